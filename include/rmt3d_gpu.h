@@ -1,0 +1,188 @@
+/* rmt3d_gpu.h -- C ABI of the B200 implementation of RMT3D's per-timestep
+ * Eulerian fluid-structure-interaction update.
+ *
+ * The reference's seam for this path is the fluid_3d class driven by the
+ * duck-typed stepper (Sim/stepper.hh:296-376) and built by run_sim
+ * (Execs/run_sim.cc:64-141).  Every entry point below replaces one member or
+ * construction step of that seam; the reference location is cited beside it.
+ * Plain C types only: no torch, no C++ types, no exceptions.  Every call
+ * returns an int status (RMT3D_OK == 0); the step codes keep the reference's
+ * values (Utilities/defs.hh:47-50).
+ *
+ * Threading: one host thread per scene handle at a time.  Device memory is
+ * owned by the handle and never exposed except through the export calls. */
+#ifndef RMT3D_GPU_H
+#define RMT3D_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define RMT3D_OK 0
+#define RMT3D_REFMAP_UPDATE_ERR 1   /* F3D_CONST::REFMAP_UPDATE_ERR */
+#define RMT3D_PROJECTION_ERR 2      /* F3D_CONST::PROJECTION_ERR */
+#define RMT3D_STEADY_SOLN_EXIT 100  /* F3D_CONST::STEADY_SOLN_EXIT */
+#define RMT3D_ERR_INVALID (-1)      /* bad argument or malformed .cfg */
+#define RMT3D_ERR_UNSUPPORTED (-2)  /* object/sim type outside this path */
+#define RMT3D_ERR_CUDA (-3)         /* CUDA runtime error (message via rmt3d_last_error) */
+#define RMT3D_ERR_EXTRAP (-4)       /* extrapolation found no eligible samples (ex.cc:253-269) */
+#define RMT3D_ERR_NAN (-5)          /* NaN in a multigrid solve (fluid_3d.cc:2227) */
+#define RMT3D_ERR_IO (-6)           /* file could not be read */
+#define RMT3D_ERR_OOM (-7)          /* device allocation failed */
+#define RMT3D_ERR_TOO_LARGE (-8)    /* size beyond a documented maximum */
+
+#define RMT3D_MAX_OBJ 16
+#define RMT3D_MAX_VEL_PROF 8
+
+/* sim types (Execs/run_sim.cc:13-32) */
+#define RMT3D_SIM_FTEST 0
+#define RMT3D_SIM_STEST 1
+#define RMT3D_SIM_OBJECTS 2
+
+/* object types (Utilities/defs.hh:64-77); this path supports the first two */
+#define RMT3D_OBJ_BASIC_SPHERE 0
+#define RMT3D_OBJ_SPHERE 1
+
+/* arithmetic forms */
+#define RMT3D_FP64 0   /* plain form: FP64 throughout */
+#define RMT3D_MIXED 1  /* FP32 multigrid V-cycles inside FP64 iterative refinement */
+
+/* One object: Sim/sim_params.cc:248-288 (basic_specs, extra_specs, srho,
+ * shear_mod, object_list). */
+typedef struct {
+    int type;
+    double basic[4];  /* centre x, y, z and primary dimension (radius) */
+    double extra[10]; /* object-specific; SPHERE: stretch dir, sqrt(lambda), omega0[3] */
+    double rho;
+    double G;
+} rmt3d_object_desc;
+
+/* Everything the reference reads from sim_params and sim_manager for this
+ * path (Sim/sim_params.cc:10-410, Sim/sim_manager.hh:164-188). */
+typedef struct {
+    int sys_size[3];
+    double bounds[6]; /* ax, bx, ay, by, az, bz */
+    int periodic[3];  /* derived from the BC sums, sim_params.cc:330-364 */
+    int bct[3][6];    /* [velocity component][face] BC type: 0 periodic, 1 Dirichlet, 2 Neumann */
+    double bcv[3][6];
+    int walls[6];
+    double wall_pos[6];
+    double wall_dist;
+    double fmu, frho, fdt_pad;
+    double dt; /* user dt ("dt" keyword); the effective dt comes from the CFL rule */
+    double T;
+    int frames;
+    int stop_short;
+    int num_iters;
+    int sim_type;
+    int has_exact;
+    int godunov;
+    int implicit_visc;
+    int vel_prof_num;
+    double vel_profile[2 * RMT3D_MAX_VEL_PROF];
+    int n_obj;
+    int nlayers;
+    int max_extrap_rs;
+    double wt_n, ex_visc_mult, ev_trans_mult, sdt_pad, dt_ex_pad, weight_fac, gravity;
+    rmt3d_object_desc obj[RMT3D_MAX_OBJ];
+    int var_den;   /* compile-time VAR_DEN in the reference (Execs/Makefile:37-42) */
+    int precision; /* RMT3D_FP64 or RMT3D_MIXED */
+} rmt3d_scene_desc;
+
+typedef struct rmt3d_scene rmt3d_scene;
+
+/* ABI check: sizeof(rmt3d_scene_desc) as compiled into the library. */
+int rmt3d_desc_sizeof(void);
+
+/* Last error message of the calling thread (static storage). */
+const char *rmt3d_last_error(void);
+
+/* Parse a .cfg file with the reference's keyword semantics
+ * (Sim/sim_params.cc:10-410; unknown keywords are an error, :317-321). */
+int rmt3d_desc_from_cfg(const char *cfg_path, rmt3d_scene_desc *out);
+
+/* Fill a descriptor with the reference's defaults (sim_params.cc:10-39). */
+int rmt3d_desc_defaults(rmt3d_scene_desc *out);
+
+/* Construct: fluid_3d::fluid_3d plus sim_manager setup (fluid_3d.cc:12-77,
+ * sim_manager.cc:37-81).  Allocates the device state on the current device.
+ * stream may be 0 (the legacy default stream) or a cudaStream_t cast to void*. */
+int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rmt3d_scene **out);
+
+/* fluid_3d::initialize (fluid_3d.cc:192-233): fields from the initial
+ * conditions, first extrapolation, dt_reg from the CFL recheck. */
+int rmt3d_initialize(rmt3d_scene *s);
+
+/* fluid_3d::set_dt (fluid_3d.hh:454-457). */
+int rmt3d_set_dt(rmt3d_scene *s, double dt);
+
+/* stepper::stepper dt fitting to frames (Sim/stepper.hh:211-227) after
+ * run_sim's min(dt_reg, dt) (run_sim.cc:100-102); writes the fitted dt and
+ * the number of steps per frame.  Pure host arithmetic. */
+int rmt3d_stepper_dt(const rmt3d_scene_desc *desc, double dt_reg, double *dt_out, int *steps_per_frame);
+
+/* fluid_3d::init_iter (fluid_3d.cc:235-287): up to num_iters pressure
+ * pre-iterations, then the t=0 stress. */
+int rmt3d_init_iter(rmt3d_scene *s);
+
+/* run_sim's whole set-up sequence: initialize, stepper dt fit, set_dt,
+ * init_iter (run_sim.cc:94-106). */
+int rmt3d_prepare(rmt3d_scene *s);
+
+/* fluid_3d::step_forward (fluid_3d.cc:429-577).  *status receives the
+ * reference's step code; the return value is RMT3D_OK unless the call itself
+ * failed. */
+int rmt3d_step(rmt3d_scene *s, int debug, int *status);
+
+/* n calls of rmt3d_step, stopping at the first non-zero status. */
+int rmt3d_run(rmt3d_scene *s, int nsteps, int *status);
+
+/* Scalars: 0 dt, 1 time, 2 dt_reg, 3 eps (transition width), 4 nt (steps
+ * taken), 5 last MAC V-cycles, 6 last FEM V-cycles, 7 total MAC V-cycles,
+ * 8 total FEM V-cycles, 9 extrapolated maps, 10 K_stiff, 11 vmax. */
+int rmt3d_get_scalar(rmt3d_scene *s, int which, double *value);
+
+/* Grid extents of the ghosted arrays: sm+4, sn+4, so+4 and the FEM node
+ * grid m,n,o (fluid_3d.cc:21-24, geometry copy for the nodal grid). */
+int rmt3d_get_dims(rmt3d_scene *s, int dims[6]);
+
+/* Field export to host memory, SoA over the ghosted (sm+4)(sn+4)(so+4)
+ * array with index i + sm4*j + smn4*k (fluid_3d.cc:24,45).
+ * which: 0..2 vel u,v,w; 3 p; 4 dp; 5 q; 6..8 dvel; 9..26 fvel[f][c];
+ *        27..35 sigma[F][c]. */
+int rmt3d_get_field(rmt3d_scene *s, int which, double *host_dst);
+
+/* Reference-map export for object slot obj (0-based): per cell the map code
+ * (-1 none, 0 primary, L>0 extrapolation layer L) and x[3], xpred[3]. */
+int rmt3d_get_refmap(rmt3d_scene *s, int obj, int *code, double *x, double *xpred);
+
+/* State import from the reference's AoS arrays (struct field 360 B, struct
+ * ref_map 488 B; F3D_Source/fields.hh:34-646) plus its extrapolated maps as
+ * (cell index, ref_map) pairs; the inverse of fluid_3d's in-memory layout. */
+int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, const void *refmap_aos,
+                           const int *ext_index, const void *ext_refmaps, int n_ext,
+                           double dt, double time);
+
+/* Export in the same AoS layout (fields.hh:34-646); extrapolated maps are
+ * written as (cell index, ref_map) pairs into ext_index/ext_refmaps of
+ * capacity max_ext, *n_ext receives the count. */
+int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *refmap_aos,
+                           int *ext_index, void *ext_refmaps, int max_ext, int *n_ext);
+
+/* Diagnostics: 0 div_u L2 of the FEM rhs (fluid_3d_utils.cc:507-653),
+ * 1 solid volume sum H(phi) dV for object 0 (compute_centroid :1348-1379). */
+int rmt3d_diag(rmt3d_scene *s, int kind, double *value);
+
+/* Synchronise the scene's stream. */
+int rmt3d_sync(rmt3d_scene *s);
+
+/* Number of kernel launches issued by this scene so far. */
+int rmt3d_launch_count(rmt3d_scene *s, long long *count);
+
+int rmt3d_scene_destroy(rmt3d_scene *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

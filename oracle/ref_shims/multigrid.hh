@@ -1,0 +1,361 @@
+/* PGMG-compatible geometric multigrid for the CPU oracle build (test
+ * infrastructure).
+ *
+ * The reference links against the external PGMG library (unpinned, absent
+ * here).  This header provides the API the reference calls -- the templated
+ * constructor, compute_rats, v_cycle, l0_error_all, l2_error_all and
+ * reg[0]->{m,n,o,mg,ng,mng,x0,r0,clear_x_field,clear_r_field} -- written from
+ * those call sites (Utilities/mg_probs.cc:3-83, F3D_Source/fluid_3d.cc:
+ * 2244-2285, 2449-2484, 2554-2712) and from textbook multigrid, not from
+ * PGMG's source.  Only the converged answer of each Poisson solve matters to
+ * the reference (mg_prob::run iterates to a max-norm residual of order 1e-13),
+ * so the V-cycle's internals are free.
+ *
+ * Design: vertex-based coarsening (coarse point I sits on fine point 2I),
+ * tensor-product linear interpolation P that reproduces constants, Galerkin
+ * coarse operators A_c = P^T A P held as full 27-point stencils, lexicographic
+ * Gauss-Seidel smoothing, and 40 smoothing sweeps on the coarsest grid.
+ * The fine-level stencil is read through the problem's external_ptr/range
+ * callbacks on every cycle, so stencils rewritten between solves are seen. */
+#ifndef RMT3D_ORACLE_PGMG_MULTIGRID_HH
+#define RMT3D_ORACLE_PGMG_MULTIGRID_HH
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <vector>
+#include "buffer.hh"
+#include "geometry.hh"
+
+class region {
+  public:
+    int m, n, o;
+    int mg, ng, og, mng;
+    double *x, *x0;
+    double *r, *r0;
+    region(int m_, int n_, int o_)
+        : m(m_), n(n_), o(o_), mg(m_ + 2), ng(n_ + 2), og(o_ + 2), mng(mg * ng),
+          x(new double[(size_t)mg * ng * og]()), x0(x + 1 + mg + mng),
+          r(new double[(size_t)m_ * n_ * o_]()), r0(r) {}
+    ~region() {
+        delete[] x;
+        delete[] r;
+    }
+    region(const region &) = delete;
+    region &operator=(const region &) = delete;
+    void clear_x_field() { memset(x, 0, sizeof(double) * (size_t)mg * ng * og); }
+    void clear_r_field() { memset(r, 0, sizeof(double) * (size_t)m * n * o); }
+    void diagnostic_A() {}
+    inline double &xa(int i, int j, int k) { return x0[i + mg * j + mng * k]; }
+};
+
+class multigrid {
+  public:
+    int v_up, v_down;
+    region **reg;
+    int nlev;
+    /* number of V-cycles run so far (diagnostics) */
+    long ncycles = 0;
+
+    template <class p_class>
+    multigrid(p_class &pr, geometry &gm, comm_buffer &) : v_up(2), v_down(2), reg(nullptr), nlev(0) {
+        p_class *pp = &pr;
+        fine_stencil = [pp](int i, int j, int k, double (&st)[27]) {
+            for (int s = 0; s < 27; s++) st[s] = 0;
+            const int xd = pp->range_xd(i, j, k), xu = pp->range_xu(i, j, k);
+            const int yd = pp->range_yd(i, j, k), yu = pp->range_yu(i, j, k);
+            const int zd = pp->range_zd(i, j, k), zu = pp->range_zu(i, j, k);
+            const double *e = pp->external_ptr(i, j, k);
+            for (int c = zd; c < zu; c++)
+                for (int b = yd; b < yu; b++)
+                    for (int a = xd; a < xu; a++) st[(a + 1) + 3 * (b + 1) + 9 * (c + 1)] = *(e++);
+        };
+        dims.push_back({gm.m, gm.n, gm.o});
+        prd[0] = gm.x_prd;
+        prd[1] = gm.y_prd;
+        prd[2] = gm.z_prd;
+        while (true) {
+            const lvl_dims &d = dims.back();
+            int nd[3];
+            bool ok = true;
+            for (int a = 0; a < 3; a++) {
+                int len = d.len[a];
+                if (prd[a]) {
+                    if (len % 2 != 0 || len < 6) ok = false;
+                    nd[a] = len / 2;
+                } else {
+                    if (len < 5) ok = false;
+                    nd[a] = (len + 1) / 2;
+                }
+            }
+            if (!ok) break;
+            dims.push_back({nd[0], nd[1], nd[2]});
+        }
+        nlev = (int)dims.size();
+        reg = new region *[nlev];
+        for (int l = 0; l < nlev; l++) reg[l] = new region(dims[l].len[0], dims[l].len[1], dims[l].len[2]);
+        ops.resize(nlev);
+        build_tables();
+    }
+    ~multigrid() {
+        for (int l = 0; l < nlev; l++) delete reg[l];
+        delete[] reg;
+    }
+    multigrid(const multigrid &) = delete;
+    multigrid &operator=(const multigrid &) = delete;
+
+    void compute_rats() {
+        load_fine();
+        for (int l = 1; l < nlev; l++) galerkin(l);
+    }
+
+    void v_cycle(int = 0) {
+        ncycles++;
+#if defined(VAR_DEN)
+        /* variable-density stencils are rewritten before every solve */
+        if (load_fine()) {
+            for (int l = 1; l < nlev; l++) galerkin(l);
+        }
+#endif
+        cycle(0);
+    }
+
+    double l0_error_all() {
+#if defined(VAR_DEN)
+        load_fine();
+#endif
+        double mx = 0;
+        region &R = *reg[0];
+        for (int k = 0; k < R.o; k++)
+            for (int j = 0; j < R.n; j++)
+                for (int i = 0; i < R.m; i++) {
+                    double res = fabs(residual(0, i, j, k));
+                    if (res > mx || std::isnan(res)) mx = res;
+                }
+        return mx;
+    }
+    double l2_error_all() {
+        double s = 0;
+        region &R = *reg[0];
+        for (int k = 0; k < R.o; k++)
+            for (int j = 0; j < R.n; j++)
+                for (int i = 0; i < R.m; i++) {
+                    double res = residual(0, i, j, k);
+                    s += res * res;
+                }
+        return s;
+    }
+    void free() {}
+
+  private:
+    struct lvl_dims {
+        int len[3];
+    };
+    std::vector<lvl_dims> dims;
+    bool prd[3];
+    std::function<void(int, int, int, double (&)[27])> fine_stencil;
+    std::vector<std::vector<double>> ops;  // 27 coefficients per point, level >= 0
+
+    /* refresh the level-0 operator from the problem; returns whether it changed */
+    bool load_fine() {
+        region &R = *reg[0];
+        std::vector<double> &A = ops[0];
+        bool changed = A.empty();
+        if (A.empty()) A.assign((size_t)27 * R.m * R.n * R.o, 0.0);
+        double st[27];
+        size_t p = 0;
+        for (int k = 0; k < R.o; k++)
+            for (int j = 0; j < R.n; j++)
+                for (int i = 0; i < R.m; i++, p++) {
+                    fine_stencil(i, j, k, st);
+                    for (int s = 0; s < 27; s++) {
+                        if (A[27 * p + s] != st[s]) changed = true;
+                        A[27 * p + s] = st[s];
+                    }
+                }
+        return changed;
+    }
+
+    inline int wrap(int l, int a, int v) const {
+        int len = dims[l].len[a];
+        if (prd[a]) {
+            v %= len;
+            if (v < 0) v += len;
+            return v;
+        }
+        return (v < 0 || v >= len) ? -1 : v;
+    }
+
+    /* per level and axis: wrapped neighbour index (or -1) of point i at offset q */
+    std::vector<std::vector<int>> nbr[3];
+    void build_tables() {
+        for (int a = 0; a < 3; a++) {
+            nbr[a].resize(nlev);
+            for (int l = 0; l < nlev; l++) {
+                int len = dims[l].len[a];
+                nbr[a][l].resize(3 * len);
+                for (int i = 0; i < len; i++)
+                    for (int q = -1; q <= 1; q++) nbr[a][l][3 * i + q + 1] = wrap(l, a, i + q);
+            }
+        }
+    }
+
+    inline double residual(int l, int i, int j, int k) {
+        region &R = *reg[l];
+        const double *a = ops[l].data() + 27 * ((size_t)i + (size_t)R.m * (j + (size_t)R.n * k));
+        double s = R.r0[i + R.m * (j + R.n * k)];
+        const int *ti = nbr[0][l].data() + 3 * i, *tj = nbr[1][l].data() + 3 * j, *tk = nbr[2][l].data() + 3 * k;
+        for (int c = 0; c < 3; c++) {
+            int kk = tk[c];
+            if (kk < 0) continue;
+            for (int b = 0; b < 3; b++) {
+                int jj = tj[b];
+                if (jj < 0) continue;
+                const double *xr = R.x0 + R.mg * jj + R.mng * kk;
+                const double *ar = a + 3 * b + 9 * c;
+                for (int q = 0; q < 3; q++) {
+                    int ii = ti[q];
+                    if (ii < 0) continue;
+                    s -= ar[q] * xr[ii];
+                }
+            }
+        }
+        return s;
+    }
+
+    void smooth(int l, int sweeps) {
+        region &R = *reg[l];
+        for (int sw = 0; sw < sweeps; sw++)
+            for (int k = 0; k < R.o; k++)
+                for (int j = 0; j < R.n; j++)
+                    for (int i = 0; i < R.m; i++) {
+                        const double *a = ops[l].data() + 27 * ((size_t)i + (size_t)R.m * (j + (size_t)R.n * k));
+                        double d = a[13];
+                        double res = residual(l, i, j, k);
+                        R.xa(i, j, k) += res / d;
+                    }
+    }
+
+    /* 1D interpolation weights: fine index f receives w0*c[I0] + w1*c[I1] */
+    inline int pweights(int l, int a, int f, int (&ci)[2], double (&w)[2]) const {
+        int nc = dims[l + 1].len[a];
+        if (f % 2 == 0) {
+            ci[0] = f / 2;
+            w[0] = 1;
+            return 1;
+        }
+        int I = f / 2, J = I + 1;
+        if (prd[a]) J %= nc;
+        if (J < nc) {
+            ci[0] = I;
+            w[0] = 0.5;
+            ci[1] = J;
+            w[1] = 0.5;
+            return 2;
+        }
+        ci[0] = I;
+        w[0] = 1;
+        return 1;
+    }
+
+    void galerkin(int lc) {
+        const int lf = lc - 1;
+        region &F = *reg[lf];
+        region &C = *reg[lc];
+        std::vector<double> &Ac = ops[lc];
+        Ac.assign((size_t)27 * C.m * C.n * C.o, 0.0);
+        const std::vector<double> &Af = ops[lf];
+        for (int k = 0; k < F.o; k++)
+            for (int j = 0; j < F.n; j++)
+                for (int i = 0; i < F.m; i++) {
+                    int ci[3][2];
+                    double cw[3][2];
+                    int cn[3];
+                    cn[0] = pweights(lf, 0, i, ci[0], cw[0]);
+                    cn[1] = pweights(lf, 1, j, ci[1], cw[1]);
+                    cn[2] = pweights(lf, 2, k, ci[2], cw[2]);
+                    const double *a = Af.data() + 27 * ((size_t)i + (size_t)F.m * (j + (size_t)F.n * k));
+                    for (int s = 0; s < 27; s++) {
+                        double co = a[s];
+                        if (co == 0) continue;
+                        int q = s % 3 - 1, b = (s / 3) % 3 - 1, c = s / 9 - 1;
+                        int ii = wrap(lf, 0, i + q), jj = wrap(lf, 1, j + b), kk = wrap(lf, 2, k + c);
+                        if (ii < 0 || jj < 0 || kk < 0) continue;
+                        int di[3][2];
+                        double dw[3][2];
+                        int dn[3];
+                        dn[0] = pweights(lf, 0, ii, di[0], dw[0]);
+                        dn[1] = pweights(lf, 1, jj, di[1], dw[1]);
+                        dn[2] = pweights(lf, 2, kk, di[2], dw[2]);
+                        for (int z0 = 0; z0 < cn[2]; z0++)
+                            for (int y0 = 0; y0 < cn[1]; y0++)
+                                for (int x0 = 0; x0 < cn[0]; x0++) {
+                                    double wi = cw[0][x0] * cw[1][y0] * cw[2][z0] * co;
+                                    int I[3] = {ci[0][x0], ci[1][y0], ci[2][z0]};
+                                    double *row = Ac.data() + 27 * ((size_t)I[0] + (size_t)C.m * (I[1] + (size_t)C.n * I[2]));
+                                    for (int z1 = 0; z1 < dn[2]; z1++)
+                                        for (int y1 = 0; y1 < dn[1]; y1++)
+                                            for (int x1 = 0; x1 < dn[0]; x1++) {
+                                                int J[3] = {di[0][x1], di[1][y1], di[2][z1]};
+                                                int off[3];
+                                                for (int a2 = 0; a2 < 3; a2++) {
+                                                    int dlt = J[a2] - I[a2];
+                                                    int len = dims[lc].len[a2];
+                                                    if (prd[a2]) {
+                                                        if (dlt > 1) dlt -= len;
+                                                        if (dlt < -1) dlt += len;
+                                                    }
+                                                    off[a2] = dlt;
+                                                }
+                                                row[(off[0] + 1) + 3 * (off[1] + 1) + 9 * (off[2] + 1)] +=
+                                                    wi * dw[0][x1] * dw[1][y1] * dw[2][z1];
+                                            }
+                                }
+                    }
+                }
+    }
+
+    void cycle(int l) {
+        if (l == nlev - 1) {
+            smooth(l, 40);
+            return;
+        }
+        smooth(l, v_down);
+        region &F = *reg[l];
+        region &C = *reg[l + 1];
+        C.clear_r_field();
+        C.clear_x_field();
+        for (int k = 0; k < F.o; k++)
+            for (int j = 0; j < F.n; j++)
+                for (int i = 0; i < F.m; i++) {
+                    double res = residual(l, i, j, k);
+                    int ci[3][2];
+                    double cw[3][2];
+                    int cn[3];
+                    cn[0] = pweights(l, 0, i, ci[0], cw[0]);
+                    cn[1] = pweights(l, 1, j, ci[1], cw[1]);
+                    cn[2] = pweights(l, 2, k, ci[2], cw[2]);
+                    for (int z = 0; z < cn[2]; z++)
+                        for (int y = 0; y < cn[1]; y++)
+                            for (int x = 0; x < cn[0]; x++)
+                                C.r0[ci[0][x] + C.m * (ci[1][y] + C.n * ci[2][z])] += cw[0][x] * cw[1][y] * cw[2][z] * res;
+                }
+        cycle(l + 1);
+        for (int k = 0; k < F.o; k++)
+            for (int j = 0; j < F.n; j++)
+                for (int i = 0; i < F.m; i++) {
+                    int ci[3][2];
+                    double cw[3][2];
+                    int cn[3];
+                    cn[0] = pweights(l, 0, i, ci[0], cw[0]);
+                    cn[1] = pweights(l, 1, j, ci[1], cw[1]);
+                    cn[2] = pweights(l, 2, k, ci[2], cw[2]);
+                    double e = 0;
+                    for (int z = 0; z < cn[2]; z++)
+                        for (int y = 0; y < cn[1]; y++)
+                            for (int x = 0; x < cn[0]; x++) e += cw[0][x] * cw[1][y] * cw[2][z] * C.xa(ci[0][x], ci[1][y], ci[2][z]);
+                    F.xa(i, j, k) += e;
+                }
+        smooth(l, v_up);
+    }
+};
+#endif

@@ -1,0 +1,216 @@
+"""rmt3d_b200: B200 implementation of RMT3D's per-timestep Eulerian FSI update.
+
+Host-side mirror of the reference's seam for this path:
+
+* :class:`Scene` stands in for ``fluid_3d`` (F3D_Source/fluid_3d.hh:37-467):
+  ``initialize``, ``set_dt``, ``init_iter``, ``step_forward`` keep the
+  reference's names, argument meaning and integer return codes.
+* :class:`Stepper` stands in for ``stepper`` (Sim/stepper.hh:22-376): dt
+  fitting to frames and the frame/step loop with ``stop_short``.
+* :func:`run_sim` is the ``run_sim`` driver sequence (Execs/run_sim.cc:39-141).
+
+All work runs in the CUDA library ``librmt3d_gpu.so`` through the C ABI of
+include/rmt3d_gpu.h; there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import FP64, MIXED, PROJECTION_ERR, REFMAP_UPDATE_ERR, STEADY_SOLN_EXIT  # noqa: F401
+from ._lib import OK as NORMAL_EXIT
+from ._lib import RMT3DError, SceneDesc
+
+FIELD_INDEX = {"u": 0, "v": 1, "w": 2, "p": 3, "dp": 4, "q": 5, "du": 6, "dv": 7, "dw": 8}
+for _f in range(6):
+    for _c in range(3):
+        FIELD_INDEX["fvel%d%d" % (_f, _c)] = 9 + 3 * _f + _c
+for _F in range(3):
+    for _c in range(3):
+        FIELD_INDEX["sigma%d%d" % (_F, _c)] = 27 + 3 * _F + _c
+
+
+def lib():
+    return _lib.load()
+
+
+def desc_from_cfg(path):
+    """sim_params(cfg) (Sim/sim_params.cc:10-410) into a SceneDesc."""
+    L = lib()
+    d = SceneDesc()
+    _lib.check(L.rmt3d_desc_from_cfg(str(path).encode(), ctypes.byref(d)))
+    return d
+
+
+def desc_defaults():
+    L = lib()
+    d = SceneDesc()
+    _lib.check(L.rmt3d_desc_defaults(ctypes.byref(d)))
+    return d
+
+
+def stepper_dt(desc, dt_reg):
+    """stepper dt fit (Sim/stepper.hh:220-225) -> (dt, steps per frame)."""
+    L = lib()
+    dt = ctypes.c_double()
+    steps = ctypes.c_int()
+    _lib.check(L.rmt3d_stepper_dt(ctypes.byref(desc), dt_reg, ctypes.byref(dt), ctypes.byref(steps)))
+    return dt.value, steps.value
+
+
+class Scene:
+    """One simulation scene on the current CUDA device (``fluid_3d``)."""
+
+    def __init__(self, desc, stream=None):
+        L = lib()
+        self.desc = desc
+        h = ctypes.c_void_p()
+        st = ctypes.c_void_p(stream if stream is not None else 0)
+        _lib.check(L.rmt3d_scene_create(ctypes.byref(desc), st, ctypes.byref(h)))
+        self._h = h
+        dims = (ctypes.c_int * 6)()
+        _lib.check(L.rmt3d_get_dims(h, dims))
+        self.sm4, self.sn4, self.so4, self.fm, self.fn, self.fo = list(dims)
+        self.ncell = self.sm4 * self.sn4 * self.so4
+
+    @classmethod
+    def from_cfg(cls, path, **overrides):
+        d = desc_from_cfg(path)
+        for k, v in overrides.items():
+            setattr(d, k, v)
+        return cls(d)
+
+    # -- the fluid_3d members the stepper and run_sim use -------------------
+    def initialize(self):
+        _lib.check(lib().rmt3d_initialize(self._h))
+        return 1  # init_err: started from scratch (fluid_3d.cc:193-196)
+
+    def set_dt(self, dt):
+        _lib.check(lib().rmt3d_set_dt(self._h, dt))
+
+    def init_iter(self, init_err=1):
+        if init_err > 0:
+            _lib.check(lib().rmt3d_init_iter(self._h))
+
+    def prepare(self):
+        _lib.check(lib().rmt3d_prepare(self._h))
+
+    def step_forward(self, debug=0):
+        st = ctypes.c_int()
+        _lib.check(lib().rmt3d_step(self._h, debug, ctypes.byref(st)))
+        return st.value
+
+    def run(self, nsteps):
+        st = ctypes.c_int()
+        _lib.check(lib().rmt3d_run(self._h, nsteps, ctypes.byref(st)))
+        return st.value
+
+    def sync(self):
+        _lib.check(lib().rmt3d_sync(self._h))
+
+    # -- state access ---------------------------------------------------------
+    def scalar(self, which):
+        v = ctypes.c_double()
+        _lib.check(lib().rmt3d_get_scalar(self._h, which, ctypes.byref(v)))
+        return v.value
+
+    @property
+    def dt(self):
+        return self.scalar(0)
+
+    @property
+    def time(self):
+        return self.scalar(1)
+
+    @property
+    def dt_reg(self):
+        return self.scalar(2)
+
+    def field(self, name):
+        """Field over the ghosted box as an array of shape (so+4, sn+4, sm+4)."""
+        out = np.empty(self.ncell, dtype=np.float64)
+        idx = FIELD_INDEX[name] if isinstance(name, str) else int(name)
+        _lib.check(lib().rmt3d_get_field(self._h, idx, out.ctypes.data_as(ctypes.c_void_p)))
+        return out.reshape(self.so4, self.sn4, self.sm4)
+
+    def refmap(self, obj=0):
+        code = np.empty(self.ncell, dtype=np.int32)
+        x = np.empty(3 * self.ncell, dtype=np.float64)
+        xp = np.empty(3 * self.ncell, dtype=np.float64)
+        _lib.check(lib().rmt3d_get_refmap(self._h, obj, code.ctypes.data_as(ctypes.c_void_p),
+                                          x.ctypes.data_as(ctypes.c_void_p), xp.ctypes.data_as(ctypes.c_void_p)))
+        shp = (self.so4, self.sn4, self.sm4)
+        return code.reshape(shp), x.reshape((3,) + shp), xp.reshape((3,) + shp)
+
+    def import_reference(self, field_aos, refmap_aos, ext_index, ext_maps, dt, time):
+        fa = np.ascontiguousarray(field_aos)
+        ra = np.ascontiguousarray(refmap_aos) if refmap_aos is not None else None
+        ei = np.ascontiguousarray(ext_index, dtype=np.int32)
+        em = np.ascontiguousarray(ext_maps)
+        _lib.check(lib().rmt3d_import_reference(
+            self._h, fa.ctypes.data_as(ctypes.c_void_p),
+            ra.ctypes.data_as(ctypes.c_void_p) if ra is not None else None,
+            ei.ctypes.data_as(ctypes.c_void_p), em.ctypes.data_as(ctypes.c_void_p), len(ei), dt, time))
+
+    def diag(self, kind=0):
+        v = ctypes.c_double()
+        _lib.check(lib().rmt3d_diag(self._h, kind, ctypes.byref(v)))
+        return v.value
+
+    def launches(self):
+        c = ctypes.c_longlong()
+        _lib.check(lib().rmt3d_launch_count(self._h, ctypes.byref(c)))
+        return c.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rmt3d_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Stepper:
+    """Frame/step loop of the reference's stepper (Sim/stepper.hh:211-376)."""
+
+    def __init__(self, desc, scene):
+        self.dt, self.steps = stepper_dt(desc, desc.dt)
+        self.frames = desc.frames
+        self.total = (self.frames - 1) * self.steps
+        self.stop_short = desc.stop_short if desc.stop_short > 0 else self.total + 1
+        self.curr_tot_step = 0
+        scene.set_dt(self.dt)
+
+    def run(self, scene):
+        scene.set_dt(self.dt)
+        err = 0
+        for _frame in range(1, self.frames):
+            if self.curr_tot_step >= self.stop_short:
+                break
+            for _s in range(self.steps):
+                if self.curr_tot_step >= self.stop_short:
+                    break
+                self.curr_tot_step += 1
+                err = scene.step_forward(0)
+                if err not in (NORMAL_EXIT, STEADY_SOLN_EXIT):
+                    raise RMT3DError(err, "Stepper: Something went wrong, sorry.")
+        return err
+
+
+def run_sim(cfg_path, **overrides):
+    """The run_sim driver sequence (Execs/run_sim.cc:64-141); returns the scene."""
+    desc = desc_from_cfg(cfg_path)
+    for k, v in overrides.items():
+        setattr(desc, k, v)
+    scene = Scene(desc)
+    init_err = scene.initialize()
+    if scene.dt_reg < desc.dt:
+        desc.dt = scene.dt_reg
+    sim = Stepper(desc, scene)
+    scene.init_iter(init_err)
+    sim.run(scene)
+    return scene

@@ -1,0 +1,147 @@
+"""ctypes binding of the C ABI in include/rmt3d_gpu.h.
+
+The library is the in-tree ``librmt3d_gpu.so``; importing this module fails
+loudly when it is missing -- there is no CPU fallback for the FSI step.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librmt3d_gpu.so")
+
+MAX_OBJ = 16
+MAX_VEL_PROF = 8
+
+OK = 0
+REFMAP_UPDATE_ERR = 1
+PROJECTION_ERR = 2
+STEADY_SOLN_EXIT = 100
+ERR_INVALID = -1
+ERR_UNSUPPORTED = -2
+ERR_CUDA = -3
+ERR_EXTRAP = -4
+ERR_NAN = -5
+ERR_IO = -6
+ERR_OOM = -7
+ERR_TOO_LARGE = -8
+
+SIM_FTEST, SIM_STEST, SIM_OBJECTS = 0, 1, 2
+OBJ_BASIC_SPHERE, OBJ_SPHERE = 0, 1
+FP64, MIXED = 0, 1
+
+
+class ObjectDesc(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("basic", ctypes.c_double * 4),
+        ("extra", ctypes.c_double * 10),
+        ("rho", ctypes.c_double),
+        ("G", ctypes.c_double),
+    ]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("sys_size", ctypes.c_int * 3),
+        ("bounds", ctypes.c_double * 6),
+        ("periodic", ctypes.c_int * 3),
+        ("bct", (ctypes.c_int * 6) * 3),
+        ("bcv", (ctypes.c_double * 6) * 3),
+        ("walls", ctypes.c_int * 6),
+        ("wall_pos", ctypes.c_double * 6),
+        ("wall_dist", ctypes.c_double),
+        ("fmu", ctypes.c_double),
+        ("frho", ctypes.c_double),
+        ("fdt_pad", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("T", ctypes.c_double),
+        ("frames", ctypes.c_int),
+        ("stop_short", ctypes.c_int),
+        ("num_iters", ctypes.c_int),
+        ("sim_type", ctypes.c_int),
+        ("has_exact", ctypes.c_int),
+        ("godunov", ctypes.c_int),
+        ("implicit_visc", ctypes.c_int),
+        ("vel_prof_num", ctypes.c_int),
+        ("vel_profile", ctypes.c_double * (2 * MAX_VEL_PROF)),
+        ("n_obj", ctypes.c_int),
+        ("nlayers", ctypes.c_int),
+        ("max_extrap_rs", ctypes.c_int),
+        ("wt_n", ctypes.c_double),
+        ("ex_visc_mult", ctypes.c_double),
+        ("ev_trans_mult", ctypes.c_double),
+        ("sdt_pad", ctypes.c_double),
+        ("dt_ex_pad", ctypes.c_double),
+        ("weight_fac", ctypes.c_double),
+        ("gravity", ctypes.c_double),
+        ("obj", ObjectDesc * MAX_OBJ),
+        ("var_den", ctypes.c_int),
+        ("precision", ctypes.c_int),
+    ]
+
+
+# entry points declared in include/rmt3d_gpu.h: name -> (restype, argtypes)
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_DP = ctypes.POINTER(ctypes.c_double)
+_IP = ctypes.POINTER(ctypes.c_int)
+SIGNATURES = {
+    "rmt3d_desc_sizeof": (_I, []),
+    "rmt3d_last_error": (ctypes.c_char_p, []),
+    "rmt3d_desc_from_cfg": (_I, [ctypes.c_char_p, ctypes.POINTER(SceneDesc)]),
+    "rmt3d_desc_defaults": (_I, [ctypes.POINTER(SceneDesc)]),
+    "rmt3d_scene_create": (_I, [ctypes.POINTER(SceneDesc), _P, ctypes.POINTER(_P)]),
+    "rmt3d_initialize": (_I, [_P]),
+    "rmt3d_set_dt": (_I, [_P, _D]),
+    "rmt3d_stepper_dt": (_I, [ctypes.POINTER(SceneDesc), _D, _DP, _IP]),
+    "rmt3d_init_iter": (_I, [_P]),
+    "rmt3d_prepare": (_I, [_P]),
+    "rmt3d_step": (_I, [_P, _I, _IP]),
+    "rmt3d_run": (_I, [_P, _I, _IP]),
+    "rmt3d_get_scalar": (_I, [_P, _I, _DP]),
+    "rmt3d_get_dims": (_I, [_P, _IP]),
+    "rmt3d_get_field": (_I, [_P, _I, _P]),
+    "rmt3d_get_refmap": (_I, [_P, _I, _P, _P, _P]),
+    "rmt3d_import_reference": (_I, [_P, _P, _P, _P, _P, _I, _D, _D]),
+    "rmt3d_export_reference": (_I, [_P, _P, _P, _P, _P, _I, _IP]),
+    "rmt3d_diag": (_I, [_P, _I, _DP]),
+    "rmt3d_sync": (_I, [_P]),
+    "rmt3d_launch_count": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
+    "rmt3d_scene_destroy": (_I, [_P]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the library (once) and attach the prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "rmt3d_b200: CUDA library %s is missing; build it with "
+            "`python -m rmt3d_b200.build` (there is no CPU fallback)" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.rmt3d_desc_sizeof() != ctypes.sizeof(SceneDesc):
+        raise ImportError("rmt3d_b200: descriptor size mismatch between ctypes and the library")
+    _lib = lib
+    return lib
+
+
+class RMT3DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("rmt3d error %d: %s" % (code, msg))
+        self.code = code
+
+
+def check(code):
+    if code != OK:
+        msg = _lib.rmt3d_last_error().decode() if _lib is not None else ""
+        raise RMT3DError(code, msg)
+    return code

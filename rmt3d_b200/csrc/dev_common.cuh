@@ -1,0 +1,136 @@
+// Device-side definitions shared by every kernel of the FSI step.
+//
+// Layout: every per-cell quantity is a separate FP64 array (SoA) over the
+// reference's ghosted box of (sm+4)(sn+4)(so+4) cells, with the reference's
+// index i + sm4*j + smn4*k on absolute (ghost-inclusive) coordinates
+// (F3D_Source/fluid_3d.cc:21-24).  Interior cells have absolute indices
+// 2..sm+1.  Keeping the reference's index space makes every ghost-frame rule
+// (physical BCs, periodic wrap, extrapolation into ghosts) carry over
+// one-to-one, and each array is contiguous along x for coalesced access.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rmt3d {
+
+constexpr int kMaxObj = 16;
+constexpr double kBig = 1.e200;  // "unset" marker for grad_phi (fields.hh:338)
+
+// Object parameters consumed inside kernels (Sim/object.hh:76-123,
+// Sim/sim_manager.hh:15-74).
+struct obj_dev {
+    int type;
+    double c[3];
+    double R;
+    double eig[3];   // SPHERE initial-map scale per axis (object.hh:100-114)
+    double omega[3]; // initial spin
+    double G, rho, ex_mu, ev_trans_mult;
+};
+
+// Per-scene constants passed by value to kernels.
+struct grid_dev {
+    int sm, sn, so;       // interior cells
+    int sm4, sn4, so4;    // ghosted extents
+    int smn4;             // sm4*sn4
+    int ncell;            // sm4*sn4*so4
+    int prd[3];           // periodic flags
+    int fm, fn, fo;       // FEM node grid (m+1 per non-periodic axis)
+    double dx, dy, dz, dxsp, dysp, dzsp;
+    double ax, ay, az;
+    double mu;            // fluid dynamic viscosity
+    double frho;
+    double eps, tf1, tf2, tf3;  // transition zone constants (sim_manager.cc:37-47)
+    int n_obj;
+    int sim_type;
+    int has_exact;
+    double gravity;
+    double K_stiff, wall_dist, winv, min_wall_acc, wall_acc_mult;
+    int walls[6];
+    double wall_pos[6];
+    obj_dev obj[kMaxObj];
+};
+
+__host__ __device__ inline int gidx(const grid_dev &g, int i, int j, int k) { return i + g.sm4 * j + g.smn4 * k; }
+
+// ---- scalar helpers of the Godunov scheme (fluid_3d.cc:2310-2340) -------
+__device__ inline double rmin(double x, double y) { return (x < y) ? x : y; }
+__device__ inline double rsign(double x) { return (x >= 0) ? 1 : -1; }
+
+__device__ inline double del_lim(double u0, double u1, double u2) {
+    double t1 = 2 * (u1 - u0);
+    double t2 = 2 * (u2 - u1);
+    if (t1 * t2 > 0) return rmin(fabs(t1), fabs(t2));
+    return 0;
+}
+__device__ inline double del_f(double u0, double u1, double u2) {
+    double dlim = del_lim(u0, u1, u2);
+    double cen = 0.5 * (u2 - u0);
+    return rsign(cen) * rmin(fabs(cen), dlim);
+}
+// 4th-order monotonicity-limited slope, Yu (2003) Eq. 3.25-3.26
+__device__ inline double mono_diff(double u0, double u1, double u2, double u3, double u4) {
+    double dlim = del_lim(u1, u2, u3);
+    double cen = 0.5 * (u3 - u1);
+    double neigh_delf = (del_f(u0, u1, u2) + del_f(u2, u3, u4)) / 6.0;
+    return rsign(cen) * rmin(dlim, fabs(4.0 / 3.0 * cen - neigh_delf));
+}
+
+// ---- transition-zone functions (sim_manager.hh:259-280) ------------------
+__device__ inline double heaviside(const grid_dev &g, double phi) {
+    if (phi >= g.eps) return 0;
+    if (phi <= -g.eps) return 1;
+    double tmp = 0.5 - phi * g.tf1 - sin(g.tf3 * phi) * g.tf2;
+    if (tmp < 0) tmp = 0.;
+    else if (tmp > 1) tmp = 1;
+    return tmp;
+}
+__device__ inline double tderiv_func_in(const grid_dev &g, double x) {
+    double tmp = 0;
+    if (x > -g.eps && x < g.eps) tmp = 0.5 + 0.5 * cos(x * g.tf3);
+    return tmp;
+}
+__device__ inline double coll_func(const grid_dev &g, double x) { return x > g.eps ? 0 : (0.5 - x * g.tf1); }
+
+// level set of object o evaluated at reference-map value xi
+// (basic_sphere::phi, Sim/object.cc:76-82; SPHERE inherits it)
+__device__ inline double obj_phi(const grid_dev &g, int o, double x0, double x1, double x2) {
+    const obj_dev &ob = g.obj[o];
+    double sq = 0;
+    sq += (x0 - ob.c[0]) * (x0 - ob.c[0]);
+    sq += (x1 - ob.c[1]) * (x1 - ob.c[1]);
+    sq += (x2 - ob.c[2]) * (x2 - ob.c[2]);
+    return sqrt(sq) - ob.R;
+}
+
+// physical coordinate of absolute index i along an axis (fluid_3d.cc:137-139)
+__device__ inline double coord(double a, int i, double h) { return a + ((double)(i - 2) + 0.5) * h; }
+
+// Reference-map storage of one object slot: one map per (object, cell) at
+// most, as in the reference where a cell holds either the primary map or one
+// extrapolated map of each object (extrap_mmap.cc:60-200).
+struct objmap_dev {
+    int *code;       // -1 none, 0 primary, L >= 1 extrapolation layer L
+    double *x[3];    // reference map
+    double *xp[3];   // predicted reference map
+    double *fx[18];  // face states fx[f][c] (fields.hh:296)
+    double *gp[9];   // grad_phi[F][c] (fields.hh:310)
+    double *det[3];  // detF per lower face (fields.hh:308)
+    // snapshot of the previous extrapolated maps (temp_extraps, fluid_3d.hh:122)
+    int *code_prev;
+    double *x_prev[3];
+    double *gp_prev[9];
+};
+
+// All device arrays of a scene.
+struct fields_dev {
+    double *vel[3];
+    double *p, *dp, *q;
+    double *dvel[3];
+    double *fvel[18];
+    double *sigma[9];
+    double *rho;  // VAR_DEN density per cell (fluid_3d.hh:160)
+    objmap_dev om[kMaxObj];
+    unsigned int *flags;  // scratch per-cell flags (extrapolation frontier)
+};
+
+}  // namespace rmt3d

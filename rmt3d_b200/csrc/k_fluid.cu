@@ -1,0 +1,813 @@
+// Fluid-side kernels of the FSI step: ghost frames, stress, Godunov edge
+// states and upwinding, the explicit momentum update and the two projection
+// right-hand sides / corrections.  Each kernel cites the reference loop it
+// replaces; floating-point expressions keep the reference's association order
+// so that, built without FMA contraction, results track the reference's CPU
+// run to rounding.
+#include "dev_common.cuh"
+#include "kernels.h"
+
+namespace rmt3d {
+
+// -------------------------------------------------------------------------
+// Periodic ghost copy: replaces fluid_3d::communicate<flags> on one rank
+// (fluid_3d_comm.cc:76-198), where each ghost region whose direction has only
+// periodic components receives the interior slab from the opposite side.
+// corner != 0 selects the nodal table (fluid_3d_comm.cc:55-58), whose extent
+// along a non-periodic axis is one node longer.
+// -------------------------------------------------------------------------
+__global__ void k_periodic_copy(grid_dev g, ptr_list pl, int corner) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.sm4 || j >= g.sn4 || k >= g.so4) return;
+    const int c[3] = {i, j, k};
+    const int s[3] = {g.sm, g.sn, g.so};
+    int src[3];
+    bool ghost = false;
+    for (int d = 0; d < 3; d++) {
+        int len = s[d] + ((corner && !g.prd[d]) ? 1 : 0);
+        if (c[d] >= 2 && c[d] < 2 + len) {
+            src[d] = c[d];
+            continue;
+        }
+        if (!g.prd[d]) return;  // wall ghost: not filled by the exchange
+        ghost = true;
+        src[d] = (c[d] < 2) ? c[d] + s[d] : c[d] - s[d];
+    }
+    if (!ghost) return;
+    int dst = gidx(g, i, j, k), from = gidx(g, src[0], src[1], src[2]);
+    for (int a = 0; a < pl.n; a++) pl.p[a][dst] = pl.p[a][from];
+    for (int a = 0; a < pl.ni; a++) pl.ip[a][dst] = pl.ip[a][from];
+}
+
+// -------------------------------------------------------------------------
+// Physical BC ghost fill of one face, face_gm::set_ghost_cc
+// (fields.hh:765-800): both ghost layers, the whole tangential extent.
+// -------------------------------------------------------------------------
+__global__ void k_bc_cc(grid_dev g, int face, bc_face bc, double *u, double *v, double *w) {
+    const int n = face / 2;
+    const int lower = (face % 2 == 0);
+    const int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
+    const int ext[3] = {g.sm4, g.sn4, g.so4};
+    const int len[3] = {g.sm, g.sn, g.so};
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    int b = blockIdx.y * blockDim.y + threadIdx.y;
+    int layer = blockIdx.z + 1;  // 1 or 2
+    if (a >= ext[t0] || b >= ext[t1]) return;
+    int gc[3], mc[3];
+    gc[t0] = mc[t0] = a;
+    gc[t1] = mc[t1] = b;
+    if (lower) {
+        gc[n] = 2 - layer;
+        mc[n] = 2 + layer - 1;
+    } else {
+        gc[n] = 2 + len[n] - 1 + layer;
+        mc[n] = 2 + len[n] - layer;
+    }
+    const int gi = gidx(g, gc[0], gc[1], gc[2]);
+    const int mi = gidx(g, mc[0], mc[1], mc[2]);
+    const double sgn = lower ? -1 : 1;
+    const double dn = 2 * fabs(0.5 * bc.h * (2 * layer - 1));
+    double *vel[3] = {u, v, w};
+    for (int c = 0; c < 3; c++) {
+        if (bc.bct[c] == 1) vel[c][gi] = 2 * bc.bcv[c] - vel[c][mi];
+        else vel[c][gi] = sgn * dn * bc.bcv[c] + vel[c][mi];
+    }
+}
+
+// -------------------------------------------------------------------------
+// Face-velocity BC of one face, face_gm::set_ghost_cf / compute_ghost_cf
+// (fields.hh:804-849): the boundary face of the outermost interior layer and
+// the matching face of the inner ghost layer.
+// -------------------------------------------------------------------------
+__global__ void k_bc_cf(grid_dev g, int face, bc_face bc, const fields_dev *F) {
+    const int n = face / 2;
+    const int lower = (face % 2 == 0);
+    const int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
+    const int ext[3] = {g.sm4, g.sn4, g.so4};
+    const int len[3] = {g.sm, g.sn, g.so};
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    int b = blockIdx.y * blockDim.y + threadIdx.y;
+    if (a >= ext[t0] || b >= ext[t1]) return;
+    int gc[3], y0[3], y1[3];
+    gc[t0] = y0[t0] = y1[t0] = a;
+    gc[t1] = y0[t1] = y1[t1] = b;
+    if (lower) {
+        gc[n] = 1;
+        y0[n] = 2;
+        y1[n] = 3;
+    } else {
+        gc[n] = 2 + len[n];
+        y0[n] = 1 + len[n];
+        y1[n] = len[n];
+    }
+    const int gi = gidx(g, gc[0], gc[1], gc[2]);
+    const int i0 = gidx(g, y0[0], y0[1], y0[2]);
+    const int i1 = gidx(g, y1[0], y1[1], y1[2]);
+    const double sgn = lower ? -1 : 1;
+    const int inner = 2 * n + (lower ? 1 : 0);
+    for (int c = 0; c < 3; c++) {
+        double f = bc.bcv[c];
+        if (bc.bct[c] == 2) f = (3 * bc.h * bc.bcv[c] * sgn + 9 * F->vel[c][i0] - F->vel[c][i1]) * 0.125;
+        F->fvel[3 * face + c][i0] = f;
+        F->fvel[3 * inner + c][gi] = f;
+    }
+}
+
+// -------------------------------------------------------------------------
+// Stress on the three lower faces, fluid_3d::compute_stress
+// (fluid_3d.cc:1360-1461) with solid_stress (:1777-1997), fluid_stress
+// (:2001-2031) and collision_stress (:1465-1773).  One thread per cell over
+// relative cells -1..s+1.
+// -------------------------------------------------------------------------
+__device__ inline bool has_map(const objmap_dev &m, int ind) { return m.code[ind] >= 0; }
+
+__device__ inline double map_phi(const grid_dev &g, const objmap_dev &m, int o, int ind) {
+    return obj_phi(g, o, m.x[0][ind], m.x[1][ind], m.x[2][ind]);
+}
+
+// Collision stress between maps of different objects sharing a cell,
+// fluid_3d::collision_stress (fluid_3d.cc:1465-1773).  The reference derives
+// the neighbour positions from the cell's offset relative to the first
+// interior cell (unpack_index(eid), :1476), so its box check runs on shifted
+// coordinates; that is reproduced, including C++ truncating division.
+template <int FF>
+__device__ void collision_face(const grid_dev &g, const fields_dev *__restrict__ F, int i, int j, int k, int ind,
+                               const int *order, int nmaps, double out[3]) {
+    const int strides[3] = {1, g.sm4, g.smn4};
+    const double facs[3] = {g.dxsp, g.dysp, g.dzsp};
+    const int strd = strides[FF];
+    const int ad1 = (FF + 1) % 3, ad2 = (FF + 2) % 3;
+    const int ext[3] = {g.sm4, g.sn4, g.so4};
+    const int G0 = gidx(g, 2, 2, 2);
+    const int eid = ind - G0;
+    int lp[3];
+    lp[2] = eid / g.smn4;
+    lp[1] = (eid % g.smn4) / g.sm4;
+    lp[0] = eid % g.sm4;
+    auto nbo = [&](const objmap_dev &m, int da, int sa, int db, int sb) -> int {
+        int p[3] = {lp[0], lp[1], lp[2]};
+        p[da] += sa;
+        p[db] += sb;
+        for (int d = 0; d < 3; d++)
+            if (p[d] < 0 || p[d] >= ext[d]) return -1;
+        int q = ind + sa * strides[da] + sb * strides[db];
+        if (q < 0 || q >= g.ncell) return -1;
+        return m.code[q] >= 0 ? q : -1;
+    };
+    auto grad = [&](const objmap_dev &m, int o, int rn, int q1p, int q1p1, int q1m, int q1m1, int q2p, int q2p1,
+                    int q2m, int q2m1, double dph[3]) {
+        dph[FF] = facs[FF] * (map_phi(g, m, o, ind) - map_phi(g, m, o, rn));
+        dph[ad1] = 0.25 * facs[ad1] *
+                   (map_phi(g, m, o, q1p) + map_phi(g, m, o, q1p1) - map_phi(g, m, o, q1m) - map_phi(g, m, o, q1m1));
+        dph[ad2] = 0.25 * facs[ad2] *
+                   (map_phi(g, m, o, q2p) + map_phi(g, m, o, q2p1) - map_phi(g, m, o, q2m) - map_phi(g, m, o, q2m1));
+        double nrm = 0;
+        for (int c = 0; c < 3; c++) nrm += dph[c] * dph[c];
+        if (nrm > 0) {
+            nrm = sqrt(nrm);
+            for (int c = 0; c < 3; c++) dph[c] /= nrm;
+        }
+    };
+    for (int ii = 0; ii < nmaps - 1; ii++) {
+        const int o0 = order[ii];
+        const objmap_dev &m0 = F->om[o0];
+        const double G0m = g.obj[o0].G;
+        int rn0 = nbo(m0, FF, -1, FF, 0);
+        if (rn0 < 0) continue;
+        double phiv0 = 0.5 * (map_phi(g, m0, o0, ind) + map_phi(g, m0, o0, rn0));
+        if (phiv0 > g.eps) continue;
+        int a1 = nbo(m0, ad1, 1, FF, 0), a2 = nbo(m0, ad1, 1, FF, -1), a3 = nbo(m0, ad1, -1, FF, 0),
+            a4 = nbo(m0, ad1, -1, FF, -1);
+        int b1 = nbo(m0, ad2, 1, FF, 0), b2 = nbo(m0, ad2, 1, FF, -1), b3 = nbo(m0, ad2, -1, FF, 0),
+            b4 = nbo(m0, ad2, -1, FF, -1);
+        if (a1 < 0 || a2 < 0 || a3 < 0 || a4 < 0 || b1 < 0 || b2 < 0 || b3 < 0 || b4 < 0) continue;
+        double d0[3];
+        grad(m0, o0, rn0, a1, a2, a3, a4, b1, b2, b3, b4, d0);
+        for (int jj = ii + 1; jj < nmaps; jj++) {
+            const int o1 = order[jj];
+            const objmap_dev &m1 = F->om[o1];
+            int rn1 = ind - strd;
+            if (rn1 < 0 || m1.code[rn1] < 0) continue;
+            double phiv1 = 0.5 * (map_phi(g, m1, o1, ind) + map_phi(g, m1, o1, rn1));
+            if (phiv1 > g.eps || phiv0 + phiv1 > g.eps) continue;
+            int c1 = nbo(m1, ad1, 1, FF, 0), c2 = nbo(m1, ad1, 1, FF, -1), c3 = nbo(m1, ad1, -1, FF, 0),
+                c4 = nbo(m1, ad1, -1, FF, -1);
+            int e1 = nbo(m1, ad2, 1, FF, 0), e2 = nbo(m1, ad2, 1, FF, -1), e3 = nbo(m1, ad2, -1, FF, 0),
+                e4 = nbo(m1, ad2, -1, FF, -1);
+            if (c1 < 0 || c2 < 0 || c3 < 0 || c4 < 0 || e1 < 0 || e2 < 0 || e3 < 0 || e4 < 0) continue;
+            double d1[3];
+            grad(m1, o1, rn1, c1, c2, c3, c4, e1, e2, e3, e4, d1);
+            double nv[3], den = 0;
+            for (int nn = 0; nn < 3; nn++) {
+                nv[nn] = d1[nn] - d0[nn];
+                den += nv[nn] * nv[nn];
+            }
+            den = sqrt(den);
+            if (den < 100. * 2.220446049250313e-16) continue;
+            for (int nn = 0; nn < 3; nn++) nv[nn] /= den;
+            const double G1m = g.obj[o1].G;
+            double cf = G0m * coll_func(g, phiv0) + G1m * coll_func(g, phiv1);
+            double cs[3][3];
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) cs[a][b] = -cf * nv[a] * nv[b];
+            double avg = (cs[0][0] + cs[1][1] + cs[2][2]) / 3.;
+            for (int b = 0; b < 3; b++) cs[b][b] -= avg;
+            for (int a = 0; a < 3; a++) out[a] += cs[FF][a];
+        }
+    }
+}
+
+template <int FF>
+__device__ void face_stress(const grid_dev &g, const fields_dev *__restrict__ F, int i, int j, int k, int ind,
+                            bool collide) {
+    const int strides[3] = {1, g.sm4, g.smn4};
+    const double facs[3] = {g.dxsp, g.dysp, g.dzsp};
+    const int strd = strides[FF];
+    const int ad1 = (FF + 1) % 3, ad2 = (FF + 2) % 3;
+    const int pos[3] = {i, j, k};
+    const int ext[3] = {g.sm4, g.sn4, g.so4};
+    double ss[3] = {0, 0, 0};
+    double sfrac = 0;
+    // maps in the reference's order: the primary first, then extrapolations
+    int order[kMaxObj];
+    int nmaps = 0, prim = -1;
+    for (int o = 0; o < g.n_obj; o++) {
+        int cd = F->om[o].code[ind];
+        if (cd == 0) prim = o;
+    }
+    if (prim >= 0) order[nmaps++] = prim;
+    for (int o = 0; o < g.n_obj; o++)
+        if (o != prim && F->om[o].code[ind] > 0) order[nmaps++] = o;
+
+    for (int mi = 0; mi < nmaps; mi++) {
+        const int o = order[mi];
+        const objmap_dev &m = F->om[o];
+        for (int c = 0; c < 3; c++) m.gp[3 * FF + c][ind] = -kBig;
+        m.det[FF][ind] = -kBig;
+        // neighbour inside the local box (get_refmap with a position check)
+        auto nb = [&](int da, int sa, int db, int sb) -> int {
+            int p[3] = {pos[0], pos[1], pos[2]};
+            p[da] += sa;
+            p[db] += sb;
+            for (int d = 0; d < 3; d++)
+                if (p[d] < 0 || p[d] >= ext[d]) return -1;
+            int q = gidx(g, p[0], p[1], p[2]);
+            return has_map(m, q) ? q : -1;
+        };
+        int rn = nb(FF, -1, FF, 0);
+        if (rn < 0) continue;
+        const double ph = map_phi(g, m, o, ind);
+        const double phn = map_phi(g, m, o, rn);
+        double phiv = 0.5 * (ph + phn);
+        if (phiv > g.eps) continue;
+        double tf = heaviside(g, phiv);
+        sfrac += tf;
+        const obj_dev &ob = g.obj[o];
+        double G = ob.G * tf;
+        int r1p = nb(ad1, 1, FF, 0), r1p1 = nb(ad1, 1, FF, -1), r1m = nb(ad1, -1, FF, 0), r1m1 = nb(ad1, -1, FF, -1);
+        int r2p = nb(ad2, 1, FF, 0), r2p1 = nb(ad2, 1, FF, -1), r2m = nb(ad2, -1, FF, 0), r2m1 = nb(ad2, -1, FF, -1);
+        if (r1p < 0 || r1p1 < 0 || r1m < 0 || r1m1 < 0 || r2p < 0 || r2p1 < 0 || r2m < 0 || r2m1 < 0) continue;
+        double gph[3];
+        gph[FF] = facs[FF] * (ph - phn);
+        gph[ad1] = 0.25 * facs[ad1] *
+                   (map_phi(g, m, o, r1p) + map_phi(g, m, o, r1p1) - map_phi(g, m, o, r1m) - map_phi(g, m, o, r1m1));
+        gph[ad2] = 0.25 * facs[ad2] *
+                   (map_phi(g, m, o, r2p) + map_phi(g, m, o, r2p1) - map_phi(g, m, o, r2m) - map_phi(g, m, o, r2m1));
+        {  // ref_map::normalize_grad_phi (fields.hh:382-394)
+            double nrm = 0;
+            for (int c = 0; c < 3; c++) nrm += gph[c] * gph[c];
+            nrm = sqrt(nrm);
+            if (nrm != 0.) {
+                double ninv = 1. / nrm;
+                for (int c = 0; c < 3; c++) gph[c] = ninv * gph[c];
+            }
+        }
+        for (int c = 0; c < 3; c++) m.gp[3 * FF + c][ind] = gph[c];
+        double dR[3][3];
+        for (int nn = 0; nn < 3; nn++) {
+            dR[FF][nn] = facs[FF] * (m.x[nn][ind] - m.x[nn][rn]);
+            dR[ad1][nn] = 0.25 * facs[ad1] * (m.x[nn][r1p] + m.x[nn][r1p1] - m.x[nn][r1m] - m.x[nn][r1m1]);
+            dR[ad2][nn] = 0.25 * facs[ad2] * (m.x[nn][r2p] + m.x[nn][r2p1] - m.x[nn][r2m] - m.x[nn][r2m1]);
+        }
+        // grad_xi(i,j) = dR[j][i], row-major (matlib.hh:160-175)
+        double v[9] = {dR[0][0], dR[1][0], dR[2][0], dR[0][1], dR[1][1], dR[2][1], dR[0][2], dR[1][2], dR[2][2]};
+        // matrix::inverse via the transposed cofactors (matlib.hh:303-329)
+        double d = v[0] * (v[4] * v[8] - v[5] * v[7]) + v[3] * (v[2] * v[7] - v[1] * v[8]) + v[6] * (v[1] * v[5] - v[2] * v[4]);
+        double Fm[9];
+        for (int jj = 0; jj < 3; jj++)
+            for (int ii = 0; ii < 3; ii++) {
+                double cof = v[3 * ((ii + 1) % 3) + (jj + 1) % 3] * v[3 * ((ii + 2) % 3) + (jj + 2) % 3] -
+                             v[3 * ((ii + 1) % 3) + (jj + 2) % 3] * v[3 * ((ii + 2) % 3) + (jj + 1) % 3];
+                Fm[3 * jj + ii] = cof / d;
+            }
+        m.det[FF][ind] = Fm[0] * (Fm[4] * Fm[8] - Fm[5] * Fm[7]) + Fm[3] * (Fm[2] * Fm[7] - Fm[1] * Fm[8]) +
+                         Fm[6] * (Fm[1] * Fm[5] - Fm[2] * Fm[4]);
+        // left Cauchy-Green F F^T as a symmetric matrix (matlib.hh:214-229)
+        double sg[3][3];
+        for (int a = 0; a < 3; a++)
+            for (int b = a; b < 3; b++) {
+                double val = 0;
+                for (int kk = 0; kk < 3; kk++) val += Fm[3 * a + kk] * Fm[3 * b + kk];
+                sg[a][b] = sg[b][a] = val;
+            }
+        double avg = (sg[0][0] + sg[1][1] + sg[2][2]) / 3.0;
+        for (int nn = 0; nn < 3; nn++) sg[nn][nn] -= avg;
+        double ex_mu = ob.ex_mu * tf * (1 + ob.ev_trans_mult * tderiv_func_in(g, phiv));
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) sg[a][b] *= G;
+        for (int nn = 0; nn < 3; nn++) {
+            const double *vn = F->vel[nn];
+            const double *vF = F->vel[FF];
+            ss[nn] += sg[FF][nn];
+            double tang;
+            if (nn == FF) {
+                tang = vn[ind] - vn[ind - strd];
+            } else {
+                int sn_ = strides[nn];
+                tang = 0.25 * (vF[ind + sn_] + vF[ind + sn_ - strd] - vF[ind - sn_] - vF[ind - sn_ - strd]);
+            }
+            ss[nn] += ex_mu * facs[FF] * ((vn[ind] - vn[ind - strd]) + tang);
+        }
+    }
+    double out[3];
+    if (sfrac >= 1) {
+        for (int s = 0; s < 3; s++) out[s] = ss[s] / sfrac;
+    } else {
+        double fs[3];
+        for (int nn = 0; nn < 3; nn++) fs[nn] = g.mu * facs[FF] * (F->vel[nn][ind] - F->vel[nn][ind - strd]);
+        for (int s = 0; s < 3; s++) out[s] = (1 - sfrac) * fs[s] + ss[s];
+    }
+    if (collide && nmaps > 1) collision_face<FF>(g, F, i, j, k, ind, order, nmaps, out);
+    for (int s = 0; s < 3; s++) F->sigma[3 * FF + s][ind] = out[s];
+}
+
+__global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.sm + 2 || j > g.sn + 2 || k > g.so + 2) return;
+    const int ind = gidx(g, i, j, k);
+    face_stress<0>(g, F, i, j, k, ind, true);
+    face_stress<1>(g, F, i, j, k, ind, true);
+    face_stress<2>(g, F, i, j, k, ind, true);
+}
+
+// -------------------------------------------------------------------------
+// Acceleration at a cell centre, fluid_3d::acceleration (fluid_3d.cc:980-1033)
+// with neg_pres_grad (:2347-2361) and the sim_manager body/solid forces
+// (Sim/sim_manager.cc:133-295).
+// -------------------------------------------------------------------------
+__device__ inline void solid_accel(const grid_dev &g, int o, const double rv[3], double x, double y, double z,
+                                   double t, double &fx, double &fy, double &fz) {
+    fx = fy = fz = 0;
+    if (g.sim_type != 2) return;  // base sim_manager: no solid forces
+    // sim_objects::solid_acceleration (sim_manager.cc:212-295) with the
+    // average object velocities at their reset value 0 (no macro output)
+    double krep = g.min_wall_acc;
+    double phiv = obj_phi(g, o, rv[0], rv[1], rv[2]);
+    const double h[3] = {g.dx, g.dy, g.dz};
+    const double hs[3] = {g.dxsp, g.dysp, g.dzsp};
+    const double pos[3] = {x, y, z};
+    double f[3] = {0, 0, 0};
+    for (int a = 0; a < 3; a++) {
+        // wall_trans_func(phiv, h, 1/h) (sim_manager.hh:281-285)
+        double wt;
+        if (phiv < -h[a]) wt = 1;
+        else if (phiv < h[a]) wt = 0.5 * (1 - phiv * hs[a]);
+        else wt = 0;
+        if (g.walls[2 * a]) {
+            double dist = pos[a] - g.wall_pos[2 * a];
+            if (dist <= g.wall_dist) {
+                double xx = dist * g.winv;
+                double del = (xx <= 0) ? 100 : (1 - xx) / xx;
+                f[a] += del * krep * wt;
+            }
+        }
+        if (g.walls[2 * a + 1]) {
+            double dist = g.wall_pos[2 * a + 1] - pos[a];
+            if (dist <= g.wall_dist) {
+                double xx = dist * g.winv;
+                double del = (xx <= 0) ? 100 : (1 - xx) / xx;
+                f[a] -= del * krep * wt;
+            }
+        }
+    }
+    fx = f[0];
+    fy = f[1];
+    fz = f[2];
+    double f_norm = sqrt(fx * fx + fy * fy + fz * fz);
+    if (f_norm >= g.K_stiff) {
+        double nf = g.K_stiff / f_norm;
+        fx *= nf;
+        fy *= nf;
+        fz *= nf;
+    }
+    // spheres have no anchors: dtoe1 = dtoe2 = 2 eps gives K = 0 (object.hh:62-64)
+    double Kh = g.K_stiff * heaviside(g, 2 * g.eps) * heaviside(g, 2 * g.eps);
+    fx -= Kh * 0;
+    fy -= Kh * 0;
+    fz -= Kh * 0;
+    fz += g.gravity * heaviside(g, phiv);
+}
+
+__device__ inline void fluid_accel(const grid_dev &g, double x, double y, double z, double t, double &fx, double &fy,
+                                   double &fz) {
+    if (g.sim_type == 0) {  // sim_ftest::fluid_acceleration (sim_manager.cc:169-178)
+        const double PI = 3.14159265358979323846;
+        double mu = g.mu;
+        fx = (12 * PI * cos(2 * PI * y) * cos(2 * PI * z) * (-6 * PI * mu * cos(2 * PI * t) + sin(2 * PI * t)) *
+                  sin(2 * PI * x) +
+              PI * cos(2 * PI * t) * cos(2 * PI * t) * (2 + cos(4 * PI * y) + cos(4 * PI * z)) * sin(4 * PI * x)) /
+             4;
+        fy = -(PI * cos(2 * PI * t) * cos(2 * PI * t) * (-1 + cos(4 * PI * x) - 2 * cos(4 * PI * z)) * sin(4 * PI * y)) / 8;
+        fz = -(PI * cos(2 * PI * t) * cos(2 * PI * t) * (-1 + cos(4 * PI * x) - 2 * cos(4 * PI * y)) * sin(4 * PI * z)) / 8;
+    } else if (g.sim_type == 2) {  // sim_objects: gravity (sim_manager.hh:400-404)
+        fx = fy = 0;
+        fz = 0;
+        fz += g.gravity;
+    } else {
+        fx = fy = fz = 0;
+    }
+}
+
+__device__ void acceleration(const grid_dev &g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                             const double *lz, int i, int j, int k, double t, bool var_den, double acc[3]) {
+    const int ind = gidx(g, i, j, k);
+    const int s1 = g.sm4, s2 = g.smn4;
+    for (int c = 0; c < 3; c++) {
+        const double *s0 = F->sigma[c], *sy = F->sigma[3 + c], *sz = F->sigma[6 + c];
+        acc[c] += g.dxsp * (s0[ind + 1] - s0[ind]) + g.dysp * (sy[ind + s1] - sy[ind]) + g.dzsp * (sz[ind + s2] - sz[ind]);
+    }
+    // neg_pres_grad: -grad p from the 8 nodal pressures around the cell
+    double pr[8];
+    for (int n = 0; n < 8; n++) pr[n] = F->p[ind + n % 2 + s1 * ((n / 2) % 2) + (n / 4) * s2];
+    double xa = 0, ya = 0, za = 0;
+    for (int n = 0; n < 4; n++) {
+        xa += pr[2 * n + 1] - pr[2 * n];
+        int yi = (n / 2) * 4 + n % 2;
+        ya += pr[yi + 2] - pr[yi];
+        za += pr[n + 4] - pr[n];
+    }
+    xa *= -0.25 * g.dxsp;
+    ya *= -0.25 * g.dysp;
+    za *= -0.25 * g.dzsp;
+    double tmp[3] = {xa, ya, za};
+    for (int c = 0; c < 3; c++) {
+        acc[c] += tmp[c];
+        if (var_den) acc[c] /= F->rho[ind];
+    }
+    for (int c = 0; c < 3; c++) tmp[c] = 0.;
+    double anc[3] = {0, 0, 0};
+    double sfrac = 0;
+    const double xx = lx[i], yy = ly[j], zz = lz[k];
+    for (int o = 0; o < g.n_obj; o++) {
+        const objmap_dev &m = F->om[o];
+        if (m.code[ind] < 0) continue;
+        double rv[3] = {m.x[0][ind], m.x[1][ind], m.x[2][ind]};
+        double phiv = obj_phi(g, o, rv[0], rv[1], rv[2]);
+        if (phiv < g.eps) {
+            double lfrac = heaviside(g, phiv);
+            solid_accel(g, o, rv, xx, yy, zz, t, anc[0], anc[1], anc[2]);
+            for (int nn = 0; nn < 3; nn++) tmp[nn] += anc[nn];
+            sfrac += lfrac;
+        }
+    }
+    if (sfrac > 1.)
+        for (int nn = 0; nn < 3; nn++) tmp[nn] /= sfrac;
+    for (int nn = 0; nn < 3; nn++) acc[nn] += tmp[nn];
+    if (sfrac < 1.) {
+        fluid_accel(g, xx, yy, zz, t, anc[0], anc[1], anc[2]);
+        for (int nn = 0; nn < 3; nn++) acc[nn] += anc[nn] * (1 - sfrac);
+    }
+}
+
+// -------------------------------------------------------------------------
+// Limited slopes + half-step edge extrapolation of the velocity:
+// normal_derivatives_velocity (fluid_3d.cc:582-617) fused with
+// compute_half_time_edge_velocities (:1038-1066) and field::godunov_extrap
+// (fields.hh:147-177, non-TANG branch).  Interior cells.
+// -------------------------------------------------------------------------
+__global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                           const double *lz, double cdt, double time, int var_den) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
+    if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
+    const int ind = gidx(g, i, j, k);
+    const int strides[3] = {1, g.sm4, g.smn4};
+    const double dhsp[3] = {g.dxsp, g.dysp, g.dzsp};
+    double nv[3][3];
+    double vel[3];
+    for (int c = 0; c < 3; c++) vel[c] = F->vel[c][ind];
+    for (int d = 0; d < 3; d++) {
+        int s = strides[d];
+        for (int c = 0; c < 3; c++) {
+            const double *u = F->vel[c];
+            nv[d][c] = dhsp[d] * mono_diff(u[ind - 2 * s], u[ind - s], u[ind], u[ind + s], u[ind + 2 * s]);
+        }
+    }
+    double acc[3] = {0, 0, 0};
+    acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
+    const double dh2[3] = {g.dx / 2, g.dy / 2, g.dz / 2};
+    const double dt2 = cdt / 2.0;
+    double adv[3] = {0, 0, 0};
+    for (int a = 0; a < 3; a++) {
+        for (int b = 0; b < 3; b++) adv[a] -= vel[b] * nv[b][a];
+        adv[a] *= dt2;
+    }
+    for (int f = 0; f < 6; f++) {
+        int dim = f / 2;
+        double d = dh2[dim] * (2 * (f % 2) - 1);
+        for (int c = 0; c < 3; c++) F->fvel[3 * f + c][ind] = vel[c] + d * nv[dim][c] + adv[c] + dt2 * acc[c];
+    }
+}
+
+// -------------------------------------------------------------------------
+// Godunov upwinding on every upper face from relative index -1,
+// fluid_3d::godunov_upwinding_set (fluid_3d.cc:811-944) with
+// godunov_set_velocity (:2156-2176) and godunov_set_refmap (:2184-2204).
+// The reference-map pairs are upwinded first, with the fluid states still
+// unmodified, exactly as the reference's per-cell loop does.
+// -------------------------------------------------------------------------
+__device__ inline void set_refmap(double norml, double normr, double &ml, double &vl, double &wl, double &mr,
+                                  double &vr, double &wr) {
+    if (norml + normr > 0 && norml > 0) {
+        mr = ml;
+        vr = vl;
+        wr = wl;
+    } else if (norml + normr < 0 && normr < 0) {
+        ml = mr;
+        vl = vr;
+        wl = wr;
+    } else {
+        double t = 0.5 * (ml + mr);
+        ml = mr = t;
+        t = 0.5 * (vl + vr);
+        vl = vr = t;
+        t = 0.5 * (wl + wr);
+        wl = wr = t;
+    }
+}
+
+__global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
+    const int ind = gidx(g, i, j, k);
+    const int strides[3] = {1, g.sm4, g.smn4};
+    for (int o = 0; o < g.n_obj; o++) {
+        const objmap_dev &m = F->om[o];
+        int cd = m.code[ind];
+        if (cd < 0) continue;
+        bool go = (cd == 0);
+        if (!go) {  // an extrapolated map with a primary neighbour on its upper side (neigh_inside)
+            for (int d = 0; d < 3 && !go; d++)
+                if (m.code[ind + strides[d]] == 0) go = true;
+        }
+        if (!go) continue;
+        for (int dir = 0; dir < 3; dir++) {
+            const int nb = ind + strides[dir];
+            const int ff = 2 * dir + 1, nf = ff ^ 1;
+            const int a1 = (dir + 1) % 3, a2 = (dir + 2) % 3;
+            double norml = F->fvel[3 * ff + dir][ind];
+            double normr = F->fvel[3 * nf + dir][nb];
+            double ml = m.fx[3 * ff + dir][ind], vl = m.fx[3 * ff + a1][ind], wl = m.fx[3 * ff + a2][ind];
+            double mr = m.fx[3 * nf + dir][nb], vr = m.fx[3 * nf + a1][nb], wr = m.fx[3 * nf + a2][nb];
+            set_refmap(norml, normr, ml, vl, wl, mr, vr, wr);
+            m.fx[3 * ff + dir][ind] = ml;
+            m.fx[3 * ff + a1][ind] = vl;
+            m.fx[3 * ff + a2][ind] = wl;
+            m.fx[3 * nf + dir][nb] = mr;
+            m.fx[3 * nf + a1][nb] = vr;
+            m.fx[3 * nf + a2][nb] = wr;
+        }
+    }
+    for (int dir = 0; dir < 3; dir++) {
+        const int nb = ind + strides[dir];
+        const int ff = 2 * dir + 1, nf = ff ^ 1;
+        const int a1 = (dir + 1) % 3, a2 = (dir + 2) % 3;
+        double nl = F->fvel[3 * ff + dir][ind], vl = F->fvel[3 * ff + a1][ind], wl = F->fvel[3 * ff + a2][ind];
+        double nr = F->fvel[3 * nf + dir][nb], vr = F->fvel[3 * nf + a1][nb], wr = F->fvel[3 * nf + a2][nb];
+        if (nl + nr > 0 && nl > 0) {
+            nr = nl;
+            vr = vl;
+            wr = wl;
+        } else if (nl + nr < 0 && nr < 0) {
+            nl = nr;
+            vl = vr;
+            wl = wr;
+        } else {
+            nl = nr = 0;
+            double t = 0.5 * (vl + vr);
+            vl = vr = t;
+            t = 0.5 * (wl + wr);
+            wl = wr = t;
+        }
+        F->fvel[3 * ff + dir][ind] = nl;
+        F->fvel[3 * ff + a1][ind] = vl;
+        F->fvel[3 * ff + a2][ind] = wl;
+        F->fvel[3 * nf + dir][nb] = nr;
+        F->fvel[3 * nf + a1][nb] = vr;
+        F->fvel[3 * nf + a2][nb] = wr;
+    }
+}
+
+// -------------------------------------------------------------------------
+// MAC projection: rhs (fill_mac_rhs, fluid_3d.cc:2244-2265), solution
+// extraction (:2268-2281) and face correction (subtract_q_grad, :2284-2304).
+// -------------------------------------------------------------------------
+__global__ void k_mac_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, double cdt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.sm || j >= g.sn || k >= g.so) return;
+    const int ind = gidx(g, i + 2, j + 2, k + 2);
+    const double fac = g.dx / (2 * cdt);
+    double s = 0;
+    for (int f = 0; f < 3; f++) s += fac * (F->fvel[3 * (2 * f + 1) + f][ind] - F->fvel[3 * (2 * f) + f][ind]);
+    r[i + g.sm * (j + g.sn * k)] = s;
+}
+
+__global__ void k_mac_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.sm || j >= g.sn || k >= g.so) return;
+    F->q[gidx(g, i + 2, j + 2, k + 2)] = x[i + g.sm * (j + g.sn * k)];
+}
+
+__global__ void k_sub_qgrad(grid_dev g, const fields_dev *__restrict__ F, double cdt, int var_den) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
+    if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
+    const int ind = gidx(g, i, j, k);
+    const int strides[3] = {1, g.sm4, g.smn4};
+    const double fac = 2 * cdt * g.dxsp;
+    const double *q = F->q;
+    for (int f = 0; f < 3; f++) {
+        int s = strides[f];
+        double down, up;
+        if (var_den) {
+            const double *rho = F->rho;
+            down = fac * (q[ind] - q[ind - s]) / (0.5 * (rho[ind] + rho[ind - s]));
+            up = fac * (q[ind + s] - q[ind]) / (0.5 * (rho[ind + s] + rho[ind]));
+        } else {
+            down = fac * (q[ind] - q[ind - s]);
+            up = fac * (q[ind + s] - q[ind]);
+        }
+        F->fvel[3 * (2 * f) + f][ind] -= down;
+        F->fvel[3 * (2 * f + 1) + f][ind] -= up;
+    }
+}
+
+// -------------------------------------------------------------------------
+// Explicit momentum update, fluid_3d::compute_ustar (fluid_3d.cc:1309-1352).
+// -------------------------------------------------------------------------
+__global__ void k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                        const double *lz, double cdt, double time, int var_den) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
+    if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
+    const int ind = gidx(g, i, j, k);
+    double acc[3] = {0, 0, 0};
+    acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
+    double fv[18];
+    for (int a = 0; a < 18; a++) fv[a] = F->fvel[a][ind];
+    double avgs[3];
+    avgs[0] = -0.5 * cdt * (fv[0] + fv[3]) * g.dxsp;
+    avgs[1] = -0.5 * cdt * (fv[3 * 2 + 1] + fv[3 * 3 + 1]) * g.dysp;
+    avgs[2] = -0.5 * cdt * (fv[3 * 4 + 2] + fv[3 * 5 + 2]) * g.dzsp;
+    double dv[3];
+    for (int d = 0; d < 3; d++) {
+        dv[d] = avgs[0] * (fv[3 + d] - fv[d]) + avgs[1] * (fv[9 + d] - fv[6 + d]) + avgs[2] * (fv[15 + d] - fv[12 + d]);
+        acc[d] *= cdt;
+    }
+    for (int d = 0; d < 3; d++) dv[d] += acc[d];
+    for (int d = 0; d < 3; d++) {
+        double dd = 0.;
+        dd += dv[d];
+        F->dvel[d][ind] = dd;
+        F->vel[d][ind] += dd;
+    }
+}
+
+// -------------------------------------------------------------------------
+// FEM projection right-hand side, fluid_3d::fill_pp_rhs (fluid_3d.cc:
+// 2554-2649), written as a gather over the (up to) eight elements around each
+// node in the reference's element order, followed by the domain-face flux
+// terms in face order.  One thread per FEM node.
+// -------------------------------------------------------------------------
+__device__ inline bool elem_in_domain(const grid_dev &g, int ei, int ej, int ek) {
+    return (g.prd[0] || (ei >= 0 && ei <= g.sm - 1)) && (g.prd[1] || (ej >= 0 && ej <= g.sn - 1)) &&
+           (g.prd[2] || (ek >= 0 && ek <= g.so - 1));
+}
+
+__global__ void k_fem_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, gradphi_t gp) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    int b = blockIdx.y * blockDim.y + threadIdx.y;
+    int c = blockIdx.z * blockDim.z + threadIdx.z;
+    if (a >= g.fm || b >= g.fn || c >= g.fo) return;
+    double s = 0;
+    // element (ei,ej,ek) touches node (a,b,c) as local node (a-ei)+2(b-ej)+4(c-ek)
+    for (int ek = c - 1; ek <= c; ek++)
+        for (int ej = b - 1; ej <= b; ej++)
+            for (int ei = a - 1; ei <= a; ei++) {
+                if (ei < -1 || ej < -1 || ek < -1) continue;
+                if (ei > g.fm - 1 || ej > g.fn - 1 || ek > g.fo - 1) continue;
+                if (!elem_in_domain(g, ei, ej, ek)) continue;
+                const int n = (a - ei) + 2 * (b - ej) + 4 * (c - ek);
+                const int ind = gidx(g, ei + 2, ej + 2, ek + 2);
+                double val = 0;
+                for (int l = 0; l < 3; l++) val += F->dvel[l][ind] * gp.v[n][l];
+                s += val;
+            }
+    // domain-face flux terms of non-periodic faces (fluid_3d.cc:2585-2645)
+    const int node[3] = {a, b, c};
+    const int fdim[3] = {g.fm, g.fn, g.fo};
+    for (int face = 0; face < 6; face++) {
+        const int nd = face / 2;
+        if (g.prd[nd]) continue;
+        const int side = face % 2;
+        // nodes on this face: node[nd] == 0 (lower) or == len (upper)
+        if (node[nd] != (side ? fdim[nd] - 1 : 0)) continue;
+        const int t0 = (nd == 0) ? 1 : 0, t1 = (nd == 2) ? 1 : 2;
+        // boundary cells around the node in the reference's loop order
+        for (int c1 = node[t1] - 1; c1 <= node[t1]; c1++)
+            for (int c0 = node[t0] - 1; c0 <= node[t0]; c0++) {
+                int e[3];
+                e[nd] = side ? fdim[nd] - 2 : 0;
+                e[t0] = c0;
+                e[t1] = c1;
+                if (e[t0] < -1 || e[t1] < -1) continue;
+                const int lens[3] = {g.sm, g.sn, g.so};
+                if (e[t0] > lens[t0] || e[t1] > lens[t1]) continue;
+                if (!elem_in_domain(g, e[0], e[1], e[2])) continue;
+                int inds[3];
+                inds[nd] = side;
+                inds[t0] = node[t0] - e[t0];
+                inds[t1] = node[t1] - e[t1];
+                // node validity as in map_ref_to_local
+                bool ok = true;
+                for (int d = 0; d < 3; d++) {
+                    int nn = e[d] + inds[d];
+                    if (nn > fdim[d] - 1) ok = false;
+                    if (e[d] < 0 && inds[d] == 0) ok = false;
+                }
+                if (!ok) continue;
+                const int lid = inds[0] + 2 * inds[1] + 4 * inds[2];
+                const int cell = gidx(g, e[0] + 2, e[1] + 2, e[2] + 2);
+                double val = -F->fvel[3 * face + nd][cell] * gp.v[lid][nd];
+                s += val;
+            }
+    }
+    r[a + g.fm * (b + g.fn * c)] = s;
+}
+
+// p += x - mean, dp = x - mean over FEM nodes (extract_pp_soln, :2685-2712)
+__global__ void k_fem_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x, const double *mean) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    int b = blockIdx.y * blockDim.y + threadIdx.y;
+    int c = blockIdx.z * blockDim.z + threadIdx.z;
+    if (a >= g.fm || b >= g.fn || c >= g.fo) return;
+    const double m = *mean;
+    const double v = x[a + g.fm * (b + g.fn * c)];
+    const int ind = gidx(g, a + 2, b + 2, c + 2);
+    F->p[ind] += (v - m);
+    F->dp[ind] = (v - m);
+}
+
+// u, dvel -= dt grad(dp), subtract_pres_grad (:2717-2753) with neg_pres_dgrad
+__global__ void k_sub_pgrad(grid_dev g, const fields_dev *__restrict__ F, double dt, int var_den) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
+    if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
+    const int ind = gidx(g, i, j, k);
+    const int s1 = g.sm4, s2 = g.smn4;
+    double pr[8];
+    for (int n = 0; n < 8; n++) pr[n] = F->dp[ind + n % 2 + s1 * ((n / 2) % 2) + (n / 4) * s2];
+    double xa = 0, ya = 0, za = 0;
+    for (int n = 0; n < 4; n++) {
+        xa += pr[2 * n + 1] - pr[2 * n];
+        int yi = (n / 2) * 4 + n % 2;
+        ya += pr[yi + 2] - pr[yi];
+        za += pr[n + 4] - pr[n];
+    }
+    xa *= -0.25 * g.dxsp;
+    ya *= -0.25 * g.dysp;
+    za *= -0.25 * g.dzsp;
+    double npg[3] = {xa, ya, za};
+    for (int c = 0; c < 3; c++) {
+        if (var_den) npg[c] *= dt / F->rho[ind];
+        else npg[c] *= dt;
+        F->vel[c][ind] += npg[c];
+        F->dvel[c][ind] += npg[c];
+    }
+}
+
+}  // namespace rmt3d

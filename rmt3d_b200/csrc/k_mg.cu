@@ -1,0 +1,527 @@
+// Multigrid kernels and V-cycle driver (see mg.h).
+//
+// Operators (rediscretised on every level, nothing stored):
+//  * MAC, cell centred: 7-point [1 ... -6]; at a wall the missing face
+//    neighbour moves onto the centre (Neumann fix of stencil_set::set_partials
+//    with macfix, mg_probs.hh:281-343).  Coarsening pairs cells; restriction
+//    sums the 8 children with weight 1/2 (the (2h)^2 scaling of the coarse
+//    operator); prolongation is cell-centred trilinear (3/4, 1/4 per axis,
+//    constant extension at walls).  Red-black Gauss-Seidel smoothing.
+//  * FEM, nodal: 27-point Q1 stencil 32/-2/-1 (faces 0); each entry is halved
+//    once per non-periodic axis on which the node lies on the boundary and the
+//    offset along that axis is zero (set_partials(false)).  Vertex coarsening
+//    (coarse node I on fine node 2I), trilinear prolongation P and restriction
+//    P^T/2, which equals the Galerkin operator P^T A P of this stencil.
+//    Eight-colour Gauss-Seidel (exact GS ordering for a 27-point stencil).
+// Residual max norms are reduced with warp shuffles and one atomic per warp.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "host_common.h"
+#include "mg.h"
+#include "rmt3d_gpu.h"
+
+namespace rmt3d {
+
+struct lvl_dev {
+    int n0, n1, n2;
+    int p0, p1, p2;
+};
+
+__device__ __forceinline__ int wrapi(int v, int n, int prd) {
+    if (v < 0) return prd ? v + n : -1;
+    if (v >= n) return prd ? v - n : -1;
+    return v;
+}
+
+// ---- operator application -------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T mac_offdiag(const lvl_dev L, const T *__restrict__ x, int i, int j, int k, T &diag) {
+    T s = 0;
+    int missing = 0;
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int c[3] = {i, j, k};
+    const int st[3] = {1, L.n0, L.n0 * L.n1};
+    const int base = i + L.n0 * (j + L.n1 * k);
+    for (int d = 0; d < 3; d++) {
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+            int v = wrapi(c[d] + sgn, n[d], p[d]);
+            if (v < 0) {
+                missing++;
+                continue;
+            }
+            s += x[base + (v - c[d]) * st[d]];
+        }
+    }
+    diag = (T)(-6 + missing);
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T fem_offdiag(const lvl_dev L, const T *__restrict__ x, int i, int j, int k, T &diag) {
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int c[3] = {i, j, k};
+    bool bd[3];
+    for (int d = 0; d < 3; d++) bd[d] = !p[d] && (c[d] == 0 || c[d] == n[d] - 1);
+    int nb[3][3];
+    for (int d = 0; d < 3; d++)
+        for (int o = -1; o <= 1; o++) nb[d][o + 1] = wrapi(c[d] + o, n[d], p[d]);
+    T s = 0;
+    for (int oc = 0; oc < 3; oc++) {
+        int kk = nb[2][oc];
+        if (kk < 0) continue;
+        for (int ob = 0; ob < 3; ob++) {
+            int jj = nb[1][ob];
+            if (jj < 0) continue;
+            const T *row = x + (size_t)L.n0 * (jj + (size_t)L.n1 * kk);
+            for (int oa = 0; oa < 3; oa++) {
+                int ii = nb[0][oa];
+                if (ii < 0) continue;
+                int nz = (oa != 1) + (ob != 1) + (oc != 1);
+                if (nz == 0 || nz == 1) continue;  // centre handled below, faces are 0
+                T co = (nz == 2) ? (T)-2 : (T)-1;
+                int halve = (bd[0] && oa == 1) + (bd[1] && ob == 1) + (bd[2] && oc == 1);
+                if (halve == 1) co *= (T)0.5;
+                else if (halve == 2) co *= (T)0.25;
+                s += co * row[ii];
+            }
+        }
+    }
+    int hc = bd[0] + bd[1] + bd[2];
+    diag = (T)32 / (T)(1 << hc);
+    return s;
+}
+
+// ---- smoothing -------------------------------------------------------------
+template <typename T>
+__global__ void k_mac_rb(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int colour) {
+    int hi = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (j >= L.n1 || k >= L.n2) return;
+    int i = 2 * hi + ((j + k + colour) & 1);
+    if (i >= L.n0) return;
+    T diag;
+    T s = mac_offdiag(L, x, i, j, k, diag);
+    int id = i + L.n0 * (j + L.n1 * k);
+    x[id] = (r[id] - s) / diag;
+}
+
+template <typename T>
+__global__ void k_fem_gs(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int colour) {
+    int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + (colour & 1);
+    int j = 2 * (blockIdx.y * blockDim.y + threadIdx.y) + ((colour >> 1) & 1);
+    int k = 2 * (blockIdx.z * blockDim.z + threadIdx.z) + ((colour >> 2) & 1);
+    if (i >= L.n0 || j >= L.n1 || k >= L.n2) return;
+    T diag;
+    T s = fem_offdiag(L, x, i, j, k, diag);
+    int id = i + L.n0 * (j + L.n1 * k);
+    x[id] = (r[id] - s) / diag;
+}
+
+// residual res = r - A x, and max |res| into *mx (as ordered bit pattern)
+template <typename T, int KIND>
+__global__ void k_resid(lvl_dev L, const T *__restrict__ x, const T *__restrict__ r, T *__restrict__ res,
+                        unsigned long long *mx) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    double a = 0;
+    if (i < L.n0 && j < L.n1 && k < L.n2) {
+        T diag;
+        T s = (KIND == 0) ? mac_offdiag(L, x, i, j, k, diag) : fem_offdiag(L, x, i, j, k, diag);
+        int id = i + L.n0 * (j + L.n1 * k);
+        T v = r[id] - s - diag * x[id];
+        if (res) res[id] = v;
+        a = fabs((double)v);
+        if (a != a) a = __longlong_as_double(0x7ff8000000000000LL);
+    }
+    if (mx) {
+        unsigned long long b = (unsigned long long)__double_as_longlong(a);
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
+            b = t > b ? t : b;
+        }
+        if ((threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) % 32 == 0) atomicMax(mx, b);
+    }
+}
+
+// ---- grid transfer ---------------------------------------------------------
+template <typename T>
+__global__ void k_mac_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, T *__restrict__ rc) {
+    int I = blockIdx.x * blockDim.x + threadIdx.x;
+    int J = blockIdx.y * blockDim.y + threadIdx.y;
+    int K = blockIdx.z * blockDim.z + threadIdx.z;
+    if (I >= C.n0 || J >= C.n1 || K >= C.n2) return;
+    T s = 0;
+    for (int c = 0; c < 2; c++)
+        for (int b = 0; b < 2; b++)
+            for (int a = 0; a < 2; a++) s += res[(2 * I + a) + F.n0 * ((2 * J + b) + F.n1 * (2 * K + c))];
+    rc[I + C.n0 * (J + C.n1 * K)] = (T)0.5 * s;
+}
+
+template <typename T>
+__global__ void k_mac_prolong(lvl_dev F, lvl_dev C, T *__restrict__ x, const T *__restrict__ xc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= F.n0 || j >= F.n1 || k >= F.n2) return;
+    const int f[3] = {i, j, k};
+    const int nc[3] = {C.n0, C.n1, C.n2}, p[3] = {C.p0, C.p1, C.p2};
+    int ci[3][2];
+    T w[3][2];
+    for (int d = 0; d < 3; d++) {
+        int I = f[d] >> 1;
+        int J = wrapi(I + ((f[d] & 1) ? 1 : -1), nc[d], p[d]);
+        ci[d][0] = I;
+        if (J < 0) {
+            w[d][0] = 1;
+            ci[d][1] = I;
+            w[d][1] = 0;
+        } else {
+            w[d][0] = (T)0.75;
+            ci[d][1] = J;
+            w[d][1] = (T)0.25;
+        }
+    }
+    T e = 0;
+    for (int c = 0; c < 2; c++)
+        for (int b = 0; b < 2; b++)
+            for (int a = 0; a < 2; a++) {
+                T wt = w[0][a] * w[1][b] * w[2][c];
+                if (wt != 0) e += wt * xc[ci[0][a] + C.n0 * (ci[1][b] + C.n1 * ci[2][c])];
+            }
+    x[i + F.n0 * (j + F.n1 * k)] += e;
+}
+
+template <typename T>
+__global__ void k_fem_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, T *__restrict__ rc) {
+    int I = blockIdx.x * blockDim.x + threadIdx.x;
+    int J = blockIdx.y * blockDim.y + threadIdx.y;
+    int K = blockIdx.z * blockDim.z + threadIdx.z;
+    if (I >= C.n0 || J >= C.n1 || K >= C.n2) return;
+    const int nf[3] = {F.n0, F.n1, F.n2}, p[3] = {F.p0, F.p1, F.p2};
+    const int c[3] = {I, J, K};
+    int idx[3][3];
+    T w[3][3];
+    for (int d = 0; d < 3; d++)
+        for (int o = -1; o <= 1; o++) {
+            int v = wrapi(2 * c[d] + o, nf[d], p[d]);
+            idx[d][o + 1] = v;
+            w[d][o + 1] = (v < 0) ? (T)0 : (o == 0 ? (T)1 : (T)0.5);
+        }
+    T s = 0;
+    for (int oc = 0; oc < 3; oc++) {
+        if (idx[2][oc] < 0) continue;
+        for (int ob = 0; ob < 3; ob++) {
+            if (idx[1][ob] < 0) continue;
+            for (int oa = 0; oa < 3; oa++) {
+                if (idx[0][oa] < 0) continue;
+                s += w[0][oa] * w[1][ob] * w[2][oc] * res[idx[0][oa] + F.n0 * (idx[1][ob] + F.n1 * idx[2][oc])];
+            }
+        }
+    }
+    rc[I + C.n0 * (J + C.n1 * K)] = (T)0.5 * s;
+}
+
+template <typename T>
+__global__ void k_fem_prolong(lvl_dev F, lvl_dev C, T *__restrict__ x, const T *__restrict__ xc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= F.n0 || j >= F.n1 || k >= F.n2) return;
+    const int f[3] = {i, j, k};
+    const int nc[3] = {C.n0, C.n1, C.n2}, p[3] = {C.p0, C.p1, C.p2};
+    int ci[3][2];
+    T w[3][2];
+    int cnt[3];
+    for (int d = 0; d < 3; d++) {
+        if ((f[d] & 1) == 0) {
+            ci[d][0] = f[d] >> 1;
+            w[d][0] = 1;
+            cnt[d] = 1;
+        } else {
+            ci[d][0] = f[d] >> 1;
+            ci[d][1] = wrapi((f[d] >> 1) + 1, nc[d], p[d]);
+            w[d][0] = w[d][1] = (T)0.5;
+            cnt[d] = 2;
+        }
+    }
+    T e = 0;
+    for (int c = 0; c < cnt[2]; c++)
+        for (int b = 0; b < cnt[1]; b++)
+            for (int a = 0; a < cnt[0]; a++)
+                e += w[0][a] * w[1][b] * w[2][c] * xc[ci[0][a] + C.n0 * (ci[1][b] + C.n1 * ci[2][c])];
+    x[i + F.n0 * (j + F.n1 * k)] += e;
+}
+
+// coarsest grid: many Gauss-Seidel sweeps inside one thread block
+template <typename T, int KIND>
+__global__ void k_coarse_solve(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int sweeps) {
+    const int np = L.n0 * L.n1 * L.n2;
+    for (int p = threadIdx.x; p < np; p += blockDim.x) x[p] = 0;
+    __syncthreads();
+    const int ncol = (KIND == 0) ? 2 : 8;
+    for (int s = 0; s < sweeps; s++)
+        for (int col = 0; col < ncol; col++) {
+            for (int p = threadIdx.x; p < np; p += blockDim.x) {
+                int i = p % L.n0, j = (p / L.n0) % L.n1, k = p / (L.n0 * L.n1);
+                int my = (KIND == 0) ? ((i + j + k) & 1) : ((i & 1) | ((j & 1) << 1) | ((k & 1) << 2));
+                if (my != col) continue;
+                T diag;
+                T sum = (KIND == 0) ? mac_offdiag(L, x, i, j, k, diag) : fem_offdiag(L, x, i, j, k, diag);
+                x[p] = (r[p] - sum) / diag;
+            }
+            __syncthreads();
+        }
+}
+
+// FP64 <-> FP32 helpers of the mixed form
+__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, size_t n) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_add_f32(double *__restrict__ a, const float *__restrict__ b, size_t n) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] += (double)b[i];
+}
+template <typename T>
+__global__ void k_zero(T *a, size_t n) {
+    size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 0;
+}
+
+// ---- host side -----------------------------------------------------------
+static lvl_dev dev_of(const mg_level &l) { return lvl_dev{l.n[0], l.n[1], l.n[2], l.prd[0], l.prd[1], l.prd[2]}; }
+
+static dim3 blk3() { return dim3(32, 4, 2); }
+static dim3 grid3(int a, int b, int c) { return dim3((a + 31) / 32, (b + 3) / 4, (c + 1) / 2); }
+
+void mg_pred_state::update(int extras) {
+    double dV = iV - V_avg;
+    int exreduce = static_cast<int>(dV / sqrt(V_var));
+    exreduce = exreduce > 0 ? exreduce : 0;
+    iV += iP * extras * (extras + 1) / 2 - 1 - exreduce;
+    if (iV < iP) iV = 2 * iP - 1;
+    V_avg = (1 - alpha) * V_avg + alpha * iV;
+    V_var = (1 - alpha) * (V_var + alpha * dV * dV);
+}
+
+mg_solver::~mg_solver() {
+    for (auto &l : lv) {
+        cudaFree(l.x);
+        cudaFree(l.r);
+        cudaFree(l.res);
+        cudaFree(l.xs);
+        cudaFree(l.rs);
+        cudaFree(l.ress);
+    }
+    cudaFree(d_max);
+    cudaFreeHost(h_max);
+}
+
+int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_form, cudaStream_t st) {
+    kind = k;
+    mixed = mixed_form;
+    const double eps = 2.220446049250313e-16;
+    // tolerances of simp_fem / simp_mac (mg_probs.hh:483-485, :516-518)
+    max_norm_tol = (k == MG_FEM) ? 32 * eps * 1e2 : 6 * eps * 1e2;
+    mg_level L0;
+    for (int d = 0; d < 3; d++) {
+        L0.n[d] = n[d];
+        L0.prd[d] = prd[d];
+    }
+    lv.push_back(L0);
+    while (true) {
+        const mg_level &f = lv.back();
+        if (f.npts() <= 512) break;
+        mg_level c;
+        bool ok = true;
+        for (int d = 0; d < 3; d++) {
+            c.prd[d] = f.prd[d];
+            int len = f.n[d];
+            if (k == MG_MAC) {
+                if (len % 2 != 0 || len < 4) ok = false;
+                c.n[d] = len / 2;
+            } else if (f.prd[d]) {
+                if (len % 2 != 0 || len < 4) ok = false;
+                c.n[d] = len / 2;
+            } else {
+                if ((len - 1) % 2 != 0 || len < 3) ok = false;
+                c.n[d] = (len - 1) / 2 + 1;
+            }
+        }
+        if (!ok) break;
+        lv.push_back(c);
+    }
+    if (lv.back().npts() > 4096) return fail(RMT3D_ERR_UNSUPPORTED, "grid does not coarsen to a small enough level");
+    for (auto &l : lv) {
+        size_t b = l.npts() * sizeof(double);
+        if (cudaMalloc(&l.x, b) != cudaSuccess || cudaMalloc(&l.r, b) != cudaSuccess ||
+            cudaMalloc(&l.res, b) != cudaSuccess)
+            return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
+        cudaMemsetAsync(l.x, 0, b, st);
+        cudaMemsetAsync(l.r, 0, b, st);
+        cudaMemsetAsync(l.res, 0, b, st);
+        if (mixed) {
+            size_t bf = l.npts() * sizeof(float);
+            if (cudaMalloc(&l.xs, bf) != cudaSuccess || cudaMalloc(&l.rs, bf) != cudaSuccess ||
+                cudaMalloc(&l.ress, bf) != cudaSuccess)
+                return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
+            cudaMemsetAsync(l.xs, 0, bf, st);
+            cudaMemsetAsync(l.rs, 0, bf, st);
+            cudaMemsetAsync(l.ress, 0, bf, st);
+        }
+    }
+    if (cudaMalloc(&d_max, sizeof(double)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
+    if (cudaMallocHost(&h_max, sizeof(double)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "pinned allocation failed");
+    return 0;
+}
+
+#define LAUNCH(...)                           \
+    do {                                      \
+        __VA_ARGS__;                          \
+        if (launches) (*launches)++;          \
+    } while (0)
+
+void mg_solver::smooth(int l, int sweeps, cudaStream_t st) {
+    mg_level &L = lv[l];
+    lvl_dev d = dev_of(L);
+    for (int s = 0; s < sweeps; s++) {
+        if (kind == MG_MAC) {
+            dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
+            for (int c = 0; c < 2; c++) LAUNCH(k_mac_rb<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c));
+        } else {
+            dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, ((L.n[2] + 1) / 2 + 1) / 2);
+            for (int c = 0; c < 8; c++) LAUNCH(k_fem_gs<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c));
+        }
+    }
+}
+
+void mg_solver::smooth_f32(int l, int sweeps, cudaStream_t st) {
+    mg_level &L = lv[l];
+    lvl_dev d = dev_of(L);
+    for (int s = 0; s < sweeps; s++) {
+        if (kind == MG_MAC) {
+            dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
+            for (int c = 0; c < 2; c++) LAUNCH(k_mac_rb<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+        } else {
+            dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, ((L.n[2] + 1) / 2 + 1) / 2);
+            for (int c = 0; c < 8; c++) LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+        }
+    }
+}
+
+void mg_solver::cycle(int l, cudaStream_t st) {
+    mg_level &F = lv[l];
+    lvl_dev fd = dev_of(F);
+    if (l == (int)lv.size() - 1) {
+        if (kind == MG_MAC) LAUNCH(k_coarse_solve<double, 0><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
+        else LAUNCH(k_coarse_solve<double, 1><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
+        return;
+    }
+    smooth(l, v_down, st);
+    mg_level &C = lv[l + 1];
+    lvl_dev cd = dev_of(C);
+    dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
+    if (kind == MG_MAC) {
+        LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
+        LAUNCH(k_mac_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r));
+    } else {
+        LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
+        LAUNCH(k_fem_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r));
+    }
+    if (l + 1 < (int)lv.size() - 1) {
+        size_t nc = C.npts();
+        LAUNCH(k_zero<double><<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(C.x, nc));
+    }
+    cycle(l + 1, st);
+    if (kind == MG_MAC) LAUNCH(k_mac_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, F.x, C.x));
+    else LAUNCH(k_fem_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, F.x, C.x));
+    smooth(l, v_up, st);
+}
+
+void mg_solver::cycle_f32(int l, cudaStream_t st) {
+    mg_level &F = lv[l];
+    lvl_dev fd = dev_of(F);
+    if (l == (int)lv.size() - 1) {
+        if (kind == MG_MAC) LAUNCH(k_coarse_solve<float, 0><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
+        else LAUNCH(k_coarse_solve<float, 1><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
+        return;
+    }
+    smooth_f32(l, v_down, st);
+    mg_level &C = lv[l + 1];
+    lvl_dev cd = dev_of(C);
+    dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
+    if (kind == MG_MAC) {
+        LAUNCH((k_resid<float, 0><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr)));
+        LAUNCH(k_mac_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs));
+    } else {
+        LAUNCH((k_resid<float, 1><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr)));
+        LAUNCH(k_fem_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs));
+    }
+    if (l + 1 < (int)lv.size() - 1) {
+        size_t nc = C.npts();
+        LAUNCH(k_zero<float><<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(C.xs, nc));
+    }
+    cycle_f32(l + 1, st);
+    if (kind == MG_MAC) LAUNCH(k_mac_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, F.xs, C.xs));
+    else LAUNCH(k_fem_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, F.xs, C.xs));
+    smooth_f32(l, v_up, st);
+}
+
+// One refinement step of the mixed form: FP64 residual, FP32 V-cycle on the
+// correction, FP64 update.
+void mg_solver::refine_step(cudaStream_t st) {
+    mg_level &F = lv[0];
+    lvl_dev fd = dev_of(F);
+    dim3 gf = grid3(F.n[0], F.n[1], F.n[2]);
+    size_t n = F.npts();
+    unsigned nb = (unsigned)((n + 255) / 256);
+    if (kind == MG_MAC) LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
+    else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
+    LAUNCH(k_to_f32<<<nb, 256, 0, st>>>(F.res, F.rs, n));
+    LAUNCH(k_zero<float><<<nb, 256, 0, st>>>(F.xs, n));
+    cycle_f32(0, st);
+    LAUNCH(k_add_f32<<<nb, 256, 0, st>>>(F.x, F.xs, n));
+}
+
+void mg_solver::vcycle(cudaStream_t st) {
+    cycles_total++;
+    last_cycles++;
+    if (mixed) refine_step(st);
+    else cycle(0, st);
+}
+
+double mg_solver::residual_max(cudaStream_t st) {
+    mg_level &F = lv[0];
+    lvl_dev fd = dev_of(F);
+    dim3 gf = grid3(F.n[0], F.n[1], F.n[2]);
+    cudaMemsetAsync(d_max, 0, sizeof(double), st);
+    if (kind == MG_MAC)
+        LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, (unsigned long long *)d_max)));
+    else
+        LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, (unsigned long long *)d_max)));
+    cudaMemcpyAsync(h_max, d_max, sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return *h_max;
+}
+
+double mg_solver::run(cudaStream_t st) {
+    const int hard_cap = 20;
+    last_cycles = 0;
+    for (int i = 0; i < pred.iters(); i++) vcycle(st);
+    double res = residual_max(st);
+    int extra = 0;
+    while (res > max_norm_tol && extra < hard_cap) {
+        extra++;
+        for (int n = 0; n < extra; n++) vcycle(st);
+        res = residual_max(st);
+    }
+    for (int i = 0; i < 2; i++) vcycle(st);
+    pred.update(extra);
+    return res;
+}
+
+}  // namespace rmt3d

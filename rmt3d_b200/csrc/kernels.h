@@ -1,0 +1,43 @@
+// Kernel declarations and small by-value argument structs shared between the
+// kernel translation units and the host orchestration (scene.cu).
+#pragma once
+#include "dev_common.cuh"
+
+namespace rmt3d {
+
+// arrays touched by one periodic ghost exchange
+struct ptr_list {
+    double *p[40];
+    int *ip[4];
+    int n, ni;
+};
+
+// one physical boundary face (face_gm, fields.hh:661-850)
+struct bc_face {
+    int bct[3];
+    double bcv[3];
+    double h;
+};
+
+// FEM element-integrated basis gradients (fluid_3d.cc:2506-2517)
+struct gradphi_t {
+    double v[8][3];
+};
+
+__global__ void k_periodic_copy(grid_dev g, ptr_list pl, int corner);
+__global__ void k_bc_cc(grid_dev g, int face, bc_face bc, double *u, double *v, double *w);
+__global__ void k_bc_cf(grid_dev g, int face, bc_face bc, const fields_dev *F);
+__global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F);
+__global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                           const double *lz, double cdt, double time, int var_den);
+__global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F);
+__global__ void k_mac_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, double cdt);
+__global__ void k_mac_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x);
+__global__ void k_sub_qgrad(grid_dev g, const fields_dev *__restrict__ F, double cdt, int var_den);
+__global__ void k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                        const double *lz, double cdt, double time, int var_den);
+__global__ void k_fem_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, gradphi_t gp);
+__global__ void k_fem_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x, const double *mean);
+__global__ void k_sub_pgrad(grid_dev g, const fields_dev *__restrict__ F, double dt, int var_den);
+
+}  // namespace rmt3d

@@ -1,0 +1,74 @@
+// Device-resident geometric multigrid for the two pressure Poisson problems of
+// the step: the cell-centred 7-point MAC problem (simp_mac,
+// Utilities/mg_probs.hh:497-530) and the nodal 27-point Q1 FEM problem
+// (simp_fem, :458-495).  The V-cycle control reproduces mg_prob::run and
+// mg_pred (Utilities/mg_probs.cc:3-83, mg_probs.hh:37-78): the predicted
+// number of cycles, extra rounds until the max-norm residual is below the
+// problem's tolerance (at most 20 rounds), then two insurance cycles.
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+
+namespace rmt3d {
+
+enum mg_kind { MG_MAC = 0, MG_FEM = 1 };
+
+struct mg_level {
+    int n[3];
+    int prd[3];
+    double *x = nullptr;    // solution
+    double *r = nullptr;    // source
+    double *res = nullptr;  // residual scratch
+    float *xs = nullptr, *rs = nullptr, *ress = nullptr;  // FP32 copies (mixed form)
+    size_t npts() const { return (size_t)n[0] * n[1] * n[2]; }
+};
+
+// mg_pred (mg_probs.hh:37-78); alpha is the integer quotient 1/(3*iP) = 0
+// exactly as the reference computes it, so the averages never move.
+struct mg_pred_state {
+    int iP = 16;
+    int iV = 32;
+    double V_avg = 32;
+    double V_var = 1e6;
+    double alpha = 1 / (3 * 16);
+    int iters() const { return iV / iP; }
+    void update(int extras);
+};
+
+class mg_solver {
+  public:
+    mg_kind kind;
+    std::vector<mg_level> lv;
+    double max_norm_tol;
+    int v_up = 2, v_down = 2;
+    mg_pred_state pred;
+    long long cycles_total = 0;
+    int last_cycles = 0;
+    bool mixed = false;  // FP32 cycles inside FP64 iterative refinement
+    long long *launches = nullptr;
+
+    mg_solver() = default;
+    mg_solver(const mg_solver &) = delete;
+    mg_solver &operator=(const mg_solver &) = delete;
+    ~mg_solver();
+    // n: fine points per axis; prd: periodic flags
+    int setup(mg_kind k, const int n[3], const int prd[3], bool mixed_form, cudaStream_t st);
+    double *rhs() { return lv[0].r; }
+    double *sol() { return lv[0].x; }
+    // one solve with the reference's control logic; returns the final max-norm
+    // residual (NaN propagates)
+    double run(cudaStream_t st);
+    double residual_max(cudaStream_t st);
+    void vcycle(cudaStream_t st);
+
+  private:
+    double *d_max = nullptr;   // device scalar for reductions
+    double *h_max = nullptr;   // pinned host mirror
+    void cycle(int l, cudaStream_t st);
+    void cycle_f32(int l, cudaStream_t st);
+    void smooth(int l, int sweeps, cudaStream_t st);
+    void smooth_f32(int l, int sweeps, cudaStream_t st);
+    void refine_step(cudaStream_t st);
+};
+
+}  // namespace rmt3d

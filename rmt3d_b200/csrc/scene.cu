@@ -1,0 +1,1199 @@
+// Scene object and C ABI: construction (fluid_3d ctor + sim_manager set-up),
+// initialisation (fluid_3d::initialize / init_iter), the time step
+// (fluid_3d::step_forward, F3D_Source/fluid_3d.cc:429-577) as a sequence of
+// device kernels on the scene's stream, and state import/export in the
+// reference's AoS layout.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "host_common.h"
+#include "kernels.h"
+#include "mg.h"
+#include "rmt3d_gpu.h"
+#include "solid.h"
+
+namespace rmt3d {
+
+static thread_local std::string g_err;
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+}  // namespace rmt3d
+
+using namespace rmt3d;
+
+extern "C" const char *rmt3d_last_error(void) { return g_err.c_str(); }
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(RMT3D_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// host-side mirrors of the reference's object and manager arithmetic
+// ---------------------------------------------------------------------------
+namespace {
+
+struct host_obj {
+    int type;
+    double c[3], R, eig[3], omega[3];
+    double rho, G, cs, ex_visc_mult, ev_trans_mult, dt_pad, dt_ex_pad, ex_mu, volume;
+    // basic_sphere::phi (object.cc:76-82)
+    double phi(const double xi[3]) const {
+        double sq = 0;
+        for (int i = 0; i < 3; i++) sq += (xi[i] - c[i]) * (xi[i] - c[i]);
+        return sqrt(sq) - R;
+    }
+    // object::rm0 / sphere::rm0 (object.hh:40-42, :110-114)
+    void rm0(const double x[3], double xi[3]) const {
+        if (type == RMT3D_OBJ_SPHERE)
+            for (int i = 0; i < 3; i++) xi[i] = (x[i] - c[i]) * eig[i] + c[i];
+        else
+            for (int i = 0; i < 3; i++) xi[i] = x[i];
+    }
+    // object::velocity (object.hh:48-54)
+    void velocity(const double rv[3], double &u, double &v, double &w) const {
+        double L[3];
+        for (int i = 0; i < 3; i++) L[i] = rv[i] - c[i];
+        u += omega[1] * L[2] - omega[2] * L[1];
+        v -= omega[0] * L[2] - omega[2] * L[0];
+        w += omega[0] * L[1] - omega[1] * L[0];
+    }
+    // sl_mat::cfl (sim_manager.hh:59-64)
+    double cfl(double dx) const {
+        double xxsp3 = 3 / (dx * dx);
+        double dt1 = 0.5 * rho / (ex_mu * (ev_trans_mult + 1) * xxsp3) * dt_ex_pad;
+        double dt0 = dx / cs * dt_pad;
+        return (dt0 < dt1) ? dt0 : dt1;
+    }
+};
+
+inline dim3 blk() { return dim3(32, 4, 2); }
+inline dim3 grd(int a, int b, int c) { return dim3((a + 31) / 32, (b + 3) / 4, (c + 1) / 2); }
+inline unsigned lin_blocks(int n) { return (unsigned)((n + 255) / 256); }
+
+}  // namespace
+
+struct rmt3d_scene {
+    rmt3d_scene_desc d;
+    grid_dev g;
+    fields_dev hF;
+    fields_dev *dF = nullptr;
+    cudaStream_t st = 0;
+    bool own_stream = false;
+    std::vector<void *> allocs;
+    double *lx = nullptr, *ly = nullptr, *lz = nullptr;
+    std::vector<double> hlx, hly, hlz;
+    host_obj obj[RMT3D_MAX_OBJ];
+    mg_solver mac, fem;
+    gradphi_t gradphi;
+    bc_face faces[6];
+    bool wall[6];
+    double dt = 0, time = 0, dt_reg = 0, eps = 0, vmax = 1, K_stiff = 0;
+    double min_wall_acc = 0, wall_acc_mult = 0;
+    int nt = 0;
+    long long launches = 0;
+    // extrapolation scratch
+    uint8_t *lay = nullptr, *inl = nullptr;
+    int *front[2] = {nullptr, nullptr};
+    int *counters = nullptr;  // [0..1] frontier sizes, [2] extrapolation errors, [3] corrector problems,
+                              // [4] redraw fatal, [5] refmap-derivative errors
+    int *h_counters = nullptr;
+    double *d_mean = nullptr;
+    double *h_scalar = nullptr;
+    double *d_red = nullptr;
+
+    template <typename T>
+    int alloc(T **p, size_t n) {
+        if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "device allocation failed");
+        allocs.push_back(*p);
+        cudaMemsetAsync(*p, 0, n * sizeof(T), st);
+        return 0;
+    }
+    void count(int n = 1) { launches += n; }
+};
+
+// ---------------------------------------------------------------------------
+// ghost-frame helpers
+// ---------------------------------------------------------------------------
+static void periodic(rmt3d_scene *s, std::initializer_list<double *> arrs, std::initializer_list<int *> iarrs,
+                     int corner) {
+    if (!(s->g.prd[0] || s->g.prd[1] || s->g.prd[2])) return;
+    ptr_list pl;
+    pl.n = 0;
+    pl.ni = 0;
+    for (double *a : arrs) pl.p[pl.n++] = a;
+    for (int *a : iarrs) pl.ip[pl.ni++] = a;
+    k_periodic_copy<<<grd(s->g.sm4, s->g.sn4, s->g.so4), blk(), 0, s->st>>>(s->g, pl, corner);
+    s->count();
+}
+
+// fill_boundary_cc: set_bc_cc then communicate<1> (fluid_3d.cc:145-152)
+static void fill_boundary_cc(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    for (int f = 0; f < 6; f++) {
+        if (!s->wall[f]) continue;
+        int n = f / 2;
+        int ext[3] = {g.sm4, g.sn4, g.so4};
+        int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
+        dim3 gr((ext[t0] + 31) / 32, (ext[t1] + 7) / 8, 2);
+        k_bc_cc<<<gr, dim3(32, 8, 1), 0, s->st>>>(g, f, s->faces[f], s->hF.vel[0], s->hF.vel[1], s->hF.vel[2]);
+        s->count();
+    }
+    periodic(s, {s->hF.vel[0], s->hF.vel[1], s->hF.vel[2]}, {}, 0);
+}
+
+// fill_boundary_cf: set_bc_cf then communicate<4> (fluid_3d.cc:155-165)
+static void fill_boundary_cf(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    for (int f = 0; f < 6; f++) {
+        if (!s->wall[f]) continue;
+        int n = f / 2;
+        int ext[3] = {g.sm4, g.sn4, g.so4};
+        int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
+        dim3 gr((ext[t0] + 31) / 32, (ext[t1] + 7) / 8, 1);
+        k_bc_cf<<<gr, dim3(32, 8, 1), 0, s->st>>>(g, f, s->faces[f], s->dF);
+        s->count();
+    }
+    if (g.prd[0] || g.prd[1] || g.prd[2]) {
+        ptr_list pl;
+        pl.n = 18;
+        pl.ni = 0;
+        for (int a = 0; a < 18; a++) pl.p[a] = s->hF.fvel[a];
+        k_periodic_copy<<<grd(g.sm4, g.sn4, g.so4), blk(), 0, s->st>>>(g, pl, 0);
+        s->count();
+    }
+}
+
+// communicate<2>: p, dp, q on the nodal table
+static void comm_pressure(rmt3d_scene *s) { periodic(s, {s->hF.p, s->hF.dp, s->hF.q}, {}, 1); }
+// communicate<2048>: dvel
+static void comm_dvel(rmt3d_scene *s) { periodic(s, {s->hF.dvel[0], s->hF.dvel[1], s->hF.dvel[2]}, {}, 0); }
+
+// communicate<4|64> + communicate_extrap_fx: face states of the maps
+static void comm_face_maps(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    if (!(g.prd[0] || g.prd[1] || g.prd[2])) return;
+    for (int o = 0; o < g.n_obj; o++) {
+        ptr_list pl;
+        pl.n = 18;
+        pl.ni = 0;
+        for (int a = 0; a < 18; a++) pl.p[a] = s->hF.om[o].fx[a];
+        k_periodic_copy<<<grd(g.sm4, g.sn4, g.so4), blk(), 0, s->st>>>(g, pl, 0);
+        s->count();
+    }
+}
+
+// communicate<8> + <16|32>: the primary maps' id, x and xpred
+static void comm_primary(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    if (!(g.prd[0] || g.prd[1] || g.prd[2])) return;
+    for (int o = 0; o < g.n_obj; o++) {
+        objmap_dev &m = s->hF.om[o];
+        ptr_list pl;
+        pl.n = 0;
+        for (int a = 0; a < 3; a++) pl.p[pl.n++] = m.x[a];
+        for (int a = 0; a < 3; a++) pl.p[pl.n++] = m.xp[a];
+        pl.ni = 1;
+        pl.ip[0] = m.code;
+        k_periodic_copy<<<grd(g.sm4, g.sn4, g.so4), blk(), 0, s->st>>>(g, pl, 0);
+        s->count();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// extrapolation, fluid_3d::extrapolate (fluid_3d_ex.cc:31-47)
+// ---------------------------------------------------------------------------
+static void extrapolate(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    const int nb = lin_blocks(g.ncell);
+    const int per_warp_blocks = 148 * 8;
+    for (int o = 0; o < g.n_obj; o++) {
+        k_lay_init<<<nb, 256, 0, s->st>>>(g, s->dF, o, s->lay, s->inl);
+        cudaMemsetAsync(s->counters, 0, 2 * sizeof(int), s->st);
+        k_lay_push<<<nb, 256, 0, s->st>>>(g, nullptr, nullptr, 1, s->lay, s->inl, 1);
+        k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, 1);
+        k_lay_compact<<<nb, 256, 0, s->st>>>(g, s->inl, s->front[0], s->counters + 0);
+        s->count(4);
+        int cur = 0;
+        for (int L = 1; L <= s->d.nlayers; L++) {
+            k_extrap_layer<<<per_warp_blocks, 128, 0, s->st>>>(g, s->dF, o, s->front[cur], s->counters + cur, L,
+                                                               s->d.max_extrap_rs, s->d.weight_fac, s->lx, s->ly,
+                                                               s->lz, s->counters + 2);
+            k_layer_ghost_copy<<<nb, 256, 0, s->st>>>(g, s->dF, o, L);
+            s->count(2);
+            if (L < s->d.nlayers) {
+                int nxt = cur ^ 1;
+                cudaMemsetAsync(s->counters + nxt, 0, sizeof(int), s->st);
+                k_lay_push<<<per_warp_blocks, 256, 0, s->st>>>(g, s->front[cur], s->counters + cur, 0, s->lay, s->inl,
+                                                               L + 1);
+                k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, L + 1);
+                k_lay_compact<<<nb, 256, 0, s->st>>>(g, s->inl, s->front[nxt], s->counters + nxt);
+                s->count(3);
+                cur = nxt;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host initial conditions (fluid_3d.cc:292-400) -- evaluated on the host
+// exactly as the reference does, then uploaded
+// ---------------------------------------------------------------------------
+static void host_velocity(rmt3d_scene *s, double x, double y, double z, double &u, double &v, double &w) {
+    const rmt3d_scene_desc &d = s->d;
+    if (d.sim_type == RMT3D_SIM_FTEST) {  // sim_ftest::velocity (sim_manager.cc:139-146)
+        u = -sin(2 * M_PI * x) * cos(2 * M_PI * y) * cos(2 * M_PI * z);
+        v = 0.5 * cos(2 * M_PI * x) * sin(2 * M_PI * y) * cos(2 * M_PI * z);
+        w = 0.5 * cos(2 * M_PI * x) * cos(2 * M_PI * y) * sin(2 * M_PI * z);
+    } else if (d.sim_type == RMT3D_SIM_STEST) {  // sim_stest::velocity (:203-210)
+        const double a = 0.01, k = 2 * M_PI;
+        u = 2 * M_PI * a * sin(k * z);
+        v = 2 * M_PI * a * sin(k * z);
+        w = 0;
+    } else {  // sim_manager::velocity (:102-131)
+        u = 0;
+        v = 0;
+        w = 0;
+        const double coords[3] = {x, y, z};
+        double rx[3] = {0, 0, 0};
+        for (int i = 0; i < d.vel_prof_num; i++) {
+            int vt = static_cast<int>(d.vel_profile[2 * i]);
+            double amp = d.vel_profile[2 * i + 1];
+            if (vt == 0) continue;
+            else if (vt == 1) u += amp;
+            else if (vt == 2) v += amp;
+            else if (vt == 3) w += amp;
+        }
+        for (int i = 0; i < d.n_obj; i++) {
+            s->obj[i].rm0(coords, rx);
+            if (s->obj[i].phi(rx) < 0.) s->obj[i].velocity(rx, u, v, w);
+        }
+    }
+    double tmp = sqrt(u * u + v * v + w * w);
+    if (tmp > s->vmax) s->vmax = tmp;
+}
+
+static void host_exact(rmt3d_scene *s, double x, double y, double z, double t, double h, double &u, double &v,
+                       double &w, double &p) {
+    const rmt3d_scene_desc &d = s->d;
+    if (d.sim_type == RMT3D_SIM_FTEST) {  // sim_ftest::exact (sim_manager.cc:152-167)
+        host_velocity(s, x, y, z, u, v, w);
+        u *= cos(2 * M_PI * t);
+        v *= cos(2 * M_PI * t);
+        w *= cos(2 * M_PI * t);
+        x -= 0.5 * h;
+        y -= 0.5 * h;
+        z -= 0.5 * h;
+        p = 3 * M_PI * d.fmu * cos(2 * M_PI * x) * cos(2 * M_PI * y) * cos(2 * M_PI * z);
+        p *= (cos(2 * M_PI * t) - sin(2 * M_PI * t) / (6 * M_PI * d.fmu));
+    } else if (d.sim_type == RMT3D_SIM_STEST) {  // sim_stest::exact (:187-197)
+        const double a = 0.01, k = 2 * M_PI, om = 2 * M_PI;
+        u = om * a * sin(k * z - om * t);
+        v = om * a * sin(k * z - om * t);
+        w = 0;
+        z -= 0.5 * h;
+        p = -s->obj[0].G * a * a * k * (-k * cos(2 * (k * z - om * t)) + cos(2 * om * t - k) * sin(k)) / 3;
+    } else {
+        u = v = w = p = 0;
+    }
+}
+
+static double host_pressure(rmt3d_scene *s, double x, double y, double z) {
+    const rmt3d_scene_desc &d = s->d;
+    if (d.sim_type == RMT3D_SIM_FTEST) return 3 * M_PI * d.fmu * cos(2 * M_PI * x) * cos(2 * M_PI * y) * cos(2 * M_PI * z);
+    if (d.sim_type == RMT3D_SIM_STEST) {
+        const double a = 0.01, k = 2 * M_PI;
+        return -s->obj[0].G * a * a * k * (-k * cos(2 * k * z) + cos(-k) * sin(k)) / 3;
+    }
+    return 0;
+}
+
+// obligatory_cfl_recheck (sim_manager.cc:56-66)
+static void cfl_recheck(rmt3d_scene *s) {
+    double dh = std::min(s->g.dx, std::min(s->g.dy, s->g.dz));
+    double dt_min = s->d.fdt_pad * dh / s->vmax;
+    if (s->dt_reg > dt_min) {
+        s->dt_reg = dt_min;
+        if (s->d.dt < s->dt_reg) s->dt_reg = s->d.dt;
+    }
+    s->K_stiff = 0.0025 / (s->dt_reg * s->dt_reg);
+    s->g.K_stiff = s->K_stiff;
+}
+
+// init_fluid (fluid_3d.cc:292-320): every cell reset (p kept), velocities from
+// the initial condition, periodic exchange, CFL recheck, dt = dt_reg
+static int init_fluid(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    const size_t n = g.ncell;
+    std::vector<double> u(n), v(n), w(n);
+    for (int k = 0; k < g.so4; k++)
+        for (int j = 0; j < g.sn4; j++)
+            for (int i = 0; i < g.sm4; i++) {
+                double p, t[3];
+                if (s->d.has_exact) host_exact(s, s->hlx[i], s->hly[j], s->hlz[k], s->time, g.dx, t[0], t[1], t[2], p);
+                else host_velocity(s, s->hlx[i], s->hly[j], s->hlz[k], t[0], t[1], t[2]);
+                size_t id = gidx(g, i, j, k);
+                u[id] = t[0];
+                v[id] = t[1];
+                w[id] = t[2];
+            }
+    CK(cudaMemcpyAsync(s->hF.vel[0], u.data(), n * 8, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->hF.vel[1], v.data(), n * 8, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->hF.vel[2], w.data(), n * 8, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemsetAsync(s->hF.q, 0, n * 8, s->st));
+    CK(cudaMemsetAsync(s->hF.dp, 0, n * 8, s->st));
+    for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(s->hF.dvel[c], 0, n * 8, s->st));
+    for (int c = 0; c < 18; c++) CK(cudaMemsetAsync(s->hF.fvel[c], 0, n * 8, s->st));
+    for (int c = 0; c < 9; c++) CK(cudaMemsetAsync(s->hF.sigma[c], 0, n * 8, s->st));
+    if (s->d.var_den) {
+        std::vector<double> r(n, s->d.frho);
+        CK(cudaMemcpyAsync(s->hF.rho, r.data(), n * 8, cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    CK(cudaStreamSynchronize(s->st));
+    periodic(s, {s->hF.vel[0], s->hF.vel[1], s->hF.vel[2]}, {}, 0);
+    cfl_recheck(s);
+    s->dt = s->dt_reg;
+    return 0;
+}
+
+// init_pres (fluid_3d.cc:326-343)
+static int init_pres(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    const size_t n = g.ncell;
+    std::vector<double> p(n);
+    CK(cudaMemcpyAsync(p.data(), s->hF.p, n * 8, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    double hdx = g.dx * 0.5, hdy = g.dy * 0.5, hdz = g.dz * 0.5;
+    for (int k = 2; k < g.so4 - 1; k++)
+        for (int j = 2; j < g.sn4 - 1; j++)
+            for (int i = 2; i < g.sm4 - 1; i++)
+                p[gidx(g, i, j, k)] = host_pressure(s, s->hlx[i] - hdx, s->hly[j] - hdy, s->hlz[k] - hdz);
+    CK(cudaMemcpyAsync(s->hF.p, p.data(), n * 8, cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemsetAsync(s->hF.q, 0, n * 8, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    comm_pressure(s);
+    return 0;
+}
+
+// init_refmap (fluid_3d.cc:348-400): every map reset; interior cells take the
+// initial map of each object in turn and belong to the first object whose
+// level set is negative there
+static int init_refmap(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    const size_t n = g.ncell;
+    if (g.n_obj == 0) return 0;
+    std::vector<int> code(n);
+    std::vector<double> X[3], init_gp(n, -kBig);
+    for (int c = 0; c < 3; c++) X[c].assign(n, 0.0);
+    std::vector<int> owner(n, -1);
+    for (int k = 2; k < g.so4 - 2; k++)
+        for (int j = 2; j < g.sn4 - 2; j++)
+            for (int i = 2; i < g.sm4 - 2; i++) {
+                size_t id = gidx(g, i, j, k);
+                double tx[3] = {s->hlx[i], s->hly[j], s->hlz[k]};
+                double xi[3];
+                bool found = false;
+                for (int o = 0; o < g.n_obj; o++) {
+                    s->obj[o].rm0(tx, xi);
+                    for (int c = 0; c < 3; c++) X[c][id] = xi[c];
+                    if (s->obj[o].phi(xi) < 0) {
+                        if (!found) {
+                            owner[id] = o;
+                            found = true;
+                        } else {
+                            return fail(RMT3D_ERR_INVALID, "init_refmap: overlapping primary points");
+                        }
+                    }
+                }
+            }
+    for (int o = 0; o < g.n_obj; o++) {
+        objmap_dev &m = s->hF.om[o];
+        for (size_t id = 0; id < n; id++) code[id] = (owner[id] == o) ? 0 : -1;
+        CK(cudaMemcpy(m.code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+        for (int c = 0; c < 3; c++) {
+            CK(cudaMemcpy(m.x[c], X[c].data(), n * 8, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(m.xp[c], X[c].data(), n * 8, cudaMemcpyHostToDevice));
+        }
+        for (int c = 0; c < 9; c++) CK(cudaMemcpy(m.gp[c], init_gp.data(), n * 8, cudaMemcpyHostToDevice));
+        for (int c = 0; c < 18; c++) CK(cudaMemsetAsync(m.fx[c], 0, n * 8, s->st));
+    }
+    comm_primary(s);
+    return 0;
+}
+
+// update_rho (fluid_3d.cc:1104-1143), VAR_DEN only
+__global__ void k_update_rho(grid_dev g, const fields_dev *__restrict__ F) {
+    int ind = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ind >= g.ncell) return;
+    double sfrac = 0, srho = 0;
+    int prim = -1;
+    for (int o = 0; o < g.n_obj; o++)
+        if (F->om[o].code[ind] == 0) prim = o;
+    if (prim >= 0) {
+        const objmap_dev &m = F->om[prim];
+        double t = heaviside(g, obj_phi(g, prim, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
+        srho += t * g.obj[prim].rho;
+        sfrac += t;
+    }
+    for (int o = 0; o < g.n_obj; o++) {
+        const objmap_dev &m = F->om[o];
+        if (m.code[ind] <= 0) continue;
+        double t = heaviside(g, obj_phi(g, o, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
+        srho += t * g.obj[o].rho;
+        sfrac += t;
+    }
+    if (sfrac > 1.) srho /= sfrac;
+    else srho += (1 - sfrac) * g.frho;
+    F->rho[ind] = srho;
+}
+
+static void update_rho(rmt3d_scene *s) {
+    if (!s->d.var_den) return;
+    k_update_rho<<<lin_blocks(s->g.ncell), 256, 0, s->st>>>(s->g, s->dF);
+    s->count();
+}
+
+// init_extrapolate (fluid_3d_ex.cc:16-27)
+static void init_extrapolate(rmt3d_scene *s) {
+    if (s->g.n_obj == 0) return;
+    extrapolate(s);
+    k_extraps_full<<<lin_blocks(s->g.ncell), 256, 0, s->st>>>(s->g, s->dF);
+    s->count();
+}
+
+// compute_grad_basis (fluid_3d.cc:2506-2517), evaluated with the current dt
+static void compute_grad_basis(rmt3d_scene *s) {
+    double fac = 3 * s->g.dx / s->dt;
+    for (int i = 0; i < 8; i++) {
+        s->gradphi.v[i][0] = (2 * (i % 2) - 1) * fac;
+        s->gradphi.v[i][1] = (2 * ((i / 2) % 2) - 1) * fac;
+        s->gradphi.v[i][2] = (2 * (i / 4) - 1) * fac;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// step phases
+// ---------------------------------------------------------------------------
+static void compute_stress(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    k_stress<<<grd(g.sm + 3, g.sn + 3, g.so + 3), blk(), 0, s->st>>>(g, s->dF);
+    s->count();
+}
+
+static int mac_solve(rmt3d_scene *s, double cdt) {
+    const grid_dev &g = s->g;
+    update_rho(s);
+    k_mac_rhs<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.rhs(), cdt);
+    s->count();
+    double res = s->mac.run(s->st);
+    if (std::isnan(res)) return fail(RMT3D_ERR_NAN, "fluid_3d::mac_solve(): NaN detected in multigrid solve");
+    k_mac_extract<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.sol());
+    s->count();
+    comm_pressure(s);
+    k_sub_qgrad<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, cdt, s->d.var_den);
+    s->count();
+    return 0;
+}
+
+__global__ void k_mean(const double *x, size_t n, double scale, double *out) {
+    double sum = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        sum += x[i] * scale;
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    __shared__ double sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = (threadIdx.x < blockDim.x / 32) ? sh[threadIdx.x] : 0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) atomicAdd(out, v);
+    }
+}
+
+// pp_solve (fluid_3d.cc:2653-2681): 0 or PROJECTION_ERR
+static int pp_solve(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    update_rho(s);
+    k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
+    s->count();
+    double res = s->fem.run(s->st);
+    if (std::isnan(res)) return 1;
+    size_t nn = (size_t)g.fm * g.fn * g.fo;
+    cudaMemsetAsync(s->d_mean, 0, sizeof(double), s->st);
+    k_mean<<<148, 256, 0, s->st>>>(s->fem.sol(), nn, 1 / (double)nn, s->d_mean);
+    k_fem_extract<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.sol(), s->d_mean);
+    s->count(2);
+    comm_pressure(s);
+    k_sub_pgrad<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->d.var_den);
+    s->count();
+    return 0;
+}
+
+// update_reference_map (fluid_3d.cc:1149-1255); returns the problem count
+static int update_reference_map(rmt3d_scene *s, double cdt, int *prob) {
+    const grid_dev &g = s->g;
+    *prob = 0;
+    if (g.n_obj == 0) return 0;
+    k_refmap_predict<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, cdt);
+    k_snapshot_reset<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
+    s->count(2);
+    comm_primary(s);
+    extrapolate(s);
+    k_refmap_correct<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->counters + 3);
+    s->count();
+    update_rho(s);
+    CK(cudaMemcpyAsync(s->h_counters, s->counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (s->h_counters[2] > 0) return fail(RMT3D_ERR_EXTRAP, "Extrapolation failed: no eligible points or degenerate matrix");
+    if (s->h_counters[5] > 0)
+        return fail(RMT3D_ERR_EXTRAP, "normal_derivatives_refmap: missing necessary cells to carry out finite differences");
+    *prob = s->h_counters[3];
+    return 0;
+}
+
+static int step_forward(rmt3d_scene *s, int debug) {
+    const grid_dev &g = s->g;
+    (void)debug;
+    s->nt++;
+    CK(cudaMemsetAsync(s->counters + 2, 0, 6 * sizeof(int), s->st));
+    compute_stress(s);
+    k_edge_vel<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, s->time,
+                                                            s->d.var_den);
+    s->count();
+    if (g.n_obj > 0) {
+        k_edge_refmap<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->counters + 5);
+        s->count();
+    }
+    s->time += 0.5 * s->dt;
+    fill_boundary_cf(s);
+    comm_face_maps(s);
+    k_upwind<<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
+    s->count();
+    fill_boundary_cf(s);
+    int e = mac_solve(s, s->dt);
+    if (e) return e;
+    fill_boundary_cf(s);
+    int prob = 0;
+    e = update_reference_map(s, s->dt, &prob);
+    if (e) return e;
+    if (prob) {
+        k_refmap_revert<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
+        s->count();
+        return RMT3D_REFMAP_UPDATE_ERR;
+    }
+    compute_stress(s);
+    k_ustar<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, s->time, s->d.var_den);
+    s->count();
+    fill_boundary_cc(s);
+    comm_dvel(s);
+    s->time += 0.5 * s->dt;
+    if (pp_solve(s)) return RMT3D_PROJECTION_ERR;
+    if (g.n_obj > 0) {
+        k_refmap_full<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
+        s->count();
+        update_rho(s);
+        k_redraw<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->d.nlayers, s->counters + 4);
+        s->count();
+    }
+    fill_boundary_cc(s);
+    comm_dvel(s);
+    if (g.n_obj > 0) {
+        CK(cudaMemcpyAsync(s->h_counters, s->counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        if (s->h_counters[4] > 0)
+            return fail(RMT3D_ERR_INVALID, "redraw_boundary(): Two deep maps try to be inside a cell at the same time!");
+    }
+    CK(cudaGetLastError());
+    return RMT3D_OK;
+}
+
+// div_u (fluid_3d_utils.cc:507-560): weighted L2 norm of the FEM rhs
+__global__ void k_divu(grid_dev g, const double *r, double *out) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    int b = blockIdx.y * blockDim.y + threadIdx.y;
+    int c = blockIdx.z * blockDim.z + threadIdx.z;
+    double v = 0;
+    if (a < g.fm && b < g.fn && c < g.fo) {
+        double nk = (c == 0 || c == g.fo - 1) ? 0.5 : 1.0;
+        if (g.prd[2]) nk = 1.0;
+        double nj = (b == 0 || b == g.fn - 1) ? 0.5 : 1.0;
+        if (g.prd[1]) nj = 1.0;
+        double ni = (a == 0 || a == g.fm - 1) ? 0.5 : 1.0;
+        if (g.prd[0]) ni = 1.0;
+        double rr = r[a + g.fm * (b + g.fn * c)];
+        v = ni * nj * nk * rr * rr;
+    }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) % 32 == 0) atomicAdd(out, v);
+}
+
+static int div_u(rmt3d_scene *s, double *out) {
+    const grid_dev &g = s->g;
+    k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
+    CK(cudaMemsetAsync(s->d_red, 0, sizeof(double), s->st));
+    k_divu<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->fem.rhs(), s->d_red);
+    s->count(2);
+    CK(cudaMemcpyAsync(s->h_scalar, s->d_red, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    *out = sqrt(*s->h_scalar / ((double)g.fm * g.fn * g.fo));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rmt3d_scene **out) {
+    if (!desc || !out) return fail(RMT3D_ERR_INVALID, "null argument");
+    *out = nullptr;
+    const rmt3d_scene_desc &d = *desc;
+    for (int a = 0; a < 3; a++)
+        if (d.sys_size[a] < 4 || d.sys_size[a] > 1024) return fail(RMT3D_ERR_INVALID, "sys_size outside 4..1024");
+    if (d.n_obj < 0 || d.n_obj > RMT3D_MAX_OBJ) return fail(RMT3D_ERR_TOO_LARGE, "n_obj outside 0..16");
+    if (d.implicit_visc) return fail(RMT3D_ERR_UNSUPPORTED, "implicit viscosity is outside this path");
+    if (!d.godunov) return fail(RMT3D_ERR_UNSUPPORTED, "only the Godunov scheme is on this path");
+    if (d.sim_type == RMT3D_SIM_STEST) return fail(RMT3D_ERR_UNSUPPORTED, "stest (shear cube object) is outside this path");
+    for (int o = 0; o < d.n_obj; o++)
+        if (d.obj[o].type != RMT3D_OBJ_BASIC_SPHERE && d.obj[o].type != RMT3D_OBJ_SPHERE)
+            return fail(RMT3D_ERR_UNSUPPORTED, "object type " + std::to_string(d.obj[o].type) + " is outside this path");
+    if (d.nlayers < 1 || d.nlayers > 60) return fail(RMT3D_ERR_INVALID, "nlayers outside 1..60");
+
+    rmt3d_scene *s = new rmt3d_scene();
+    s->d = d;
+    if (stream) {
+        s->st = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete s;
+            return fail(RMT3D_ERR_CUDA, "stream creation failed");
+        }
+        s->own_stream = true;
+    }
+    grid_dev &g = s->g;
+    memset(&g, 0, sizeof(g));
+    g.sm = d.sys_size[0];
+    g.sn = d.sys_size[1];
+    g.so = d.sys_size[2];
+    g.sm4 = g.sm + 4;
+    g.sn4 = g.sn + 4;
+    g.so4 = g.so + 4;
+    g.smn4 = g.sm4 * g.sn4;
+    g.ncell = g.smn4 * g.so4;
+    for (int a = 0; a < 3; a++) g.prd[a] = d.periodic[a];
+    g.fm = g.sm + (g.prd[0] ? 0 : 1);
+    g.fn = g.sn + (g.prd[1] ? 0 : 1);
+    g.fo = g.so + (g.prd[2] ? 0 : 1);
+    // sim_params.cc:368-370
+    double lxx = d.bounds[1] - d.bounds[0], lyy = d.bounds[3] - d.bounds[2], lzz = d.bounds[5] - d.bounds[4];
+    g.dx = lxx / d.sys_size[0];
+    g.dy = lyy / d.sys_size[1];
+    g.dz = lzz / d.sys_size[2];
+    g.dxsp = 1.0 / g.dx;
+    g.dysp = 1.0 / g.dy;
+    g.dzsp = 1.0 / g.dz;
+    g.ax = d.bounds[0];
+    g.ay = d.bounds[2];
+    g.az = d.bounds[4];
+    g.mu = d.fmu;
+    g.frho = d.frho;
+    g.n_obj = d.n_obj;
+    g.sim_type = d.sim_type;
+    g.has_exact = d.has_exact;
+    g.gravity = d.gravity;
+    for (int f = 0; f < 6; f++) {
+        g.walls[f] = d.walls[f];
+        g.wall_pos[f] = d.wall_pos[f];
+    }
+    g.wall_dist = d.wall_dist;
+    g.winv = 1 / d.wall_dist;
+    const double dh = std::min(g.dx, std::min(g.dy, g.dz));
+
+    // sim_manager::create_objs (sim_manager.cc:68-81)
+    for (int o = 0; o < d.n_obj; o++) {
+        host_obj &ob = s->obj[o];
+        const rmt3d_object_desc &od = d.obj[o];
+        ob.type = od.type;
+        for (int c = 0; c < 3; c++) ob.c[c] = od.basic[c];
+        ob.R = od.basic[3];
+        ob.rho = od.rho;
+        ob.G = od.G;
+        ob.cs = sqrt(ob.G / ob.rho);
+        ob.ex_visc_mult = d.ex_visc_mult;
+        ob.ev_trans_mult = d.ev_trans_mult;
+        ob.dt_pad = d.sdt_pad;
+        ob.dt_ex_pad = d.dt_ex_pad;
+        ob.ex_mu = ob.ex_visc_mult * d.fmu;  // the override at sim_manager.cc:72
+        ob.volume = M_PI * 4 / 3 * pow(ob.R, 3);
+        for (int c = 0; c < 3; c++) {
+            ob.eig[c] = 1;
+            ob.omega[c] = 0;
+        }
+        if (ob.type == RMT3D_OBJ_SPHERE) {
+            int sd = int(od.extra[0]);
+            double sl = od.extra[1];
+            for (int c = 0; c < 3; c++) {
+                ob.eig[c] = sl;
+                ob.omega[c] = od.extra[2 + c];
+            }
+            ob.eig[sd] = 1. / (sl * sl);
+        }
+        obj_dev &gd = g.obj[o];
+        gd.type = ob.type;
+        for (int c = 0; c < 3; c++) {
+            gd.c[c] = ob.c[c];
+            gd.eig[c] = ob.eig[c];
+            gd.omega[c] = ob.omega[c];
+        }
+        gd.R = ob.R;
+        gd.G = ob.G;
+        gd.rho = ob.rho;
+        gd.ex_mu = ob.ex_mu;
+        gd.ev_trans_mult = ob.ev_trans_mult;
+    }
+    // sim_manager::setup_const (sim_manager.cc:37-53)
+    {
+        double xxsp3 = 3.0 / (dh * dh);
+        double dt_s = 100000;
+        for (int o = 0; o < d.n_obj; o++) {
+            double odt = s->obj[o].cfl(dh);
+            if (odt < dt_s) dt_s = odt;
+        }
+        double dt_f = 0.5 * d.frho / (d.fmu * xxsp3) * d.fdt_pad;
+        s->dt_reg = (dt_s < dt_f) ? dt_s : dt_f;
+        s->eps = d.wt_n * dh;
+        g.eps = s->eps;
+        g.tf1 = 0.5 / s->eps;
+        g.tf2 = 0.5 / M_PI;
+        g.tf3 = M_PI / s->eps;
+        if (d.dt < s->dt_reg) s->dt_reg = d.dt;
+        s->K_stiff = 0.0025 / (s->dt_reg * s->dt_reg);
+        g.K_stiff = s->K_stiff;
+    }
+    // vmax: sim_manager ctor value 1; sim_objects::set_wall_acc (sim_manager.hh:411-444)
+    s->vmax = 1;
+    if (d.sim_type == RMT3D_SIM_OBJECTS) {
+        double winv = g.winv;
+        s->min_wall_acc = 20 * winv;
+        double mvsq = -1, mvol = -1;
+        for (int o = 0; o < d.n_obj; o++) {
+            double rho_s = s->obj[o].rho;
+            double vsq = 0.5 * fabs((rho_s - d.frho) * d.gravity) / d.frho;
+            double mvol_fact = s->obj[o].volume / s->obj[o].R / s->obj[o].R;
+            vsq *= mvol_fact;
+            if (vsq > mvsq) mvsq = vsq;
+            if (mvol_fact > mvol) mvol = mvol_fact;
+            double support_acc = fabs((rho_s - d.frho) * d.gravity * winv * mvol_fact / rho_s);
+            if (support_acc > s->min_wall_acc) s->min_wall_acc = support_acc;
+        }
+        s->wall_acc_mult = 0.5 * mvol * pow(winv, 2);
+        mvsq = sqrt(mvsq);
+        s->vmax = mvsq;  // NaN without objects, exactly as in the reference
+    }
+    g.min_wall_acc = s->min_wall_acc;
+    g.wall_acc_mult = s->wall_acc_mult;
+    // fluid_3d::setup_faces (fluid_3d.cc:2952-2974)
+    for (int f = 0; f < 6; f++) {
+        for (int c = 0; c < 3; c++) {
+            s->faces[f].bct[c] = d.bct[c][f];
+            s->faces[f].bcv[c] = d.bcv[c][f];
+            if (d.bct[c][f] == 1 && d.bcv[c][f] > s->vmax) s->vmax = d.bcv[c][f];
+        }
+        s->faces[f].h = (f / 2 == 0) ? g.dx : ((f / 2 == 1) ? g.dy : g.dz);
+        s->wall[f] = !g.prd[f / 2];
+        if (s->wall[f])
+            for (int c = 0; c < 3; c++)
+                if (d.bct[c][f] != 1 && d.bct[c][f] != 2) {
+                    rmt3d_scene_destroy(s);
+                    return fail(RMT3D_ERR_INVALID, "bad boundary condition type");
+                }
+    }
+    s->dt = d.dt;
+
+    // coordinates (fluid_3d.cc:137-139)
+    s->hlx.resize(g.sm4);
+    s->hly.resize(g.sn4);
+    s->hlz.resize(g.so4);
+    for (int i = 0; i < g.sm4; i++) s->hlx[i] = g.ax + (0 + i - 2 + 0.5) * g.dx;
+    for (int j = 0; j < g.sn4; j++) s->hly[j] = g.ay + (0 + j - 2 + 0.5) * g.dy;
+    for (int k = 0; k < g.so4; k++) s->hlz[k] = g.az + (0 + k - 2 + 0.5) * g.dz;
+
+    // device state
+    const size_t n = g.ncell;
+    int e = 0;
+    fields_dev &F = s->hF;
+    memset(&F, 0, sizeof(F));
+    for (int c = 0; c < 3 && !e; c++) e |= s->alloc(&F.vel[c], n) | s->alloc(&F.dvel[c], n);
+    e |= s->alloc(&F.p, n) | s->alloc(&F.dp, n) | s->alloc(&F.q, n);
+    for (int c = 0; c < 18 && !e; c++) e |= s->alloc(&F.fvel[c], n);
+    for (int c = 0; c < 9 && !e; c++) e |= s->alloc(&F.sigma[c], n);
+    if (d.var_den) e |= s->alloc(&F.rho, n);
+    for (int o = 0; o < d.n_obj && !e; o++) {
+        objmap_dev &m = F.om[o];
+        e |= s->alloc(&m.code, n) | s->alloc(&m.code_prev, n);
+        for (int c = 0; c < 3; c++) e |= s->alloc(&m.x[c], n) | s->alloc(&m.xp[c], n) | s->alloc(&m.x_prev[c], n) | s->alloc(&m.det[c], n);
+        for (int c = 0; c < 18; c++) e |= s->alloc(&m.fx[c], n);
+        for (int c = 0; c < 9; c++) e |= s->alloc(&m.gp[c], n) | s->alloc(&m.gp_prev[c], n);
+        cudaMemsetAsync(m.code, 0xff, n * sizeof(int), s->st);
+        cudaMemsetAsync(m.code_prev, 0xff, n * sizeof(int), s->st);
+    }
+    e |= s->alloc(&s->lx, g.sm4) | s->alloc(&s->ly, g.sn4) | s->alloc(&s->lz, g.so4);
+    e |= s->alloc(&s->dF, 1);
+    if (d.n_obj > 0) {
+        e |= s->alloc(&s->lay, n) | s->alloc(&s->inl, n) | s->alloc(&s->front[0], n) | s->alloc(&s->front[1], n);
+    }
+    e |= s->alloc(&s->counters, 8) | s->alloc(&s->d_mean, 1) | s->alloc(&s->d_red, 1);
+    if (e) {
+        rmt3d_scene_destroy(s);
+        return RMT3D_ERR_OOM;
+    }
+    cudaMallocHost(&s->h_counters, 8 * sizeof(int));
+    cudaMallocHost(&s->h_scalar, sizeof(double));
+    cudaMemcpyAsync(s->lx, s->hlx.data(), g.sm4 * 8, cudaMemcpyHostToDevice, s->st);
+    cudaMemcpyAsync(s->ly, s->hly.data(), g.sn4 * 8, cudaMemcpyHostToDevice, s->st);
+    cudaMemcpyAsync(s->lz, s->hlz.data(), g.so4 * 8, cudaMemcpyHostToDevice, s->st);
+    cudaMemcpyAsync(s->dF, &F, sizeof(F), cudaMemcpyHostToDevice, s->st);
+    s->mac.launches = &s->launches;
+    s->fem.launches = &s->launches;
+    int nm[3] = {g.sm, g.sn, g.so}, nf[3] = {g.fm, g.fn, g.fo};
+    bool mixed = d.precision == RMT3D_MIXED;
+    if ((e = s->mac.setup(MG_MAC, nm, g.prd, mixed, s->st)) != 0 || (e = s->fem.setup(MG_FEM, nf, g.prd, mixed, s->st)) != 0) {
+        rmt3d_scene_destroy(s);
+        return e;
+    }
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) {
+        rmt3d_scene_destroy(s);
+        return fail(RMT3D_ERR_CUDA, "scene set-up failed");
+    }
+    *out = s;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_initialize(rmt3d_scene *s) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    s->time = 0;
+    int e;
+    if ((e = init_fluid(s))) return e;
+    if ((e = init_pres(s))) return e;
+    if ((e = init_refmap(s))) return e;
+    init_extrapolate(s);
+    update_rho(s);
+    fill_boundary_cc(s);
+    compute_grad_basis(s);
+    CK(cudaMemcpyAsync(s->h_counters, s->counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (s->h_counters[2] > 0) return fail(RMT3D_ERR_EXTRAP, "Extrapolation failed: no eligible points or degenerate matrix");
+    CK(cudaGetLastError());
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_set_dt(rmt3d_scene *s, double dt) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    s->dt = dt;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_init_iter(rmt3d_scene *s) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    const double tol = 1e-4;
+    for (int i = 0; i < s->d.num_iters; i++) {
+        s->time = 0;
+        fill_boundary_cc(s);
+        int e = step_forward(s, 0);
+        if (e < 0) return e;
+        double divu;
+        if ((e = div_u(s, &divu))) return e;
+        if ((e = init_fluid(s))) return e;
+        if ((e = init_refmap(s))) return e;
+        if (s->g.n_obj > 0) {
+            k_reset_extraps<<<lin_blocks(s->g.ncell), 256, 0, s->st>>>(s->g, s->dF);
+            s->count();
+        }
+        init_extrapolate(s);
+        update_rho(s);
+        if (divu < tol) break;
+    }
+    s->nt = 0;
+    s->time = 0.0;
+    compute_stress(s);
+    CK(cudaStreamSynchronize(s->st));
+    CK(cudaGetLastError());
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_prepare(rmt3d_scene *s) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    int e = rmt3d_initialize(s);
+    if (e) return e;
+    double dt;
+    if ((e = rmt3d_stepper_dt(&s->d, s->dt_reg, &dt, nullptr))) return e;
+    s->dt = dt;
+    if ((e = rmt3d_init_iter(s))) return e;
+    s->dt = dt;  // stepper::run re-links dt (stepper.hh:336)
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_step(rmt3d_scene *s, int debug, int *status) {
+    if (!s || !status) return fail(RMT3D_ERR_INVALID, "null argument");
+    int e = step_forward(s, debug);
+    if (e < 0) {
+        *status = e;
+        return e;
+    }
+    *status = e;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_run(rmt3d_scene *s, int nsteps, int *status) {
+    if (!s || !status) return fail(RMT3D_ERR_INVALID, "null argument");
+    *status = 0;
+    for (int i = 0; i < nsteps; i++) {
+        int e = rmt3d_step(s, 0, status);
+        if (e) return e;
+        if (*status) return RMT3D_OK;
+    }
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_get_scalar(rmt3d_scene *s, int which, double *v) {
+    if (!s || !v) return fail(RMT3D_ERR_INVALID, "null argument");
+    switch (which) {
+        case 0: *v = s->dt; break;
+        case 1: *v = s->time; break;
+        case 2: *v = s->dt_reg; break;
+        case 3: *v = s->eps; break;
+        case 4: *v = s->nt; break;
+        case 5: *v = s->mac.last_cycles; break;
+        case 6: *v = s->fem.last_cycles; break;
+        case 7: *v = (double)s->mac.cycles_total; break;
+        case 8: *v = (double)s->fem.cycles_total; break;
+        case 9: {
+            long long cnt = 0;
+            std::vector<int> code(s->g.ncell);
+            for (int o = 0; o < s->g.n_obj; o++) {
+                CK(cudaMemcpy(code.data(), s->hF.om[o].code, s->g.ncell * sizeof(int), cudaMemcpyDeviceToHost));
+                for (int c : code) cnt += (c > 0);
+            }
+            *v = (double)cnt;
+            break;
+        }
+        case 10: *v = s->K_stiff; break;
+        case 11: *v = s->vmax; break;
+        default: return fail(RMT3D_ERR_INVALID, "unknown scalar");
+    }
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_get_dims(rmt3d_scene *s, int dims[6]) {
+    if (!s || !dims) return fail(RMT3D_ERR_INVALID, "null argument");
+    dims[0] = s->g.sm4;
+    dims[1] = s->g.sn4;
+    dims[2] = s->g.so4;
+    dims[3] = s->g.fm;
+    dims[4] = s->g.fn;
+    dims[5] = s->g.fo;
+    return RMT3D_OK;
+}
+
+static double *field_ptr(rmt3d_scene *s, int which) {
+    fields_dev &F = s->hF;
+    if (which >= 0 && which < 3) return F.vel[which];
+    if (which == 3) return F.p;
+    if (which == 4) return F.dp;
+    if (which == 5) return F.q;
+    if (which >= 6 && which < 9) return F.dvel[which - 6];
+    if (which >= 9 && which < 27) return F.fvel[which - 9];
+    if (which >= 27 && which < 36) return F.sigma[which - 27];
+    return nullptr;
+}
+
+extern "C" int rmt3d_get_field(rmt3d_scene *s, int which, double *dst) {
+    if (!s || !dst) return fail(RMT3D_ERR_INVALID, "null argument");
+    double *p = field_ptr(s, which);
+    if (!p) return fail(RMT3D_ERR_INVALID, "unknown field");
+    CK(cudaStreamSynchronize(s->st));
+    CK(cudaMemcpy(dst, p, s->g.ncell * sizeof(double), cudaMemcpyDeviceToHost));
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_get_refmap(rmt3d_scene *s, int obj, int *code, double *x, double *xpred) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (obj < 0 || obj >= s->g.n_obj) return fail(RMT3D_ERR_INVALID, "object index out of range");
+    const size_t n = s->g.ncell;
+    objmap_dev &m = s->hF.om[obj];
+    CK(cudaStreamSynchronize(s->st));
+    if (code) CK(cudaMemcpy(code, m.code, n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int c = 0; c < 3; c++) {
+        if (x) CK(cudaMemcpy(x + c * n, m.x[c], n * 8, cudaMemcpyDeviceToHost));
+        if (xpred) CK(cudaMemcpy(xpred + c * n, m.xp[c], n * 8, cudaMemcpyDeviceToHost));
+    }
+    return RMT3D_OK;
+}
+
+// AoS offsets of struct field (360 B) and struct ref_map (488 B), fields.hh
+namespace {
+// field: vel[3], p, dp, q, dvel[3], nv_der[3][3], fvel[6][3], sigma[3][3]
+constexpr int F_VEL = 0, F_P = 3, F_DP = 4, F_Q = 5, F_DVEL = 6, F_FVEL = 18, F_SIGMA = 36, F_N = 45;
+// ref_map (in doubles after the 8-byte id word): x[3], xpred[3], nv_der[3][3],
+// fx[6][3], sigma[3][3], elastic_energy[3], detF[3], grad_phi[3][3], act_power[3]
+constexpr int R_X = 1, R_XP = 4, R_FX = 16, R_DET = 46, R_GP = 49;
+}  // namespace
+
+extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, const void *refmap_aos,
+                                      const int *ext_index, const void *ext_refmaps, int n_ext, double dt,
+                                      double time) {
+    if (!s || !field_aos) return fail(RMT3D_ERR_INVALID, "null argument");
+    const size_t n = s->g.ncell;
+    const double *fa = (const double *)field_aos;
+    std::vector<double> buf(n);
+    auto put = [&](double *dst, const double *src, int stride, int off) -> int {
+        for (size_t i = 0; i < n; i++) buf[i] = src[i * stride + off];
+        CK(cudaMemcpy(dst, buf.data(), n * 8, cudaMemcpyHostToDevice));
+        return 0;
+    };
+    int e = 0;
+    for (int c = 0; c < 3; c++) e |= put(s->hF.vel[c], fa, F_N, F_VEL + c) | put(s->hF.dvel[c], fa, F_N, F_DVEL + c);
+    e |= put(s->hF.p, fa, F_N, F_P) | put(s->hF.dp, fa, F_N, F_DP) | put(s->hF.q, fa, F_N, F_Q);
+    for (int c = 0; c < 18; c++) e |= put(s->hF.fvel[c], fa, F_N, F_FVEL + c);
+    for (int c = 0; c < 9; c++) e |= put(s->hF.sigma[c], fa, F_N, F_SIGMA + c);
+    if (e) return e;
+    const int no = s->g.n_obj;
+    if (no > 0 && refmap_aos) {
+        std::vector<int> code(n);
+        std::vector<double> X(n * 3), XP(n * 3), FX(n * 18), GP(n * 9), DT(n * 3);
+        auto rd = [&](const unsigned char *rec, int off) { return ((const double *)rec)[off]; };
+        for (int o = 0; o < no; o++) {
+            std::fill(code.begin(), code.end(), -1);
+            std::fill(GP.begin(), GP.end(), -kBig);
+            const unsigned char *ra = (const unsigned char *)refmap_aos;
+            auto take = [&](size_t cell, const unsigned char *rec, int cd) {
+                code[cell] = cd;
+                for (int c = 0; c < 3; c++) {
+                    X[c * n + cell] = rd(rec, R_X + c);
+                    XP[c * n + cell] = rd(rec, R_XP + c);
+                    DT[c * n + cell] = rd(rec, R_DET + c);
+                }
+                for (int c = 0; c < 18; c++) FX[c * n + cell] = rd(rec, R_FX + c);
+                for (int c = 0; c < 9; c++) GP[c * n + cell] = rd(rec, R_GP + c);
+            };
+            for (size_t i = 0; i < n; i++) {
+                const unsigned char *rec = ra + i * 488;
+                unsigned int cc = *(const unsigned int *)rec;
+                if ((int)(cc & 1023) == o + 1) take(i, rec, (cc >> 10) & 63);
+            }
+            const unsigned char *ea = (const unsigned char *)ext_refmaps;
+            for (int q = 0; q < n_ext; q++) {
+                const unsigned char *rec = ea + (size_t)q * 488;
+                unsigned int cc = *(const unsigned int *)rec;
+                if ((int)(cc & 1023) == o + 1) take(ext_index[q], rec, (cc >> 10) & 63);
+            }
+            objmap_dev &m = s->hF.om[o];
+            CK(cudaMemcpy(m.code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+            for (int c = 0; c < 3; c++) {
+                CK(cudaMemcpy(m.x[c], X.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(m.xp[c], XP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(m.det[c], DT.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+            }
+            for (int c = 0; c < 18; c++) CK(cudaMemcpy(m.fx[c], FX.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+            for (int c = 0; c < 9; c++) CK(cudaMemcpy(m.gp[c], GP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+        }
+    }
+    s->dt = dt;
+    s->time = time;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *refmap_aos, int *ext_index,
+                                      void *ext_refmaps, int max_ext, int *n_ext) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    const size_t n = s->g.ncell;
+    CK(cudaStreamSynchronize(s->st));
+    std::vector<double> buf(n);
+    if (field_aos) {
+        double *fa = (double *)field_aos;
+        memset(fa, 0, n * 360);
+        auto get = [&](const double *src, int off) -> int {
+            CK(cudaMemcpy(buf.data(), src, n * 8, cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; i++) fa[i * F_N + off] = buf[i];
+            return 0;
+        };
+        int e = 0;
+        for (int c = 0; c < 3; c++) e |= get(s->hF.vel[c], F_VEL + c) | get(s->hF.dvel[c], F_DVEL + c);
+        e |= get(s->hF.p, F_P) | get(s->hF.dp, F_DP) | get(s->hF.q, F_Q);
+        for (int c = 0; c < 18; c++) e |= get(s->hF.fvel[c], F_FVEL + c);
+        for (int c = 0; c < 9; c++) e |= get(s->hF.sigma[c], F_SIGMA + c);
+        if (e) return e;
+    }
+    int ne = 0;
+    if (refmap_aos) memset(refmap_aos, 0, n * 488);
+    std::vector<int> code(n);
+    std::vector<double> X(3 * n), XP(3 * n), FX(18 * n), GP(9 * n);
+    for (int o = 0; o < s->g.n_obj; o++) {
+        objmap_dev &m = s->hF.om[o];
+        CK(cudaMemcpy(code.data(), m.code, n * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int c = 0; c < 3; c++) {
+            CK(cudaMemcpy(X.data() + c * n, m.x[c], n * 8, cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(XP.data() + c * n, m.xp[c], n * 8, cudaMemcpyDeviceToHost));
+        }
+        for (int c = 0; c < 18; c++) CK(cudaMemcpy(FX.data() + c * n, m.fx[c], n * 8, cudaMemcpyDeviceToHost));
+        for (int c = 0; c < 9; c++) CK(cudaMemcpy(GP.data() + c * n, m.gp[c], n * 8, cudaMemcpyDeviceToHost));
+        auto fill = [&](unsigned char *rec, size_t cell, int cd) {
+            *(unsigned int *)rec = (unsigned)(o + 1) | ((unsigned)cd << 10);
+            double *r = (double *)rec;
+            for (int c = 0; c < 3; c++) {
+                r[R_X + c] = X[c * n + cell];
+                r[R_XP + c] = XP[c * n + cell];
+            }
+            for (int c = 0; c < 18; c++) r[R_FX + c] = FX[c * n + cell];
+            for (int c = 0; c < 9; c++) r[R_GP + c] = GP[c * n + cell];
+        };
+        for (size_t i = 0; i < n; i++) {
+            if (code[i] == 0 && refmap_aos) fill((unsigned char *)refmap_aos + i * 488, i, 0);
+            if (code[i] > 0) {
+                if (ne < max_ext && ext_refmaps && ext_index) {
+                    ext_index[ne] = (int)i;
+                    fill((unsigned char *)ext_refmaps + (size_t)ne * 488, i, code[i]);
+                }
+                ne++;
+            }
+        }
+    }
+    if (n_ext) *n_ext = ne;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_diag(rmt3d_scene *s, int kind, double *value) {
+    if (!s || !value) return fail(RMT3D_ERR_INVALID, "null argument");
+    if (kind == 0) return div_u(s, value);
+    return fail(RMT3D_ERR_INVALID, "unknown diagnostic");
+}
+
+extern "C" int rmt3d_sync(rmt3d_scene *s) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    CK(cudaStreamSynchronize(s->st));
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_launch_count(rmt3d_scene *s, long long *count) {
+    if (!s || !count) return fail(RMT3D_ERR_INVALID, "null argument");
+    *count = s->launches;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_scene_destroy(rmt3d_scene *s) {
+    if (!s) return RMT3D_OK;
+    cudaStreamSynchronize(s->st);
+    for (void *p : s->allocs) cudaFree(p);
+    if (s->h_counters) cudaFreeHost(s->h_counters);
+    if (s->h_scalar) cudaFreeHost(s->h_scalar);
+    if (s->own_stream) cudaStreamDestroy(s->st);
+    delete s;
+    return RMT3D_OK;
+}
