@@ -88,6 +88,10 @@ typedef struct {
     rmt3d_object_desc obj[RMT3D_MAX_OBJ];
     int var_den;   /* compile-time VAR_DEN in the reference (Execs/Makefile:37-42) */
     int precision; /* RMT3D_FP64 or RMT3D_MIXED */
+    int mg_exact;  /* 0: the reference's V-cycle control (residual tolerance of
+                      mg_probs.hh:483-518); 1: additionally iterate every
+                      Poisson solve until its residual stops shrinking, so
+                      results are free of tolerance-level noise */
 } rmt3d_scene_desc;
 
 typedef struct rmt3d_scene rmt3d_scene;
@@ -134,6 +138,14 @@ int rmt3d_prepare(rmt3d_scene *s);
  * reference's step code; the return value is RMT3D_OK unless the call itself
  * failed. */
 int rmt3d_step(rmt3d_scene *s, int debug, int *status);
+
+/* The first last_phase (1..9) phase groups of one step_forward, for
+ * phase-by-phase inspection: 1 compute_stress; 2 normal derivatives and
+ * half-time edge states; 3 face BCs and Godunov upwinding; 4 MAC projection;
+ * 5 update_reference_map; 6 compute_stress; 7 compute_ustar and cell BCs;
+ * 8 pp_solve; 9 full reference-map update, redraw_boundary and cell BCs.
+ * These are the member calls of fluid_3d.cc:470-560 in order. */
+int rmt3d_step_phases(rmt3d_scene *s, int last_phase, int *status);
 
 /* n calls of rmt3d_step, stopping at the first non-zero status. */
 int rmt3d_run(rmt3d_scene *s, int nsteps, int *status);

@@ -7,6 +7,11 @@
  *
  * Usage: ref_driver <file.cfg> <steps> <out.bin>
  *   steps = 0 writes the state after init_iter, before the first step.
+ *        ref_driver <file.cfg> <steps> <prefix> phases
+ *   runs <steps> steps, writes <prefix>_P0.bin, then runs the next step as
+ *   the nine phase groups of fluid_3d::step_forward (fluid_3d.cc:429-577),
+ *   calling the same members in the same order, and writes <prefix>_P<k>.bin
+ *   after group k.
  *
  * Output layout (little endian):
  *   char[4] "RMTD"; int32 version=1;
@@ -82,8 +87,54 @@ int main(int argc, char *argv[]) {
     f3d.dt = sim.dt;
     f3d.init_iter(init_err);
 
+    const bool phases = argc > 4 && strcmp(argv[4], "phases") == 0;
     double t0 = MPI_Wtime();
     if (nsteps > 0) sim.run(f3d);
+    if (phases) {
+        char fn[1024];
+        auto out = [&](int k) {
+            snprintf(fn, sizeof(fn), "%s_P%d.bin", argv[3], k);
+            dump(f3d, nsteps, fn);
+        };
+        f3d.set_dt(sim.dt);
+        out(0);
+        f3d.nt++;
+        f3d.compute_stress(false);
+        out(1);
+        f3d.normal_derivatives_velocity(f3d.dt, false);
+        f3d.normal_derivatives_refmap(f3d.dt, false);
+        f3d.compute_half_time_edge_velocities(f3d.dt, false);
+        f3d.compute_half_time_edge_refmap(f3d.dt, false);
+        f3d.time += 0.5 * f3d.dt;
+        out(2);
+        f3d.fill_boundary_cf(false);
+        f3d.godunov_upwinding_set(false, false);
+        f3d.fill_boundary_cf(false);
+        out(3);
+        f3d.mac_solve(f3d.dt, false);
+        f3d.fill_boundary_cf(false);
+        out(4);
+        int err = f3d.update_reference_map(f3d.dt, false);
+        if (err) printf("# ref_driver: update_reference_map error %d\n", err);
+        out(5);
+        f3d.compute_stress(false);
+        out(6);
+        f3d.compute_ustar(f3d.dt, false);
+        f3d.fill_boundary_cc(false);
+        f3d.communicate<2048>();
+        f3d.time += 0.5 * f3d.dt;
+        out(7);
+        f3d.pp_solve(false);
+        out(8);
+        f3d.update_reference_map_full(false);
+        f3d.redraw_boundary(false);
+        f3d.fill_boundary_cc(false);
+        f3d.communicate<2048>();
+        out(9);
+        printf("# ref_driver: phases written\n");
+        delete mgmt;
+        return 0;
+    }
     double t1 = MPI_Wtime();
     printf("# ref_driver: %d steps in %.6f s (dt %.17g)\n", nsteps, t1 - t0, f3d.dt);
     f3d.watch.report();

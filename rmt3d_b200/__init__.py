@@ -100,6 +100,27 @@ class Scene:
         _lib.check(lib().rmt3d_step(self._h, debug, ctypes.byref(st)))
         return st.value
 
+    def step_phases(self, last_phase):
+        """The first `last_phase` phase groups of one step (inspection)."""
+        st = ctypes.c_int()
+        _lib.check(lib().rmt3d_step_phases(self._h, last_phase, ctypes.byref(st)))
+        return st.value
+
+    def export_reference(self):
+        """State in the reference's AoS layout: (fields, refmaps, ext_index, ext_maps)."""
+        from oracle.refdump import FIELD_DT, REFMAP_DT
+        fields = np.zeros(self.ncell, dtype=FIELD_DT)
+        rm = np.zeros(self.ncell, dtype=REFMAP_DT)
+        n = ctypes.c_int()
+        _lib.check(lib().rmt3d_export_reference(self._h, fields.ctypes.data_as(ctypes.c_void_p),
+                                                rm.ctypes.data_as(ctypes.c_void_p), None, None, 0,
+                                                ctypes.byref(n)))
+        idx = np.zeros(max(n.value, 1), dtype=np.int32)
+        ext = np.zeros(max(n.value, 1), dtype=REFMAP_DT)
+        _lib.check(lib().rmt3d_export_reference(self._h, None, None, idx.ctypes.data_as(ctypes.c_void_p),
+                                                ext.ctypes.data_as(ctypes.c_void_p), n.value, ctypes.byref(n)))
+        return fields, rm, idx[:n.value], ext[:n.value]
+
     def run(self, nsteps):
         st = ctypes.c_int()
         _lib.check(lib().rmt3d_run(self._h, nsteps, ctypes.byref(st)))

@@ -77,6 +77,7 @@ class SceneDesc(ctypes.Structure):
         ("obj", ObjectDesc * MAX_OBJ),
         ("var_den", ctypes.c_int),
         ("precision", ctypes.c_int),
+        ("mg_exact", ctypes.c_int),
     ]
 
 
@@ -99,6 +100,7 @@ SIGNATURES = {
     "rmt3d_prepare": (_I, [_P]),
     "rmt3d_step": (_I, [_P, _I, _IP]),
     "rmt3d_run": (_I, [_P, _I, _IP]),
+    "rmt3d_step_phases": (_I, [_P, _I, _IP]),
     "rmt3d_get_scalar": (_I, [_P, _I, _DP]),
     "rmt3d_get_dims": (_I, [_P, _IP]),
     "rmt3d_get_field": (_I, [_P, _I, _P]),

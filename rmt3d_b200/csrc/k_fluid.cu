@@ -119,7 +119,7 @@ __global__ void k_bc_cf(grid_dev g, int face, bc_face bc, const fields_dev *F) {
 // Stress on the three lower faces, fluid_3d::compute_stress
 // (fluid_3d.cc:1360-1461) with solid_stress (:1777-1997), fluid_stress
 // (:2001-2031) and collision_stress (:1465-1773).  One thread per cell over
-// relative cells -1..s+1.
+// relative cells -1..s+1 inclusive, i.e. absolute 1..s+3.
 // -------------------------------------------------------------------------
 __device__ inline bool has_map(const objmap_dev &m, int ind) { return m.code[ind] >= 0; }
 
@@ -347,7 +347,7 @@ __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (i > g.sm + 2 || j > g.sn + 2 || k > g.so + 2) return;
+    if (i > g.sm + 3 || j > g.sn + 3 || k > g.so + 3) return;
     const int ind = gidx(g, i, j, k);
     face_stress<0>(g, F, i, j, k, ind, true);
     face_stress<1>(g, F, i, j, k, ind, true);

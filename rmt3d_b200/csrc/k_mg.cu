@@ -520,6 +520,15 @@ double mg_solver::run(cudaStream_t st) {
         res = residual_max(st);
     }
     for (int i = 0; i < 2; i++) vcycle(st);
+    if (exact) {
+        double prev = 1e300;
+        res = residual_max(st);
+        for (int it = 0; it < 60 && res > 0 && res < 0.7 * prev; it++) {
+            vcycle(st);
+            prev = res;
+            res = residual_max(st);
+        }
+    }
     pred.update(extra);
     return res;
 }

@@ -45,6 +45,7 @@ class mg_solver {
     long long cycles_total = 0;
     int last_cycles = 0;
     bool mixed = false;  // FP32 cycles inside FP64 iterative refinement
+    bool exact = false;  // iterate each solve until the residual stagnates
     long long *launches = nullptr;
 
     mg_solver() = default;

@@ -485,7 +485,7 @@ static void compute_grad_basis(rmt3d_scene *s) {
 // ---------------------------------------------------------------------------
 static void compute_stress(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    k_stress<<<grd(g.sm + 3, g.sn + 3, g.so + 3), blk(), 0, s->st>>>(g, s->dF);
+    k_stress<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF);
     s->count();
 }
 
@@ -560,12 +560,13 @@ static int update_reference_map(rmt3d_scene *s, double cdt, int *prob) {
     return 0;
 }
 
-static int step_forward(rmt3d_scene *s, int debug) {
+static int step_forward(rmt3d_scene *s, int debug, int stop = 99) {
     const grid_dev &g = s->g;
     (void)debug;
     s->nt++;
     CK(cudaMemsetAsync(s->counters + 2, 0, 6 * sizeof(int), s->st));
     compute_stress(s);
+    if (stop <= 1) return RMT3D_OK;
     k_edge_vel<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, s->time,
                                                             s->d.var_den);
     s->count();
@@ -574,14 +575,17 @@ static int step_forward(rmt3d_scene *s, int debug) {
         s->count();
     }
     s->time += 0.5 * s->dt;
+    if (stop <= 2) return RMT3D_OK;
     fill_boundary_cf(s);
     comm_face_maps(s);
     k_upwind<<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
     s->count();
     fill_boundary_cf(s);
+    if (stop <= 3) return RMT3D_OK;
     int e = mac_solve(s, s->dt);
     if (e) return e;
     fill_boundary_cf(s);
+    if (stop <= 4) return RMT3D_OK;
     int prob = 0;
     e = update_reference_map(s, s->dt, &prob);
     if (e) return e;
@@ -590,13 +594,17 @@ static int step_forward(rmt3d_scene *s, int debug) {
         s->count();
         return RMT3D_REFMAP_UPDATE_ERR;
     }
+    if (stop <= 5) return RMT3D_OK;
     compute_stress(s);
+    if (stop <= 6) return RMT3D_OK;
     k_ustar<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, s->time, s->d.var_den);
     s->count();
     fill_boundary_cc(s);
     comm_dvel(s);
     s->time += 0.5 * s->dt;
+    if (stop <= 7) return RMT3D_OK;
     if (pp_solve(s)) return RMT3D_PROJECTION_ERR;
+    if (stop <= 8) return RMT3D_OK;
     if (g.n_obj > 0) {
         k_refmap_full<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
         s->count();
@@ -864,6 +872,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     s->fem.launches = &s->launches;
     int nm[3] = {g.sm, g.sn, g.so}, nf[3] = {g.fm, g.fn, g.fo};
     bool mixed = d.precision == RMT3D_MIXED;
+    s->mac.exact = s->fem.exact = d.mg_exact != 0;
     if ((e = s->mac.setup(MG_MAC, nm, g.prd, mixed, s->st)) != 0 || (e = s->fem.setup(MG_FEM, nf, g.prd, mixed, s->st)) != 0) {
         rmt3d_scene_destroy(s);
         return e;
@@ -948,6 +957,16 @@ extern "C" int rmt3d_step(rmt3d_scene *s, int debug, int *status) {
         return e;
     }
     *status = e;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_step_phases(rmt3d_scene *s, int last_phase, int *status) {
+    if (!s || !status) return fail(RMT3D_ERR_INVALID, "null argument");
+    if (last_phase < 1 || last_phase > 9) return fail(RMT3D_ERR_INVALID, "phase outside 1..9");
+    int e = step_forward(s, 0, last_phase);
+    *status = e;
+    if (e < 0) return e;
+    CK(cudaStreamSynchronize(s->st));
     return RMT3D_OK;
 }
 

@@ -4,10 +4,12 @@ Runs the reference solver (compiled from its own sources by oracle/Makefile
 into oracle/_ref/ref_driver) on small seeded workloads and stores, for each
 saved step count, the state the FSI step reads and writes: velocities and
 nodal pressure over the ghosted box, the primary reference maps and the
-extrapolated maps.  Usage (in the build container, where the reference is
-present):
+extrapolated maps.  The oracle's Poisson solves run with RMT3D_SHIM_EXACT=1
+(converged to round-off on every solve), so the fixtures carry no
+residual-tolerance noise.  Usage (in the build container, where the reference
+is present):
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle all nofma && python tests/golden/make_golden.py
 """
 import os
 import subprocess
@@ -24,6 +26,8 @@ from oracle import refdump  # noqa: E402
 from rmt3d_b200 import scenes  # noqa: E402
 
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+# the reference rebuilt without FMA contraction (make -C oracle nofma)
+DRIVER_NOFMA = os.path.join(ROOT, "oracle", "_ref", "nofma", "ref_driver")
 
 # name -> (cfg text, saved step counts)
 CASES = {
@@ -59,24 +63,55 @@ def compact(d):
     return out
 
 
-def run(cfg_text, steps, workdir):
+def run(cfg_text, steps, workdir, driver=DRIVER, exact="1"):
     cfg = os.path.join(workdir, "case.cfg")
     with open(cfg, "w") as fh:
         fh.write(cfg_text)
     out = os.path.join(workdir, "s%d.bin" % steps)
-    subprocess.run([DRIVER, cfg, str(steps), out], check=True, capture_output=True, cwd=workdir)
+    env = dict(os.environ, RMT3D_SHIM_EXACT=exact)
+    subprocess.run([driver, cfg, str(steps), out], check=True, capture_output=True, cwd=workdir, env=env)
     return refdump.read(out)
 
 
+def _rel(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def envelope(cfg_text, steps, base, workdir):
+    """Rounding envelope of the reference at this state: the largest rel-L2
+    change of (velocity vector, pressure, reference map) between the fixture
+    and two other valid roundings of the same computation -- the build without
+    FMA contraction, and the reference's own residual-tolerance multigrid
+    control instead of round-off convergence."""
+    shp = base["shape"]
+    sl = (slice(2, -2),) * 3
+    vb = base["fields"]["vel"].reshape(shp + (3,))[sl]
+    pb = base["fields"]["p"].reshape(shp)[sl]
+    env = np.zeros(3)
+    for drv, ex in ((DRIVER_NOFMA, "1"), (DRIVER, "0")):
+        d = run(cfg_text, steps, workdir, drv, ex)
+        v = d["fields"]["vel"].reshape(shp + (3,))[sl]
+        p = d["fields"]["p"].reshape(shp)[sl]
+        x_b = base["refmaps"]["x"][base["refmaps"]["c"] != 0]
+        x_d = d["refmaps"]["x"][d["refmaps"]["c"] != 0]
+        xe = _rel(x_d, x_b) if x_b.shape == x_d.shape and x_b.size else 0.0
+        env = np.maximum(env, [_rel(v, vb), _rel(p, pb), xe])
+    return env
+
+
 def main():
-    if not os.path.exists(DRIVER):
-        sys.exit("build the reference first: make -C oracle")
+    if not (os.path.exists(DRIVER) and os.path.exists(DRIVER_NOFMA)):
+        sys.exit("build the reference first: make -C oracle all nofma")
     with tempfile.TemporaryDirectory() as wd:
         for name, (txt, steps) in CASES.items():
             arrays = {"cfg": np.frombuffer(txt.encode(), dtype=np.uint8)}
             for k in steps:
-                for key, val in compact(run(txt, k, wd)).items():
+                d = run(txt, k, wd)
+                for key, val in compact(d).items():
                     arrays["s%d_%s" % (k, key)] = val
+                arrays["s%d_env" % k] = envelope(txt, k, d, wd)
+                print(name, k, "envelope", arrays["s%d_env" % k])
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
             print("wrote", name)
         for name, (txt, k) in LONG.items():
@@ -92,7 +127,9 @@ def main():
                 "v": vel[:, 1].reshape(shp)[sl].copy(),
                 "w": vel[:, 2].reshape(shp)[sl].copy(),
                 "p": d["fields"]["p"].reshape(shp)[sl].copy(),
+                "env": envelope(txt, k, d, wd),
             }
+            print(name, "envelope", arrays["env"])
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
             print("wrote", name)
 

@@ -20,7 +20,8 @@ def test_fixture_reproduces_from_reference(tmp_path, name, k):
     fx = H.load_fixture(name)
     cfg = H.fixture_cfg(fx, str(tmp_path / "case.cfg"))
     out = str(tmp_path / "o.bin")
-    subprocess.run([DRIVER, cfg, str(k), out], check=True, capture_output=True, cwd=str(tmp_path))
+    env = dict(os.environ, RMT3D_SHIM_EXACT="1")
+    subprocess.run([DRIVER, cfg, str(k), out], check=True, capture_output=True, cwd=str(tmp_path), env=env)
     d = refdump.read(out)
     st = H.state(fx, k)
     assert d["dt"] == st["dt"] and d["time"] == st["time"]
