@@ -186,6 +186,25 @@ int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *refmap_aos,
  * 1 solid volume sum H(phi) dV for object 0 (compute_centroid :1348-1379). */
 int rmt3d_diag(rmt3d_scene *s, int kind, double *value);
 
+/* Allocation-free divergence diagnostic (no counterpart in the reference; it
+ * is an addition of this library).  Same value as rmt3d_diag(s, 0, ...) for
+ * a scene with the given grid, computed from caller-owned device arrays, for
+ * hosts that cannot allocate device memory when they need it (a host running
+ * inside a memory pool it must not grow, or a plugin only handed device
+ * pointers).  The scratch is a fixed array inside the library sized for at
+ * most 274,625 FEM nodes (65^3, a 64^3 box with walls); larger grids return
+ * RMT3D_ERR_TOO_LARGE.  No cudaMalloc/cudaFree or allocating library call is
+ * made.  The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress), so make that first call outside any stream capture.
+ * Every call shares the array: calls that overlap on the GPU race.
+ *   dvel[3]: du, dv, dw over the ghosted box (sys_size+4 per axis);
+ *   face_normal_vel[6]: for each wall face f, fvel[f][f/2] over the same box
+ *   (may be NULL for periodic faces); dt_basis: the dt the FEM basis was built
+ *   with (dt_reg); stream: cudaStream_t or 0; norm_out: host result. */
+int rmt3d_div_u_noalloc(const int sys_size[3], const int periodic[3], const double bounds[6],
+                        double dt_basis, const double *const dvel[3],
+                        const double *const face_normal_vel[6], void *stream, double *norm_out);
+
 /* Synchronise the scene's stream. */
 int rmt3d_sync(rmt3d_scene *s);
 

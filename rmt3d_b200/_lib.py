@@ -111,6 +111,7 @@ SIGNATURES = {
     "rmt3d_sync": (_I, [_P]),
     "rmt3d_launch_count": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "rmt3d_scene_destroy": (_I, [_P]),
+    "rmt3d_div_u_noalloc": (_I, [_IP, _IP, _DP, _D, ctypes.POINTER(_P), ctypes.POINTER(_P), _P, _DP]),
 }
 
 _lib = None

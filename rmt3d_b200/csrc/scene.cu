@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1214,5 +1215,120 @@ extern "C" int rmt3d_scene_destroy(rmt3d_scene *s) {
     if (s->h_scalar) cudaFreeHost(s->h_scalar);
     if (s->own_stream) cudaStreamDestroy(s->st);
     delete s;
+    return RMT3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the divergence diagnostic.
+//
+// Some hosts cannot allocate device memory at the point where they want this
+// diagnostic: a host that runs inside a memory pool it must not grow, a plugin
+// that is only handed device pointers by its host application, or code that
+// must not synchronise the device through cudaMalloc/cudaFree.  For them the
+// scratch of div_u -- the FEM right-hand side over the node grid, the
+// reduction accumulator and the small argument block the kernels read --
+// lives in the fixed array below instead of in per-scene allocations.
+//
+// The array is sized for at most kNoallocMaxNodes FEM nodes (65^3, the node
+// grid of a 64^3 box with walls) and is held by every GPU that loads this
+// library until the process exits.  All calls share it and it keeps the last
+// call's contents: the accumulator is cleared on every call, and calls that
+// overlap on the GPU (different streams or threads) race on it.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoallocMaxNodes = 65 * 65 * 65;
+constexpr size_t kNoallocHeader = 16384;  // accumulator + argument block, 256-aligned
+constexpr size_t kNoallocBytes = kNoallocHeader + kNoallocMaxNodes * sizeof(double);
+static_assert(sizeof(fields_dev) + 256 <= kNoallocHeader, "argument block does not fit");
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+std::vector<unsigned char *> g_noalloc_addr;  // per device, set up on first use
+
+// Device address of the scratch array for the current device.  The symbol's
+// name in host code is only a host-side stand-in, so the address is looked up
+// once per device with that device current.
+int noalloc_scratch(unsigned char **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(RMT3D_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if ((int)g_noalloc_addr.size() <= dev) g_noalloc_addr.resize(dev + 1, nullptr);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(RMT3D_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        g_noalloc_addr[dev] = (unsigned char *)p;
+    }
+    *out = g_noalloc_addr[dev];
+    return RMT3D_OK;
+}
+}  // namespace
+
+extern "C" int rmt3d_div_u_noalloc(const int sys_size[3], const int periodic[3], const double bounds[6],
+                                   double dt_basis, const double *const dvel[3],
+                                   const double *const face_normal_vel[6], void *stream, double *norm_out) {
+    if (!sys_size || !periodic || !bounds || !dvel || !norm_out) return fail(RMT3D_ERR_INVALID, "null argument");
+    for (int c = 0; c < 3; c++)
+        if (!dvel[c]) return fail(RMT3D_ERR_INVALID, "null dvel pointer");
+    grid_dev g;
+    memset(&g, 0, sizeof(g));
+    g.sm = sys_size[0];
+    g.sn = sys_size[1];
+    g.so = sys_size[2];
+    if (g.sm < 1 || g.sn < 1 || g.so < 1) return fail(RMT3D_ERR_INVALID, "sys_size must be positive");
+    for (int a = 0; a < 3; a++) g.prd[a] = periodic[a] ? 1 : 0;
+    g.fm = g.sm + (g.prd[0] ? 0 : 1);
+    g.fn = g.sn + (g.prd[1] ? 0 : 1);
+    g.fo = g.so + (g.prd[2] ? 0 : 1);
+    const size_t nodes = (size_t)g.fm * g.fn * g.fo;
+    if (nodes > kNoallocMaxNodes)
+        return fail(RMT3D_ERR_TOO_LARGE, "rmt3d_div_u_noalloc: at most 274625 FEM nodes (65^3); got " +
+                                             std::to_string(nodes));
+    for (int f = 0; f < 6; f++)
+        if (!g.prd[f / 2] && (!face_normal_vel || !face_normal_vel[f]))
+            return fail(RMT3D_ERR_INVALID, "a wall face needs its normal face-velocity array");
+    g.sm4 = g.sm + 4;
+    g.sn4 = g.sn + 4;
+    g.so4 = g.so + 4;
+    g.smn4 = g.sm4 * g.sn4;
+    g.ncell = g.smn4 * g.so4;
+    g.dx = (bounds[1] - bounds[0]) / g.sm;
+    g.dy = (bounds[3] - bounds[2]) / g.sn;
+    g.dz = (bounds[5] - bounds[4]) / g.so;
+    // compute_grad_basis (fluid_3d.cc:2506-2517)
+    gradphi_t gp;
+    const double fac = 3 * g.dx / dt_basis;
+    for (int i = 0; i < 8; i++) {
+        gp.v[i][0] = (2 * (i % 2) - 1) * fac;
+        gp.v[i][1] = (2 * ((i / 2) % 2) - 1) * fac;
+        gp.v[i][2] = (2 * (i / 4) - 1) * fac;
+    }
+    // argument block: only the arrays div_u reads
+    static thread_local fields_dev hf;
+    memset(&hf, 0, sizeof(hf));
+    for (int c = 0; c < 3; c++) hf.dvel[c] = const_cast<double *>(dvel[c]);
+    for (int f = 0; f < 6; f++)
+        if (face_normal_vel && face_normal_vel[f]) hf.fvel[3 * f + f / 2] = const_cast<double *>(face_normal_vel[f]);
+    unsigned char *base = nullptr;
+    int e = noalloc_scratch(&base);
+    if (e) return e;
+    cudaStream_t st = (cudaStream_t)stream;
+    double *acc = (double *)base;
+    fields_dev *dF = (fields_dev *)(base + 256);
+    double *rhs = (double *)(base + kNoallocHeader);
+    CK(cudaMemsetAsync(acc, 0, sizeof(double), st));
+    CK(cudaMemcpyAsync(dF, &hf, sizeof(hf), cudaMemcpyHostToDevice, st));
+    k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, st>>>(g, dF, rhs, gp);
+    k_divu<<<grd(g.fm, g.fn, g.fo), blk(), 0, st>>>(g, rhs, acc);
+    double sum = 0;
+    CK(cudaMemcpyAsync(&sum, acc, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    *norm_out = sqrt(sum / ((double)g.fm * g.fn * g.fo));
     return RMT3D_OK;
 }

@@ -175,7 +175,8 @@ def test_nan_input_is_reported(tmp_path):
     try:
         st0 = H.state(fx, 0)
         fa, ra, ei, em = H.to_aos(st0)
-        fa["vel"][len(fa) // 2, 0] = np.nan
+        so4, sn4, sm4 = st0["shape"]
+        fa["vel"][10 + sm4 * (10 + sn4 * 10), 0] = np.nan  # an interior cell
         sc.import_reference(fa, ra, ei, em, H.state(fx, 1)["dt"], 0.0)
         assert sc.step_forward(0) == R.PROJECTION_ERR
     finally:
