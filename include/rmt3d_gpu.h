@@ -205,6 +205,18 @@ int rmt3d_div_u_noalloc(const int sys_size[3], const int periodic[3], const doub
                         double dt_basis, const double *const dvel[3],
                         const double *const face_normal_vel[6], void *stream, double *norm_out);
 
+/* Launch timing of one kernel class for roofline measurement (no counterpart
+ * in the reference, which has no device code): kernel 0 = FEM Gauss-Seidel
+ * colour pass on the finest level, 1 = MAC red-black pass on the finest level,
+ * -1 = off.  CUDA events are recorded on the scene's stream around each
+ * launch of that class, up to max_launches launches. */
+int rmt3d_profile_kernel(rmt3d_scene *s, int kernel, int max_launches);
+
+/* Sum of the timed launches' durations (ms), their count, and their
+ * algorithmic bytes (8 B per point of the level read for x, plus the updated
+ * colour's r read and x write). */
+int rmt3d_profile_read(rmt3d_scene *s, double *ms_total, long long *launches, double *bytes_total);
+
 /* Synchronise the scene's stream. */
 int rmt3d_sync(rmt3d_scene *s);
 

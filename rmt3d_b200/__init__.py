@@ -178,6 +178,17 @@ class Scene:
         _lib.check(lib().rmt3d_diag(self._h, kind, ctypes.byref(v)))
         return v.value
 
+    def profile_kernel(self, kernel, max_launches=100000):
+        """Time launches of one kernel class (0 FEM GS fine level, 1 MAC RB fine level, -1 off)."""
+        _lib.check(lib().rmt3d_profile_kernel(self._h, kernel, max_launches))
+
+    def profile_read(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        b = ctypes.c_double()
+        _lib.check(lib().rmt3d_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(b)))
+        return ms.value, n.value, b.value
+
     def launches(self):
         c = ctypes.c_longlong()
         _lib.check(lib().rmt3d_launch_count(self._h, ctypes.byref(c)))

@@ -111,6 +111,8 @@ SIGNATURES = {
     "rmt3d_sync": (_I, [_P]),
     "rmt3d_launch_count": (_I, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "rmt3d_scene_destroy": (_I, [_P]),
+    "rmt3d_profile_kernel": (_I, [_P, _I, _I]),
+    "rmt3d_profile_read": (_I, [_P, _DP, ctypes.POINTER(ctypes.c_longlong), _DP]),
     "rmt3d_div_u_noalloc": (_I, [_IP, _IP, _DP, _D, ctypes.POINTER(_P), ctypes.POINTER(_P), _P, _DP]),
 }
 

@@ -12,11 +12,16 @@
 //    offset along that axis is zero (set_partials(false)).  Vertex coarsening
 //    (coarse node I on fine node 2I), trilinear prolongation P and restriction
 //    P^T/2, which equals the Galerkin operator P^T A P of this stencil.
-//    Eight-colour Gauss-Seidel (exact GS ordering for a 27-point stencil).
+//    Four-colour Gauss-Seidel (exact GS ordering: the face entries are zero).
+//  * Coarsest level: a dense inverse of A + (alpha/n) 1 1^T, precomputed on the
+//    host; for the singular Neumann/periodic operators (null space = the
+//    constants) it returns the solution orthogonal to the constants.
 // Residual max norms are reduced with warp shuffles and one atomic per warp.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "host_common.h"
 #include "mg.h"
@@ -108,11 +113,15 @@ __global__ void k_mac_rb(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, 
     x[id] = (r[id] - s) / diag;
 }
 
+// The Q1 stencil couples a node only to its edge and corner neighbours (the
+// face entries are zero), so colouring by the parities of i and j alone never
+// puts two coupled nodes in one colour: four colour passes are an exact
+// Gauss-Seidel sweep.
 template <typename T>
 __global__ void k_fem_gs(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int colour) {
     int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + (colour & 1);
     int j = 2 * (blockIdx.y * blockDim.y + threadIdx.y) + ((colour >> 1) & 1);
-    int k = 2 * (blockIdx.z * blockDim.z + threadIdx.z) + ((colour >> 2) & 1);
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i >= L.n0 || j >= L.n1 || k >= L.n2) return;
     T diag;
     T s = fem_offdiag(L, x, i, j, k, diag);
@@ -149,7 +158,8 @@ __global__ void k_resid(lvl_dev L, const T *__restrict__ x, const T *__restrict_
 
 // ---- grid transfer ---------------------------------------------------------
 template <typename T>
-__global__ void k_mac_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, T *__restrict__ rc) {
+__global__ void k_mac_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, T *__restrict__ rc,
+                               T *__restrict__ xc0) {
     int I = blockIdx.x * blockDim.x + threadIdx.x;
     int J = blockIdx.y * blockDim.y + threadIdx.y;
     int K = blockIdx.z * blockDim.z + threadIdx.z;
@@ -159,6 +169,7 @@ __global__ void k_mac_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, 
         for (int b = 0; b < 2; b++)
             for (int a = 0; a < 2; a++) s += res[(2 * I + a) + F.n0 * ((2 * J + b) + F.n1 * (2 * K + c))];
     rc[I + C.n0 * (J + C.n1 * K)] = (T)0.5 * s;
+    xc0[I + C.n0 * (J + C.n1 * K)] = 0;
 }
 
 template <typename T>
@@ -196,7 +207,8 @@ __global__ void k_mac_prolong(lvl_dev F, lvl_dev C, T *__restrict__ x, const T *
 }
 
 template <typename T>
-__global__ void k_fem_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, T *__restrict__ rc) {
+__global__ void k_fem_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, T *__restrict__ rc,
+                               T *__restrict__ xc0) {
     int I = blockIdx.x * blockDim.x + threadIdx.x;
     int J = blockIdx.y * blockDim.y + threadIdx.y;
     int K = blockIdx.z * blockDim.z + threadIdx.z;
@@ -223,6 +235,7 @@ __global__ void k_fem_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, 
         }
     }
     rc[I + C.n0 * (J + C.n1 * K)] = (T)0.5 * s;
+    xc0[I + C.n0 * (J + C.n1 * K)] = 0;
 }
 
 template <typename T>
@@ -256,7 +269,23 @@ __global__ void k_fem_prolong(lvl_dev F, lvl_dev C, T *__restrict__ x, const T *
     x[i + F.n0 * (j + F.n1 * k)] += e;
 }
 
-// coarsest grid: many Gauss-Seidel sweeps inside one thread block
+// coarsest grid: x = B r with the precomputed dense inverse B (row-major)
+template <typename T>
+__global__ void k_coarse_dense(int np, const double *__restrict__ B, T *__restrict__ x, const T *__restrict__ r) {
+    __shared__ double rs[1024];
+    for (int p = threadIdx.x; p < np; p += blockDim.x) rs[p] = (double)r[p];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int row = blockIdx.x * (blockDim.x >> 5) + warp; row < np; row += gridDim.x * (blockDim.x >> 5)) {
+        const double *b = B + (size_t)row * np;
+        double acc = 0;
+        for (int c = lane; c < np; c += 32) acc += b[c] * rs[c];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) x[row] = (T)acc;
+    }
+}
+
+// coarsest grid fallback: many Gauss-Seidel sweeps inside one thread block
 template <typename T, int KIND>
 __global__ void k_coarse_solve(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int sweeps) {
     const int np = L.n0 * L.n1 * L.n2;
@@ -308,6 +337,110 @@ void mg_pred_state::update(int extras) {
     V_var = (1 - alpha) * (V_var + alpha * dV * dV);
 }
 
+// Host copy of the level operator, for the coarsest-grid inverse.
+static void host_stencil_row(mg_kind kind, const mg_level &L, int i, int j, int k, std::vector<double> &row) {
+    const int n[3] = {L.n[0], L.n[1], L.n[2]};
+    const int c[3] = {i, j, k};
+    auto wrap = [&](int v, int d) -> int {
+        if (v < 0) return L.prd[d] ? v + n[d] : -1;
+        if (v >= n[d]) return L.prd[d] ? v - n[d] : -1;
+        return v;
+    };
+    const int me = i + n[0] * (j + n[1] * k);
+    if (kind == MG_MAC) {
+        int missing = 0;
+        for (int d = 0; d < 3; d++)
+            for (int sg = -1; sg <= 1; sg += 2) {
+                int q[3] = {i, j, k};
+                q[d] = wrap(c[d] + sg, d);
+                if (q[d] < 0) {
+                    missing++;
+                    continue;
+                }
+                row[q[0] + n[0] * (q[1] + n[1] * q[2])] += 1;
+            }
+        row[me] += -6 + missing;
+        return;
+    }
+    bool bd[3];
+    for (int d = 0; d < 3; d++) bd[d] = !L.prd[d] && (c[d] == 0 || c[d] == n[d] - 1);
+    for (int oc = -1; oc <= 1; oc++)
+        for (int ob = -1; ob <= 1; ob++)
+            for (int oa = -1; oa <= 1; oa++) {
+                int q[3] = {wrap(i + oa, 0), wrap(j + ob, 1), wrap(k + oc, 2)};
+                if (q[0] < 0 || q[1] < 0 || q[2] < 0) continue;
+                int nz = (oa != 0) + (ob != 0) + (oc != 0);
+                double co = (nz == 0) ? 32 : (nz == 1 ? 0 : (nz == 2 ? -2 : -1));
+                int halve = (bd[0] && oa == 0) + (bd[1] && ob == 0) + (bd[2] && oc == 0);
+                co /= (double)(1 << halve);
+                row[q[0] + n[0] * (q[1] + n[1] * q[2])] += co;
+            }
+}
+
+// Dense inverse of the coarsest operator.  The operators here are singular
+// with the constants as null space (Neumann walls or periodic wrap); adding
+// (alpha/n) 1 1^T with alpha = mean diagonal makes the matrix SPD and its
+// inverse maps every right-hand side to the solution of the projected system
+// that is orthogonal to the constants.
+int mg_solver::build_dense(cudaStream_t st) {
+    const mg_level &L = lv.back();
+    const int np = (int)L.npts();
+    if (np > 1024) return 0;  // Gauss-Seidel fallback
+    std::vector<double> A((size_t)np * np, 0.0), row(np);
+    double dsum = 0, rsum_max = 0;
+    for (int k = 0; k < L.n[2]; k++)
+        for (int j = 0; j < L.n[1]; j++)
+            for (int i = 0; i < L.n[0]; i++) {
+                std::fill(row.begin(), row.end(), 0.0);
+                host_stencil_row(kind, L, i, j, k, row);
+                int me = i + L.n[0] * (j + L.n[1] * k);
+                double rs = 0;
+                for (int c = 0; c < np; c++) {
+                    A[(size_t)me * np + c] = row[c];
+                    rs += row[c];
+                }
+                dsum += row[me];
+                rsum_max = std::max(rsum_max, std::fabs(rs));
+            }
+    if (rsum_max < 1e-12) {
+        double alpha = dsum / np;
+        for (size_t e = 0; e < A.size(); e++) A[e] += alpha / np;
+    }
+    // Gauss-Jordan with partial pivoting
+    std::vector<double> B((size_t)np * np, 0.0);
+    for (int r = 0; r < np; r++) B[(size_t)r * np + r] = 1;
+    for (int col = 0; col < np; col++) {
+        int piv = col;
+        for (int r = col + 1; r < np; r++)
+            if (std::fabs(A[(size_t)r * np + col]) > std::fabs(A[(size_t)piv * np + col])) piv = r;
+        if (piv != col)
+            for (int c = 0; c < np; c++) {
+                std::swap(A[(size_t)piv * np + c], A[(size_t)col * np + c]);
+                std::swap(B[(size_t)piv * np + c], B[(size_t)col * np + c]);
+            }
+        double d = A[(size_t)col * np + col];
+        if (d == 0) return 0;  // keep the Gauss-Seidel fallback
+        double inv = 1 / d;
+        for (int c = 0; c < np; c++) {
+            A[(size_t)col * np + c] *= inv;
+            B[(size_t)col * np + c] *= inv;
+        }
+        for (int r = 0; r < np; r++) {
+            if (r == col) continue;
+            double f = A[(size_t)r * np + col];
+            if (f == 0) continue;
+            for (int c = 0; c < np; c++) {
+                A[(size_t)r * np + c] -= f * A[(size_t)col * np + c];
+                B[(size_t)r * np + c] -= f * B[(size_t)col * np + c];
+            }
+        }
+    }
+    if (cudaMalloc(&dense, B.size() * sizeof(double)) != cudaSuccess) return 1;
+    cudaMemcpyAsync(dense, B.data(), B.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaStreamSynchronize(st);
+    return 0;
+}
+
 mg_solver::~mg_solver() {
     for (auto &l : lv) {
         cudaFree(l.x);
@@ -318,6 +451,7 @@ mg_solver::~mg_solver() {
         cudaFree(l.ress);
     }
     cudaFree(d_max);
+    cudaFree(dense);
     cudaFreeHost(h_max);
 }
 
@@ -374,6 +508,7 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
             cudaMemsetAsync(l.ress, 0, bf, st);
         }
     }
+    if (build_dense(st)) return fail(RMT3D_ERR_OOM, "coarse inverse allocation failed");
     if (cudaMalloc(&d_max, sizeof(double)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
     if (cudaMallocHost(&h_max, sizeof(double)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "pinned allocation failed");
     return 0;
@@ -388,13 +523,25 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
 void mg_solver::smooth(int l, int sweeps, cudaStream_t st) {
     mg_level &L = lv[l];
     lvl_dev d = dev_of(L);
+    // algorithmic bytes of one colour pass: read x of the whole level, read r
+    // and write x of the updated colour
+    const double npts = (double)L.npts();
+    const bool timed = prof && l == 0 && prof->target == (kind == MG_FEM ? 0 : 1);
     for (int s = 0; s < sweeps; s++) {
         if (kind == MG_MAC) {
             dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
-            for (int c = 0; c < 2; c++) LAUNCH(k_mac_rb<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c));
+            for (int c = 0; c < 2; c++) {
+                if (timed) prof->begin(st);
+                LAUNCH(k_mac_rb<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c));
+                if (timed) prof->end(st, npts / 2, 8.0 * (npts + npts / 2 + npts / 2));
+            }
         } else {
-            dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, ((L.n[2] + 1) / 2 + 1) / 2);
-            for (int c = 0; c < 8; c++) LAUNCH(k_fem_gs<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c));
+            dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, (L.n[2] + 1) / 2);
+            for (int c = 0; c < 4; c++) {
+                if (timed) prof->begin(st);
+                LAUNCH(k_fem_gs<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c));
+                if (timed) prof->end(st, npts / 4, 8.0 * (npts + npts / 4 + npts / 4));
+            }
         }
     }
 }
@@ -407,8 +554,8 @@ void mg_solver::smooth_f32(int l, int sweeps, cudaStream_t st) {
             dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 2; c++) LAUNCH(k_mac_rb<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
         } else {
-            dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, ((L.n[2] + 1) / 2 + 1) / 2);
-            for (int c = 0; c < 8; c++) LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+            dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, (L.n[2] + 1) / 2);
+            for (int c = 0; c < 4; c++) LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
         }
     }
 }
@@ -417,7 +564,8 @@ void mg_solver::cycle(int l, cudaStream_t st) {
     mg_level &F = lv[l];
     lvl_dev fd = dev_of(F);
     if (l == (int)lv.size() - 1) {
-        if (kind == MG_MAC) LAUNCH(k_coarse_solve<double, 0><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
+        if (dense) LAUNCH(k_coarse_dense<double><<<16, 256, 0, st>>>((int)F.npts(), dense, F.x, F.r));
+        else if (kind == MG_MAC) LAUNCH(k_coarse_solve<double, 0><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
         else LAUNCH(k_coarse_solve<double, 1><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
         return;
     }
@@ -427,14 +575,10 @@ void mg_solver::cycle(int l, cudaStream_t st) {
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
     if (kind == MG_MAC) {
         LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
-        LAUNCH(k_mac_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r));
+        LAUNCH(k_mac_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r, C.x));
     } else {
         LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
-        LAUNCH(k_fem_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r));
-    }
-    if (l + 1 < (int)lv.size() - 1) {
-        size_t nc = C.npts();
-        LAUNCH(k_zero<double><<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(C.x, nc));
+        LAUNCH(k_fem_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r, C.x));
     }
     cycle(l + 1, st);
     if (kind == MG_MAC) LAUNCH(k_mac_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, F.x, C.x));
@@ -446,7 +590,8 @@ void mg_solver::cycle_f32(int l, cudaStream_t st) {
     mg_level &F = lv[l];
     lvl_dev fd = dev_of(F);
     if (l == (int)lv.size() - 1) {
-        if (kind == MG_MAC) LAUNCH(k_coarse_solve<float, 0><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
+        if (dense) LAUNCH(k_coarse_dense<float><<<16, 256, 0, st>>>((int)F.npts(), dense, F.xs, F.rs));
+        else if (kind == MG_MAC) LAUNCH(k_coarse_solve<float, 0><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
         else LAUNCH(k_coarse_solve<float, 1><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
         return;
     }
@@ -456,14 +601,10 @@ void mg_solver::cycle_f32(int l, cudaStream_t st) {
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
     if (kind == MG_MAC) {
         LAUNCH((k_resid<float, 0><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr)));
-        LAUNCH(k_mac_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs));
+        LAUNCH(k_mac_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs, C.xs));
     } else {
         LAUNCH((k_resid<float, 1><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr)));
-        LAUNCH(k_fem_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs));
-    }
-    if (l + 1 < (int)lv.size() - 1) {
-        size_t nc = C.npts();
-        LAUNCH(k_zero<float><<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(C.xs, nc));
+        LAUNCH(k_fem_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs, C.xs));
     }
     cycle_f32(l + 1, st);
     if (kind == MG_MAC) LAUNCH(k_mac_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, F.xs, C.xs));

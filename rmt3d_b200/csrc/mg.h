@@ -13,6 +13,27 @@ namespace rmt3d {
 
 enum mg_kind { MG_MAC = 0, MG_FEM = 1 };
 
+// Opt-in launch timing of one kernel class: CUDA events recorded on the
+// launching stream around each launch, summed on read.
+struct kernel_profiler {
+    int target = -1;  // 0 fem_gs (fine level), 1 mac_rb (fine level)
+    std::vector<cudaEvent_t> ev;
+    size_t used = 0;
+    double points = 0;  // points updated by the timed launches
+    double bytes = 0;   // algorithmic bytes of the timed launches
+    void begin(cudaStream_t st) {
+        if (used + 2 > ev.size()) return;
+        cudaEventRecord(ev[used], st);
+    }
+    void end(cudaStream_t st, double pts, double byt) {
+        if (used + 2 > ev.size()) return;
+        cudaEventRecord(ev[used + 1], st);
+        used += 2;
+        points += pts;
+        bytes += byt;
+    }
+};
+
 struct mg_level {
     int n[3];
     int prd[3];
@@ -47,6 +68,7 @@ class mg_solver {
     bool mixed = false;  // FP32 cycles inside FP64 iterative refinement
     bool exact = false;  // iterate each solve until the residual stagnates
     long long *launches = nullptr;
+    kernel_profiler *prof = nullptr;
 
     mg_solver() = default;
     mg_solver(const mg_solver &) = delete;
@@ -64,6 +86,8 @@ class mg_solver {
 
   private:
     double *d_max = nullptr;   // device scalar for reductions
+    double *dense = nullptr;   // inverse of the coarsest operator (row-major), or null
+    int build_dense(cudaStream_t st);
     double *h_max = nullptr;   // pinned host mirror
     void cycle(int l, cudaStream_t st);
     void cycle_f32(int l, cudaStream_t st);

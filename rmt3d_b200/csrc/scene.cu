@@ -101,6 +101,7 @@ struct rmt3d_scene {
     double min_wall_acc = 0, wall_acc_mult = 0;
     int nt = 0;
     long long launches = 0;
+    kernel_profiler prof;
     // extrapolation scratch
     uint8_t *lay = nullptr, *inl = nullptr;
     int *front[2] = {nullptr, nullptr};
@@ -871,6 +872,8 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     cudaMemcpyAsync(s->dF, &F, sizeof(F), cudaMemcpyHostToDevice, s->st);
     s->mac.launches = &s->launches;
     s->fem.launches = &s->launches;
+    s->mac.prof = &s->prof;
+    s->fem.prof = &s->prof;
     int nm[3] = {g.sm, g.sn, g.so}, nf[3] = {g.fm, g.fn, g.fo};
     bool mixed = d.precision == RMT3D_MIXED;
     s->mac.exact = s->fem.exact = d.mg_exact != 0;
@@ -1207,9 +1210,41 @@ extern "C" int rmt3d_launch_count(rmt3d_scene *s, long long *count) {
     return RMT3D_OK;
 }
 
+extern "C" int rmt3d_profile_kernel(rmt3d_scene *s, int kernel, int max_launches) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (kernel < -1 || kernel > 1) return fail(RMT3D_ERR_INVALID, "unknown kernel class");
+    CK(cudaStreamSynchronize(s->st));
+    for (cudaEvent_t e : s->prof.ev) cudaEventDestroy(e);
+    s->prof.ev.clear();
+    s->prof.used = 0;
+    s->prof.points = s->prof.bytes = 0;
+    s->prof.target = kernel;
+    if (kernel >= 0) {
+        s->prof.ev.resize(2 * (size_t)max_launches);
+        for (auto &e : s->prof.ev) CK(cudaEventCreate(&e));
+    }
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_profile_read(rmt3d_scene *s, double *ms_total, long long *launches, double *bytes_total) {
+    if (!s || !ms_total || !launches || !bytes_total) return fail(RMT3D_ERR_INVALID, "null argument");
+    CK(cudaStreamSynchronize(s->st));
+    double tot = 0;
+    for (size_t i = 0; i + 1 < s->prof.used; i += 2) {
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, s->prof.ev[i], s->prof.ev[i + 1]));
+        tot += ms;
+    }
+    *ms_total = tot;
+    *launches = (long long)(s->prof.used / 2);
+    *bytes_total = s->prof.bytes;
+    return RMT3D_OK;
+}
+
 extern "C" int rmt3d_scene_destroy(rmt3d_scene *s) {
     if (!s) return RMT3D_OK;
     cudaStreamSynchronize(s->st);
+    for (cudaEvent_t e : s->prof.ev) cudaEventDestroy(e);
     for (void *p : s->allocs) cudaFree(p);
     if (s->h_counters) cudaFreeHost(s->h_counters);
     if (s->h_scalar) cudaFreeHost(s->h_scalar);

@@ -1,0 +1,21 @@
+import sys, os, tempfile
+sys.path.insert(0, os.path.abspath('.'))
+import rmt3d_b200 as R
+from rmt3d_b200 import scenes
+n = int(sys.argv[1]) if len(sys.argv) > 1 else 64
+steps = int(sys.argv[2]) if len(sys.argv) > 2 else 2
+prec = int(sys.argv[3]) if len(sys.argv) > 3 else 0
+wd = tempfile.mkdtemp()
+cfg = scenes.write(os.path.join(wd, 'w.cfg'), scenes.cavity_sphere(n, 100000, radius=0.2))
+d = R.desc_from_cfg(cfg); d.precision = prec
+sc = R.Scene(d)
+sc.prepare()
+sc.step_forward(0)
+sc.sync()
+print('PREP_LAUNCHES=%d' % sc.launches())
+l0 = sc.launches()
+for _ in range(steps):
+    sc.step_forward(0)
+sc.sync()
+print('STEP_LAUNCHES=%d' % (sc.launches() - l0))
+print('MG', sc.scalar(5), sc.scalar(6))
