@@ -1,5 +1,12 @@
+"""Profiling driver: set up the bench workload, step once, then run N steps.
+
+    python -m rmt3d_b200.prof_step [n=64] [steps=2] [precision=0]
+
+Prints PREP_LAUNCHES (kernel launches before the profiled steps, for ncu -s)
+and STEP_LAUNCHES (launches of the profiled steps, for ncu -c).
+"""
 import sys, os, tempfile
-sys.path.insert(0, os.path.abspath('.'))
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 import rmt3d_b200 as R
 from rmt3d_b200 import scenes
 n = int(sys.argv[1]) if len(sys.argv) > 1 else 64
