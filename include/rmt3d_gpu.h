@@ -14,6 +14,8 @@
 #ifndef RMT3D_GPU_H
 #define RMT3D_GPU_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -216,6 +218,64 @@ int rmt3d_profile_kernel(rmt3d_scene *s, int kernel, int max_launches);
  * algorithmic bytes (8 B per point of the level read for x, plus the updated
  * colour's r read and x write). */
 int rmt3d_profile_read(rmt3d_scene *s, double *ms_total, long long *launches, double *bytes_total);
+
+/* ---- batched form ------------------------------------------------------
+ * Many independent scenes (uneven grid sizes allowed) stepped together: each
+ * scene keeps its own state and stream, and a pool of host threads issues
+ * their steps so the kernels of many scenes overlap on the device.  No
+ * counterpart in the reference, which runs one scene per process. */
+typedef struct rmt3d_batch rmt3d_batch;
+int rmt3d_batch_create(const rmt3d_scene_desc *descs, int nscenes, int host_threads, rmt3d_batch **out);
+/* run_sim's set-up (rmt3d_prepare) of every scene */
+int rmt3d_batch_prepare(rmt3d_batch *b);
+/* every scene advances nsteps steps; status[i] receives scene i's step code */
+int rmt3d_batch_step(rmt3d_batch *b, int nsteps, int *status);
+int rmt3d_batch_size(rmt3d_batch *b, int *n);
+int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out);
+/* choose (v_down, v_up) per distinct grid size by timing candidates on a
+ * probe scene (the reference's mg_opt searches the same pair,
+ * Utilities/mg_probs.hh:80-208); tuned_out gets (cells, v_down, v_up) */
+int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out);
+int rmt3d_batch_destroy(rmt3d_batch *b);
+
+/* Multigrid smoothing counts of one scene (V(v_down, v_up) cycles). */
+int rmt3d_scene_set_smoothing(rmt3d_scene *s, int v_down, int v_up);
+
+/* Device bytes a scene with this descriptor allocates (admission control). */
+size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d);
+
+/* Sums of u^2, v^2, w^2, p^2 over the interior cells: a compact fingerprint of
+ * a scene's state. */
+int rmt3d_scene_checksum(rmt3d_scene *s, double out[4]);
+
+/* ---- serving loop ------------------------------------------------------ */
+typedef struct {
+    double arrival_s;      /* arrival time after the start of rmt3d_serve */
+    int steps;             /* steps to run after the set-up */
+    rmt3d_scene_desc desc;
+} rmt3d_request;
+
+typedef struct {
+    double admit_s, finish_s, latency_s; /* latency = finish - arrival */
+    double step_p50_ms, step_p99_ms;
+    double checksum[4];                  /* rmt3d_scene_checksum of the final state */
+    int steps_done;
+    int status;
+} rmt3d_request_result;
+
+typedef struct {
+    double wall_s;
+    double request_p50_s, request_p99_s;
+    double step_p50_ms, step_p99_ms;
+    double cellsteps_per_s;
+    int requests;
+} rmt3d_serve_summary;
+
+/* Run a request stream: admission when a slot (max_slots concurrent scenes)
+ * is free and the request's footprint fits hbm_budget bytes; admitted scenes
+ * run concurrently, each on its own stream; results[i] for request i. */
+int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budget, int max_slots,
+                rmt3d_request_result *results, rmt3d_serve_summary *summary);
 
 /* Synchronise the scene's stream. */
 int rmt3d_sync(rmt3d_scene *s);

@@ -189,6 +189,21 @@ class Scene:
         _lib.check(lib().rmt3d_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(b)))
         return ms.value, n.value, b.value
 
+    def set_smoothing(self, v_down, v_up):
+        """Multigrid V(v_down, v_up) smoothing counts of both solvers."""
+        _lib.check(lib().rmt3d_scene_set_smoothing(self._h, v_down, v_up))
+
+    def checksum(self):
+        """Sums of u^2, v^2, w^2, p^2 over the interior cells."""
+        out = (ctypes.c_double * 4)()
+        _lib.check(lib().rmt3d_scene_checksum(self._h, out))
+        return tuple(out)
+
+    @property
+    def device_bytes(self):
+        """Device bytes the scene holds."""
+        return int(self.scalar(12))
+
     def launches(self):
         c = ctypes.c_longlong()
         _lib.check(lib().rmt3d_launch_count(self._h, ctypes.byref(c)))
@@ -246,3 +261,91 @@ def run_sim(cfg_path, **overrides):
     scene.init_iter(init_err)
     sim.run(scene)
     return scene
+
+
+def footprint(desc):
+    """Device bytes a scene with this descriptor allocates (admission control)."""
+    return int(lib().rmt3d_scene_footprint(ctypes.byref(desc)))
+
+
+class Batch:
+    """Independent scenes stepped together, each on its own stream; a pool of
+    host threads issues their steps so the kernels of many scenes overlap."""
+
+    def __init__(self, descs, host_threads=0):
+        L = lib()
+        arr = (SceneDesc * len(descs))(*descs)
+        h = ctypes.c_void_p()
+        _lib.check(L.rmt3d_batch_create(arr, len(descs), host_threads, ctypes.byref(h)))
+        self._h = h
+        self.n = len(descs)
+
+    def prepare(self):
+        _lib.check(lib().rmt3d_batch_prepare(self._h))
+
+    def step(self, nsteps=1):
+        st = (ctypes.c_int * self.n)()
+        _lib.check(lib().rmt3d_batch_step(self._h, nsteps, st))
+        return list(st)
+
+    def scene_handle(self, i):
+        h = ctypes.c_void_p()
+        _lib.check(lib().rmt3d_batch_scene(self._h, i, ctypes.byref(h)))
+        return h
+
+    def checksum(self, i):
+        out = (ctypes.c_double * 4)()
+        _lib.check(lib().rmt3d_scene_checksum(self.scene_handle(i), out))
+        return tuple(out)
+
+    def field(self, i, name):
+        h = self.scene_handle(i)
+        dims = (ctypes.c_int * 6)()
+        _lib.check(lib().rmt3d_get_dims(h, dims))
+        n = dims[0] * dims[1] * dims[2]
+        out = np.empty(n, dtype=np.float64)
+        idx = FIELD_INDEX[name] if isinstance(name, str) else int(name)
+        _lib.check(lib().rmt3d_get_field(h, idx, out.ctypes.data_as(ctypes.c_void_p)))
+        return out.reshape(dims[2], dims[1], dims[0])
+
+    def autotune(self, probe_steps=3):
+        """Per grid size: {cells: (v_down, v_up)} chosen by timing candidates."""
+        buf = (ctypes.c_int * (3 * self.n))()
+        n = ctypes.c_int()
+        _lib.check(lib().rmt3d_batch_autotune(self._h, probe_steps, buf, self.n, ctypes.byref(n)))
+        return {buf[3 * i]: (buf[3 * i + 1], buf[3 * i + 2]) for i in range(min(n.value, self.n))}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().rmt3d_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve(requests, hbm_budget, max_slots):
+    """Run a request stream [(arrival_s, steps, desc), ...] through the serving
+    loop; returns (per-request result dicts, summary dict)."""
+    L = lib()
+    n = len(requests)
+    reqs = (_lib.Request * n)()
+    for i, (arr, steps, desc) in enumerate(requests):
+        reqs[i].arrival_s = arr
+        reqs[i].steps = steps
+        reqs[i].desc = desc
+    res = (_lib.RequestResult * n)()
+    summ = _lib.ServeSummary()
+    _lib.check(L.rmt3d_serve(reqs, n, hbm_budget, max_slots, res, ctypes.byref(summ)))
+
+    def as_dict(st):
+        out = {}
+        for name, _t in st._fields_:
+            v = getattr(st, name)
+            out[name] = tuple(v) if hasattr(v, "__len__") else v
+        return out
+
+    return [as_dict(r) for r in res], as_dict(summ)

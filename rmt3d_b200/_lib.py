@@ -81,6 +81,26 @@ class SceneDesc(ctypes.Structure):
     ]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("arrival_s", ctypes.c_double), ("steps", ctypes.c_int), ("desc", SceneDesc)]
+
+
+class RequestResult(ctypes.Structure):
+    _fields_ = [
+        ("admit_s", ctypes.c_double), ("finish_s", ctypes.c_double), ("latency_s", ctypes.c_double),
+        ("step_p50_ms", ctypes.c_double), ("step_p99_ms", ctypes.c_double),
+        ("checksum", ctypes.c_double * 4), ("steps_done", ctypes.c_int), ("status", ctypes.c_int),
+    ]
+
+
+class ServeSummary(ctypes.Structure):
+    _fields_ = [
+        ("wall_s", ctypes.c_double), ("request_p50_s", ctypes.c_double), ("request_p99_s", ctypes.c_double),
+        ("step_p50_ms", ctypes.c_double), ("step_p99_ms", ctypes.c_double),
+        ("cellsteps_per_s", ctypes.c_double), ("requests", ctypes.c_int),
+    ]
+
+
 # entry points declared in include/rmt3d_gpu.h: name -> (restype, argtypes)
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -113,6 +133,18 @@ SIGNATURES = {
     "rmt3d_scene_destroy": (_I, [_P]),
     "rmt3d_profile_kernel": (_I, [_P, _I, _I]),
     "rmt3d_profile_read": (_I, [_P, _DP, ctypes.POINTER(ctypes.c_longlong), _DP]),
+    "rmt3d_batch_create": (_I, [ctypes.POINTER(SceneDesc), _I, _I, ctypes.POINTER(_P)]),
+    "rmt3d_batch_prepare": (_I, [_P]),
+    "rmt3d_batch_step": (_I, [_P, _I, _IP]),
+    "rmt3d_batch_size": (_I, [_P, _IP]),
+    "rmt3d_batch_scene": (_I, [_P, _I, ctypes.POINTER(_P)]),
+    "rmt3d_batch_autotune": (_I, [_P, _I, _IP, _I, _IP]),
+    "rmt3d_batch_destroy": (_I, [_P]),
+    "rmt3d_scene_set_smoothing": (_I, [_P, _I, _I]),
+    "rmt3d_scene_footprint": (ctypes.c_size_t, [ctypes.POINTER(SceneDesc)]),
+    "rmt3d_scene_checksum": (_I, [_P, _DP]),
+    "rmt3d_serve": (_I, [ctypes.POINTER(Request), _I, ctypes.c_size_t, _I,
+                         ctypes.POINTER(RequestResult), ctypes.POINTER(ServeSummary)]),
     "rmt3d_div_u_noalloc": (_I, [_IP, _IP, _DP, _D, ctypes.POINTER(_P), ctypes.POINTER(_P), _P, _DP]),
 }
 

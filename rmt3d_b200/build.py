@@ -22,7 +22,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "--fmad=false",
                    "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
                    "-I" + INCLUDE, "-I" + CSRC]
-CU_SOURCES = ["k_fluid.cu", "k_mg.cu", "k_solid.cu", "scene.cu", "batch.cu"]
+CU_SOURCES = ["k_fluid.cu", "k_mg.cu", "k_mgp.cu", "k_solid.cu", "scene.cu", "batch.cu"]
+# per-file extra flags: the persistent multigrid kernel exchanges data between
+# CTAs inside one launch, so its global loads bypass the (non-coherent) L1
+PER_FILE = {"k_mgp.cu": ["-Xptxas", "-dlcm=cg"]}
 CC_SOURCES = ["cfg.cc"]
 
 
@@ -52,7 +55,7 @@ def build(verbose=False):
             continue
         obj = os.path.join(BUILD, src + ".o")
         if _stale(obj, [path] + headers):
-            _run([NVCC] + CU_FLAGS + ["-c", path, "-o", obj])
+            _run([NVCC] + CU_FLAGS + PER_FILE.get(src, []) + ["-c", path, "-o", obj])
             if verbose:
                 print("built", obj)
         objs.append(obj)

@@ -1,0 +1,321 @@
+// Batched form: many independent scenes stepped together.
+//
+// Every scene keeps its own device state and its own CUDA stream; a pool of
+// host threads issues the scenes' steps so that the small kernels of many
+// scenes overlap on the device (uneven grid sizes need no padding: each scene
+// launches its own grids).  Scenes are assigned to threads by a greedy
+// balance of cells.  An autotuner picks the multigrid smoothing counts per
+// grid size by timing candidate (v_down, v_up) pairs on a probe scene.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "host_common.h"
+#include "rmt3d_gpu.h"
+
+// knobs shared with scene.cu (defined there)
+extern "C" int rmt3d_scene_set_smoothing(rmt3d_scene *s, int v_down, int v_up);
+
+struct rmt3d_batch {
+    std::vector<rmt3d_scene *> scenes;
+    std::vector<rmt3d_scene_desc> descs;
+    std::vector<std::vector<int>> groups;  // scene indices per host thread
+    std::vector<int> status;
+    std::map<int, std::pair<int, int>> tuned;  // grid cells -> (v_down, v_up)
+    int nthreads = 1;
+};
+
+namespace {
+
+long long cells(const rmt3d_scene_desc &d) { return (long long)d.sys_size[0] * d.sys_size[1] * d.sys_size[2]; }
+
+// run fn(scene index) for every scene, each host thread over its group
+template <typename F>
+int for_all(rmt3d_batch *b, F fn) {
+    std::vector<int> err(b->groups.size(), 0);
+    std::vector<std::string> msg(b->groups.size());
+    std::vector<std::thread> th;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    for (size_t t = 0; t < b->groups.size(); t++) {
+        th.emplace_back([&, t]() {
+            cudaSetDevice(dev);
+            for (int i : b->groups[t]) {
+                int e = fn(i);
+                if (e && !err[t]) {
+                    err[t] = e;
+                    msg[t] = rmt3d_last_error();
+                }
+            }
+        });
+    }
+    for (auto &x : th) x.join();
+    for (size_t t = 0; t < err.size(); t++)
+        if (err[t]) return rmt3d::fail(err[t], msg[t]);
+    return RMT3D_OK;
+}
+
+}  // namespace
+
+extern "C" int rmt3d_batch_create(const rmt3d_scene_desc *descs, int nscenes, int host_threads,
+                                  rmt3d_batch **out) {
+    if (!descs || !out || nscenes < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "bad batch arguments");
+    *out = nullptr;
+    rmt3d_batch *b = new rmt3d_batch();
+    b->descs.assign(descs, descs + nscenes);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    for (int i = 0; i < nscenes; i++) {
+        rmt3d_scene *s = nullptr;
+        int e = rmt3d_scene_create(&descs[i], nullptr, &s);
+        if (e) {
+            for (auto *x : b->scenes) rmt3d_scene_destroy(x);
+            delete b;
+            return e;
+        }
+        b->scenes.push_back(s);
+    }
+    b->status.assign(nscenes, 0);
+    int nt = host_threads > 0 ? host_threads : (int)std::thread::hardware_concurrency();
+    nt = std::max(1, std::min(nt, nscenes));
+    b->nthreads = nt;
+    b->groups.assign(nt, {});
+    // greedy balance by cells, largest first
+    std::vector<int> order(nscenes);
+    for (int i = 0; i < nscenes; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int c) { return cells(descs[a]) > cells(descs[c]); });
+    std::vector<long long> load(nt, 0);
+    for (int i : order) {
+        int t = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        b->groups[t].push_back(i);
+        load[t] += cells(descs[i]);
+    }
+    *out = b;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_batch_prepare(rmt3d_batch *b) {
+    if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
+    return for_all(b, [&](int i) { return rmt3d_prepare(b->scenes[i]); });
+}
+
+extern "C" int rmt3d_batch_step(rmt3d_batch *b, int nsteps, int *status) {
+    if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
+    int e = for_all(b, [&](int i) {
+        int st = 0;
+        int r = rmt3d_run(b->scenes[i], nsteps, &st);
+        b->status[i] = st;
+        return r;
+    });
+    if (status)
+        for (size_t i = 0; i < b->status.size(); i++) status[i] = b->status[i];
+    return e;
+}
+
+extern "C" int rmt3d_batch_size(rmt3d_batch *b, int *n) {
+    if (!b || !n) return rmt3d::fail(RMT3D_ERR_INVALID, "null argument");
+    *n = (int)b->scenes.size();
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
+    if (!b || !out || i < 0 || i >= (int)b->scenes.size()) return rmt3d::fail(RMT3D_ERR_INVALID, "bad scene index");
+    *out = b->scenes[i];
+    return RMT3D_OK;
+}
+
+// Autotune the multigrid smoothing counts per grid size: for each distinct
+// size in the batch, a probe copy of the first scene of that size is set up
+// and stepped `probe_steps` times per candidate; the fastest candidate is
+// applied to every scene of that size.  tuned_out (optional, 3 ints per
+// distinct size: cells, v_down, v_up) receives the choices.
+extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out) {
+    if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
+    static const int cand[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
+    std::map<long long, int> first;
+    for (size_t i = 0; i < b->descs.size(); i++)
+        if (!first.count(cells(b->descs[i]))) first[cells(b->descs[i])] = (int)i;
+    int written = 0;
+    for (auto &kv : first) {
+        rmt3d_scene *probe = nullptr;
+        int e = rmt3d_scene_create(&b->descs[kv.second], nullptr, &probe);
+        if (e) return e;
+        if ((e = rmt3d_prepare(probe))) {
+            rmt3d_scene_destroy(probe);
+            return e;
+        }
+        double best = 1e300;
+        int bd = 2, bu = 2;
+        for (auto &c : cand) {
+            rmt3d_scene_set_smoothing(probe, c[0], c[1]);
+            int st = 0;
+            rmt3d_run(probe, 1, &st);  // settle the cycle predictor
+            rmt3d_sync(probe);
+            auto t0 = std::chrono::steady_clock::now();
+            rmt3d_run(probe, probe_steps, &st);
+            rmt3d_sync(probe);
+            double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (st == 0 && dt < best) {
+                best = dt;
+                bd = c[0];
+                bu = c[1];
+            }
+        }
+        rmt3d_scene_destroy(probe);
+        b->tuned[(int)kv.first] = {bd, bu};
+        for (size_t i = 0; i < b->descs.size(); i++)
+            if (cells(b->descs[i]) == kv.first) rmt3d_scene_set_smoothing(b->scenes[i], bd, bu);
+        if (tuned_out && written < max_out) {
+            tuned_out[3 * written] = (int)kv.first;
+            tuned_out[3 * written + 1] = bd;
+            tuned_out[3 * written + 2] = bu;
+        }
+        written++;
+    }
+    if (n_out) *n_out = written;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_batch_destroy(rmt3d_batch *b) {
+    if (!b) return RMT3D_OK;
+    for (auto *s : b->scenes) rmt3d_scene_destroy(s);
+    delete b;
+    return RMT3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Serving loop: requests arrive over time; each is admitted when a slot (a
+// host worker with its own stream) is free and its device footprint fits the
+// remaining HBM budget.  Admitted requests run concurrently on the device
+// (continuous batching: a request that arrives while others run starts as
+// soon as a slot and memory free up, without waiting for a batch boundary).
+// Per-step and per-request latencies are recorded.
+// ---------------------------------------------------------------------------
+extern "C" int rmt3d_scene_checksum(rmt3d_scene *s, double out[4]);
+extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d);
+
+namespace {
+double pct(std::vector<double> v, double q) {
+    if (v.empty()) return 0;
+    std::sort(v.begin(), v.end());
+    double pos = q * (v.size() - 1);
+    size_t lo = (size_t)pos, hi = std::min(lo + 1, v.size() - 1);
+    return v[lo] + (pos - lo) * (v[hi] - v[lo]);
+}
+}  // namespace
+
+extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budget, int max_slots,
+                           rmt3d_request_result *results, rmt3d_serve_summary *summary) {
+    if (!reqs || nreq < 1 || !results || max_slots < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "bad serve arguments");
+    for (int i = 0; i < nreq; i++)
+        if (rmt3d_scene_footprint(&reqs[i].desc) > hbm_budget)
+            return rmt3d::fail(RMT3D_ERR_TOO_LARGE, "request " + std::to_string(i) + " exceeds the HBM budget");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::mutex mu;
+    std::vector<char> taken(nreq, 0);
+    size_t used = 0;
+    int done = 0;
+    std::atomic<int> first_err{0};
+    std::string err_msg;
+    std::vector<std::vector<double>> step_ms(nreq);
+    const auto t0 = std::chrono::steady_clock::now();
+    auto now_s = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    std::vector<long long> cellsteps(max_slots, 0);
+    auto worker = [&](int slot) {
+        cudaSetDevice(dev);
+        while (true) {
+            int pick = -1;
+            size_t fp = 0;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (done >= nreq || first_err) return;
+                double t = now_s();
+                // earliest arrived request that fits the free budget
+                for (int i = 0; i < nreq; i++) {
+                    if (taken[i] || reqs[i].arrival_s > t) continue;
+                    size_t f = rmt3d_scene_footprint(&reqs[i].desc);
+                    if (used + f <= hbm_budget) {
+                        pick = i;
+                        fp = f;
+                        break;
+                    }
+                }
+                if (pick >= 0) {
+                    taken[pick] = 1;
+                    used += fp;
+                } else {
+                    bool any_left = false;
+                    for (int i = 0; i < nreq; i++)
+                        if (!taken[i]) any_left = true;
+                    if (!any_left) return;
+                }
+            }
+            if (pick < 0) {
+                std::this_thread::sleep_for(std::chrono::microseconds(200));
+                continue;
+            }
+            rmt3d_request_result &R = results[pick];
+            memset(&R, 0, sizeof(R));
+            R.admit_s = now_s();
+            rmt3d_scene *s = nullptr;
+            int e = rmt3d_scene_create(&reqs[pick].desc, nullptr, &s);
+            if (!e) e = rmt3d_prepare(s);
+            int st = 0;
+            for (int k = 0; !e && k < reqs[pick].steps && st == 0; k++) {
+                auto a = std::chrono::steady_clock::now();
+                e = rmt3d_step(s, 0, &st);
+                if (!e) e = rmt3d_sync(s);
+                step_ms[pick].push_back(
+                    1e3 * std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count());
+            }
+            if (!e) e = rmt3d_scene_checksum(s, R.checksum);
+            R.finish_s = now_s();
+            R.latency_s = R.finish_s - reqs[pick].arrival_s;
+            R.status = e ? e : st;
+            R.steps_done = (int)step_ms[pick].size();
+            R.step_p50_ms = pct(step_ms[pick], 0.5);
+            R.step_p99_ms = pct(step_ms[pick], 0.99);
+            cellsteps[slot] += (long long)R.steps_done * reqs[pick].desc.sys_size[0] * reqs[pick].desc.sys_size[1] *
+                               reqs[pick].desc.sys_size[2];
+            if (e && !first_err.exchange(e)) {
+                std::lock_guard<std::mutex> lk(mu);
+                err_msg = rmt3d_last_error();
+            }
+            rmt3d_scene_destroy(s);
+            std::lock_guard<std::mutex> lk(mu);
+            used -= fp;
+            done++;
+        }
+    };
+    std::vector<std::thread> th;
+    for (int k = 0; k < max_slots; k++) th.emplace_back(worker, k);
+    for (auto &x : th) x.join();
+    const double wall = now_s();
+    if (summary) {
+        std::vector<double> lat, steps;
+        long long cs = 0;
+        for (int i = 0; i < nreq; i++) {
+            lat.push_back(results[i].latency_s);
+            steps.insert(steps.end(), step_ms[i].begin(), step_ms[i].end());
+        }
+        for (long long c : cellsteps) cs += c;
+        summary->wall_s = wall;
+        summary->request_p50_s = pct(lat, 0.5);
+        summary->request_p99_s = pct(lat, 0.99);
+        summary->step_p50_ms = pct(steps, 0.5);
+        summary->step_p99_ms = pct(steps, 0.99);
+        summary->cellsteps_per_s = cs / wall;
+        summary->requests = nreq;
+    }
+    if (first_err) return rmt3d::fail(first_err, err_msg);
+    return RMT3D_OK;
+}

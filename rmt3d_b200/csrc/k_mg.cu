@@ -19,84 +19,17 @@
 // Residual max norms are reduced with warp shuffles and one atomic per warp.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <vector>
 
 #include "host_common.h"
 #include "mg.h"
+#include "mg_ops.cuh"
 #include "rmt3d_gpu.h"
 
 namespace rmt3d {
-
-struct lvl_dev {
-    int n0, n1, n2;
-    int p0, p1, p2;
-};
-
-__device__ __forceinline__ int wrapi(int v, int n, int prd) {
-    if (v < 0) return prd ? v + n : -1;
-    if (v >= n) return prd ? v - n : -1;
-    return v;
-}
-
-// ---- operator application -------------------------------------------------
-template <typename T>
-__device__ __forceinline__ T mac_offdiag(const lvl_dev L, const T *__restrict__ x, int i, int j, int k, T &diag) {
-    T s = 0;
-    int missing = 0;
-    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
-    const int c[3] = {i, j, k};
-    const int st[3] = {1, L.n0, L.n0 * L.n1};
-    const int base = i + L.n0 * (j + L.n1 * k);
-    for (int d = 0; d < 3; d++) {
-        for (int sgn = -1; sgn <= 1; sgn += 2) {
-            int v = wrapi(c[d] + sgn, n[d], p[d]);
-            if (v < 0) {
-                missing++;
-                continue;
-            }
-            s += x[base + (v - c[d]) * st[d]];
-        }
-    }
-    diag = (T)(-6 + missing);
-    return s;
-}
-
-template <typename T>
-__device__ __forceinline__ T fem_offdiag(const lvl_dev L, const T *__restrict__ x, int i, int j, int k, T &diag) {
-    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
-    const int c[3] = {i, j, k};
-    bool bd[3];
-    for (int d = 0; d < 3; d++) bd[d] = !p[d] && (c[d] == 0 || c[d] == n[d] - 1);
-    int nb[3][3];
-    for (int d = 0; d < 3; d++)
-        for (int o = -1; o <= 1; o++) nb[d][o + 1] = wrapi(c[d] + o, n[d], p[d]);
-    T s = 0;
-    for (int oc = 0; oc < 3; oc++) {
-        int kk = nb[2][oc];
-        if (kk < 0) continue;
-        for (int ob = 0; ob < 3; ob++) {
-            int jj = nb[1][ob];
-            if (jj < 0) continue;
-            const T *row = x + (size_t)L.n0 * (jj + (size_t)L.n1 * kk);
-            for (int oa = 0; oa < 3; oa++) {
-                int ii = nb[0][oa];
-                if (ii < 0) continue;
-                int nz = (oa != 1) + (ob != 1) + (oc != 1);
-                if (nz == 0 || nz == 1) continue;  // centre handled below, faces are 0
-                T co = (nz == 2) ? (T)-2 : (T)-1;
-                int halve = (bd[0] && oa == 1) + (bd[1] && ob == 1) + (bd[2] && oc == 1);
-                if (halve == 1) co *= (T)0.5;
-                else if (halve == 2) co *= (T)0.25;
-                s += co * row[ii];
-            }
-        }
-    }
-    int hc = bd[0] + bd[1] + bd[2];
-    diag = (T)32 / (T)(1 << hc);
-    return s;
-}
 
 // ---- smoothing -------------------------------------------------------------
 template <typename T>
@@ -306,6 +239,10 @@ __global__ void k_coarse_solve(lvl_dev L, T *__restrict__ x, const T *__restrict
         }
 }
 
+// the coarse-level part of a V-cycle (levels cf..nlev-1) in one CTA
+template <typename T>
+__global__ void __launch_bounds__(512) k_mg_coarse(pmg_args A, int cf) { coarse_cycle<T>(A, cf); }
+
 // FP64 <-> FP32 helpers of the mixed form
 __global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, size_t n) {
     size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -385,7 +322,7 @@ static void host_stencil_row(mg_kind kind, const mg_level &L, int i, int j, int 
 int mg_solver::build_dense(cudaStream_t st) {
     const mg_level &L = lv.back();
     const int np = (int)L.npts();
-    if (np > 1024) return 0;  // Gauss-Seidel fallback
+    if (np > 1024) return 0;  // Gauss-Seidel fallback (mg_solver::footprint uses the same bound)
     std::vector<double> A((size_t)np * np, 0.0), row(np);
     double dsum = 0, rsum_max = 0;
     for (int k = 0; k < L.n[2]; k++)
@@ -452,15 +389,12 @@ mg_solver::~mg_solver() {
     }
     cudaFree(d_max);
     cudaFree(dense);
+    cudaFree(pstate);
     cudaFreeHost(h_max);
 }
 
-int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_form, cudaStream_t st) {
-    kind = k;
-    mixed = mixed_form;
-    const double eps = 2.220446049250313e-16;
-    // tolerances of simp_fem / simp_mac (mg_probs.hh:483-485, :516-518)
-    max_norm_tol = (k == MG_FEM) ? 32 * eps * 1e2 : 6 * eps * 1e2;
+int mg_solver::plan(mg_kind k, const int n[3], const int prd[3], std::vector<mg_level> &lv) {
+    lv.clear();
     mg_level L0;
     for (int d = 0; d < 3; d++) {
         L0.n[d] = n[d];
@@ -469,7 +403,7 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
     lv.push_back(L0);
     while (true) {
         const mg_level &f = lv.back();
-        if (f.npts() <= 512) break;
+        if (f.npts() <= 128) break;
         mg_level c;
         bool ok = true;
         for (int d = 0; d < 3; d++) {
@@ -490,11 +424,33 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
         lv.push_back(c);
     }
     if (lv.back().npts() > 4096) return fail(RMT3D_ERR_UNSUPPORTED, "grid does not coarsen to a small enough level");
+    if ((int)lv.size() > kMaxLev) return fail(RMT3D_ERR_UNSUPPORTED, "too many multigrid levels");
+    return 0;
+}
+
+size_t mg_solver::footprint(mg_kind k, const int n[3], const int prd[3], bool mixed_form) {
+    std::vector<mg_level> v;
+    if (plan(k, n, prd, v)) return 0;
+    size_t b = 0;
+    for (auto &l : v) b += l.npts() * (3 * sizeof(double) + (mixed_form ? 3 * sizeof(float) : 0));
+    if (v.back().npts() <= 1024) b += v.back().npts() * v.back().npts() * sizeof(double);  // coarsest inverse
+    return b + sizeof(double);
+}
+
+int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_form, cudaStream_t st) {
+    kind = k;
+    mixed = mixed_form;
+    const double eps = 2.220446049250313e-16;
+    // tolerances of simp_fem / simp_mac (mg_probs.hh:483-485, :516-518)
+    max_norm_tol = (k == MG_FEM) ? 32 * eps * 1e2 : 6 * eps * 1e2;
+    int pe = plan(k, n, prd, lv);
+    if (pe) return pe;
     for (auto &l : lv) {
         size_t b = l.npts() * sizeof(double);
         if (cudaMalloc(&l.x, b) != cudaSuccess || cudaMalloc(&l.r, b) != cudaSuccess ||
             cudaMalloc(&l.res, b) != cudaSuccess)
             return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
+        bytes_alloc += 3 * b;
         cudaMemsetAsync(l.x, 0, b, st);
         cudaMemsetAsync(l.r, 0, b, st);
         cudaMemsetAsync(l.res, 0, b, st);
@@ -503,13 +459,30 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
             if (cudaMalloc(&l.xs, bf) != cudaSuccess || cudaMalloc(&l.rs, bf) != cudaSuccess ||
                 cudaMalloc(&l.ress, bf) != cudaSuccess)
                 return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
+            bytes_alloc += 3 * bf;
             cudaMemsetAsync(l.xs, 0, bf, st);
             cudaMemsetAsync(l.rs, 0, bf, st);
             cudaMemsetAsync(l.ress, 0, bf, st);
         }
     }
     if (build_dense(st)) return fail(RMT3D_ERR_OOM, "coarse inverse allocation failed");
+    if (dense) bytes_alloc += lv.back().npts() * lv.back().npts() * sizeof(double);
+    cf = (int)lv.size() - 1;
+    for (int l = 0; l < (int)lv.size(); l++)
+        if (lv[l].npts() <= (size_t)kCoarsePts) {
+            cf = l;
+            break;
+        }
+    {
+        const char *e = getenv("RMT3D_MG_PERSISTENT");
+        persistent = (e && e[0] == '1');
+    }
+    if (persistent) {
+        int pe = setup_persistent(st);
+        if (pe) return pe;
+    }
     if (cudaMalloc(&d_max, sizeof(double)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
+    bytes_alloc += sizeof(double);
     if (cudaMallocHost(&h_max, sizeof(double)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "pinned allocation failed");
     return 0;
 }
@@ -560,9 +533,38 @@ void mg_solver::smooth_f32(int l, int sweeps, cudaStream_t st) {
     }
 }
 
+// level table of the coarse sub-cycle kernel
+static pmg_args coarse_args(const mg_solver &m) {
+    pmg_args A;
+    memset(&A, 0, sizeof(A));
+    A.kind = (m.kind == MG_MAC) ? 0 : 1;
+    A.nlev = (int)m.lv.size();
+    for (int l = 0; l < A.nlev && l < kMaxLev; l++) {
+        pmg_level &P = A.lv[l];
+        for (int d = 0; d < 3; d++) {
+            P.n[d] = m.lv[l].n[d];
+            P.prd[d] = m.lv[l].prd[d];
+        }
+        P.x = m.lv[l].x;
+        P.r = m.lv[l].r;
+        P.res = m.lv[l].res;
+        P.xs = m.lv[l].xs;
+        P.rs = m.lv[l].rs;
+        P.ress = m.lv[l].ress;
+    }
+    A.dense = m.dense;
+    A.v_up = m.v_up;
+    A.v_down = m.v_down;
+    return A;
+}
+
 void mg_solver::cycle(int l, cudaStream_t st) {
     mg_level &F = lv[l];
     lvl_dev fd = dev_of(F);
+    if (l == cf && l < (int)lv.size() - 1) {
+        LAUNCH(k_mg_coarse<double><<<1, 512, 0, st>>>(coarse_args(*this), l));
+        return;
+    }
     if (l == (int)lv.size() - 1) {
         if (dense) LAUNCH(k_coarse_dense<double><<<16, 256, 0, st>>>((int)F.npts(), dense, F.x, F.r));
         else if (kind == MG_MAC) LAUNCH(k_coarse_solve<double, 0><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
@@ -589,6 +591,10 @@ void mg_solver::cycle(int l, cudaStream_t st) {
 void mg_solver::cycle_f32(int l, cudaStream_t st) {
     mg_level &F = lv[l];
     lvl_dev fd = dev_of(F);
+    if (l == cf && l < (int)lv.size() - 1) {
+        LAUNCH(k_mg_coarse<float><<<1, 512, 0, st>>>(coarse_args(*this), l));
+        return;
+    }
     if (l == (int)lv.size() - 1) {
         if (dense) LAUNCH(k_coarse_dense<float><<<16, 256, 0, st>>>((int)F.npts(), dense, F.xs, F.rs));
         else if (kind == MG_MAC) LAUNCH(k_coarse_solve<float, 0><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
@@ -650,6 +656,7 @@ double mg_solver::residual_max(cudaStream_t st) {
 }
 
 double mg_solver::run(cudaStream_t st) {
+    if (persistent) return run_persistent(st);
     const int hard_cap = 20;
     last_cycles = 0;
     for (int i = 0; i < pred.iters(); i++) vcycle(st);

@@ -76,17 +76,30 @@ class mg_solver {
     ~mg_solver();
     // n: fine points per axis; prd: periodic flags
     int setup(mg_kind k, const int n[3], const int prd[3], bool mixed_form, cudaStream_t st);
+    // the level hierarchy setup() builds; 0 or an error code
+    static int plan(mg_kind k, const int n[3], const int prd[3], std::vector<mg_level> &out);
+    // device bytes setup() allocates for this hierarchy (0 if it cannot coarsen)
+    static size_t footprint(mg_kind k, const int n[3], const int prd[3], bool mixed_form);
+    size_t bytes_alloc = 0;  // device bytes held
     double *rhs() { return lv[0].r; }
     double *sol() { return lv[0].x; }
     // one solve with the reference's control logic; returns the final max-norm
     // residual (NaN propagates)
     double run(cudaStream_t st);
+    // one cooperative launch per solve with the control loop on the device
+    bool persistent = false;
+    double *dense = nullptr;  // inverse of the coarsest operator (row-major), or null
+    int cf = 0;  // first level whose whole sub-cycle runs in one CTA
+    bool hard_error = false;  // the persistent launch failed or its barrier timed out
+    int setup_persistent(cudaStream_t st);
+    double run_persistent(cudaStream_t st);
     double residual_max(cudaStream_t st);
     void vcycle(cudaStream_t st);
 
   private:
     double *d_max = nullptr;   // device scalar for reductions
-    double *dense = nullptr;   // inverse of the coarsest operator (row-major), or null
+    void *pstate = nullptr;    // persistent solver: predictor state, barrier, partial maxima
+    int pgrid = 0;
     int build_dense(cudaStream_t st);
     double *h_max = nullptr;   // pinned host mirror
     void cycle(int l, cudaStream_t st);

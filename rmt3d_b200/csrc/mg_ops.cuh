@@ -1,0 +1,330 @@
+// Multigrid operator helpers shared by the per-launch V-cycle (k_mg.cu) and
+// the persistent solver (k_mgp.cu): rediscretised MAC 7-point and FEM Q1
+// 27-point stencils with the boundary rules of stencil_set::set_partials
+// (Utilities/mg_probs.hh:281-343).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace rmt3d {
+
+struct lvl_dev {
+    int n0, n1, n2;
+    int p0, p1, p2;
+};
+
+__host__ __device__ __forceinline__ int wrapi(int v, int n, int prd) {
+    if (v < 0) return prd ? v + n : -1;
+    if (v >= n) return prd ? v - n : -1;
+    return v;
+}
+
+// ---- operator application -------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T mac_offdiag(const lvl_dev L, const T *__restrict__ x, int i, int j, int k, T &diag) {
+    if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
+        const int sy = L.n0, sz = L.n0 * L.n1;
+        const T *c = x + i + sy * j + sz * k;
+        diag = (T)-6;
+        return ((c[-1] + c[1]) + (c[-sy] + c[sy])) + (c[-sz] + c[sz]);
+    }
+    T s = 0;
+    int missing = 0;
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int c[3] = {i, j, k};
+    const int st[3] = {1, L.n0, L.n0 * L.n1};
+    const int base = i + L.n0 * (j + L.n1 * k);
+    for (int d = 0; d < 3; d++) {
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+            int v = wrapi(c[d] + sgn, n[d], p[d]);
+            if (v < 0) {
+                missing++;
+                continue;
+            }
+            s += x[base + (v - c[d]) * st[d]];
+        }
+    }
+    diag = (T)(-6 + missing);
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T fem_offdiag(const lvl_dev L, const T *__restrict__ x, int i, int j, int k, T &diag) {
+    if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
+        // interior node: edges -2, corners -1, faces 0
+        const int sy = L.n0, sz = L.n0 * L.n1;
+        const T *c = x + i + sy * j + sz * k;
+        const T *zm = c - sz, *zp = c + sz;
+        T e = (c[-1 - sy] + c[1 - sy]) + (c[-1 + sy] + c[1 + sy]);
+        e += (zm[-1] + zm[1]) + (zm[-sy] + zm[sy]);
+        e += (zp[-1] + zp[1]) + (zp[-sy] + zp[sy]);
+        T q = (zm[-1 - sy] + zm[1 - sy]) + (zm[-1 + sy] + zm[1 + sy]);
+        q += (zp[-1 - sy] + zp[1 - sy]) + (zp[-1 + sy] + zp[1 + sy]);
+        diag = (T)32;
+        return (T)-2 * e - q;
+    }
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int c[3] = {i, j, k};
+    bool bd[3];
+    for (int d = 0; d < 3; d++) bd[d] = !p[d] && (c[d] == 0 || c[d] == n[d] - 1);
+    int nb[3][3];
+    for (int d = 0; d < 3; d++)
+        for (int o = -1; o <= 1; o++) nb[d][o + 1] = wrapi(c[d] + o, n[d], p[d]);
+    T s = 0;
+    for (int oc = 0; oc < 3; oc++) {
+        int kk = nb[2][oc];
+        if (kk < 0) continue;
+        for (int ob = 0; ob < 3; ob++) {
+            int jj = nb[1][ob];
+            if (jj < 0) continue;
+            const T *row = x + (size_t)L.n0 * (jj + (size_t)L.n1 * kk);
+            for (int oa = 0; oa < 3; oa++) {
+                int ii = nb[0][oa];
+                if (ii < 0) continue;
+                int nz = (oa != 1) + (ob != 1) + (oc != 1);
+                if (nz == 0 || nz == 1) continue;  // centre handled below, faces are 0
+                T co = (nz == 2) ? (T)-2 : (T)-1;
+                int halve = (bd[0] && oa == 1) + (bd[1] && ob == 1) + (bd[2] && oc == 1);
+                if (halve == 1) co *= (T)0.5;
+                else if (halve == 2) co *= (T)0.25;
+                s += co * row[ii];
+            }
+        }
+    }
+    int hc = bd[0] + bd[1] + bd[2];
+    diag = (T)32 / (T)(1 << hc);
+    return s;
+}
+
+
+constexpr int kCoarsePts = 1000;
+constexpr int kMaxLev = 12;
+constexpr int kThreads = 256;
+
+struct pmg_level {
+    int n[3];
+    int prd[3];
+    double *x, *r, *res;
+    float *xs, *rs, *ress;
+};
+
+struct pmg_args {
+    int kind;  // 0 MAC, 1 FEM
+    int nlev;
+    int cf;    // first level handled by CTA 0 alone
+    pmg_level lv[kMaxLev];
+    const double *dense;  // inverse of the coarsest operator, or null
+    double tol;
+    int v_up, v_down;
+    int exact, mixed;
+    int *pred_iV;
+    double *pred_avg, *pred_var;
+    unsigned *bar;      // [0] arrival count, [1] generation
+    double *partial;    // per-CTA residual maxima
+    double *out;        // [0] final residual, [1] V-cycles run, [2] extra rounds
+    int *err;           // barrier timeout
+};
+
+__device__ __forceinline__ lvl_dev ldev(const pmg_level &L) {
+    return lvl_dev{L.n[0], L.n[1], L.n[2], L.prd[0], L.prd[1], L.prd[2]};
+}
+
+// ---- one phase over a level, for the points [t0, total) with stride ts ----
+template <typename T>
+__device__ void ph_smooth_colour(int kind, const lvl_dev L, T *x, const T *r, int colour, int t0, int ts) {
+    if (kind == 0) {
+        const int h = (L.n0 + 1) / 2;
+        const int tot = h * L.n1 * L.n2;
+        for (int t = t0; t < tot; t += ts) {
+            int hi = t % h, j = (t / h) % L.n1, k = t / (h * L.n1);
+            int i = 2 * hi + ((j + k + colour) & 1);
+            if (i >= L.n0) continue;
+            T diag;
+            T s = mac_offdiag(L, x, i, j, k, diag);
+            int id = i + L.n0 * (j + L.n1 * k);
+            x[id] = (r[id] - s) / diag;
+        }
+    } else {
+        const int ha = (L.n0 + 1) / 2, hb = (L.n1 + 1) / 2;
+        const int tot = ha * hb * L.n2;
+        for (int t = t0; t < tot; t += ts) {
+            int a = t % ha, b = (t / ha) % hb, k = t / (ha * hb);
+            int i = 2 * a + (colour & 1), j = 2 * b + ((colour >> 1) & 1);
+            if (i >= L.n0 || j >= L.n1) continue;
+            T diag;
+            T s = fem_offdiag(L, x, i, j, k, diag);
+            int id = i + L.n0 * (j + L.n1 * k);
+            x[id] = (r[id] - s) / diag;
+        }
+    }
+}
+
+template <typename T>
+__device__ double ph_resid(int kind, const lvl_dev L, const T *x, const T *r, T *res, int t0, int ts) {
+    const int tot = L.n0 * L.n1 * L.n2;
+    double mx = 0;
+    for (int t = t0; t < tot; t += ts) {
+        int i = t % L.n0, j = (t / L.n0) % L.n1, k = t / (L.n0 * L.n1);
+        T diag;
+        T s = (kind == 0) ? mac_offdiag(L, x, i, j, k, diag) : fem_offdiag(L, x, i, j, k, diag);
+        T v = r[t] - s - diag * x[t];
+        if (res) res[t] = v;
+        double a = fabs((double)v);
+        if (a != a || a > mx) mx = a;  // NaN sticks
+    }
+    return mx;
+}
+
+template <typename T>
+__device__ void ph_restrict(int kind, const lvl_dev F, const lvl_dev C, const T *res, T *rc, T *xc, int t0, int ts) {
+    const int tot = C.n0 * C.n1 * C.n2;
+    for (int t = t0; t < tot; t += ts) {
+        int I = t % C.n0, J = (t / C.n0) % C.n1, K = t / (C.n0 * C.n1);
+        T s = 0;
+        if (kind == 0) {
+            for (int c = 0; c < 2; c++)
+                for (int b = 0; b < 2; b++)
+                    for (int a = 0; a < 2; a++) s += res[(2 * I + a) + F.n0 * ((2 * J + b) + F.n1 * (2 * K + c))];
+        } else {
+            const int nf[3] = {F.n0, F.n1, F.n2}, p[3] = {F.p0, F.p1, F.p2};
+            const int cc[3] = {I, J, K};
+            int idx[3][3];
+            T w[3][3];
+            for (int d = 0; d < 3; d++)
+                for (int o = -1; o <= 1; o++) {
+                    int v = wrapi(2 * cc[d] + o, nf[d], p[d]);
+                    idx[d][o + 1] = v;
+                    w[d][o + 1] = (v < 0) ? (T)0 : (o == 0 ? (T)1 : (T)0.5);
+                }
+            for (int oc = 0; oc < 3; oc++) {
+                if (idx[2][oc] < 0) continue;
+                for (int ob = 0; ob < 3; ob++) {
+                    if (idx[1][ob] < 0) continue;
+                    for (int oa = 0; oa < 3; oa++) {
+                        if (idx[0][oa] < 0) continue;
+                        s += w[0][oa] * w[1][ob] * w[2][oc] *
+                             res[idx[0][oa] + F.n0 * (idx[1][ob] + F.n1 * idx[2][oc])];
+                    }
+                }
+            }
+        }
+        rc[t] = (T)0.5 * s;
+        xc[t] = 0;
+    }
+}
+
+template <typename T>
+__device__ void ph_prolong(int kind, const lvl_dev F, const lvl_dev C, T *x, const T *xc, int t0, int ts) {
+    const int tot = F.n0 * F.n1 * F.n2;
+    const int nc[3] = {C.n0, C.n1, C.n2}, p[3] = {C.p0, C.p1, C.p2};
+    for (int t = t0; t < tot; t += ts) {
+        int i = t % F.n0, j = (t / F.n0) % F.n1, k = t / (F.n0 * F.n1);
+        const int f[3] = {i, j, k};
+        int ci[3][2];
+        T w[3][2];
+        int cnt[3];
+        for (int d = 0; d < 3; d++) {
+            if (kind == 0) {
+                int I = f[d] >> 1;
+                int J = wrapi(I + ((f[d] & 1) ? 1 : -1), nc[d], p[d]);
+                ci[d][0] = I;
+                if (J < 0) {
+                    w[d][0] = 1;
+                    cnt[d] = 1;
+                } else {
+                    w[d][0] = (T)0.75;
+                    ci[d][1] = J;
+                    w[d][1] = (T)0.25;
+                    cnt[d] = 2;
+                }
+            } else if ((f[d] & 1) == 0) {
+                ci[d][0] = f[d] >> 1;
+                w[d][0] = 1;
+                cnt[d] = 1;
+            } else {
+                ci[d][0] = f[d] >> 1;
+                ci[d][1] = wrapi((f[d] >> 1) + 1, nc[d], p[d]);
+                w[d][0] = w[d][1] = (T)0.5;
+                cnt[d] = 2;
+            }
+        }
+        T e = 0;
+        for (int c = 0; c < cnt[2]; c++)
+            for (int b = 0; b < cnt[1]; b++)
+                for (int a = 0; a < cnt[0]; a++)
+                    e += w[0][a] * w[1][b] * w[2][c] * xc[ci[0][a] + C.n0 * (ci[1][b] + C.n1 * ci[2][c])];
+        x[t] += e;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T *LX(const pmg_level &L) {
+    if constexpr (sizeof(T) == 8) return (T *)L.x;
+    else return (T *)L.xs;
+}
+template <typename T>
+__device__ __forceinline__ T *LR(const pmg_level &L) {
+    if constexpr (sizeof(T) == 8) return (T *)L.r;
+    else return (T *)L.rs;
+}
+template <typename T>
+__device__ __forceinline__ T *LS(const pmg_level &L) {
+    if constexpr (sizeof(T) == 8) return (T *)L.res;
+    else return (T *)L.ress;
+}
+
+// coarse levels cf..nlev-1 of one V-cycle inside the calling CTA
+template <typename T>
+__device__ void coarse_cycle(const pmg_args &A, int cf) {
+    const int t0 = threadIdx.x, ts = blockDim.x;
+    const int nc = A.kind == 0 ? 2 : 4;
+    for (int l = cf; l < A.nlev - 1; l++) {
+        const pmg_level &F = A.lv[l];
+        for (int s = 0; s < A.v_down; s++)
+            for (int c = 0; c < nc; c++) {
+                ph_smooth_colour<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), c, t0, ts);
+                __syncthreads();
+            }
+        ph_resid<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), LS<T>(F), t0, ts);
+        __syncthreads();
+        const pmg_level &C = A.lv[l + 1];
+        ph_restrict<T>(A.kind, ldev(F), ldev(C), LS<T>(F), LR<T>(C), LX<T>(C), t0, ts);
+        __syncthreads();
+    }
+    {  // coarsest level
+        const pmg_level &L = A.lv[A.nlev - 1];
+        const int np = L.n[0] * L.n[1] * L.n[2];
+        T *x = LX<T>(L);
+        const T *r = LR<T>(L);
+        if (A.dense) {
+            for (int row = t0; row < np; row += ts) {
+                const double *b = A.dense + (size_t)row * np;
+                double acc = 0;
+                for (int c = 0; c < np; c++) acc += b[c] * (double)r[c];
+                x[row] = (T)acc;
+            }
+            __syncthreads();
+        } else {
+            for (int p = t0; p < np; p += ts) x[p] = 0;
+            __syncthreads();
+            for (int s = 0; s < 80; s++)
+                for (int c = 0; c < nc; c++) {
+                    ph_smooth_colour<T>(A.kind, ldev(L), x, r, c, t0, ts);
+                    __syncthreads();
+                }
+        }
+    }
+    for (int l = A.nlev - 2; l >= cf; l--) {
+        const pmg_level &F = A.lv[l];
+        const pmg_level &C = A.lv[l + 1];
+        ph_prolong<T>(A.kind, ldev(F), ldev(C), LX<T>(F), LX<T>(C), t0, ts);
+        __syncthreads();
+        for (int s = 0; s < A.v_up; s++)
+            for (int c = 0; c < nc; c++) {
+                ph_smooth_colour<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), c, t0, ts);
+                __syncthreads();
+            }
+    }
+}
+
+}  // namespace rmt3d

@@ -108,19 +108,30 @@ struct rmt3d_scene {
     int *counters = nullptr;  // [0..1] frontier sizes, [2] extrapolation errors, [3] corrector problems,
                               // [4] redraw fatal, [5] refmap-derivative errors
     int *h_counters = nullptr;
-    double *d_mean = nullptr;
+    double *d_mean = nullptr;  // [0] mean, [1..] per-block partial sums
+    unsigned *mean_ticket = nullptr;
     double *h_scalar = nullptr;
     double *d_red = nullptr;
+    size_t dev_bytes = 0;  // bytes held through alloc()
 
     template <typename T>
     int alloc(T **p, size_t n) {
         if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "device allocation failed");
         allocs.push_back(*p);
+        dev_bytes += n * sizeof(T);
         cudaMemsetAsync(*p, 0, n * sizeof(T), st);
         return 0;
     }
     void count(int n = 1) { launches += n; }
 };
+
+// A blocking copy ordered on the scene's (non-blocking) stream: plain
+// cudaMemcpy runs on the legacy stream, which does not wait for it.
+static cudaError_t copy_sync(rmt3d_scene *s, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, s->st);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s->st);
+}
 
 // ---------------------------------------------------------------------------
 // ghost-frame helpers
@@ -420,12 +431,12 @@ static int init_refmap(rmt3d_scene *s) {
     for (int o = 0; o < g.n_obj; o++) {
         objmap_dev &m = s->hF.om[o];
         for (size_t id = 0; id < n; id++) code[id] = (owner[id] == o) ? 0 : -1;
-        CK(cudaMemcpy(m.code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+        CK(copy_sync(s, m.code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice));
         for (int c = 0; c < 3; c++) {
-            CK(cudaMemcpy(m.x[c], X[c].data(), n * 8, cudaMemcpyHostToDevice));
-            CK(cudaMemcpy(m.xp[c], X[c].data(), n * 8, cudaMemcpyHostToDevice));
+            CK(copy_sync(s, m.x[c], X[c].data(), n * 8, cudaMemcpyHostToDevice));
+            CK(copy_sync(s, m.xp[c], X[c].data(), n * 8, cudaMemcpyHostToDevice));
         }
-        for (int c = 0; c < 9; c++) CK(cudaMemcpy(m.gp[c], init_gp.data(), n * 8, cudaMemcpyHostToDevice));
+        for (int c = 0; c < 9; c++) CK(copy_sync(s, m.gp[c], init_gp.data(), n * 8, cudaMemcpyHostToDevice));
         for (int c = 0; c < 18; c++) CK(cudaMemsetAsync(m.fx[c], 0, n * 8, s->st));
     }
     comm_primary(s);
@@ -497,6 +508,7 @@ static int mac_solve(rmt3d_scene *s, double cdt) {
     k_mac_rhs<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.rhs(), cdt);
     s->count();
     double res = s->mac.run(s->st);
+    if (s->mac.hard_error) return RMT3D_ERR_CUDA;
     if (std::isnan(res)) return fail(RMT3D_ERR_NAN, "fluid_3d::mac_solve(): NaN detected in multigrid solve");
     k_mac_extract<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.sol());
     s->count();
@@ -506,18 +518,38 @@ static int mac_solve(rmt3d_scene *s, double cdt) {
     return 0;
 }
 
-__global__ void k_mean(const double *x, size_t n, double scale, double *out) {
+// Mean of x in a fixed summation order: each block writes its partial sum,
+// and the last block to finish adds the partials in block order, so the
+// result does not depend on scheduling (scenes give the same answer alone
+// and when they share the device with others).
+constexpr int kMeanBlocks = 148;
+
+__global__ void k_mean(const double *x, size_t n, double scale, double *out, unsigned *ticket) {
     double sum = 0;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         sum += x[i] * scale;
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     __shared__ double sh[32];
+    __shared__ bool last;
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = sum;
     __syncthreads();
     if (threadIdx.x < 32) {
         double v = (threadIdx.x < blockDim.x / 32) ? sh[threadIdx.x] : 0;
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) atomicAdd(out, v);
+        if (threadIdx.x == 0) {
+            out[1 + blockIdx.x] = v;
+            __threadfence();
+            last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const volatile double *part = out + 1;
+        double t = 0;
+        for (unsigned b = 0; b < gridDim.x; b++) t += part[b];
+        out[0] = t;
+        *ticket = 0;
     }
 }
 
@@ -528,10 +560,10 @@ static int pp_solve(rmt3d_scene *s) {
     k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
     s->count();
     double res = s->fem.run(s->st);
+    if (s->fem.hard_error) return -1;
     if (std::isnan(res)) return 1;
     size_t nn = (size_t)g.fm * g.fn * g.fo;
-    cudaMemsetAsync(s->d_mean, 0, sizeof(double), s->st);
-    k_mean<<<148, 256, 0, s->st>>>(s->fem.sol(), nn, 1 / (double)nn, s->d_mean);
+    k_mean<<<kMeanBlocks, 256, 0, s->st>>>(s->fem.sol(), nn, 1 / (double)nn, s->d_mean, s->mean_ticket);
     k_fem_extract<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.sol(), s->d_mean);
     s->count(2);
     comm_pressure(s);
@@ -605,7 +637,11 @@ static int step_forward(rmt3d_scene *s, int debug, int stop = 99) {
     comm_dvel(s);
     s->time += 0.5 * s->dt;
     if (stop <= 7) return RMT3D_OK;
-    if (pp_solve(s)) return RMT3D_PROJECTION_ERR;
+    {
+        int pe = pp_solve(s);
+        if (pe < 0) return RMT3D_ERR_CUDA;
+        if (pe) return RMT3D_PROJECTION_ERR;
+    }
     if (stop <= 8) return RMT3D_OK;
     if (g.n_obj > 0) {
         k_refmap_full<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
@@ -669,6 +705,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
         if (d.sys_size[a] < 4 || d.sys_size[a] > 1024) return fail(RMT3D_ERR_INVALID, "sys_size outside 4..1024");
     if (d.n_obj < 0 || d.n_obj > RMT3D_MAX_OBJ) return fail(RMT3D_ERR_TOO_LARGE, "n_obj outside 0..16");
     if (d.implicit_visc) return fail(RMT3D_ERR_UNSUPPORTED, "implicit viscosity is outside this path");
+    if (d.var_den) return fail(RMT3D_ERR_UNSUPPORTED, "variable-density multigrid operators are not built yet");
     if (!d.godunov) return fail(RMT3D_ERR_UNSUPPORTED, "only the Godunov scheme is on this path");
     if (d.sim_type == RMT3D_SIM_STEST) return fail(RMT3D_ERR_UNSUPPORTED, "stest (shear cube object) is outside this path");
     for (int o = 0; o < d.n_obj; o++)
@@ -859,7 +896,8 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     if (d.n_obj > 0) {
         e |= s->alloc(&s->lay, n) | s->alloc(&s->inl, n) | s->alloc(&s->front[0], n) | s->alloc(&s->front[1], n);
     }
-    e |= s->alloc(&s->counters, 8) | s->alloc(&s->d_mean, 1) | s->alloc(&s->d_red, 1);
+    e |= s->alloc(&s->counters, 8) | s->alloc(&s->d_mean, 1 + kMeanBlocks) | s->alloc(&s->d_red, 4) |
+         s->alloc(&s->mean_ticket, 1);
     if (e) {
         rmt3d_scene_destroy(s);
         return RMT3D_ERR_OOM;
@@ -1001,7 +1039,7 @@ extern "C" int rmt3d_get_scalar(rmt3d_scene *s, int which, double *v) {
             long long cnt = 0;
             std::vector<int> code(s->g.ncell);
             for (int o = 0; o < s->g.n_obj; o++) {
-                CK(cudaMemcpy(code.data(), s->hF.om[o].code, s->g.ncell * sizeof(int), cudaMemcpyDeviceToHost));
+                CK(copy_sync(s, code.data(), s->hF.om[o].code, s->g.ncell * sizeof(int), cudaMemcpyDeviceToHost));
                 for (int c : code) cnt += (c > 0);
             }
             *v = (double)cnt;
@@ -1009,6 +1047,7 @@ extern "C" int rmt3d_get_scalar(rmt3d_scene *s, int which, double *v) {
         }
         case 10: *v = s->K_stiff; break;
         case 11: *v = s->vmax; break;
+        case 12: *v = (double)(s->dev_bytes + s->mac.bytes_alloc + s->fem.bytes_alloc); break;
         default: return fail(RMT3D_ERR_INVALID, "unknown scalar");
     }
     return RMT3D_OK;
@@ -1042,7 +1081,7 @@ extern "C" int rmt3d_get_field(rmt3d_scene *s, int which, double *dst) {
     double *p = field_ptr(s, which);
     if (!p) return fail(RMT3D_ERR_INVALID, "unknown field");
     CK(cudaStreamSynchronize(s->st));
-    CK(cudaMemcpy(dst, p, s->g.ncell * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(copy_sync(s, dst, p, s->g.ncell * sizeof(double), cudaMemcpyDeviceToHost));
     return RMT3D_OK;
 }
 
@@ -1052,10 +1091,10 @@ extern "C" int rmt3d_get_refmap(rmt3d_scene *s, int obj, int *code, double *x, d
     const size_t n = s->g.ncell;
     objmap_dev &m = s->hF.om[obj];
     CK(cudaStreamSynchronize(s->st));
-    if (code) CK(cudaMemcpy(code, m.code, n * sizeof(int), cudaMemcpyDeviceToHost));
+    if (code) CK(copy_sync(s, code, m.code, n * sizeof(int), cudaMemcpyDeviceToHost));
     for (int c = 0; c < 3; c++) {
-        if (x) CK(cudaMemcpy(x + c * n, m.x[c], n * 8, cudaMemcpyDeviceToHost));
-        if (xpred) CK(cudaMemcpy(xpred + c * n, m.xp[c], n * 8, cudaMemcpyDeviceToHost));
+        if (x) CK(copy_sync(s, x + c * n, m.x[c], n * 8, cudaMemcpyDeviceToHost));
+        if (xpred) CK(copy_sync(s, xpred + c * n, m.xp[c], n * 8, cudaMemcpyDeviceToHost));
     }
     return RMT3D_OK;
 }
@@ -1078,7 +1117,7 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
     std::vector<double> buf(n);
     auto put = [&](double *dst, const double *src, int stride, int off) -> int {
         for (size_t i = 0; i < n; i++) buf[i] = src[i * stride + off];
-        CK(cudaMemcpy(dst, buf.data(), n * 8, cudaMemcpyHostToDevice));
+        CK(copy_sync(s, dst, buf.data(), n * 8, cudaMemcpyHostToDevice));
         return 0;
     };
     int e = 0;
@@ -1118,14 +1157,14 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
                 if ((int)(cc & 1023) == o + 1) take(ext_index[q], rec, (cc >> 10) & 63);
             }
             objmap_dev &m = s->hF.om[o];
-            CK(cudaMemcpy(m.code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+            CK(copy_sync(s, m.code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice));
             for (int c = 0; c < 3; c++) {
-                CK(cudaMemcpy(m.x[c], X.data() + c * n, n * 8, cudaMemcpyHostToDevice));
-                CK(cudaMemcpy(m.xp[c], XP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
-                CK(cudaMemcpy(m.det[c], DT.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+                CK(copy_sync(s, m.x[c], X.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+                CK(copy_sync(s, m.xp[c], XP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+                CK(copy_sync(s, m.det[c], DT.data() + c * n, n * 8, cudaMemcpyHostToDevice));
             }
-            for (int c = 0; c < 18; c++) CK(cudaMemcpy(m.fx[c], FX.data() + c * n, n * 8, cudaMemcpyHostToDevice));
-            for (int c = 0; c < 9; c++) CK(cudaMemcpy(m.gp[c], GP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+            for (int c = 0; c < 18; c++) CK(copy_sync(s, m.fx[c], FX.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+            for (int c = 0; c < 9; c++) CK(copy_sync(s, m.gp[c], GP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
         }
     }
     s->dt = dt;
@@ -1143,7 +1182,7 @@ extern "C" int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *ref
         double *fa = (double *)field_aos;
         memset(fa, 0, n * 360);
         auto get = [&](const double *src, int off) -> int {
-            CK(cudaMemcpy(buf.data(), src, n * 8, cudaMemcpyDeviceToHost));
+            CK(copy_sync(s, buf.data(), src, n * 8, cudaMemcpyDeviceToHost));
             for (size_t i = 0; i < n; i++) fa[i * F_N + off] = buf[i];
             return 0;
         };
@@ -1160,13 +1199,13 @@ extern "C" int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *ref
     std::vector<double> X(3 * n), XP(3 * n), FX(18 * n), GP(9 * n);
     for (int o = 0; o < s->g.n_obj; o++) {
         objmap_dev &m = s->hF.om[o];
-        CK(cudaMemcpy(code.data(), m.code, n * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(copy_sync(s, code.data(), m.code, n * sizeof(int), cudaMemcpyDeviceToHost));
         for (int c = 0; c < 3; c++) {
-            CK(cudaMemcpy(X.data() + c * n, m.x[c], n * 8, cudaMemcpyDeviceToHost));
-            CK(cudaMemcpy(XP.data() + c * n, m.xp[c], n * 8, cudaMemcpyDeviceToHost));
+            CK(copy_sync(s, X.data() + c * n, m.x[c], n * 8, cudaMemcpyDeviceToHost));
+            CK(copy_sync(s, XP.data() + c * n, m.xp[c], n * 8, cudaMemcpyDeviceToHost));
         }
-        for (int c = 0; c < 18; c++) CK(cudaMemcpy(FX.data() + c * n, m.fx[c], n * 8, cudaMemcpyDeviceToHost));
-        for (int c = 0; c < 9; c++) CK(cudaMemcpy(GP.data() + c * n, m.gp[c], n * 8, cudaMemcpyDeviceToHost));
+        for (int c = 0; c < 18; c++) CK(copy_sync(s, FX.data() + c * n, m.fx[c], n * 8, cudaMemcpyDeviceToHost));
+        for (int c = 0; c < 9; c++) CK(copy_sync(s, GP.data() + c * n, m.gp[c], n * 8, cudaMemcpyDeviceToHost));
         auto fill = [&](unsigned char *rec, size_t cell, int cd) {
             *(unsigned int *)rec = (unsigned)(o + 1) | ((unsigned)cd << 10);
             double *r = (double *)rec;
@@ -1207,6 +1246,64 @@ extern "C" int rmt3d_sync(rmt3d_scene *s) {
 extern "C" int rmt3d_launch_count(rmt3d_scene *s, long long *count) {
     if (!s || !count) return fail(RMT3D_ERR_INVALID, "null argument");
     *count = s->launches;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_scene_set_smoothing(rmt3d_scene *s, int v_down, int v_up) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (v_down < 0 || v_up < 0 || v_down + v_up < 1 || v_down > 8 || v_up > 8)
+        return fail(RMT3D_ERR_INVALID, "smoothing counts outside 0..8 (sum >= 1)");
+    s->mac.v_down = s->fem.v_down = v_down;
+    s->mac.v_up = s->fem.v_up = v_up;
+    return RMT3D_OK;
+}
+
+extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
+    // mirrors the allocations of rmt3d_scene_create and mg_solver::setup
+    if (!d || d->sys_size[0] < 1 || d->sys_size[1] < 1 || d->sys_size[2] < 1) return 0;
+    const size_t n = (size_t)(d->sys_size[0] + 4) * (d->sys_size[1] + 4) * (d->sys_size[2] + 4);
+    size_t b = n * sizeof(double) * (36 + (d->var_den ? 1 : 0));
+    b += (size_t)d->n_obj * n * (2 * sizeof(int) + 48 * sizeof(double));
+    if (d->n_obj > 0) b += n * (2 * sizeof(uint8_t) + 2 * sizeof(int));
+    b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);
+    b += sizeof(fields_dev) + 8 * sizeof(int) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);
+    int prd[3], nm[3], nf[3];
+    for (int a = 0; a < 3; a++) {
+        prd[a] = d->periodic[a] != 0;
+        nm[a] = d->sys_size[a];
+        nf[a] = d->sys_size[a] + (prd[a] ? 0 : 1);
+    }
+    const bool mixed = d->precision == RMT3D_MIXED;
+    const size_t mac = mg_solver::footprint(MG_MAC, nm, prd, mixed), fem = mg_solver::footprint(MG_FEM, nf, prd, mixed);
+    if (!mac || !fem) return 0;
+    return b + mac + fem;
+}
+
+__global__ void k_checksum(grid_dev g, const fields_dev *__restrict__ F, double *out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
+    double v[4] = {0, 0, 0, 0};
+    if (i < g.sm + 2 && j < g.sn + 2 && k < g.so + 2) {
+        int ind = gidx(g, i, j, k);
+        for (int c = 0; c < 3; c++) v[c] = F->vel[c][ind] * F->vel[c][ind];
+        v[3] = F->p[ind] * F->p[ind];
+    }
+    for (int c = 0; c < 4; c++) {
+        double a = v[c];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if ((threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) % 32 == 0) atomicAdd(out + c, a);
+    }
+}
+
+extern "C" int rmt3d_scene_checksum(rmt3d_scene *s, double out[4]) {
+    if (!s || !out) return fail(RMT3D_ERR_INVALID, "null argument");
+    const grid_dev &g = s->g;
+    CK(cudaMemsetAsync(s->d_red, 0, 4 * sizeof(double), s->st));
+    k_checksum<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->d_red);
+    s->count();
+    CK(cudaMemcpyAsync(out, s->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
     return RMT3D_OK;
 }
 

@@ -1,0 +1,145 @@
+"""Batched form and serving loop against scenes stepped alone.
+
+A batch steps independent scenes of uneven grid sizes together (each on its
+own stream, kernels overlapping on the device); the serving loop admits
+requests over time under an HBM budget.  Each scene's result must be the same
+as when the scene runs alone: the kernels and their order per scene do not
+depend on what else runs, so the only differences allowed are those of the
+floating-point atomics of the checksum reduction, far below the tolerance
+used here (the step's own reductions sum in a fixed order).
+"""
+import pytest
+
+import helpers as H
+import rmt3d_b200 as R
+from rmt3d_b200 import _lib, scenes
+
+pytestmark = pytest.mark.gpu
+
+SAME_TOL = 1e-11      # batch / mix versus alone, rel-L2 per field
+CHECK_TOL = 1e-11     # checksums, relative
+
+
+def _descs(tmp_path):
+    cfgs = [
+        scenes.cavity(16, steps=4),
+        scenes.cavity_sphere(24, steps=4, radius=0.25),
+        scenes.cavity(32, steps=4, lid=0.7),
+        scenes.cavity_sphere(16, steps=4, radius=0.3, G=3.0),
+    ]
+    out = []
+    for i, c in enumerate(cfgs):
+        out.append(R.desc_from_cfg(scenes.write(str(tmp_path / ("b%d.cfg" % i)), c)))
+    return out
+
+
+def _alone(desc, steps):
+    sc = R.Scene(desc)
+    try:
+        sc.prepare()
+        assert sc.run(steps) == R.NORMAL_EXIT
+        return {f: sc.field(f) for f in ("u", "v", "w", "p")}, sc.checksum()
+    finally:
+        sc.close()
+
+
+def test_alone_is_deterministic(tmp_path):
+    """Every reduction sums in a fixed order: two runs agree bit for bit."""
+    d = _descs(tmp_path)[1]
+    a, ca = _alone(d, 3)
+    b, cb = _alone(d, 3)
+    for f in a:
+        assert (a[f] == b[f]).all(), f
+
+
+def test_batch_matches_alone(tmp_path):
+    descs = _descs(tmp_path)
+    b = R.Batch(descs, host_threads=3)
+    try:
+        b.prepare()
+        st = b.step(3)
+        assert st == [R.NORMAL_EXIT] * len(descs)
+        for i, d in enumerate(descs):
+            ref, _ = _alone(d, 3)
+            for f in ("u", "v", "w", "p"):
+                got = b.field(i, f)
+                e = H.rel_l2(got[H.INTERIOR], ref[f][H.INTERIOR])
+                assert e < SAME_TOL, (i, f, e)
+    finally:
+        b.close()
+
+
+def test_autotune_choices_and_results(tmp_path):
+    descs = _descs(tmp_path)[:3]
+    b = R.Batch(descs, host_threads=2)
+    try:
+        b.prepare()
+        tuned = b.autotune(probe_steps=2)
+        sizes = sorted({d.sys_size[0] * d.sys_size[1] * d.sys_size[2] for d in descs})
+        assert sorted(tuned) == sizes
+        for vd, vu in tuned.values():
+            assert (vd, vu) in [(2, 2), (1, 1), (1, 2), (2, 1), (3, 3)]
+        assert b.step(3) == [R.NORMAL_EXIT] * len(descs)
+        # another smoothing schedule converges to the same tolerance: the
+        # fields agree with the default schedule at the solver's tolerance
+        for i, d in enumerate(descs):
+            ref, _ = _alone(d, 3)
+            e = H.rel_l2(b.field(i, "u")[H.INTERIOR], ref["u"][H.INTERIOR])
+            assert e < 1e-6, (i, e)
+    finally:
+        b.close()
+
+
+def test_footprint_is_what_a_scene_allocates(tmp_path):
+    for d in _descs(tmp_path):
+        for prec in (R.FP64, R.MIXED):
+            d.precision = prec
+            sc = R.Scene(d)
+            try:
+                assert R.footprint(d) == sc.device_bytes
+            finally:
+                sc.close()
+
+
+def test_serve_same_alone_and_in_mix(tmp_path):
+    descs = _descs(tmp_path)
+    steps = 3
+    # staggered arrivals: later requests arrive while earlier ones run
+    reqs = [(0.0, steps, descs[0]), (0.0, steps, descs[1]), (0.02, steps, descs[2]),
+            (0.05, steps, descs[3]), (0.05, steps, descs[1]), (0.1, steps, descs[2])]
+    budget = sum(R.footprint(d) for _, _, d in reqs)
+    res, summ = R.serve(reqs, budget, max_slots=3)
+    assert summ["requests"] == len(reqs)
+    assert 0 < summ["request_p50_s"] <= summ["request_p99_s"]
+    assert 0 < summ["step_p50_ms"] <= summ["step_p99_ms"]
+    assert summ["cellsteps_per_s"] > 0
+    # the work overlapped: some request was admitted before another finished
+    spans = sorted((r["admit_s"], r["finish_s"]) for r in res)
+    assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+    for (arr, n, d), r in zip(reqs, res):
+        assert r["status"] == R.NORMAL_EXIT and r["steps_done"] == n
+        assert r["admit_s"] >= arr - 1e-6
+        _, alone = _alone(d, n)
+        for a, b in zip(r["checksum"], alone):
+            assert abs(a - b) <= CHECK_TOL * max(abs(b), 1e-300), (a, b)
+
+
+def test_serve_admission_by_budget(tmp_path):
+    descs = _descs(tmp_path)
+    big = max(R.footprint(d) for d in descs)
+    reqs = [(0.0, 2, d) for d in descs]
+    # room for one scene at a time (any two footprints exceed the budget
+    # except pairs of small scenes): overlapping spans must fit together
+    budget = int(big * 1.5)
+    res, _ = R.serve(reqs, budget, max_slots=4)
+    used = [R.footprint(d) for d in descs]
+    assert all(r["status"] == R.NORMAL_EXIT for r in res)
+    for i in range(len(res)):
+        for j in range(i + 1, len(res)):
+            overlap = res[i]["admit_s"] < res[j]["finish_s"] and res[j]["admit_s"] < res[i]["finish_s"]
+            if overlap:
+                assert used[i] + used[j] <= budget, (i, j)
+    # a request larger than the whole budget is refused up front
+    with pytest.raises(_lib.RMT3DError) as ei:
+        R.serve(reqs, big // 2, max_slots=2)
+    assert ei.value.code == _lib.ERR_TOO_LARGE
