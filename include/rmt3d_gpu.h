@@ -232,14 +232,17 @@ int rmt3d_batch_prepare(rmt3d_batch *b);
 int rmt3d_batch_step(rmt3d_batch *b, int nsteps, int *status);
 int rmt3d_batch_size(rmt3d_batch *b, int *n);
 int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out);
-/* choose (v_down, v_up) per distinct grid size by timing candidates on a
- * probe scene (the reference's mg_opt searches the same pair,
- * Utilities/mg_probs.hh:80-208); tuned_out gets (cells, v_down, v_up) */
+/* choose the multigrid schedule (v_down, v_up, coarse_pts) per distinct grid
+ * size by timing candidates on a probe scene (the reference's mg_opt searches
+ * the (v_down, v_up) pair, Utilities/mg_probs.hh:80-208); tuned_out gets
+ * (cells, v_down, v_up, coarse_pts) per size */
 int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out);
 int rmt3d_batch_destroy(rmt3d_batch *b);
 
-/* Multigrid smoothing counts of one scene (V(v_down, v_up) cycles). */
-int rmt3d_scene_set_smoothing(rmt3d_scene *s, int v_down, int v_up);
+/* Multigrid schedule of one scene: V(v_down, v_up) smoothing counts, and the
+ * largest level (points) whose whole sub-cycle runs in one thread block out of
+ * shared memory (0 keeps the current value). */
+int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts);
 
 /* Device bytes a scene with this descriptor allocates (admission control). */
 size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d);

@@ -189,9 +189,10 @@ class Scene:
         _lib.check(lib().rmt3d_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(b)))
         return ms.value, n.value, b.value
 
-    def set_smoothing(self, v_down, v_up):
-        """Multigrid V(v_down, v_up) smoothing counts of both solvers."""
-        _lib.check(lib().rmt3d_scene_set_smoothing(self._h, v_down, v_up))
+    def set_schedule(self, v_down, v_up, coarse_pts=0):
+        """Multigrid V(v_down, v_up) smoothing counts of both solvers and the
+        largest level run by the one-block coarse sub-cycle (0 keeps it)."""
+        _lib.check(lib().rmt3d_scene_set_schedule(self._h, v_down, v_up, coarse_pts))
 
     def checksum(self):
         """Sums of u^2, v^2, w^2, p^2 over the interior cells."""
@@ -309,11 +310,11 @@ class Batch:
         return out.reshape(dims[2], dims[1], dims[0])
 
     def autotune(self, probe_steps=3):
-        """Per grid size: {cells: (v_down, v_up)} chosen by timing candidates."""
-        buf = (ctypes.c_int * (3 * self.n))()
+        """Per grid size: {cells: (v_down, v_up, coarse_pts)} chosen by timing candidates."""
+        buf = (ctypes.c_int * (4 * self.n))()
         n = ctypes.c_int()
         _lib.check(lib().rmt3d_batch_autotune(self._h, probe_steps, buf, self.n, ctypes.byref(n)))
-        return {buf[3 * i]: (buf[3 * i + 1], buf[3 * i + 2]) for i in range(min(n.value, self.n))}
+        return {buf[4 * i]: tuple(buf[4 * i + 1:4 * i + 4]) for i in range(min(n.value, self.n))}
 
     def close(self):
         if getattr(self, "_h", None):

@@ -22,10 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "--fmad=false",
                    "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
                    "-I" + INCLUDE, "-I" + CSRC]
-CU_SOURCES = ["k_fluid.cu", "k_mg.cu", "k_mgp.cu", "k_solid.cu", "scene.cu", "batch.cu"]
-# per-file extra flags: the persistent multigrid kernel exchanges data between
-# CTAs inside one launch, so its global loads bypass the (non-coherent) L1
-PER_FILE = {"k_mgp.cu": ["-Xptxas", "-dlcm=cg"]}
+CU_SOURCES = ["k_fluid.cu", "k_mg.cu", "k_solid.cu", "scene.cu", "batch.cu"]
+PER_FILE = {}
 CC_SOURCES = ["cfg.cc"]
 
 

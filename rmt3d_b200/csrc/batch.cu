@@ -4,9 +4,12 @@
 // host threads issues the scenes' steps so that the small kernels of many
 // scenes overlap on the device (uneven grid sizes need no padding: each scene
 // launches its own grids).  Scenes are assigned to threads by a greedy
-// balance of cells.  An autotuner picks the multigrid smoothing counts per
-// grid size by timing candidate (v_down, v_up) pairs on a probe scene.
+// balance of cells.  An autotuner picks the multigrid schedule per grid size
+// -- smoothing counts (v_down, v_up) and the size of the levels handed to the
+// one-block shared-memory coarse sub-cycle -- by timing candidates on a probe
+// scene.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -22,14 +25,14 @@
 #include "rmt3d_gpu.h"
 
 // knobs shared with scene.cu (defined there)
-extern "C" int rmt3d_scene_set_smoothing(rmt3d_scene *s, int v_down, int v_up);
+extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts);
 
 struct rmt3d_batch {
     std::vector<rmt3d_scene *> scenes;
     std::vector<rmt3d_scene_desc> descs;
     std::vector<std::vector<int>> groups;  // scene indices per host thread
     std::vector<int> status;
-    std::map<int, std::pair<int, int>> tuned;  // grid cells -> (v_down, v_up)
+    std::map<int, std::array<int, 3>> tuned;  // grid cells -> (v_down, v_up, coarse_pts)
     int nthreads = 1;
 };
 
@@ -107,17 +110,39 @@ extern "C" int rmt3d_batch_prepare(rmt3d_batch *b) {
     return for_all(b, [&](int i) { return rmt3d_prepare(b->scenes[i]); });
 }
 
+// Each host thread queues all steps of its scenes (step-graph launches on
+// the scenes' own streams) before waiting for any of them, so that every
+// scene of the batch is in flight on the device at once.
 extern "C" int rmt3d_batch_step(rmt3d_batch *b, int nsteps, int *status) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
-    int e = for_all(b, [&](int i) {
-        int st = 0;
-        int r = rmt3d_run(b->scenes[i], nsteps, &st);
-        b->status[i] = st;
-        return r;
-    });
+    std::vector<int> err(b->groups.size(), 0);
+    std::vector<std::string> msg(b->groups.size());
+    std::vector<std::thread> th;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    for (size_t t = 0; t < b->groups.size(); t++) {
+        th.emplace_back([&, t]() {
+            cudaSetDevice(dev);
+            auto note = [&](int e) {
+                if (e && !err[t]) {
+                    err[t] = e;
+                    msg[t] = rmt3d_last_error();
+                }
+            };
+            for (int i : b->groups[t]) note(rmt3d::steps_launch(b->scenes[i], nsteps));
+            for (int i : b->groups[t]) {
+                int st = 0;
+                note(rmt3d::steps_finish(b->scenes[i], &st));
+                b->status[i] = st;
+            }
+        });
+    }
+    for (auto &x : th) x.join();
     if (status)
         for (size_t i = 0; i < b->status.size(); i++) status[i] = b->status[i];
-    return e;
+    for (size_t t = 0; t < err.size(); t++)
+        if (err[t]) return rmt3d::fail(err[t], msg[t]);
+    return RMT3D_OK;
 }
 
 extern "C" int rmt3d_batch_size(rmt3d_batch *b, int *n) {
@@ -139,7 +164,9 @@ extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
 // distinct size: cells, v_down, v_up) receives the choices.
 extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
-    static const int cand[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
+    if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
+    static const int smooth[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
+    static const int coarse[] = {1000, 5000};
     std::map<long long, int> first;
     for (size_t i = 0; i < b->descs.size(); i++)
         if (!first.count(cells(b->descs[i]))) first[cells(b->descs[i])] = (int)i;
@@ -153,30 +180,38 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
             return e;
         }
         double best = 1e300;
-        int bd = 2, bu = 2;
-        for (auto &c : cand) {
-            rmt3d_scene_set_smoothing(probe, c[0], c[1]);
-            int st = 0;
-            rmt3d_run(probe, 1, &st);  // settle the cycle predictor
-            rmt3d_sync(probe);
-            auto t0 = std::chrono::steady_clock::now();
-            rmt3d_run(probe, probe_steps, &st);
-            rmt3d_sync(probe);
-            double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-            if (st == 0 && dt < best) {
-                best = dt;
-                bd = c[0];
-                bu = c[1];
+        int bd = 2, bu = 2, bc = 5000;
+        for (int cp : coarse)
+            for (auto &c : smooth) {
+                if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], cp))) {
+                    rmt3d_scene_destroy(probe);
+                    return e;
+                }
+                int st = 0;
+                rmt3d_run(probe, 1, &st);  // settle the cycle predictor
+                rmt3d_sync(probe);
+                auto t0 = std::chrono::steady_clock::now();
+                rmt3d_run(probe, probe_steps, &st);
+                rmt3d_sync(probe);
+                double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                if (st == 0 && dt < best) {
+                    best = dt;
+                    bd = c[0];
+                    bu = c[1];
+                    bc = cp;
+                }
             }
-        }
         rmt3d_scene_destroy(probe);
-        b->tuned[(int)kv.first] = {bd, bu};
+        b->tuned[(int)kv.first] = {bd, bu, bc};
         for (size_t i = 0; i < b->descs.size(); i++)
-            if (cells(b->descs[i]) == kv.first) rmt3d_scene_set_smoothing(b->scenes[i], bd, bu);
+            if (cells(b->descs[i]) == kv.first) {
+                if ((e = rmt3d_scene_set_schedule(b->scenes[i], bd, bu, bc))) return e;
+            }
         if (tuned_out && written < max_out) {
-            tuned_out[3 * written] = (int)kv.first;
-            tuned_out[3 * written + 1] = bd;
-            tuned_out[3 * written + 2] = bu;
+            tuned_out[4 * written] = (int)kv.first;
+            tuned_out[4 * written + 1] = bd;
+            tuned_out[4 * written + 2] = bu;
+            tuned_out[4 * written + 3] = bc;
         }
         written++;
     }

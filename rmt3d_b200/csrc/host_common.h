@@ -2,6 +2,16 @@
 #pragma once
 #include <string>
 
+struct rmt3d_scene;
+
 namespace rmt3d {
 int fail(int code, const std::string &msg);
+
+// Graph-mode stepping split in two, for callers that keep many scenes in
+// flight: queue nsteps step-graph launches on the scene's stream (building
+// the graph first if needed), then wait and collect the outcome as
+// rmt3d_run does.  Scenes in profiling or eager mode run eagerly in
+// steps_launch and steps_finish only reports.
+int steps_launch(rmt3d_scene *s, int nsteps);
+int steps_finish(rmt3d_scene *s, int *status);
 }

@@ -490,11 +490,12 @@ __device__ void acceleration(const grid_dev &g, const fields_dev *__restrict__ F
 // (fields.hh:147-177, non-TANG branch).  Interior cells.
 // -------------------------------------------------------------------------
 __global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
-                           const double *lz, double cdt, double time, int var_den) {
+                           const double *lz, double cdt, const double *time_p, int var_den) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
     int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
     if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
+    const double time = *time_p;  // device-resident simulation time
     const int ind = gidx(g, i, j, k);
     const int strides[3] = {1, g.sm4, g.smn4};
     const double dhsp[3] = {g.dxsp, g.dysp, g.dzsp};
@@ -668,11 +669,12 @@ __global__ void k_sub_qgrad(grid_dev g, const fields_dev *__restrict__ F, double
 // Explicit momentum update, fluid_3d::compute_ustar (fluid_3d.cc:1309-1352).
 // -------------------------------------------------------------------------
 __global__ void k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
-                        const double *lz, double cdt, double time, int var_den) {
+                        const double *lz, double cdt, const double *time_p, int var_den) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
     int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
     if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
+    const double time = *time_p;  // device-resident simulation time
     const int ind = gidx(g, i, j, k);
     double acc[3] = {0, 0, 0};
     acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);

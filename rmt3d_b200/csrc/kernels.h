@@ -29,13 +29,13 @@ __global__ void k_bc_cc(grid_dev g, int face, bc_face bc, double *u, double *v, 
 __global__ void k_bc_cf(grid_dev g, int face, bc_face bc, const fields_dev *F);
 __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F);
 __global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
-                           const double *lz, double cdt, double time, int var_den);
+                           const double *lz, double cdt, const double *time_p, int var_den);
 __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F);
 __global__ void k_mac_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, double cdt);
 __global__ void k_mac_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x);
 __global__ void k_sub_qgrad(grid_dev g, const fields_dev *__restrict__ F, double cdt, int var_den);
 __global__ void k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
-                        const double *lz, double cdt, double time, int var_den);
+                        const double *lz, double cdt, const double *time_p, int var_den);
 __global__ void k_fem_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, gradphi_t gp);
 __global__ void k_fem_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x, const double *mean);
 __global__ void k_sub_pgrad(grid_dev g, const fields_dev *__restrict__ F, double dt, int var_den);

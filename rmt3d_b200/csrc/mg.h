@@ -44,17 +44,31 @@ struct mg_level {
     size_t npts() const { return (size_t)n[0] * n[1] * n[2]; }
 };
 
-// mg_pred (mg_probs.hh:37-78); alpha is the integer quotient 1/(3*iP) = 0
-// exactly as the reference computes it, so the averages never move.
-struct mg_pred_state {
-    int iP = 16;
-    int iV = 32;
-    double V_avg = 32;
-    double V_var = 1e6;
-    double alpha = 1 / (3 * 16);
-    int iters() const { return iV / iP; }
-    void update(int extras);
+// Device-resident control state of one solver: the mg_pred predictor
+// (mg_probs.hh:37-78; alpha is the integer quotient 1/(3*iP) = 0 exactly as
+// the reference computes it, so the averages never move) and the position in
+// the mg_prob::run loop (Utilities/mg_probs.cc:3-83).  The host reads it back
+// after a solve or a step.
+struct mg_ctl {
+    int iV;            // predicted V-cycles x iP
+    int phase;         // 0 predicted cycles, 1 extra rounds, 2 insurance, 3 stagnation loop
+    int todo;          // cycles left in the current phase
+    int extra;         // extra rounds so far
+    int it;            // stagnation-loop iterations
+    int count;         // cycles of the current solve
+    int last_cycles;   // cycles of the last finished solve
+    int active;        // the current solve continues
+    int nan;           // the last solve ended with a NaN residual
+    int pad;
+    long long cycles_total;
+    double V_avg, V_var;
+    double prev, res_out;  // previous / reported max-norm residual
 };
+
+constexpr int kMgIP = 16;
+constexpr int kMgMaxCycles = 4096;  // bound on the cycles of one solve
+
+struct graph_builder;
 
 class mg_solver {
   public:
@@ -62,13 +76,14 @@ class mg_solver {
     std::vector<mg_level> lv;
     double max_norm_tol;
     int v_up = 2, v_down = 2;
-    mg_pred_state pred;
-    long long cycles_total = 0;
+    long long cycles_total = 0;  // host mirrors of the device control state
     int last_cycles = 0;
     bool mixed = false;  // FP32 cycles inside FP64 iterative refinement
     bool exact = false;  // iterate each solve until the residual stagnates
     long long *launches = nullptr;
     kernel_profiler *prof = nullptr;
+    mg_ctl *ctl = nullptr;       // device control block (owned by the scene)
+    mg_ctl *h_ctl = nullptr;     // pinned mirror (owned by the scene)
 
     mg_solver() = default;
     mg_solver(const mg_solver &) = delete;
@@ -83,25 +98,33 @@ class mg_solver {
     size_t bytes_alloc = 0;  // device bytes held
     double *rhs() { return lv[0].r; }
     double *sol() { return lv[0].x; }
-    // one solve with the reference's control logic; returns the final max-norm
-    // residual (NaN propagates)
-    double run(cudaStream_t st);
-    // one cooperative launch per solve with the control loop on the device
-    bool persistent = false;
     double *dense = nullptr;  // inverse of the coarsest operator (row-major), or null
     int cf = 0;  // first level whose whole sub-cycle runs in one CTA
-    bool hard_error = false;  // the persistent launch failed or its barrier timed out
-    int setup_persistent(cudaStream_t st);
-    double run_persistent(cudaStream_t st);
-    double residual_max(cudaStream_t st);
-    void vcycle(cudaStream_t st);
+    int coarse_pts = 1000;  // largest level handed to the one-CTA sub-cycle
+    int set_coarse(int pts);
+
+    // One solve with the reference's control logic, issued eagerly and
+    // waited for; returns the reported max-norm residual (NaN propagates).
+    // Uses the solver's own graph unless a kernel profiler is active.
+    double run(cudaStream_t st);
+    // Append one solve to the graph `cur` is capturing: an arming kernel and a
+    // WHILE node whose body is one iteration, the residual norm and the
+    // control kernel.  Returns the kernels per loop iteration.
+    int capture_solve(cudaStream_t cur, graph_builder &gb);
+    int outside_kernels = 1;   // kernels of a solve outside its loop body
+    int body_kernels = 0;      // kernels per loop iteration (set by capture_solve)
+    void invalidate();         // drop the solver's own graph (schedule changed)
+    void sync_host_mirror();   // cycles from the pinned control mirror
 
   private:
-    double *d_max = nullptr;   // device scalar for reductions
-    void *pstate = nullptr;    // persistent solver: predictor state, barrier, partial maxima
-    int pgrid = 0;
+    unsigned long long *d_max = nullptr;  // residual max-norm (ordered bit pattern)
+    cudaGraphExec_t solve_exec = nullptr;
+    cudaStream_t cap_main = nullptr;
+    graph_builder *own_gb = nullptr;
     int build_dense(cudaStream_t st);
-    double *h_max = nullptr;   // pinned host mirror
+    int build_solve_graph();
+    void launch_body(cudaStream_t st, bool armed, unsigned long long h);
+    void iterate(cudaStream_t st);
     void cycle(int l, cudaStream_t st);
     void cycle_f32(int l, cudaStream_t st);
     void smooth(int l, int sweeps, cudaStream_t st);

@@ -1,7 +1,7 @@
-// Multigrid operator helpers shared by the per-launch V-cycle (k_mg.cu) and
-// the persistent solver (k_mgp.cu): rediscretised MAC 7-point and FEM Q1
-// 27-point stencils with the boundary rules of stencil_set::set_partials
-// (Utilities/mg_probs.hh:281-343).
+// Multigrid operator helpers of the V-cycle kernels (k_mg.cu): rediscretised
+// MAC 7-point and FEM Q1 27-point stencils with the boundary rules of
+// stencil_set::set_partials (Utilities/mg_probs.hh:281-343), and the phases of
+// the one-block coarse sub-cycle.
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -97,7 +97,6 @@ __device__ __forceinline__ T fem_offdiag(const lvl_dev L, const T *__restrict__ 
 }
 
 
-constexpr int kCoarsePts = 1000;
 constexpr int kMaxLev = 12;
 constexpr int kThreads = 256;
 
@@ -111,18 +110,9 @@ struct pmg_level {
 struct pmg_args {
     int kind;  // 0 MAC, 1 FEM
     int nlev;
-    int cf;    // first level handled by CTA 0 alone
     pmg_level lv[kMaxLev];
     const double *dense;  // inverse of the coarsest operator, or null
-    double tol;
     int v_up, v_down;
-    int exact, mixed;
-    int *pred_iV;
-    double *pred_avg, *pred_var;
-    unsigned *bar;      // [0] arrival count, [1] generation
-    double *partial;    // per-CTA residual maxima
-    double *out;        // [0] final residual, [1] V-cycles run, [2] extra rounds
-    int *err;           // barrier timeout
 };
 
 __device__ __forceinline__ lvl_dev ldev(const pmg_level &L) {
@@ -258,6 +248,19 @@ __device__ void ph_prolong(int kind, const lvl_dev F, const lvl_dev C, T *x, con
 }
 
 template <typename T>
+__device__ __forceinline__ void set_level_ptrs(pmg_level &L, T *x, T *r, T *res) {
+    if constexpr (sizeof(T) == 8) {
+        L.x = (double *)x;
+        L.r = (double *)r;
+        L.res = (double *)res;
+    } else {
+        L.xs = (float *)x;
+        L.rs = (float *)r;
+        L.ress = (float *)res;
+    }
+}
+
+template <typename T>
 __device__ __forceinline__ T *LX(const pmg_level &L) {
     if constexpr (sizeof(T) == 8) return (T *)L.x;
     else return (T *)L.xs;
@@ -297,11 +300,14 @@ __device__ void coarse_cycle(const pmg_args &A, int cf) {
         T *x = LX<T>(L);
         const T *r = LR<T>(L);
         if (A.dense) {
-            for (int row = t0; row < np; row += ts) {
+            // one warp per row of the (row-major) inverse: coalesced reads
+            const int warp = t0 >> 5, lane = t0 & 31, nw = ts >> 5;
+            for (int row = warp; row < np; row += nw) {
                 const double *b = A.dense + (size_t)row * np;
                 double acc = 0;
-                for (int c = 0; c < np; c++) acc += b[c] * (double)r[c];
-                x[row] = (T)acc;
+                for (int c = lane; c < np; c += 32) acc += b[c] * (double)r[c];
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                if (lane == 0) x[row] = (T)acc;
             }
             __syncthreads();
         } else {

@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "graph_build.h"
 #include "host_common.h"
 #include "kernels.h"
 #include "mg.h"
@@ -82,6 +83,20 @@ inline unsigned lin_blocks(int n) { return (unsigned)((n + 255) / 256); }
 
 }  // namespace
 
+// Device-resident control block of a scene, copied to a pinned mirror after
+// every solve or step: simulation time, the step graph's halt flag and status,
+// the per-step error counters and both solvers' multigrid control state.
+struct scene_ctl {
+    double time;
+    int halted;  // a step of the step graph failed: its later launches do nothing
+    int steps;   // steps the step graph has executed
+    int status;  // status of the failing step
+    int pad;
+    int counters[8];  // [0..1] frontier sizes, [2] extrapolation errors, [3] corrector problems,
+                      // [4] redraw fatal, [5] refmap-derivative errors
+    mg_ctl mac, fem;
+};
+
 struct rmt3d_scene {
     rmt3d_scene_desc d;
     grid_dev g;
@@ -105,9 +120,18 @@ struct rmt3d_scene {
     // extrapolation scratch
     uint8_t *lay = nullptr, *inl = nullptr;
     int *front[2] = {nullptr, nullptr};
-    int *counters = nullptr;  // [0..1] frontier sizes, [2] extrapolation errors, [3] corrector problems,
-                              // [4] redraw fatal, [5] refmap-derivative errors
-    int *h_counters = nullptr;
+    scene_ctl *ctl = nullptr;    // device control block
+    scene_ctl *h_ctl = nullptr;  // pinned mirror
+    int *counters = nullptr;     // = ctl->counters
+    int *h_counters = nullptr;   // = h_ctl->counters
+    // the step as one CUDA graph (built on first use, rebuilt when dt, the
+    // FEM basis or the multigrid schedule change)
+    graph_builder gb;
+    cudaGraphExec_t step_exec = nullptr;
+    bool graph_dirty = true;
+    bool capturing = false;
+    bool use_graph = true;
+    long long graph_fixed = 0;  // kernels per step outside the multigrid loops
     double *d_mean = nullptr;  // [0] mean, [1..] per-block partial sums
     unsigned *mean_ticket = nullptr;
     double *h_scalar = nullptr;
@@ -374,7 +398,7 @@ static int init_fluid(rmt3d_scene *s) {
     CK(cudaStreamSynchronize(s->st));
     periodic(s, {s->hF.vel[0], s->hF.vel[1], s->hF.vel[2]}, {}, 0);
     cfl_recheck(s);
-    s->dt = s->dt_reg;
+    rmt3d_set_dt(s, s->dt_reg);
     return 0;
 }
 
@@ -502,20 +526,95 @@ static void compute_stress(rmt3d_scene *s) {
     s->count();
 }
 
-static int mac_solve(rmt3d_scene *s, double cdt) {
+// ---- simulation time, kept on the device (read by the kernels) -----------
+__global__ void k_time_set(scene_ctl *c, double t) { c->time = t; }
+__global__ void k_time_add(scene_ctl *c, double dt_half) { c->time += dt_half; }
+
+static void set_time(rmt3d_scene *s, double t) {
+    s->time = t;
+    k_time_set<<<1, 1, 0, s->st>>>(s->ctl, t);
+    s->count();
+}
+
+// time += dt/2 (the two halves of fluid_3d::step_forward, fluid_3d.cc:456,
+// :541); the host mirror follows in eager mode and is read back after a
+// graph step
+static void advance_half(rmt3d_scene *s) {
+    if (!s->capturing) s->time += 0.5 * s->dt;
+    k_time_add<<<1, 1, 0, s->st>>>(s->ctl, 0.5 * s->dt);
+    s->count();
+}
+
+// ---- phases of fluid_3d::step_forward (fluid_3d.cc:429-577) ----------------
+// compute_half_time_edge_velocities/refmap with their limited derivatives
+static void ph_edges(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    k_edge_vel<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, &s->ctl->time,
+                                                            s->d.var_den);
+    s->count();
+    if (g.n_obj > 0) {
+        k_edge_refmap<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->counters + 5);
+        s->count();
+    }
+    advance_half(s);
+}
+
+// godunov_upwinding_set between the boundary fills
+static void ph_upwind(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    fill_boundary_cf(s);
+    comm_face_maps(s);
+    k_upwind<<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
+    s->count();
+    fill_boundary_cf(s);
+}
+
+// mac_solve (fluid_3d.cc:2209-2241) before and after the multigrid solve
+static void ph_mac_pre(rmt3d_scene *s, double cdt) {
     const grid_dev &g = s->g;
     update_rho(s);
     k_mac_rhs<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.rhs(), cdt);
     s->count();
-    double res = s->mac.run(s->st);
-    if (s->mac.hard_error) return RMT3D_ERR_CUDA;
-    if (std::isnan(res)) return fail(RMT3D_ERR_NAN, "fluid_3d::mac_solve(): NaN detected in multigrid solve");
+}
+
+static void ph_mac_post(rmt3d_scene *s, double cdt) {
+    const grid_dev &g = s->g;
     k_mac_extract<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.sol());
     s->count();
     comm_pressure(s);
     k_sub_qgrad<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, cdt, s->d.var_den);
     s->count();
-    return 0;
+    fill_boundary_cf(s);
+}
+
+// update_reference_map (fluid_3d.cc:1149-1255) up to the corrector, whose
+// problem count lands in counters[3]
+static void ph_refmap(rmt3d_scene *s, double cdt) {
+    const grid_dev &g = s->g;
+    k_refmap_predict<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, cdt);
+    k_snapshot_reset<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
+    s->count(2);
+    comm_primary(s);
+    extrapolate(s);
+    k_refmap_correct<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->counters + 3);
+    s->count();
+    update_rho(s);
+}
+
+static void ph_revert(rmt3d_scene *s) {
+    k_refmap_revert<<<lin_blocks(s->g.ncell), 256, 0, s->st>>>(s->g, s->dF);
+    s->count();
+}
+
+// compute_ustar (fluid_3d.cc:1309-1352) and its boundary fills
+static void ph_ustar(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
+    k_ustar<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, &s->ctl->time,
+                                                         s->d.var_den);
+    s->count();
+    fill_boundary_cc(s);
+    comm_dvel(s);
+    advance_half(s);
 }
 
 // Mean of x in a fixed summation order: each block writes its partial sum,
@@ -553,15 +652,16 @@ __global__ void k_mean(const double *x, size_t n, double scale, double *out, uns
     }
 }
 
-// pp_solve (fluid_3d.cc:2653-2681): 0 or PROJECTION_ERR
-static int pp_solve(rmt3d_scene *s) {
+// pp_solve (fluid_3d.cc:2653-2681) before and after the multigrid solve
+static void ph_pp_pre(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     update_rho(s);
     k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
     s->count();
-    double res = s->fem.run(s->st);
-    if (s->fem.hard_error) return -1;
-    if (std::isnan(res)) return 1;
+}
+
+static void ph_pp_post(rmt3d_scene *s) {
+    const grid_dev &g = s->g;
     size_t nn = (size_t)g.fm * g.fn * g.fo;
     k_mean<<<kMeanBlocks, 256, 0, s->st>>>(s->fem.sol(), nn, 1 / (double)nn, s->d_mean, s->mean_ticket);
     k_fem_extract<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.sol(), s->d_mean);
@@ -569,80 +669,12 @@ static int pp_solve(rmt3d_scene *s) {
     comm_pressure(s);
     k_sub_pgrad<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->d.var_den);
     s->count();
-    return 0;
 }
 
-// update_reference_map (fluid_3d.cc:1149-1255); returns the problem count
-static int update_reference_map(rmt3d_scene *s, double cdt, int *prob) {
+// update_reference_map_full, update_rho, redraw_boundary, boundary fills
+// (fluid_3d.cc:559-574)
+static void ph_final(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    *prob = 0;
-    if (g.n_obj == 0) return 0;
-    k_refmap_predict<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, cdt);
-    k_snapshot_reset<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
-    s->count(2);
-    comm_primary(s);
-    extrapolate(s);
-    k_refmap_correct<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->counters + 3);
-    s->count();
-    update_rho(s);
-    CK(cudaMemcpyAsync(s->h_counters, s->counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
-    CK(cudaStreamSynchronize(s->st));
-    if (s->h_counters[2] > 0) return fail(RMT3D_ERR_EXTRAP, "Extrapolation failed: no eligible points or degenerate matrix");
-    if (s->h_counters[5] > 0)
-        return fail(RMT3D_ERR_EXTRAP, "normal_derivatives_refmap: missing necessary cells to carry out finite differences");
-    *prob = s->h_counters[3];
-    return 0;
-}
-
-static int step_forward(rmt3d_scene *s, int debug, int stop = 99) {
-    const grid_dev &g = s->g;
-    (void)debug;
-    s->nt++;
-    CK(cudaMemsetAsync(s->counters + 2, 0, 6 * sizeof(int), s->st));
-    compute_stress(s);
-    if (stop <= 1) return RMT3D_OK;
-    k_edge_vel<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, s->time,
-                                                            s->d.var_den);
-    s->count();
-    if (g.n_obj > 0) {
-        k_edge_refmap<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->counters + 5);
-        s->count();
-    }
-    s->time += 0.5 * s->dt;
-    if (stop <= 2) return RMT3D_OK;
-    fill_boundary_cf(s);
-    comm_face_maps(s);
-    k_upwind<<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
-    s->count();
-    fill_boundary_cf(s);
-    if (stop <= 3) return RMT3D_OK;
-    int e = mac_solve(s, s->dt);
-    if (e) return e;
-    fill_boundary_cf(s);
-    if (stop <= 4) return RMT3D_OK;
-    int prob = 0;
-    e = update_reference_map(s, s->dt, &prob);
-    if (e) return e;
-    if (prob) {
-        k_refmap_revert<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
-        s->count();
-        return RMT3D_REFMAP_UPDATE_ERR;
-    }
-    if (stop <= 5) return RMT3D_OK;
-    compute_stress(s);
-    if (stop <= 6) return RMT3D_OK;
-    k_ustar<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, s->time, s->d.var_den);
-    s->count();
-    fill_boundary_cc(s);
-    comm_dvel(s);
-    s->time += 0.5 * s->dt;
-    if (stop <= 7) return RMT3D_OK;
-    {
-        int pe = pp_solve(s);
-        if (pe < 0) return RMT3D_ERR_CUDA;
-        if (pe) return RMT3D_PROJECTION_ERR;
-    }
-    if (stop <= 8) return RMT3D_OK;
     if (g.n_obj > 0) {
         k_refmap_full<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
         s->count();
@@ -652,14 +684,245 @@ static int step_forward(rmt3d_scene *s, int debug, int stop = 99) {
     }
     fill_boundary_cc(s);
     comm_dvel(s);
+}
+
+static int read_ctl(rmt3d_scene *s) {
+    CK(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(scene_ctl), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
+static int extrap_errors(rmt3d_scene *s) {
+    if (s->h_counters[2] > 0) return fail(RMT3D_ERR_EXTRAP, "Extrapolation failed: no eligible points or degenerate matrix");
+    if (s->h_counters[5] > 0)
+        return fail(RMT3D_ERR_EXTRAP, "normal_derivatives_refmap: missing necessary cells to carry out finite differences");
+    return 0;
+}
+
+// The step issued kernel by kernel with the host checking each solve and
+// each error counter where the reference does (used for the set-up
+// iterations, phase-by-phase inspection and kernel profiling).  `stop`
+// ends the step after that phase group.
+static int step_forward(rmt3d_scene *s, int debug, int stop = 99) {
+    const grid_dev &g = s->g;
+    (void)debug;
+    s->nt++;
+    CK(cudaMemsetAsync(s->counters + 2, 0, 6 * sizeof(int), s->st));
+    compute_stress(s);
+    if (stop <= 1) return RMT3D_OK;
+    ph_edges(s);
+    if (stop <= 2) return RMT3D_OK;
+    ph_upwind(s);
+    if (stop <= 3) return RMT3D_OK;
+    ph_mac_pre(s, s->dt);
+    double res = s->mac.run(s->st);
+    if (std::isnan(res)) {
+        CK(cudaGetLastError());
+        return fail(RMT3D_ERR_NAN, "fluid_3d::mac_solve(): NaN detected in multigrid solve");
+    }
+    ph_mac_post(s, s->dt);
+    if (stop <= 4) return RMT3D_OK;
     if (g.n_obj > 0) {
-        CK(cudaMemcpyAsync(s->h_counters, s->counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
-        CK(cudaStreamSynchronize(s->st));
+        ph_refmap(s, s->dt);
+        int e = read_ctl(s);
+        if (!e) e = extrap_errors(s);
+        if (e) return e;
+        if (s->h_counters[3]) {
+            ph_revert(s);
+            return RMT3D_REFMAP_UPDATE_ERR;
+        }
+    }
+    if (stop <= 5) return RMT3D_OK;
+    compute_stress(s);
+    if (stop <= 6) return RMT3D_OK;
+    ph_ustar(s);
+    if (stop <= 7) return RMT3D_OK;
+    ph_pp_pre(s);
+    res = s->fem.run(s->st);
+    if (std::isnan(res)) return RMT3D_PROJECTION_ERR;
+    ph_pp_post(s);
+    if (stop <= 8) return RMT3D_OK;
+    ph_final(s);
+    if (g.n_obj > 0) {
+        int e = read_ctl(s);
+        if (e) return e;
         if (s->h_counters[4] > 0)
             return fail(RMT3D_ERR_INVALID, "redraw_boundary(): Two deep maps try to be inside a cell at the same time!");
     }
     CK(cudaGetLastError());
     return RMT3D_OK;
+}
+
+// ---- the step as one CUDA graph --------------------------------------------
+// Gate: a step runs only while no earlier step of the graph failed; the
+// per-step error counters start at zero.
+__global__ void k_step_gate(scene_ctl *c, cudaGraphConditionalHandle h) {
+    const bool run = c->halted == 0;
+    if (run)
+        for (int i = 2; i < 8; i++) c->counters[i] = 0;
+    cudaGraphSetConditional(h, run ? 1u : 0u);
+}
+
+// After update_reference_map: continue, or revert the maps (corrector
+// problem), or neither (an error already ends the step).
+__global__ void k_step_branch(scene_ctl *c, cudaGraphConditionalHandle h_rest, cudaGraphConditionalHandle h_rev) {
+    const bool err = c->mac.nan || c->counters[2] > 0 || c->counters[5] > 0;
+    cudaGraphSetConditional(h_rest, (!err && c->counters[3] == 0) ? 1u : 0u);
+    cudaGraphSetConditional(h_rev, (!err && c->counters[3] != 0) ? 1u : 0u);
+}
+
+// The step's status, in the order the eager step reports them.
+__global__ void k_step_end(scene_ctl *c, int with_objects) {
+    int st = 0;
+    if (c->mac.nan) st = RMT3D_ERR_NAN;
+    else if (with_objects && (c->counters[2] > 0 || c->counters[5] > 0)) st = RMT3D_ERR_EXTRAP;
+    else if (with_objects && c->counters[3] != 0) st = RMT3D_REFMAP_UPDATE_ERR;
+    else if (c->fem.nan) st = RMT3D_PROJECTION_ERR;
+    else if (with_objects && c->counters[4] > 0) st = RMT3D_ERR_INVALID;
+    c->status = st;
+    c->halted = st != 0;
+    c->steps++;
+}
+
+// phases 6-9 (after a successful reference-map update)
+static int capture_rest(rmt3d_scene *s) {
+    compute_stress(s);
+    ph_ustar(s);
+    ph_pp_pre(s);
+    if (s->fem.capture_solve(s->st, s->gb) < 0) return 1;
+    s->launches += s->fem.outside_kernels;
+    ph_pp_post(s);
+    ph_final(s);
+    return 0;
+}
+
+static int build_step_graph(rmt3d_scene *s) {
+    if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
+    s->step_exec = nullptr;
+    if (s->gb.init()) return fail(RMT3D_ERR_CUDA, "stream creation failed");
+    s->gb.err = cudaSuccess;
+    s->gb.depth = 0;
+    const cudaStream_t main = s->st;
+    const long long saved = s->launches;
+    s->launches = 0;
+    s->capturing = true;
+    int bad = 0;
+    CK(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+    cudaGraphConditionalHandle h_step = s->gb.handle(main);
+    k_step_gate<<<1, 1, 0, main>>>(s->ctl, h_step);
+    s->count();
+    cudaStream_t b1 = s->gb.open(main, h_step, cudaGraphCondTypeIf);
+    if (b1) {
+        s->st = b1;
+        compute_stress(s);
+        ph_edges(s);
+        ph_upwind(s);
+        ph_mac_pre(s, s->dt);
+        if (s->mac.capture_solve(s->st, s->gb) < 0) bad = 1;
+        s->launches += s->mac.outside_kernels;
+        ph_mac_post(s, s->dt);
+        if (s->g.n_obj > 0) {
+            ph_refmap(s, s->dt);
+            cudaGraphConditionalHandle h_rev = s->gb.handle(b1), h_rest = s->gb.handle(b1);
+            k_step_branch<<<1, 1, 0, b1>>>(s->ctl, h_rest, h_rev);
+            s->count();
+            cudaStream_t b2 = s->gb.open(b1, h_rev, cudaGraphCondTypeIf);
+            if (b2) {
+                const long long l0 = s->launches;
+                s->st = b2;
+                ph_revert(s);
+                s->launches = l0;  // the revert branch is not part of a normal step
+                s->gb.close(b2);
+            }
+            b2 = s->gb.open(b1, h_rest, cudaGraphCondTypeIf);
+            if (b2) {
+                s->st = b2;
+                bad |= capture_rest(s);
+                s->gb.close(b2);
+            }
+            s->st = b1;
+        } else {
+            bad |= capture_rest(s);
+        }
+        k_step_end<<<1, 1, 0, b1>>>(s->ctl, s->g.n_obj > 0);
+        s->count();
+        s->gb.close(b1);
+    }
+    s->st = main;
+    cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(scene_ctl), cudaMemcpyDeviceToHost, main);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(main, &graph);
+    s->capturing = false;
+    s->graph_fixed = s->launches;
+    s->launches = saved;
+    if (bad || e != cudaSuccess || s->gb.err != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return fail(RMT3D_ERR_CUDA, std::string("step graph capture failed: ") +
+                                        cudaGetErrorString(e != cudaSuccess ? e : s->gb.err));
+    }
+    e = cudaGraphInstantiate(&s->step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(RMT3D_ERR_CUDA, std::string("step graph instantiation: ") + cudaGetErrorString(e));
+    s->graph_dirty = false;
+    return 0;
+}
+
+struct pending_steps {
+    long long c0, f0;
+    int steps0;
+    int eager_status;
+    int eager_err;
+};
+static thread_local std::vector<std::pair<rmt3d_scene *, pending_steps>> t_pending;
+
+static pending_steps *pending_of(rmt3d_scene *s) {
+    for (auto &p : t_pending)
+        if (p.first == s) return &p.second;
+    t_pending.push_back({s, pending_steps{}});
+    return &t_pending.back().second;
+}
+
+static int graph_launch(rmt3d_scene *s, int nsteps, pending_steps &p) {
+    if (s->graph_dirty || !s->step_exec) {
+        int e = build_step_graph(s);
+        if (e) return e;
+    }
+    p.c0 = s->mac.cycles_total;
+    p.f0 = s->fem.cycles_total;
+    p.steps0 = s->h_ctl->steps;
+    CK(cudaMemsetAsync(&s->ctl->halted, 0, sizeof(int), s->st));
+    CK(cudaMemsetAsync(&s->ctl->status, 0, sizeof(int), s->st));
+    for (int i = 0; i < nsteps; i++) CK(cudaGraphLaunch(s->step_exec, s->st));
+    return 0;
+}
+
+static int graph_finish(rmt3d_scene *s, const pending_steps &p, int *status) {
+    CK(cudaStreamSynchronize(s->st));
+    CK(cudaGetLastError());
+    const scene_ctl &h = *s->h_ctl;
+    const int done = h.steps - p.steps0;
+    s->nt += done;
+    s->time = h.time;
+    s->mac.sync_host_mirror();
+    s->fem.sync_host_mirror();
+    s->launches += (long long)done * s->graph_fixed + (s->mac.cycles_total - p.c0) * s->mac.body_kernels +
+                   (s->fem.cycles_total - p.f0) * s->fem.body_kernels;
+    *status = h.status;
+    switch (h.status) {
+        case RMT3D_ERR_NAN: return fail(RMT3D_ERR_NAN, "fluid_3d::mac_solve(): NaN detected in multigrid solve");
+        case RMT3D_ERR_EXTRAP: return extrap_errors(s);
+        case RMT3D_ERR_INVALID:
+            return fail(RMT3D_ERR_INVALID, "redraw_boundary(): Two deep maps try to be inside a cell at the same time!");
+        default: return 0;
+    }
+}
+
+static int run_graph(rmt3d_scene *s, int nsteps, int *status) {
+    pending_steps p;
+    int e = graph_launch(s, nsteps, p);
+    if (e) return e;
+    return graph_finish(s, p, status);
 }
 
 // div_u (fluid_3d_utils.cc:507-560): weighted L2 norm of the FEM rhs
@@ -896,14 +1159,36 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     if (d.n_obj > 0) {
         e |= s->alloc(&s->lay, n) | s->alloc(&s->inl, n) | s->alloc(&s->front[0], n) | s->alloc(&s->front[1], n);
     }
-    e |= s->alloc(&s->counters, 8) | s->alloc(&s->d_mean, 1 + kMeanBlocks) | s->alloc(&s->d_red, 4) |
+    e |= s->alloc(&s->ctl, 1) | s->alloc(&s->d_mean, 1 + kMeanBlocks) | s->alloc(&s->d_red, 4) |
          s->alloc(&s->mean_ticket, 1);
-    if (e) {
+    if (e || cudaMallocHost(&s->h_ctl, sizeof(scene_ctl)) != cudaSuccess ||
+        cudaMallocHost(&s->h_scalar, sizeof(double)) != cudaSuccess) {
         rmt3d_scene_destroy(s);
-        return RMT3D_ERR_OOM;
+        return fail(RMT3D_ERR_OOM, "allocation failed");
     }
-    cudaMallocHost(&s->h_counters, 8 * sizeof(int));
-    cudaMallocHost(&s->h_scalar, sizeof(double));
+    {
+        // control block: time 0, no halt, predictor state iV = 32,
+        // V_avg = 32, V_var = 1e6 (mg_pred, mg_probs.hh:44-50)
+        scene_ctl c;
+        memset(&c, 0, sizeof(c));
+        for (mg_ctl *m : {&c.mac, &c.fem}) {
+            m->iV = 2 * kMgIP;
+            m->V_avg = 2 * kMgIP;
+            m->V_var = 1e6;
+        }
+        *s->h_ctl = c;
+        cudaMemcpyAsync(s->ctl, s->h_ctl, sizeof(scene_ctl), cudaMemcpyHostToDevice, s->st);
+    }
+    s->counters = s->ctl->counters;
+    s->h_counters = s->h_ctl->counters;
+    s->mac.ctl = &s->ctl->mac;
+    s->mac.h_ctl = &s->h_ctl->mac;
+    s->fem.ctl = &s->ctl->fem;
+    s->fem.h_ctl = &s->h_ctl->fem;
+    {
+        const char *ge = getenv("RMT3D_GRAPH");
+        s->use_graph = !(ge && ge[0] == '0');
+    }
     cudaMemcpyAsync(s->lx, s->hlx.data(), g.sm4 * 8, cudaMemcpyHostToDevice, s->st);
     cudaMemcpyAsync(s->ly, s->hly.data(), g.sn4 * 8, cudaMemcpyHostToDevice, s->st);
     cudaMemcpyAsync(s->lz, s->hlz.data(), g.so4 * 8, cudaMemcpyHostToDevice, s->st);
@@ -929,7 +1214,8 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
 
 extern "C" int rmt3d_initialize(rmt3d_scene *s) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
-    s->time = 0;
+    set_time(s, 0);
+    s->graph_dirty = true;
     int e;
     if ((e = init_fluid(s))) return e;
     if ((e = init_pres(s))) return e;
@@ -938,8 +1224,8 @@ extern "C" int rmt3d_initialize(rmt3d_scene *s) {
     update_rho(s);
     fill_boundary_cc(s);
     compute_grad_basis(s);
-    CK(cudaMemcpyAsync(s->h_counters, s->counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
-    CK(cudaStreamSynchronize(s->st));
+    int re = read_ctl(s);
+    if (re) return re;
     if (s->h_counters[2] > 0) return fail(RMT3D_ERR_EXTRAP, "Extrapolation failed: no eligible points or degenerate matrix");
     CK(cudaGetLastError());
     return RMT3D_OK;
@@ -947,6 +1233,7 @@ extern "C" int rmt3d_initialize(rmt3d_scene *s) {
 
 extern "C" int rmt3d_set_dt(rmt3d_scene *s, double dt) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (dt != s->dt) s->graph_dirty = true;
     s->dt = dt;
     return RMT3D_OK;
 }
@@ -955,7 +1242,7 @@ extern "C" int rmt3d_init_iter(rmt3d_scene *s) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     const double tol = 1e-4;
     for (int i = 0; i < s->d.num_iters; i++) {
-        s->time = 0;
+        set_time(s, 0);
         fill_boundary_cc(s);
         int e = step_forward(s, 0);
         if (e < 0) return e;
@@ -972,7 +1259,7 @@ extern "C" int rmt3d_init_iter(rmt3d_scene *s) {
         if (divu < tol) break;
     }
     s->nt = 0;
-    s->time = 0.0;
+    set_time(s, 0.0);
     compute_stress(s);
     CK(cudaStreamSynchronize(s->st));
     CK(cudaGetLastError());
@@ -985,21 +1272,26 @@ extern "C" int rmt3d_prepare(rmt3d_scene *s) {
     if (e) return e;
     double dt;
     if ((e = rmt3d_stepper_dt(&s->d, s->dt_reg, &dt, nullptr))) return e;
-    s->dt = dt;
+    rmt3d_set_dt(s, dt);
     if ((e = rmt3d_init_iter(s))) return e;
-    s->dt = dt;  // stepper::run re-links dt (stepper.hh:336)
+    rmt3d_set_dt(s, dt);  // stepper::run re-links dt (stepper.hh:336)
     return RMT3D_OK;
 }
 
+// Steps run as graph launches unless a kernel profiler is active or graphs
+// are switched off (RMT3D_GRAPH=0); both forms issue the same kernels.
+static bool graph_mode(rmt3d_scene *s) { return s->use_graph && s->prof.target < 0; }
+
 extern "C" int rmt3d_step(rmt3d_scene *s, int debug, int *status) {
     if (!s || !status) return fail(RMT3D_ERR_INVALID, "null argument");
-    int e = step_forward(s, debug);
-    if (e < 0) {
-        *status = e;
-        return e;
+    if (graph_mode(s)) {
+        int e = run_graph(s, 1, status);
+        if (e < 0) *status = e;
+        return e < 0 ? e : RMT3D_OK;
     }
+    int e = step_forward(s, debug);
     *status = e;
-    return RMT3D_OK;
+    return e < 0 ? e : RMT3D_OK;
 }
 
 extern "C" int rmt3d_step_phases(rmt3d_scene *s, int last_phase, int *status) {
@@ -1015,6 +1307,12 @@ extern "C" int rmt3d_step_phases(rmt3d_scene *s, int last_phase, int *status) {
 extern "C" int rmt3d_run(rmt3d_scene *s, int nsteps, int *status) {
     if (!s || !status) return fail(RMT3D_ERR_INVALID, "null argument");
     *status = 0;
+    if (nsteps <= 0) return RMT3D_OK;
+    if (graph_mode(s)) {
+        int e = run_graph(s, nsteps, status);
+        if (e < 0) *status = e;
+        return e < 0 ? e : RMT3D_OK;
+    }
     for (int i = 0; i < nsteps; i++) {
         int e = rmt3d_step(s, 0, status);
         if (e) return e;
@@ -1022,6 +1320,32 @@ extern "C" int rmt3d_run(rmt3d_scene *s, int nsteps, int *status) {
     }
     return RMT3D_OK;
 }
+
+namespace rmt3d {
+int steps_launch(rmt3d_scene *s, int nsteps) {
+    pending_steps *p = pending_of(s);
+    *p = pending_steps{};
+    if (graph_mode(s)) return graph_launch(s, nsteps, *p);
+    p->eager_err = rmt3d_run(s, nsteps, &p->eager_status);
+    return 0;
+}
+
+int steps_finish(rmt3d_scene *s, int *status) {
+    pending_steps q = *pending_of(s);
+    for (size_t i = 0; i < t_pending.size(); i++)
+        if (t_pending[i].first == s) {
+            t_pending.erase(t_pending.begin() + i);
+            break;
+        }
+    if (!graph_mode(s)) {
+        *status = q.eager_status;
+        return q.eager_err;
+    }
+    int e = graph_finish(s, q, status);
+    if (e < 0) *status = e;
+    return e < 0 ? e : RMT3D_OK;
+}
+}  // namespace rmt3d
 
 extern "C" int rmt3d_get_scalar(rmt3d_scene *s, int which, double *v) {
     if (!s || !v) return fail(RMT3D_ERR_INVALID, "null argument");
@@ -1167,8 +1491,10 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
             for (int c = 0; c < 9; c++) CK(copy_sync(s, m.gp[c], GP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
         }
     }
-    s->dt = dt;
-    s->time = time;
+    rmt3d_set_dt(s, dt);
+    set_time(s, time);
+    s->graph_dirty = true;
+    CK(cudaStreamSynchronize(s->st));
     return RMT3D_OK;
 }
 
@@ -1249,12 +1575,18 @@ extern "C" int rmt3d_launch_count(rmt3d_scene *s, long long *count) {
     return RMT3D_OK;
 }
 
-extern "C" int rmt3d_scene_set_smoothing(rmt3d_scene *s, int v_down, int v_up) {
+extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     if (v_down < 0 || v_up < 0 || v_down + v_up < 1 || v_down > 8 || v_up > 8)
         return fail(RMT3D_ERR_INVALID, "smoothing counts outside 0..8 (sum >= 1)");
+    if (coarse_pts < 0) return fail(RMT3D_ERR_INVALID, "negative coarse level size");
     s->mac.v_down = s->fem.v_down = v_down;
     s->mac.v_up = s->fem.v_up = v_up;
+    s->mac.invalidate();
+    s->fem.invalidate();
+    s->graph_dirty = true;
+    if (coarse_pts > 0 && (s->mac.set_coarse(coarse_pts) || s->fem.set_coarse(coarse_pts)))
+        return fail(RMT3D_ERR_CUDA, "coarse multigrid kernel configuration failed");
     return RMT3D_OK;
 }
 
@@ -1266,7 +1598,7 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     b += (size_t)d->n_obj * n * (2 * sizeof(int) + 48 * sizeof(double));
     if (d->n_obj > 0) b += n * (2 * sizeof(uint8_t) + 2 * sizeof(int));
     b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);
-    b += sizeof(fields_dev) + 8 * sizeof(int) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);
+    b += sizeof(fields_dev) + sizeof(scene_ctl) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);
     int prd[3], nm[3], nf[3];
     for (int a = 0; a < 3; a++) {
         prd[a] = d->periodic[a] != 0;
@@ -1342,8 +1674,10 @@ extern "C" int rmt3d_scene_destroy(rmt3d_scene *s) {
     if (!s) return RMT3D_OK;
     cudaStreamSynchronize(s->st);
     for (cudaEvent_t e : s->prof.ev) cudaEventDestroy(e);
+    if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
+    s->gb.release();
     for (void *p : s->allocs) cudaFree(p);
-    if (s->h_counters) cudaFreeHost(s->h_counters);
+    if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->h_scalar) cudaFreeHost(s->h_scalar);
     if (s->own_stream) cudaStreamDestroy(s->st);
     delete s;

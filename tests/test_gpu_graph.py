@@ -1,0 +1,87 @@
+"""The step as one CUDA graph against the step issued kernel by kernel.
+
+The graph form captures the same kernels in the same order, with the
+multigrid cycle control and the step's branches evaluated on the device
+(WHILE and IF graph nodes).  Both forms must give bit-identical states,
+times, step counts and cycle counts, and the graph form must stop a run at
+the failing step exactly as the eager form does.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+import rmt3d_b200 as R
+from rmt3d_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(desc, graph):
+    old = os.environ.get("RMT3D_GRAPH")
+    os.environ["RMT3D_GRAPH"] = "1" if graph else "0"
+    try:
+        return R.Scene(desc)
+    finally:
+        if old is None:
+            del os.environ["RMT3D_GRAPH"]
+        else:
+            os.environ["RMT3D_GRAPH"] = old
+
+
+def _run(desc, graph, steps, chunks=1):
+    sc = _scene(desc, graph)
+    try:
+        sc.prepare()
+        l0 = sc.launches()
+        for _ in range(chunks):
+            assert sc.run(steps // chunks) == R.NORMAL_EXIT
+        out = {f: sc.field(f) for f in ("u", "v", "w", "p", "q", "dp")}
+        out["scalars"] = [sc.scalar(i) for i in (0, 1, 4, 5, 6, 7, 8)]
+        out["launches"] = sc.launches() - l0
+        if desc.n_obj:
+            out["x"] = sc.refmap(0)[1]
+        return out
+    finally:
+        sc.close()
+
+
+@pytest.mark.parametrize("kind", ["cavity", "sphere", "periodic_sphere", "mixed"])
+def test_graph_equals_eager(tmp_path, kind):
+    if kind == "cavity":
+        text = scenes.cavity(16, steps=6)
+    elif kind == "periodic_sphere":
+        text = scenes.stretched_sphere(24, steps=6, radius=0.2)
+    else:
+        text = scenes.cavity_sphere(24, steps=6, radius=0.25)
+    desc = R.desc_from_cfg(scenes.write(str(tmp_path / "g.cfg"), text))
+    if kind == "mixed":
+        desc.precision = R.MIXED
+    eager = _run(desc, False, 6)
+    graph = _run(desc, True, 6, chunks=2)
+    for k in eager:
+        if k == "launches":
+            continue
+        a, b = np.asarray(eager[k]), np.asarray(graph[k])
+        assert np.array_equal(a, b, equal_nan=True), k
+    # the graph adds its gate, branch and status kernels to every step
+    per_step = (graph["launches"] - eager["launches"]) / 6
+    assert per_step == (3 if desc.n_obj else 2), per_step
+
+
+def test_graph_run_stops_at_failing_step(tmp_path):
+    fx = H.load_fixture("cavity16")
+    sc = R.Scene.from_cfg(H.fixture_cfg(fx, str(tmp_path / "c16.cfg")))
+    try:
+        sc.prepare()
+        st0 = H.state(fx, 0)
+        fa, ra, ei, em = H.to_aos(st0)
+        so4, sn4, sm4 = st0["shape"]
+        fa["vel"][10 + sm4 * (10 + sn4 * 10), 0] = np.nan  # an interior cell
+        sc.import_reference(fa, ra, ei, em, H.state(fx, 1)["dt"], 0.0)
+        nt0 = sc.scalar(4)
+        assert sc.run(4) == R.PROJECTION_ERR
+        assert sc.scalar(4) == nt0 + 1  # the later steps did not run
+    finally:
+        sc.close()
