@@ -7,9 +7,14 @@ of radius 0.2 at the centre with G=1, solid density 1, transition width
 .cfg parameters.
 
 Our arm times the plain FP64 form and the mixed form (FP32 V-cycles inside
-FP64 refinement) on the device, then end to end through the C ABI with
-host-side result reads.  Multi-GPU runs one independent scene per rank
-(replicas: the path has no cross-scene exchange), timed as the max over ranks.
+FP64 refinement) on the device (K steps as K step-graph launches, CUDA events
+on the scene's stream), their per-step latency, then the headline form end to
+end through the C ABI with host-side result reads.  Two more forms are
+reported beside it: a batch of seeded scenes of uneven sizes stepped together,
+and a served Poisson request stream with admission by HBM footprint (p50/p99
+request and step latency) against the same stream run serially in FP64.
+Multi-GPU runs one independent scene per rank (replicas: the path has no
+cross-scene exchange), timed as the max over ranks.
 
 --impl reference times the reference's own CPU run_sim (oracle/_ref) on the
 same .cfg, one process per host core, with the reference's own step timer.
@@ -118,7 +123,7 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                       "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
@@ -153,6 +158,97 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def percentiles(xs):
+    import numpy as np
+    if not xs:
+        return None
+    return {"p50": float(np.percentile(xs, 50)), "p99": float(np.percentile(xs, 99))}
+
+
+def form_batched(R, args):
+    """Many independent seeded scenes (grid sizes from {32,48,64,96}, 1-8
+    spheres, lid speed U(0.5,1.5)), mixed precision, schedules autotuned per
+    grid size; every scene's step graph in flight at once.  Wall time around
+    the synchronous batch step (the scenes run on their own streams)."""
+    import numpy as np
+    wd = tempfile.mkdtemp(prefix="rmt3d_batch_")
+    descs, cells = [], 0
+    for seed in range(args.batch_scenes):
+        n, text = scenes.random_scene(seed, steps=100000)
+        d = R.desc_from_cfg(scenes.write(os.path.join(wd, "s%d.cfg" % seed), text))
+        d.precision = R.MIXED
+        descs.append(d)
+        cells += n ** 3
+    t0 = time.perf_counter()
+    b = R.Batch(descs)
+    b.prepare()
+    prep = time.perf_counter() - t0
+    tuned = b.autotune(probe_steps=2)
+    st = b.step(args.warmup)
+    if any(st):
+        raise RuntimeError("batched warm-up status %s" % st)
+    t0 = time.perf_counter()
+    st = b.step(args.steps)
+    wall = time.perf_counter() - t0
+    if any(st):
+        raise RuntimeError("batched step status %s" % st)
+    b.close()
+    return {"value": cells * args.steps / wall / 1e6, "unit": METRIC, "scenes": len(descs), "cells": cells,
+            "ms_per_batch_step": 1e3 * wall / args.steps, "timing": "wall clock around the synchronous batch step",
+            "prepare_s": prep, "schedules": {str(k): list(v) for k, v in tuned.items()},
+            "workload": "seeded cavities, n in {32,48,64,96}, 1-8 spheres R~U(0.08,0.15), G log-U[0.1,10], "
+                        "lid U(0.5,1.5), solid density 1, mixed precision"}
+
+
+def serve_stream(R, wd, seconds, rate, steps, seed, precision):
+    import random
+    rng = random.Random(seed)
+    sizes = [32] * 4 + [64] * 3 + [128] * 2 + [192]
+    t, reqs = 0.0, []
+    while True:
+        t += rng.expovariate(rate)
+        if t > seconds:
+            break
+        k = len(reqs)
+        n = rng.choice(sizes)
+        _, text = scenes.random_scene(seed * 100003 + k, sizes=(n,), steps=100000)
+        d = R.desc_from_cfg(scenes.write(os.path.join(wd, "r%d.cfg" % k), text))
+        d.precision = precision
+        reqs.append((t, steps, d))
+    return reqs
+
+
+def form_served(R, args):
+    """Seeded Poisson stream (lambda = 20 requests/s), grid sizes 32/64/128/192
+    in ratio 4:3:2:1, each request set up and stepped `serve_steps` steps,
+    admitted by HBM footprint; against the same stream run serially in FP64."""
+    import torch
+    wd = tempfile.mkdtemp(prefix="rmt3d_serve_")
+    free, total = torch.cuda.mem_get_info()
+    budget = int(min(free * 0.8, 120e9))
+    reqs = serve_stream(R, wd, args.serve_seconds, 20.0, args.serve_steps, 7, R.MIXED)
+    res, summ = R.serve(reqs, budget, args.serve_slots)
+    bad = [r["status"] for r in res if r["status"] != 0]
+    if bad:
+        raise RuntimeError("served requests failed: %s" % bad)
+    cells = sum(d.sys_size[0] * d.sys_size[1] * d.sys_size[2] * n for _, n, d in reqs)
+    # the same stream, plain FP64, one request after another
+    serial = serve_stream(R, wd, args.serve_seconds, 20.0, args.serve_steps, 7, R.FP64)
+    for i in range(len(serial)):
+        serial[i] = (0.0, serial[i][1], serial[i][2])
+    res_s, summ_s = R.serve(serial, budget, 1)
+    return {"value": summ["cellsteps_per_s"] / 1e6, "unit": METRIC, "requests": len(reqs),
+            "request_latency_s": {"p50": summ["request_p50_s"], "p99": summ["request_p99_s"]},
+            "step_latency_ms": {"p50": summ["step_p50_ms"], "p99": summ["step_p99_ms"]},
+            "wall_s": summ["wall_s"], "hbm_budget_gb": budget / 1e9, "slots": args.serve_slots,
+            "serial_fp64": {"value": summ_s["cellsteps_per_s"] / 1e6, "wall_s": summ_s["wall_s"],
+                            "step_latency_ms": {"p50": summ_s["step_p50_ms"], "p99": summ_s["step_p99_ms"]}},
+            "cellsteps": cells,
+            "workload": "Poisson arrivals 20/s for %g s, n in {32,64,128,192} 4:3:2:1, %d steps each (set-up "
+                        "included in the latency), mixed precision; serial_fp64 = the same stream one request at "
+                        "a time in FP64" % (args.serve_seconds, args.serve_steps)}
 
 
 def run_ours(args):
@@ -194,61 +290,95 @@ def run_ours(args):
         sc.prepare()
         return sc
 
-    def timed(sc, k, e2e=False, bufs=None):
-        for _ in range(args.warmup):
-            sc.step_forward(0)
+    def timed(sc, k):
+        """k steps as one run (k step-graph launches, one wait), CUDA events
+        on the scene's stream."""
+        if sc.run(args.warmup) != R.NORMAL_EXIT:
+            raise RuntimeError("warm-up step failed")
         barrier()
         l0 = sc.launches()
         start = torch.cuda.Event(enable_timing=True)
         stop = torch.cuda.Event(enable_timing=True)
-        t0 = time.perf_counter()
         start.record(stream)
-        for _ in range(k):
-            if e2e:
-                sc.set_dt(sc.dt)  # the step's host input
-            code = sc.step_forward(0)
-            if code != R.NORMAL_EXIT:
-                raise RuntimeError("step returned %d" % code)
-            if e2e:
-                for j, nm in enumerate(("u", "v", "w", "p")):
-                    R.lib().rmt3d_get_field(sc._h, R.FIELD_INDEX[nm], bufs[j].data_ptr())
+        code = sc.run(k)
         stop.record(stream)
         stop.synchronize()
-        wall = time.perf_counter() - t0
+        if code != R.NORMAL_EXIT:
+            raise RuntimeError("step returned %d" % code)
         ms = start.elapsed_time(stop)
         barrier()
-        return max_over_ranks(ms), sc.launches() - l0, wall
+        return max_over_ranks(ms), sc.launches() - l0
+
+    def step_latency(sc, k):
+        """per-step latency: one step per call (launch + wait), CUDA events"""
+        out = []
+        for _ in range(k):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            if sc.step_forward(0) != R.NORMAL_EXIT:
+                raise RuntimeError("step failed")
+            b.record(stream)
+            b.synchronize()
+            out.append(a.elapsed_time(b))
+        return percentiles(out)
+
+    def e2e(sc, k, bufs):
+        """through the public API with host buffers: dt in, u/v/w/p out to
+        pinned host memory every step"""
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        barrier()
+        start.record(stream)
+        for _ in range(k):
+            sc.set_dt(sc.dt)
+            if sc.step_forward(0) != R.NORMAL_EXIT:
+                raise RuntimeError("step failed")
+            for j, nm in enumerate(("u", "v", "w", "p")):
+                R.lib().rmt3d_get_field(sc._h, R.FIELD_INDEX[nm], bufs[j].data_ptr())
+        stop.record(stream)
+        stop.synchronize()
+        barrier()
+        return max_over_ranks(start.elapsed_time(stop))
 
     cells = n ** 3
     # plain FP64 form
     s64 = make(R.FP64)
     with ClockSampler(local) as clk:
-        ms64, launches64, _ = timed(s64, args.steps)
+        ms64, launches64 = timed(s64, args.steps)
     clocks = clk.summary()
     v64 = world * cells * args.steps / (ms64 / 1e3) / 1e6
+    lat64 = step_latency(s64, max(5, args.steps // 2))
     # mixed form (FP32 V-cycles inside FP64 iterative refinement)
     smx = make(R.MIXED)
-    msmx, launchesmx, _ = timed(smx, args.steps)
+    msmx, launchesmx = timed(smx, args.steps)
     vmx = world * cells * args.steps / (msmx / 1e3) / 1e6
+    latmx = step_latency(smx, max(5, args.steps // 2))
+    # both scenes have now run the same number of steps from the same state
     sl = (slice(2, -2),) * 3
-    ref = np.stack([s64.field(c)[sl] for c in "uvw"])
-    got = np.stack([smx.field(c)[sl] for c in "uvw"])
-    mixed_err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
-    p_err = float(np.linalg.norm(smx.field("p")[sl] - s64.field("p")[sl]) / np.linalg.norm(s64.field("p")[sl]))
-    mixed_ok = max(mixed_err, p_err) <= 1e-5
+    errs = {}
+    for f in ("u", "v", "w", "p"):
+        a, b = s64.field(f)[sl], smx.field(f)[sl]
+        errs[f] = float(np.linalg.norm(b - a) / np.linalg.norm(a))
+    mixed_ok = max(errs.values()) <= 1e-5
     head_form = "mixed" if (mixed_ok and vmx > v64) else "fp64"
     value = vmx if head_form == "mixed" else v64
     ms = msmx if head_form == "mixed" else ms64
     launches = launchesmx if head_form == "mixed" else launches64
-    # end to end through the C ABI: host dt in, u/v/w/p out to pinned host memory
     shp = (s64.so4, s64.sn4, s64.sm4)
     bufs = [torch.empty(shp, dtype=torch.float64, pin_memory=True) for _ in range(4)]
     sce = smx if head_form == "mixed" else s64
-    mse, _, wall_e = timed(sce, args.steps, e2e=True, bufs=bufs)
+    mse = e2e(sce, args.steps, bufs)
     ve = world * cells * args.steps / (mse / 1e3) / 1e6
     d2h = 4 * s64.ncell * 8
-    # roofline of the dominant kernel
     roof = roofline(R, sce, args)
+    for s_ in (s64, smx):
+        s_.close()
+    batched = served = None
+    if world == 1 and not args.no_batched:
+        batched = form_batched(R, args)
+    if world == 1 and not args.no_served:
+        served = form_served(R, args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and os.path.exists(RUN_SIM):
         procs = max(1, min(host_cores(), args.ref_procs))
@@ -262,12 +392,14 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if head_form == "fp64" else "f64+f32",
             "data": "synthetic (cfg-defined scene, no dataset)",
-            "config": dict(config_block(n, "state %.0f MB per scene > 126 MB L2" % (state_mb(s64))),
+            "config": dict(config_block(n, "state %.0f MB per scene > 126 MB L2" % (state_mb_desc(R, cfg))),
                            headline_form=head_form),
-            "forms": {"fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "gpu_launches": launches64},
+            "forms": {"fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "gpu_launches": launches64,
+                               "step_latency_ms": lat64},
                       "mixed": {"value": vmx, "ms_per_step": msmx / args.steps, "gpu_launches": launchesmx,
-                                "rel_l2_vel_vs_fp64": mixed_err, "rel_l2_p_vs_fp64": p_err,
-                                "steps_compared": args.warmup + args.steps}},
+                                "step_latency_ms": latmx, "rel_l2_vs_fp64": errs,
+                                "steps_compared": 2 * args.warmup + args.steps + max(5, args.steps // 2)},
+                      "batched": batched, "served": served},
             "e2e": {"value": ve, "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": roof,
@@ -275,15 +407,12 @@ def run_ours(args):
             "clocks": clocks,
         }
         print(json.dumps(line))
-    for s in (s64, smx):
-        s.close()
     if dist is not None:
         dist.destroy_process_group()
 
 
-def state_mb(sc):
-    per_cell = (36 + 50 * sc.desc.n_obj) * 8
-    return sc.ncell * per_cell / 1e6
+def state_mb_desc(R, cfg):
+    return R.footprint(R.desc_from_cfg(cfg)) / 1e6
 
 
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "traffic.json")
@@ -321,13 +450,19 @@ def roofline(R, sc, args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=64)
     ap.add_argument("--ref-procs", type=int, default=16)
     ap.add_argument("--ref-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--batch-scenes", type=int, default=32)
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--serve-steps", type=int, default=20)
+    ap.add_argument("--serve-slots", type=int, default=16)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -241,7 +241,7 @@ int rmt3d_batch_destroy(rmt3d_batch *b);
 
 /* Multigrid schedule of one scene: V(v_down, v_up) smoothing counts, and the
  * largest level (points) whose whole sub-cycle runs in one thread block out of
- * shared memory (0 keeps the current value). */
+ * shared memory (0: none; negative keeps the current value). */
 int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts);
 
 /* Device bytes a scene with this descriptor allocates (admission control). */

@@ -189,9 +189,10 @@ class Scene:
         _lib.check(lib().rmt3d_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(b)))
         return ms.value, n.value, b.value
 
-    def set_schedule(self, v_down, v_up, coarse_pts=0):
+    def set_schedule(self, v_down, v_up, coarse_pts=-1):
         """Multigrid V(v_down, v_up) smoothing counts of both solvers and the
-        largest level run by the one-block coarse sub-cycle (0 keeps it)."""
+        largest level run by the one-block coarse sub-cycle (0: none,
+        negative keeps it)."""
         _lib.check(lib().rmt3d_scene_set_schedule(self._h, v_down, v_up, coarse_pts))
 
     def checksum(self):

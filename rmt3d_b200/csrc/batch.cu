@@ -166,7 +166,7 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
     static const int smooth[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
-    static const int coarse[] = {1000, 5000};
+    static const int coarse[] = {0, 5000};
     std::map<long long, int> first;
     for (size_t i = 0; i < b->descs.size(); i++)
         if (!first.count(cells(b->descs[i]))) first[cells(b->descs[i])] = (int)i;
@@ -180,7 +180,7 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
             return e;
         }
         double best = 1e300;
-        int bd = 2, bu = 2, bc = 5000;
+        int bd = 2, bu = 2, bc = 0;
         for (int cp : coarse)
             for (auto &c : smooth) {
                 if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], cp))) {

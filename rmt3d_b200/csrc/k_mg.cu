@@ -22,6 +22,9 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "host_common.h"
@@ -354,10 +357,34 @@ static void host_stencil_row(mg_kind kind, const mg_level &L, int i, int j, int 
 // (alpha/n) 1 1^T with alpha = mean diagonal makes the matrix SPD and its
 // inverse maps every right-hand side to the solution of the projected system
 // that is orthogonal to the constants.
+// Process-wide cache of coarsest-level inverses: every solver whose coarsest
+// level has the same kind, shape and periodicity on the same device shares
+// one device copy (they are read-only), so creating many scenes of a few
+// grid sizes inverts each matrix once.
+namespace {
+struct dense_key {
+    int dev, kind, n0, n1, n2, p0, p1, p2;
+    bool operator<(const dense_key &o) const {
+        return std::tie(dev, kind, n0, n1, n2, p0, p1, p2) < std::tie(o.dev, o.kind, o.n0, o.n1, o.n2, o.p0, o.p1, o.p2);
+    }
+};
+std::mutex g_dense_mu;
+std::map<dense_key, double *> g_dense;
+}  // namespace
+
 int mg_solver::build_dense(cudaStream_t st) {
     const mg_level &L = lv.back();
     const int np = (int)L.npts();
-    if (np > 1024) return 0;  // Gauss-Seidel fallback (mg_solver::footprint uses the same bound)
+    if (np > kDenseMax) return 0;  // Gauss-Seidel fallback
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const dense_key key{dev, (int)kind, L.n[0], L.n[1], L.n[2], L.prd[0], L.prd[1], L.prd[2]};
+    std::lock_guard<std::mutex> lk(g_dense_mu);
+    auto it = g_dense.find(key);
+    if (it != g_dense.end()) {
+        dense = it->second;
+        return 0;
+    }
     std::vector<double> A((size_t)np * np, 0.0), row(np);
     double dsum = 0, rsum_max = 0;
     for (int k = 0; k < L.n[2]; k++)
@@ -393,23 +420,21 @@ int mg_solver::build_dense(cudaStream_t st) {
         double d = A[(size_t)col * np + col];
         if (d == 0) return 0;  // keep the Gauss-Seidel fallback
         double inv = 1 / d;
-        for (int c = 0; c < np; c++) {
-            A[(size_t)col * np + c] *= inv;
-            B[(size_t)col * np + c] *= inv;
-        }
+        // columns left of col are already unit vectors in A
+        for (int c = col; c < np; c++) A[(size_t)col * np + c] *= inv;
+        for (int c = 0; c < np; c++) B[(size_t)col * np + c] *= inv;
         for (int r = 0; r < np; r++) {
             if (r == col) continue;
             double f = A[(size_t)r * np + col];
             if (f == 0) continue;
-            for (int c = 0; c < np; c++) {
-                A[(size_t)r * np + c] -= f * A[(size_t)col * np + c];
-                B[(size_t)r * np + c] -= f * B[(size_t)col * np + c];
-            }
+            for (int c = col; c < np; c++) A[(size_t)r * np + c] -= f * A[(size_t)col * np + c];
+            for (int c = 0; c < np; c++) B[(size_t)r * np + c] -= f * B[(size_t)col * np + c];
         }
     }
     if (cudaMalloc(&dense, B.size() * sizeof(double)) != cudaSuccess) return 1;
     cudaMemcpyAsync(dense, B.data(), B.size() * sizeof(double), cudaMemcpyHostToDevice, st);
     cudaStreamSynchronize(st);
+    g_dense[key] = dense;
     return 0;
 }
 
@@ -445,7 +470,6 @@ mg_solver::~mg_solver() {
         cudaFree(l.ress);
     }
     cudaFree(d_max);
-    cudaFree(dense);
     invalidate();
     if (own_gb) {
         own_gb->release();
@@ -464,7 +488,7 @@ int mg_solver::plan(mg_kind k, const int n[3], const int prd[3], std::vector<mg_
     lv.push_back(L0);
     while (true) {
         const mg_level &f = lv.back();
-        if (f.npts() <= 128) break;
+        if (f.npts() <= (size_t)kDensePts) break;  // solved exactly by the dense inverse
         mg_level c;
         bool ok = true;
         for (int d = 0; d < 3; d++) {
@@ -494,7 +518,8 @@ size_t mg_solver::footprint(mg_kind k, const int n[3], const int prd[3], bool mi
     if (plan(k, n, prd, v)) return 0;
     size_t b = 0;
     for (auto &l : v) b += l.npts() * (3 * sizeof(double) + (mixed_form ? 3 * sizeof(float) : 0));
-    if (v.back().npts() <= 1024) b += v.back().npts() * v.back().npts() * sizeof(double);  // coarsest inverse
+    // the coarsest-level inverse is shared by all solvers with that level
+    // (one copy per distinct level shape in the process) and not counted here
     return b + sizeof(double);
 }
 
@@ -527,7 +552,6 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
         }
     }
     if (build_dense(st)) return fail(RMT3D_ERR_OOM, "coarse inverse allocation failed");
-    if (dense) bytes_alloc += lv.back().npts() * lv.back().npts() * sizeof(double);
     if (set_coarse(coarse_pts)) return fail(RMT3D_ERR_CUDA, "coarse multigrid kernel configuration failed");
     if (cudaMalloc(&d_max, sizeof(unsigned long long)) != cudaSuccess)
         return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
@@ -571,13 +595,23 @@ void mg_solver::smooth(int l, int sweeps, cudaStream_t st) {
 void mg_solver::smooth_f32(int l, int sweeps, cudaStream_t st) {
     mg_level &L = lv[l];
     lvl_dev d = dev_of(L);
+    const double npts = (double)L.npts();
+    const bool timed = prof && l == 0 && prof->target == (kind == MG_FEM ? 0 : 1);
     for (int s = 0; s < sweeps; s++) {
         if (kind == MG_MAC) {
             dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
-            for (int c = 0; c < 2; c++) LAUNCH(k_mac_rb<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+            for (int c = 0; c < 2; c++) {
+                if (timed) prof->begin(st);
+                LAUNCH(k_mac_rb<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+                if (timed) prof->end(st, npts / 2, 4.0 * (npts + npts / 2 + npts / 2));
+            }
         } else {
             dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, (L.n[2] + 1) / 2);
-            for (int c = 0; c < 4; c++) LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+            for (int c = 0; c < 4; c++) {
+                if (timed) prof->begin(st);
+                LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+                if (timed) prof->end(st, npts / 4, 4.0 * (npts + npts / 4 + npts / 4));
+            }
         }
     }
 }
@@ -615,7 +649,7 @@ void mg_solver::cycle(int l, cudaStream_t st) {
         return;
     }
     if (l == (int)lv.size() - 1) {
-        if (dense) LAUNCH(k_coarse_dense<double><<<16, 256, 0, st>>>((int)F.npts(), dense, F.x, F.r));
+        if (dense) LAUNCH(k_coarse_dense<double><<<((int)F.npts() + 7) / 8, 256, 0, st>>>((int)F.npts(), dense, F.x, F.r));
         else if (kind == MG_MAC) LAUNCH(k_coarse_solve<double, 0><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
         else LAUNCH(k_coarse_solve<double, 1><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
         return;
@@ -645,7 +679,7 @@ void mg_solver::cycle_f32(int l, cudaStream_t st) {
         return;
     }
     if (l == (int)lv.size() - 1) {
-        if (dense) LAUNCH(k_coarse_dense<float><<<16, 256, 0, st>>>((int)F.npts(), dense, F.xs, F.rs));
+        if (dense) LAUNCH(k_coarse_dense<float><<<((int)F.npts() + 7) / 8, 256, 0, st>>>((int)F.npts(), dense, F.xs, F.rs));
         else if (kind == MG_MAC) LAUNCH(k_coarse_solve<float, 0><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
         else LAUNCH(k_coarse_solve<float, 1><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
         return;
@@ -825,7 +859,7 @@ void mg_solver::sync_host_mirror() {
 }
 
 double mg_solver::run(cudaStream_t st) {
-    const bool host_loop = prof && prof->target >= 0;
+    const bool host_loop = !use_graph || (prof && prof->target >= 0);
     if (host_loop) {
         // launch by launch, so that the profiler's events bracket single kernels
         k_mg_begin<<<1, 1, 0, st>>>(ctl, d_max, 0, 0);

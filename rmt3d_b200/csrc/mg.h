@@ -84,6 +84,7 @@ class mg_solver {
     kernel_profiler *prof = nullptr;
     mg_ctl *ctl = nullptr;       // device control block (owned by the scene)
     mg_ctl *h_ctl = nullptr;     // pinned mirror (owned by the scene)
+    bool use_graph = true;       // false: run() issues every kernel from the host
 
     mg_solver() = default;
     mg_solver(const mg_solver &) = delete;
@@ -100,7 +101,7 @@ class mg_solver {
     double *sol() { return lv[0].x; }
     double *dense = nullptr;  // inverse of the coarsest operator (row-major), or null
     int cf = 0;  // first level whose whole sub-cycle runs in one CTA
-    int coarse_pts = 1000;  // largest level handed to the one-CTA sub-cycle
+    int coarse_pts = 0;  // largest level handed to the one-CTA sub-cycle (0: none)
     int set_coarse(int pts);
 
     // One solve with the reference's control logic, issued eagerly and

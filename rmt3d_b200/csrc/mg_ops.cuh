@@ -98,6 +98,8 @@ __device__ __forceinline__ T fem_offdiag(const lvl_dev L, const T *__restrict__ 
 
 
 constexpr int kMaxLev = 12;
+constexpr int kDensePts = 1000;  // coarsening stops at the first level with at most this many points
+constexpr int kDenseMax = 1024;  // largest level solved by a dense inverse
 constexpr int kThreads = 256;
 
 struct pmg_level {

@@ -1188,6 +1188,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     {
         const char *ge = getenv("RMT3D_GRAPH");
         s->use_graph = !(ge && ge[0] == '0');
+        s->mac.use_graph = s->fem.use_graph = s->use_graph;
     }
     cudaMemcpyAsync(s->lx, s->hlx.data(), g.sm4 * 8, cudaMemcpyHostToDevice, s->st);
     cudaMemcpyAsync(s->ly, s->hly.data(), g.sn4 * 8, cudaMemcpyHostToDevice, s->st);
@@ -1579,13 +1580,12 @@ extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, in
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     if (v_down < 0 || v_up < 0 || v_down + v_up < 1 || v_down > 8 || v_up > 8)
         return fail(RMT3D_ERR_INVALID, "smoothing counts outside 0..8 (sum >= 1)");
-    if (coarse_pts < 0) return fail(RMT3D_ERR_INVALID, "negative coarse level size");
     s->mac.v_down = s->fem.v_down = v_down;
     s->mac.v_up = s->fem.v_up = v_up;
     s->mac.invalidate();
     s->fem.invalidate();
     s->graph_dirty = true;
-    if (coarse_pts > 0 && (s->mac.set_coarse(coarse_pts) || s->fem.set_coarse(coarse_pts)))
+    if (coarse_pts >= 0 && (s->mac.set_coarse(coarse_pts) || s->fem.set_coarse(coarse_pts)))
         return fail(RMT3D_ERR_CUDA, "coarse multigrid kernel configuration failed");
     return RMT3D_OK;
 }

@@ -1,9 +1,11 @@
 """Profiling driver: set up the bench workload, step once, then run N steps.
 
-    python -m rmt3d_b200.prof_step [n=64] [steps=2] [precision=0]
+    RMT3D_GRAPH=0 python -m rmt3d_b200.prof_step [n=64] [steps=2] [precision=0]
 
 Prints PREP_LAUNCHES (kernel launches before the profiled steps, for ncu -s)
-and STEP_LAUNCHES (launches of the profiled steps, for ncu -c).
+and STEP_LAUNCHES (launches of the profiled steps, for ncu -c).  ncu cannot
+profile kernels inside graphs that hold conditional nodes, so profiling runs
+use RMT3D_GRAPH=0: the same kernels issued one by one from the host.
 """
 import sys, os, tempfile
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
