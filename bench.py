@@ -169,7 +169,8 @@ def percentiles(xs):
 
 def form_batched(R, args):
     """Many independent seeded scenes (grid sizes from {32,48,64,96}, 1-8
-    spheres, lid speed U(0.5,1.5)), mixed precision, schedules autotuned per
+    spheres with solid density U(0.8,1.2), lid speed U(0.5,1.5)),
+    variable-density projection, mixed precision, schedules autotuned per
     grid size; every scene's step graph in flight at once.  Wall time around
     the synchronous batch step (the scenes run on their own streams)."""
     import numpy as np
@@ -179,6 +180,7 @@ def form_batched(R, args):
         n, text = scenes.random_scene(seed, steps=100000)
         d = R.desc_from_cfg(scenes.write(os.path.join(wd, "s%d.cfg" % seed), text))
         d.precision = R.MIXED
+        d.var_den = 1  # solid densities U(0.8, 1.2): the variable-density projection
         descs.append(d)
         cells += n ** 3
     t0 = time.perf_counter()
@@ -199,7 +201,7 @@ def form_batched(R, args):
             "ms_per_batch_step": 1e3 * wall / args.steps, "timing": "wall clock around the synchronous batch step",
             "prepare_s": prep, "schedules": {str(k): list(v) for k, v in tuned.items()},
             "workload": "seeded cavities, n in {32,48,64,96}, 1-8 spheres R~U(0.08,0.15), G log-U[0.1,10], "
-                        "lid U(0.5,1.5), solid density 1, mixed precision"}
+                        "lid U(0.5,1.5), solid density U(0.8,1.2) (variable-density projection), mixed precision"}
 
 
 def serve_stream(R, wd, seconds, rate, steps, seed, precision):
@@ -216,6 +218,7 @@ def serve_stream(R, wd, seconds, rate, steps, seed, precision):
         _, text = scenes.random_scene(seed * 100003 + k, sizes=(n,), steps=100000)
         d = R.desc_from_cfg(scenes.write(os.path.join(wd, "r%d.cfg" % k), text))
         d.precision = precision
+        d.var_den = 1
         reqs.append((t, steps, d))
     return reqs
 

@@ -37,7 +37,7 @@ namespace rmt3d {
 
 // ---- smoothing -------------------------------------------------------------
 template <typename T>
-__global__ void k_mac_rb(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int colour) {
+__global__ void k_mac_rb(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int colour, const T *__restrict__ ri) {
     int hi = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y * blockDim.y + threadIdx.y;
     int k = blockIdx.z * blockDim.z + threadIdx.z;
@@ -45,7 +45,7 @@ __global__ void k_mac_rb(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, 
     int i = 2 * hi + ((j + k + colour) & 1);
     if (i >= L.n0) return;
     T diag;
-    T s = mac_offdiag(L, x, i, j, k, diag);
+    T s = ri ? mac_offdiag_vd(L, x, ri, i, j, k, diag) : mac_offdiag(L, x, i, j, k, diag);
     int id = i + L.n0 * (j + L.n1 * k);
     x[id] = (r[id] - s) / diag;
 }
@@ -55,13 +55,13 @@ __global__ void k_mac_rb(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, 
 // puts two coupled nodes in one colour: four colour passes are an exact
 // Gauss-Seidel sweep.
 template <typename T>
-__global__ void k_fem_gs(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int colour) {
+__global__ void k_fem_gs(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, int colour, const T *__restrict__ ri) {
     int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + (colour & 1);
     int j = 2 * (blockIdx.y * blockDim.y + threadIdx.y) + ((colour >> 1) & 1);
     int k = blockIdx.z * blockDim.z + threadIdx.z;
     if (i >= L.n0 || j >= L.n1 || k >= L.n2) return;
     T diag;
-    T s = fem_offdiag(L, x, i, j, k, diag);
+    T s = ri ? fem_offdiag_vd(L, x, ri, i, j, k, diag) : fem_offdiag(L, x, i, j, k, diag);
     int id = i + L.n0 * (j + L.n1 * k);
     x[id] = (r[id] - s) / diag;
 }
@@ -69,14 +69,14 @@ __global__ void k_fem_gs(lvl_dev L, T *__restrict__ x, const T *__restrict__ r, 
 // residual res = r - A x, and max |res| into *mx (as ordered bit pattern)
 template <typename T, int KIND>
 __global__ void k_resid(lvl_dev L, const T *__restrict__ x, const T *__restrict__ r, T *__restrict__ res,
-                        unsigned long long *mx) {
+                        unsigned long long *mx, const T *__restrict__ ri) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y * blockDim.y + threadIdx.y;
     int k = blockIdx.z * blockDim.z + threadIdx.z;
     double a = 0;
     if (i < L.n0 && j < L.n1 && k < L.n2) {
         T diag;
-        T s = (KIND == 0) ? mac_offdiag(L, x, i, j, k, diag) : fem_offdiag(L, x, i, j, k, diag);
+        T s = op_offdiag<T>(KIND, L, x, ri, i, j, k, diag);
         int id = i + L.n0 * (j + L.n1 * k);
         T v = r[id] - s - diag * x[id];
         if (res) res[id] = v;
@@ -441,7 +441,8 @@ int mg_solver::build_dense(cudaStream_t st) {
 // Choose the first level of the one-CTA coarse sub-cycle: the finest level
 // with at most `pts` points whose sub-hierarchy fits the shared-memory cap.
 int mg_solver::set_coarse(int pts) {
-    coarse_pts = pts;
+    coarse_pts = vd ? 0 : pts;
+    pts = coarse_pts;
     invalidate();
     cf = (int)lv.size() - 1;
     for (int l = 0; l < (int)lv.size(); l++)
@@ -578,14 +579,14 @@ void mg_solver::smooth(int l, int sweeps, cudaStream_t st) {
             dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 2; c++) {
                 if (timed) prof->begin(st);
-                LAUNCH(k_mac_rb<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c));
+                LAUNCH(k_mac_rb<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c, L.ri));
                 if (timed) prof->end(st, npts / 2, 8.0 * (npts + npts / 2 + npts / 2));
             }
         } else {
             dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 4; c++) {
                 if (timed) prof->begin(st);
-                LAUNCH(k_fem_gs<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c));
+                LAUNCH(k_fem_gs<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c, L.ri));
                 if (timed) prof->end(st, npts / 4, 8.0 * (npts + npts / 4 + npts / 4));
             }
         }
@@ -602,14 +603,14 @@ void mg_solver::smooth_f32(int l, int sweeps, cudaStream_t st) {
             dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 2; c++) {
                 if (timed) prof->begin(st);
-                LAUNCH(k_mac_rb<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+                LAUNCH(k_mac_rb<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c, L.ris));
                 if (timed) prof->end(st, npts / 2, 4.0 * (npts + npts / 2 + npts / 2));
             }
         } else {
             dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 4; c++) {
                 if (timed) prof->begin(st);
-                LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c));
+                LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c, L.ris));
                 if (timed) prof->end(st, npts / 4, 4.0 * (npts + npts / 4 + npts / 4));
             }
         }
@@ -659,10 +660,10 @@ void mg_solver::cycle(int l, cudaStream_t st) {
     lvl_dev cd = dev_of(C);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
     if (kind == MG_MAC) {
-        LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
+        LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
         LAUNCH(k_mac_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r, C.x));
     } else {
-        LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
+        LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
         LAUNCH(k_fem_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r, C.x));
     }
     cycle(l + 1, st);
@@ -689,10 +690,10 @@ void mg_solver::cycle_f32(int l, cudaStream_t st) {
     lvl_dev cd = dev_of(C);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
     if (kind == MG_MAC) {
-        LAUNCH((k_resid<float, 0><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr)));
+        LAUNCH((k_resid<float, 0><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr, F.ris)));
         LAUNCH(k_mac_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs, C.xs));
     } else {
-        LAUNCH((k_resid<float, 1><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr)));
+        LAUNCH((k_resid<float, 1><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr, F.ris)));
         LAUNCH(k_fem_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs, C.xs));
     }
     cycle_f32(l + 1, st);
@@ -709,8 +710,8 @@ void mg_solver::refine_step(cudaStream_t st) {
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]);
     size_t n = F.npts();
     unsigned nb = (unsigned)((n + 255) / 256);
-    if (kind == MG_MAC) LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
-    else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr)));
+    if (kind == MG_MAC) LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
+    else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
     LAUNCH(k_to_f32<<<nb, 256, 0, st>>>(F.res, F.rs, n));
     LAUNCH(k_zero<float><<<nb, 256, 0, st>>>(F.xs, n));
     cycle_f32(0, st);
@@ -808,8 +809,8 @@ void mg_solver::launch_body(cudaStream_t st, bool armed, unsigned long long h) {
     mg_level &F = lv[0];
     lvl_dev fd = dev_of(F);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]);
-    if (kind == MG_MAC) LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, d_max)));
-    else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, d_max)));
+    if (kind == MG_MAC) LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, d_max, F.ri)));
+    else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, d_max, F.ri)));
     LAUNCH(k_mg_ctl<<<1, 1, 0, st>>>(ctl, d_max, max_norm_tol, exact ? 1 : 0, h, armed ? 1 : 0));
 }
 

@@ -41,6 +41,10 @@ struct mg_level {
     double *r = nullptr;    // source
     double *res = nullptr;  // residual scratch
     float *xs = nullptr, *rs = nullptr, *ress = nullptr;  // FP32 copies (mixed form)
+    // variable density: 1/rho per cell of the level (shared with the other
+    // solver of the scene), FP64 and FP32; null for constant density
+    const double *ri = nullptr;
+    const float *ris = nullptr;
     size_t npts() const { return (size_t)n[0] * n[1] * n[2]; }
 };
 
@@ -85,6 +89,7 @@ class mg_solver {
     mg_ctl *ctl = nullptr;       // device control block (owned by the scene)
     mg_ctl *h_ctl = nullptr;     // pinned mirror (owned by the scene)
     bool use_graph = true;       // false: run() issues every kernel from the host
+    bool vd = false;             // variable density: levels carry 1/rho (no one-block coarse sub-cycle)
 
     mg_solver() = default;
     mg_solver(const mg_solver &) = delete;

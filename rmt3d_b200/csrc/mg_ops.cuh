@@ -97,6 +97,132 @@ __device__ __forceinline__ T fem_offdiag(const lvl_dev L, const T *__restrict__ 
 }
 
 
+// ---- variable density (VAR_DEN) ---------------------------------------------
+// ri: 1/rho per cell of the level (cell-centred, MAC level dimensions; for a
+// FEM level with n nodes per axis there are n-1 cells on a walled axis and n
+// on a periodic one).  Coarse levels carry the mean of their 8 children.
+
+// var_den_mac::set_stencils (Utilities/mg_probs.cc:196-308): each face
+// coefficient is the mean of 1/rho of the two cells it joins; the centre is
+// the (Neumann-fixed) centre entry times the mean of the face coefficients,
+// accumulated direction by direction as the reference does.
+template <typename T>
+__device__ __forceinline__ T mac_offdiag_vd(const lvl_dev L, const T *__restrict__ x, const T *__restrict__ ri, int i,
+                                            int j, int k, T &diag) {
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int c[3] = {i, j, k};
+    const int st[3] = {1, L.n0, L.n0 * L.n1};
+    const int base = i + L.n0 * (j + L.n1 * k);
+    const T rc = ri[base];
+    T s = 0, csum = 0;
+    int cnt = 0;
+    for (int d = 0; d < 3; d++) {
+        const int lo = wrapi(c[d] - 1, n[d], p[d]), hi = wrapi(c[d] + 1, n[d], p[d]);
+        const int il = base + (lo - c[d]) * st[d], ih = base + (hi - c[d]) * st[d];
+        if (lo >= 0 && hi >= 0) {
+            const T a1 = (T)0.5 * (ri[il] + rc), a2 = (T)0.5 * (rc + ri[ih]);
+            s += a1 * x[il] + a2 * x[ih];
+            csum += a1 + a2;
+            cnt += 2;
+        } else if (lo >= 0) {
+            const T a1 = (T)0.5 * (ri[il] + rc);
+            s += a1 * x[il];
+            csum += a1;
+            cnt += 1;
+        } else if (hi >= 0) {
+            const T a2 = (T)0.5 * (rc + ri[ih]);
+            s += a2 * x[ih];
+            csum += a2;
+            cnt += 1;
+        }
+    }
+    diag = (T)(-cnt) * (csum / (T)cnt);
+    return s;
+}
+
+// var_den_fem::set_stencils (Utilities/mg_probs.cc:97-150): every entry of the
+// (boundary-halved) Q1 stencil is scaled by the mean of 1/rho over the cells
+// adjacent to both the node and that neighbour -- 1 cell for a corner
+// neighbour, 2 for an edge neighbour, all (up to 8) for the centre -- summed
+// in the reference's cell order.
+template <typename T>
+__device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict__ x, const T *__restrict__ ri, int i,
+                                            int j, int k, T &diag) {
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int nc[3] = {p[0] ? n[0] : n[0] - 1, p[1] ? n[1] : n[1] - 1, p[2] ? n[2] : n[2] - 1};
+    const int c[3] = {i, j, k};
+    int cell[3][2];  // cells below / above the node on each axis (-1: none)
+    bool bd[3];
+    int nb[3][3];
+    for (int d = 0; d < 3; d++) {
+        bd[d] = !p[d] && (c[d] == 0 || c[d] == n[d] - 1);
+        cell[d][0] = (c[d] - 1 >= 0) ? c[d] - 1 : (p[d] ? c[d] - 1 + nc[d] : -1);
+        cell[d][1] = (c[d] < nc[d]) ? c[d] : (p[d] ? c[d] - nc[d] : -1);
+        for (int o = -1; o <= 1; o++) nb[d][o + 1] = wrapi(c[d] + o, n[d], p[d]);
+    }
+    // the up to 8 adjacent cells' 1/rho, [cz][cy][cx]
+    T v[2][2][2];
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+            for (int e = 0; e < 2; e++) {
+                const bool ok = cell[0][e] >= 0 && cell[1][b] >= 0 && cell[2][a] >= 0;
+                v[a][b][e] = ok ? ri[cell[0][e] + nc[0] * (cell[1][b] + nc[1] * cell[2][a])] : (T)0;
+            }
+    T s = 0;
+    for (int oc = 0; oc < 3; oc++) {
+        const int kk = nb[2][oc];
+        if (kk < 0) continue;
+        for (int ob = 0; ob < 3; ob++) {
+            const int jj = nb[1][ob];
+            if (jj < 0) continue;
+            for (int oa = 0; oa < 3; oa++) {
+                const int ii = nb[0][oa];
+                if (ii < 0) continue;
+                const int nz = (oa != 1) + (ob != 1) + (oc != 1);
+                if (nz <= 1) continue;  // centre handled below, faces are 0
+                T co = (nz == 2) ? (T)-2 : (T)-1;
+                const int halve = (bd[0] && oa == 1) + (bd[1] && ob == 1) + (bd[2] && oc == 1);
+                if (halve == 1) co *= (T)0.5;
+                else if (halve == 2) co *= (T)0.25;
+                // cells shared by the node and this neighbour, in (z, y, x) order
+                T sum = 0;
+                int num = 0;
+                for (int a = (oc == 2 ? 1 : 0); a <= (oc == 0 ? 0 : 1); a++) {
+                    if (cell[2][a] < 0) continue;
+                    for (int b = (ob == 2 ? 1 : 0); b <= (ob == 0 ? 0 : 1); b++) {
+                        if (cell[1][b] < 0) continue;
+                        for (int e = (oa == 2 ? 1 : 0); e <= (oa == 0 ? 0 : 1); e++) {
+                            if (cell[0][e] < 0) continue;
+                            sum += v[a][b][e];
+                            num++;
+                        }
+                    }
+                }
+                s += co * (sum / (T)num) * x[ii + L.n0 * (jj + L.n1 * kk)];
+            }
+        }
+    }
+    T sum = 0;
+    int num = 0;
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++)
+            for (int e = 0; e < 2; e++)
+                if (cell[2][a] >= 0 && cell[1][b] >= 0 && cell[0][e] >= 0) {
+                    sum += v[a][b][e];
+                    num++;
+                }
+    const int hc = bd[0] + bd[1] + bd[2];
+    diag = ((T)32 / (T)(1 << hc)) * (sum / (T)num);
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T op_offdiag(int kind, const lvl_dev L, const T *__restrict__ x, const T *__restrict__ ri,
+                                        int i, int j, int k, T &diag) {
+    if (ri) return kind == 0 ? mac_offdiag_vd(L, x, ri, i, j, k, diag) : fem_offdiag_vd(L, x, ri, i, j, k, diag);
+    return kind == 0 ? mac_offdiag(L, x, i, j, k, diag) : fem_offdiag(L, x, i, j, k, diag);
+}
+
 constexpr int kMaxLev = 12;
 constexpr int kDensePts = 1000;  // coarsening stops at the first level with at most this many points
 constexpr int kDenseMax = 1024;  // largest level solved by a dense inverse

@@ -137,6 +137,10 @@ struct rmt3d_scene {
     double *h_scalar = nullptr;
     double *d_red = nullptr;
     size_t dev_bytes = 0;  // bytes held through alloc()
+    // variable density: 1/rho per cell on every multigrid level (MAC level
+    // dimensions; the FEM levels' cells are the same), FP64 and FP32
+    std::vector<double *> rinv;
+    std::vector<float *> rinvs;
 
     template <typename T>
     int alloc(T **p, size_t n) {
@@ -499,6 +503,48 @@ static void update_rho(rmt3d_scene *s) {
     s->count();
 }
 
+// set_rhoinv (Utilities/mg_probs.cc:90-94) on the interior cells, then the
+// coarse levels as means of their 8 children
+__global__ void k_rinv_fine(grid_dev g, const fields_dev *__restrict__ F, double *ri, float *ris) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z * blockDim.z + threadIdx.z;
+    if (i >= g.sm || j >= g.sn || k >= g.so) return;
+    const double v = 1. / F->rho[gidx(g, i + 2, j + 2, k + 2)];
+    const int id = i + g.sm * (j + g.sn * k);
+    ri[id] = v;
+    if (ris) ris[id] = (float)v;
+}
+
+__global__ void k_rinv_coarse(int f0, int f1, int c0, int c1, int c2, const double *rf, double *rc, float *rcs) {
+    int I = blockIdx.x * blockDim.x + threadIdx.x;
+    int J = blockIdx.y * blockDim.y + threadIdx.y;
+    int K = blockIdx.z * blockDim.z + threadIdx.z;
+    if (I >= c0 || J >= c1 || K >= c2) return;
+    double s = 0;
+    for (int c = 0; c < 2; c++)
+        for (int b = 0; b < 2; b++)
+            for (int a = 0; a < 2; a++) s += rf[(2 * I + a) + f0 * ((2 * J + b) + f1 * (2 * K + c))];
+    const int id = I + c0 * (J + c1 * K);
+    rc[id] = 0.125 * s;
+    if (rcs) rcs[id] = (float)(0.125 * s);
+}
+
+static void update_rinv(rmt3d_scene *s) {
+    if (!s->d.var_den) return;
+    const grid_dev &g = s->g;
+    const bool f32 = s->d.precision == RMT3D_MIXED;
+    k_rinv_fine<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->rinv[0], f32 ? s->rinvs[0] : nullptr);
+    s->count();
+    for (size_t l = 1; l < s->rinv.size(); l++) {
+        const mg_level &F = s->mac.lv[l - 1], &C = s->mac.lv[l];
+        k_rinv_coarse<<<grd(C.n[0], C.n[1], C.n[2]), blk(), 0, s->st>>>(F.n[0], F.n[1], C.n[0], C.n[1], C.n[2],
+                                                                        s->rinv[l - 1], s->rinv[l],
+                                                                        f32 ? s->rinvs[l] : nullptr);
+        s->count();
+    }
+}
+
 // init_extrapolate (fluid_3d_ex.cc:16-27)
 static void init_extrapolate(rmt3d_scene *s) {
     if (s->g.n_obj == 0) return;
@@ -573,6 +619,7 @@ static void ph_upwind(rmt3d_scene *s) {
 static void ph_mac_pre(rmt3d_scene *s, double cdt) {
     const grid_dev &g = s->g;
     update_rho(s);
+    update_rinv(s);
     k_mac_rhs<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.rhs(), cdt);
     s->count();
 }
@@ -656,6 +703,7 @@ __global__ void k_mean(const double *x, size_t n, double scale, double *out, uns
 static void ph_pp_pre(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     update_rho(s);
+    update_rinv(s);
     k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
     s->count();
 }
@@ -968,7 +1016,6 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
         if (d.sys_size[a] < 4 || d.sys_size[a] > 1024) return fail(RMT3D_ERR_INVALID, "sys_size outside 4..1024");
     if (d.n_obj < 0 || d.n_obj > RMT3D_MAX_OBJ) return fail(RMT3D_ERR_TOO_LARGE, "n_obj outside 0..16");
     if (d.implicit_visc) return fail(RMT3D_ERR_UNSUPPORTED, "implicit viscosity is outside this path");
-    if (d.var_den) return fail(RMT3D_ERR_UNSUPPORTED, "variable-density multigrid operators are not built yet");
     if (!d.godunov) return fail(RMT3D_ERR_UNSUPPORTED, "only the Godunov scheme is on this path");
     if (d.sim_type == RMT3D_SIM_STEST) return fail(RMT3D_ERR_UNSUPPORTED, "stest (shear cube object) is outside this path");
     for (int o = 0; o < d.n_obj; o++)
@@ -1201,9 +1248,41 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     int nm[3] = {g.sm, g.sn, g.so}, nf[3] = {g.fm, g.fn, g.fo};
     bool mixed = d.precision == RMT3D_MIXED;
     s->mac.exact = s->fem.exact = d.mg_exact != 0;
+    s->mac.vd = s->fem.vd = d.var_den != 0;
     if ((e = s->mac.setup(MG_MAC, nm, g.prd, mixed, s->st)) != 0 || (e = s->fem.setup(MG_FEM, nf, g.prd, mixed, s->st)) != 0) {
         rmt3d_scene_destroy(s);
         return e;
+    }
+    if (d.var_den) {
+        // one 1/rho array per level, shared: FEM level l has the MAC level's cells
+        const size_t nl = s->mac.lv.size();
+        for (size_t l = 0; l < s->fem.lv.size(); l++)
+            for (int a = 0; a < 3; a++) {
+                const mg_level &F = s->fem.lv[l];
+                const int cells = F.prd[a] ? F.n[a] : F.n[a] - 1;
+                if (l >= nl || cells != s->mac.lv[l].n[a]) {
+                    rmt3d_scene_destroy(s);
+                    return fail(RMT3D_ERR_UNSUPPORTED, "variable density needs matching MAC and FEM hierarchies");
+                }
+            }
+        s->rinv.assign(nl, nullptr);
+        s->rinvs.assign(nl, nullptr);
+        for (size_t l = 0; l < nl && !e; l++) {
+            e |= s->alloc(&s->rinv[l], s->mac.lv[l].npts());
+            if (mixed) e |= s->alloc(&s->rinvs[l], s->mac.lv[l].npts());
+        }
+        if (e) {
+            rmt3d_scene_destroy(s);
+            return fail(RMT3D_ERR_OOM, "allocation failed");
+        }
+        for (size_t l = 0; l < nl; l++) {
+            s->mac.lv[l].ri = s->rinv[l];
+            s->mac.lv[l].ris = s->rinvs[l];
+            if (l < s->fem.lv.size()) {
+                s->fem.lv[l].ri = s->rinv[l];
+                s->fem.lv[l].ris = s->rinvs[l];
+            }
+        }
     }
     if (cudaStreamSynchronize(s->st) != cudaSuccess) {
         rmt3d_scene_destroy(s);
@@ -1494,6 +1573,7 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
     }
     rmt3d_set_dt(s, dt);
     set_time(s, time);
+    update_rho(s);  // the density the reference derives from the imported maps
     s->graph_dirty = true;
     CK(cudaStreamSynchronize(s->st));
     return RMT3D_OK;
@@ -1608,6 +1688,11 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     const bool mixed = d->precision == RMT3D_MIXED;
     const size_t mac = mg_solver::footprint(MG_MAC, nm, prd, mixed), fem = mg_solver::footprint(MG_FEM, nf, prd, mixed);
     if (!mac || !fem) return 0;
+    if (d->var_den) {
+        std::vector<mg_level> lv;
+        mg_solver::plan(MG_MAC, nm, prd, lv);
+        for (auto &l : lv) b += l.npts() * (sizeof(double) + (mixed ? sizeof(float) : 0));
+    }
     return b + mac + fem;
 }
 

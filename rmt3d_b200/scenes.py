@@ -62,6 +62,17 @@ def stretched_sphere(n=128, steps=500, mu=0.005, G=1.0, radius=0.3, stretch=1.3,
     return s
 
 
+def multi_sphere(n=24, steps=100, spheres=(), mu=0.01, lid=1.0, wt_n=1.5, nlayers=5, frames=100000, T=None):
+    """Lid-driven cavity holding several neo-Hookean spheres (identity maps);
+    spheres = [((cx, cy, cz), R, G, rho), ...]."""
+    s = cavity(n, steps, mu, lid, frames, T)
+    s += "wt_n %g\nnlayers %d\nn_obj %d\n" % (wt_n, nlayers, len(spheres))
+    for i, (c, r, G, rho) in enumerate(spheres):
+        s += "object_list %d 0\nbasic_specs %d %r %r %r %r\nshear_mod %d %r\nsrho %d %r\n" % (
+            i, i, c[0], c[1], c[2], r, i, G, i, rho)
+    return s
+
+
 def random_scene(seed, sizes=(32, 48, 64, 96), nobj=(1, 8), steps=100, mu=0.01):
     """One seeded multi-sphere cavity scene: radii U(0.08,0.15), centres
     rejection-sampled without overlap and at least 2 dx apart, G log-uniform in

@@ -9,7 +9,8 @@ extrapolated maps.  The oracle's Poisson solves run with RMT3D_SHIM_EXACT=1
 residual-tolerance noise.  Usage (in the build container, where the reference
 is present):
 
-    make -C oracle all nofma && python tests/golden/make_golden.py
+    make -C oracle all nofma && make -C oracle VARDEN=1 all nofma
+    python tests/golden/make_golden.py [case ...]
 """
 import os
 import subprocess
@@ -29,11 +30,20 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 # the reference rebuilt without FMA contraction (make -C oracle nofma)
 DRIVER_NOFMA = os.path.join(ROOT, "oracle", "_ref", "nofma", "ref_driver")
 
-# name -> (cfg text, saved step counts)
+# the variable-density build of the reference (make -C oracle VARDEN=1 all nofma)
+DRIVER_VD = os.path.join(ROOT, "oracle", "_ref", "ref_driver.varden")
+DRIVER_VD_NOFMA = os.path.join(ROOT, "oracle", "_ref", "nofma", "ref_driver.varden")
+
+# name -> (cfg text, saved step counts[, variable density])
 CASES = {
     "cavity16": (scenes.cavity(16, 8), [0, 1, 8]),
     "sphere24": (scenes.cavity_sphere(24, 4, radius=0.25), [0, 1, 4]),
     "stretch24": (scenes.stretched_sphere(24, 4, radius=0.2), [0, 1, 4]),
+    # solid density differs from the fluid's: the reference's VAR_DEN build
+    "varden24": (scenes.cavity_sphere(24, 4, radius=0.25, rho=1.5), [0, 1, 4], True),
+    "multi24": (scenes.multi_sphere(24, 4, spheres=[((0.3, 0.3, 0.35), 0.15, 0.5, 0.8),
+                                                  ((0.7, 0.65, 0.4), 0.15, 2.0, 1.2),
+                                                  ((0.45, 0.6, 0.72), 0.15, 1.0, 1.0)]), [0, 1, 4], True),
 }
 # longer runs stored as interior (u, v, w, p) only
 LONG = {
@@ -78,7 +88,7 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
 
 
-def envelope(cfg_text, steps, base, workdir):
+def envelope(cfg_text, steps, base, workdir, varden=False):
     """Rounding envelope of the reference at this state: the largest rel-L2
     change of (velocity vector, pressure, reference map) between the fixture
     and two other valid roundings of the same computation -- the build without
@@ -89,7 +99,8 @@ def envelope(cfg_text, steps, base, workdir):
     vb = base["fields"]["vel"].reshape(shp + (3,))[sl]
     pb = base["fields"]["p"].reshape(shp)[sl]
     env = np.zeros(3)
-    for drv, ex in ((DRIVER_NOFMA, "1"), (DRIVER, "0")):
+    drivers = ((DRIVER_VD_NOFMA, "1"), (DRIVER_VD, "0")) if varden else ((DRIVER_NOFMA, "1"), (DRIVER, "0"))
+    for drv, ex in drivers:
         d = run(cfg_text, steps, workdir, drv, ex)
         v = d["fields"]["vel"].reshape(shp + (3,))[sl]
         p = d["fields"]["p"].reshape(shp)[sl]
@@ -104,17 +115,24 @@ def main():
     if not (os.path.exists(DRIVER) and os.path.exists(DRIVER_NOFMA)):
         sys.exit("build the reference first: make -C oracle all nofma")
     with tempfile.TemporaryDirectory() as wd:
-        for name, (txt, steps) in CASES.items():
-            arrays = {"cfg": np.frombuffer(txt.encode(), dtype=np.uint8)}
+        only = sys.argv[1:]
+        for name, case in CASES.items():
+            if only and name not in only:
+                continue
+            txt, steps = case[0], case[1]
+            varden = len(case) > 2 and case[2]
+            arrays = {"cfg": np.frombuffer(txt.encode(), dtype=np.uint8), "varden": np.array(int(varden))}
             for k in steps:
-                d = run(txt, k, wd)
+                d = run(txt, k, wd, DRIVER_VD if varden else DRIVER)
                 for key, val in compact(d).items():
                     arrays["s%d_%s" % (k, key)] = val
-                arrays["s%d_env" % k] = envelope(txt, k, d, wd)
+                arrays["s%d_env" % k] = envelope(txt, k, d, wd, varden)
                 print(name, k, "envelope", arrays["s%d_env" % k])
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
             print("wrote", name)
         for name, (txt, k) in LONG.items():
+            if only and name not in only:
+                continue
             d = run(txt, k, wd)
             shp = d["shape"]
             sl = (slice(2, -2),) * 3

@@ -5,6 +5,9 @@ GPU, RMT3D_SHIM_EXACT in the oracle), so the comparison is not limited by the
 reference's residual tolerance.
 
 * One step from the reference's own state must agree to rel-L2 1e-10.
+* varden24 (one sphere of density 1.5) and multi24 (three spheres of
+  densities 0.8, 1.2, 1.0) are states of the reference's VAR_DEN build and
+  run the variable-density form (1/rho-weighted MAC and FEM operators).
 * Over several steps the reference is not reproducible even by itself below
   a rounding envelope: rebuilt without FMA contraction, or with its own
   tolerance-based multigrid control, it moves by the amount stored in each
@@ -57,13 +60,15 @@ def map_errors(scene, st):
 def make_scene(tmp_path, name, exact=1, prepare=True):
     fx = H.load_fixture(name)
     cfg = H.fixture_cfg(fx, str(tmp_path / (name + ".cfg")))
-    sc = R.Scene.from_cfg(cfg, mg_exact=exact)
+    # fixtures made with the reference's VAR_DEN build run the variable-density form
+    sc = R.Scene.from_cfg(cfg, mg_exact=exact, var_den=int(fx.get("varden", 0)))
     if prepare:
         sc.prepare()
     return fx, sc
 
 
-@pytest.mark.parametrize("name,steps", [("cavity16", [1, 8]), ("sphere24", [1, 4]), ("stretch24", [1, 4])])
+@pytest.mark.parametrize("name,steps", [("cavity16", [1, 8]), ("sphere24", [1, 4]), ("stretch24", [1, 4]),
+                                        ("varden24", [1, 4]), ("multi24", [1, 4])])
 def test_full_path_matches_reference(tmp_path, name, steps):
     """run_sim's set-up (initialize, dt fit, 5 pressure pre-iterations) and
     the first steps, against the reference's states."""
@@ -92,7 +97,7 @@ def test_full_path_matches_reference(tmp_path, name, steps):
         sc.close()
 
 
-@pytest.mark.parametrize("name", ["cavity16", "sphere24", "stretch24"])
+@pytest.mark.parametrize("name", ["cavity16", "sphere24", "stretch24", "varden24", "multi24"])
 def test_single_step_from_reference_state(tmp_path, name):
     """One step from the reference's own state (imported in its AoS layout)."""
     fx, sc = make_scene(tmp_path, name)
@@ -106,6 +111,23 @@ def test_single_step_from_reference_state(tmp_path, name):
         if sc.desc.n_obj:
             m = map_errors(sc, st1)
             assert m["prim_mismatch"] == 0 and m["ext_mismatch"] == 0 and m["xi"] < TOL, m
+    finally:
+        sc.close()
+
+
+def test_varden_fixture_discriminates(tmp_path):
+    """The variable-density fixtures really test the 1/rho-weighted operators:
+    the constant-density projection misses them by far more than TOL."""
+    fx = H.load_fixture("varden24")
+    cfg = H.fixture_cfg(fx, str(tmp_path / "v.cfg"))
+    sc = R.Scene.from_cfg(cfg, mg_exact=1, var_den=0)
+    try:
+        st0, st1 = H.state(fx, 0), H.state(fx, 1)
+        fa, ra, ei, em = H.to_aos(st0)
+        sc.import_reference(fa, ra, ei, em, st1["dt"], st0["time"])
+        assert sc.step_forward(0) == R.NORMAL_EXIT
+        e = vec_errors(sc, st1)
+        assert max(e.values()) > 1e3 * TOL, e
     finally:
         sc.close()
 

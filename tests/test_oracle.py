@@ -11,17 +11,21 @@ import helpers as H
 from oracle import refdump
 
 DRIVER = os.path.join(H.ROOT, "oracle", "_ref", "ref_driver")
-needs_ref = pytest.mark.skipif(not os.path.exists(DRIVER), reason="oracle/_ref not built here")
+DRIVER_VD = os.path.join(H.ROOT, "oracle", "_ref", "ref_driver.varden")
+needs_ref = pytest.mark.skipif(not (os.path.exists(DRIVER) and os.path.exists(DRIVER_VD)),
+                               reason="oracle/_ref not built here")
 
 
 @needs_ref
-@pytest.mark.parametrize("name,k", [("cavity16", 1), ("sphere24", 1), ("stretch24", 0)])
+@pytest.mark.parametrize("name,k", [("cavity16", 1), ("sphere24", 1), ("stretch24", 0), ("varden24", 1),
+                                    ("multi24", 1)])
 def test_fixture_reproduces_from_reference(tmp_path, name, k):
     fx = H.load_fixture(name)
     cfg = H.fixture_cfg(fx, str(tmp_path / "case.cfg"))
     out = str(tmp_path / "o.bin")
     env = dict(os.environ, RMT3D_SHIM_EXACT="1")
-    subprocess.run([DRIVER, cfg, str(k), out], check=True, capture_output=True, cwd=str(tmp_path), env=env)
+    drv = DRIVER_VD if int(fx.get("varden", 0)) else DRIVER
+    subprocess.run([drv, cfg, str(k), out], check=True, capture_output=True, cwd=str(tmp_path), env=env)
     d = refdump.read(out)
     st = H.state(fx, k)
     assert d["dt"] == st["dt"] and d["time"] == st["time"]
@@ -32,7 +36,7 @@ def test_fixture_reproduces_from_reference(tmp_path, name, k):
 
 
 def test_fixture_invariants():
-    for name in ("cavity16", "sphere24", "stretch24"):
+    for name in ("cavity16", "sphere24", "stretch24", "varden24", "multi24"):
         fx = H.load_fixture(name)
         for k in (0, 1):
             st = H.state(fx, k)
