@@ -184,8 +184,10 @@ int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, const void *re
 int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *refmap_aos,
                            int *ext_index, void *ext_refmaps, int max_ext, int *n_ext);
 
-/* Diagnostics: 0 div_u L2 of the FEM rhs (fluid_3d_utils.cc:507-653),
- * 1 solid volume sum H(phi) dV for object 0 (compute_centroid :1348-1379). */
+/* Diagnostics: 0 div_u L2 of the FEM rhs (fluid_3d_utils.cc:507-653);
+ * 1 solid volume sum H(phi) dV over the primary maps and 2-4 the centroid
+ * x, y, z (compute_centroid, :1348-1379); 5 total deviation of det F from 1
+ * and 6 its maximum (total_dev_in_detF, :1032-1084). */
 int rmt3d_diag(rmt3d_scene *s, int kind, double *value);
 
 /* Allocation-free divergence diagnostic (no counterpart in the reference; it
@@ -232,10 +234,10 @@ int rmt3d_batch_prepare(rmt3d_batch *b);
 int rmt3d_batch_step(rmt3d_batch *b, int nsteps, int *status);
 int rmt3d_batch_size(rmt3d_batch *b, int *n);
 int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out);
-/* choose the multigrid schedule (v_down, v_up, coarse_pts) per distinct grid
- * size by timing candidates on a probe scene (the reference's mg_opt searches
- * the (v_down, v_up) pair, Utilities/mg_probs.hh:80-208); tuned_out gets
- * (cells, v_down, v_up, coarse_pts) per size */
+/* choose the multigrid schedule (v_down, v_up, cluster launch) per distinct
+ * grid size by timing candidates on a probe scene (the reference's mg_opt
+ * searches the (v_down, v_up) pair, Utilities/mg_probs.hh:80-208); tuned_out
+ * gets (cells, v_down, v_up, cluster) per size */
 int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out);
 int rmt3d_batch_destroy(rmt3d_batch *b);
 
@@ -243,6 +245,12 @@ int rmt3d_batch_destroy(rmt3d_batch *b);
  * largest level (points) whose whole sub-cycle runs in one thread block out of
  * shared memory (0: none; negative keeps the current value). */
 int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts);
+
+/* How each multigrid solve is issued: 1 = the whole solve as one launch in a
+ * thread-block cluster of 8 or 16 CTAs, 0 (default) = one launch per phase
+ * inside a graph loop.  Same operators and control; the results agree to the
+ * solver tolerance. */
+int rmt3d_scene_set_mg_launch(rmt3d_scene *s, int cluster);
 
 /* Device bytes a scene with this descriptor allocates (admission control). */
 size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d);

@@ -174,6 +174,8 @@ class Scene:
             ei.ctypes.data_as(ctypes.c_void_p), em.ctypes.data_as(ctypes.c_void_p), len(ei), dt, time))
 
     def diag(self, kind=0):
+        """0 div_u, 1 solid volume, 2-4 solid centroid, 5 total and 6 maximum
+        deviation of det F from 1."""
         v = ctypes.c_double()
         _lib.check(lib().rmt3d_diag(self._h, kind, ctypes.byref(v)))
         return v.value
@@ -194,6 +196,11 @@ class Scene:
         largest level run by the one-block coarse sub-cycle (0: none,
         negative keeps it)."""
         _lib.check(lib().rmt3d_scene_set_schedule(self._h, v_down, v_up, coarse_pts))
+
+    def set_mg_launch(self, cluster):
+        """1: each multigrid solve as one thread-block-cluster launch; 0: one
+        launch per phase in a graph loop."""
+        _lib.check(lib().rmt3d_scene_set_mg_launch(self._h, int(cluster)))
 
     def checksum(self):
         """Sums of u^2, v^2, w^2, p^2 over the interior cells."""
@@ -311,7 +318,7 @@ class Batch:
         return out.reshape(dims[2], dims[1], dims[0])
 
     def autotune(self, probe_steps=3):
-        """Per grid size: {cells: (v_down, v_up, coarse_pts)} chosen by timing candidates."""
+        """Per grid size: {cells: (v_down, v_up, cluster)} chosen by timing candidates."""
         buf = (ctypes.c_int * (4 * self.n))()
         n = ctypes.c_int()
         _lib.check(lib().rmt3d_batch_autotune(self._h, probe_steps, buf, self.n, ctypes.byref(n)))

@@ -5,9 +5,9 @@
 // scenes overlap on the device (uneven grid sizes need no padding: each scene
 // launches its own grids).  Scenes are assigned to threads by a greedy
 // balance of cells.  An autotuner picks the multigrid schedule per grid size
-// -- smoothing counts (v_down, v_up) and the size of the levels handed to the
-// one-block shared-memory coarse sub-cycle -- by timing candidates on a probe
-// scene.
+// -- smoothing counts (v_down, v_up) and whether each solve runs as one
+// thread-block-cluster launch or as per-phase launches -- by timing
+// candidates on a probe scene.
 #include <algorithm>
 #include <array>
 #include <atomic>
@@ -26,13 +26,14 @@
 
 // knobs shared with scene.cu (defined there)
 extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts);
+extern "C" int rmt3d_scene_set_mg_launch(rmt3d_scene *s, int cluster);
 
 struct rmt3d_batch {
     std::vector<rmt3d_scene *> scenes;
     std::vector<rmt3d_scene_desc> descs;
     std::vector<std::vector<int>> groups;  // scene indices per host thread
     std::vector<int> status;
-    std::map<int, std::array<int, 3>> tuned;  // grid cells -> (v_down, v_up, coarse_pts)
+    std::map<int, std::array<int, 3>> tuned;  // grid cells -> (v_down, v_up, cluster launch)
     int nthreads = 1;
 };
 
@@ -166,7 +167,6 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
     static const int smooth[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
-    static const int coarse[] = {0, 5000};
     std::map<long long, int> first;
     for (size_t i = 0; i < b->descs.size(); i++)
         if (!first.count(cells(b->descs[i]))) first[cells(b->descs[i])] = (int)i;
@@ -181,14 +181,15 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
         }
         double best = 1e300;
         int bd = 2, bu = 2, bc = 0;
-        for (int cp : coarse)
+        for (int cl : {1, 0})
             for (auto &c : smooth) {
-                if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], cp))) {
+                if (rmt3d_scene_set_mg_launch(probe, cl)) continue;  // clusters unavailable
+                if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], 0))) {
                     rmt3d_scene_destroy(probe);
                     return e;
                 }
                 int st = 0;
-                rmt3d_run(probe, 1, &st);  // settle the cycle predictor
+                rmt3d_run(probe, 1, &st);  // settle the cycle predictor, build the graph
                 rmt3d_sync(probe);
                 auto t0 = std::chrono::steady_clock::now();
                 rmt3d_run(probe, probe_steps, &st);
@@ -198,14 +199,15 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
                     best = dt;
                     bd = c[0];
                     bu = c[1];
-                    bc = cp;
+                    bc = cl;
                 }
             }
         rmt3d_scene_destroy(probe);
         b->tuned[(int)kv.first] = {bd, bu, bc};
         for (size_t i = 0; i < b->descs.size(); i++)
             if (cells(b->descs[i]) == kv.first) {
-                if ((e = rmt3d_scene_set_schedule(b->scenes[i], bd, bu, bc))) return e;
+                if ((e = rmt3d_scene_set_schedule(b->scenes[i], bd, bu, 0))) return e;
+                if ((e = rmt3d_scene_set_mg_launch(b->scenes[i], bc))) return e;
             }
         if (tuned_out && written < max_out) {
             tuned_out[4 * written] = (int)kv.first;

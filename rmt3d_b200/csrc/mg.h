@@ -90,6 +90,15 @@ class mg_solver {
     mg_ctl *h_ctl = nullptr;     // pinned mirror (owned by the scene)
     bool use_graph = true;       // false: run() issues every kernel from the host
     bool vd = false;             // variable density: levels carry 1/rho (no one-block coarse sub-cycle)
+    // one launch per solve in a thread-block cluster (k_mgc.cu), or (default)
+    // one launch per phase inside a graph WHILE loop; measured on a B200 the
+    // per-phase launches over the whole GPU win for a single scene (64^3:
+    // 4.1 vs 14 ms per step), and the batch autotuner picks per grid size
+    int cluster_size = 0;        // CTAs per cluster supported here (0: none)
+    bool use_cluster = false;
+    bool cluster_mode() const { return use_cluster && cluster_size > 0; }
+    int setup_cluster();
+    cudaError_t launch_cluster(cudaStream_t st);
 
     mg_solver() = default;
     mg_solver(const mg_solver &) = delete;
@@ -120,9 +129,11 @@ class mg_solver {
     int outside_kernels = 1;   // kernels of a solve outside its loop body
     int body_kernels = 0;      // kernels per loop iteration (set by capture_solve)
     void invalidate();         // drop the solver's own graph (schedule changed)
+    void release();            // free the device memory (stream-ordered, on the set-up stream)
     void sync_host_mirror();   // cycles from the pinned control mirror
 
   private:
+    cudaStream_t alloc_stream = nullptr;
     unsigned long long *d_max = nullptr;  // residual max-norm (ordered bit pattern)
     cudaGraphExec_t solve_exec = nullptr;
     cudaStream_t cap_main = nullptr;

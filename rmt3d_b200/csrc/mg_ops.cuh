@@ -168,6 +168,41 @@ __device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict
                 const bool ok = cell[0][e] >= 0 && cell[1][b] >= 0 && cell[2][a] >= 0;
                 v[a][b][e] = ok ? ri[cell[0][e] + nc[0] * (cell[1][b] + nc[1] * cell[2][a])] : (T)0;
             }
+    if (!bd[0] && !bd[1] && !bd[2]) {
+        // interior node (all 8 cells exist, no halving): the same entries in
+        // closed form -- corners take one cell, edges the mean of two (lower
+        // index first), the centre the mean of all eight in (z, y, x) order
+        const int sy = L.n0, sz = L.n0 * L.n1;
+        T s = 0;
+        for (int oc = 0; oc < 3; oc++) {
+            const int kk = nb[2][oc];
+            for (int ob = 0; ob < 3; ob++) {
+                const int jj = nb[1][ob];
+                for (int oa = 0; oa < 3; oa++) {
+                    const int nz = (oa != 1) + (ob != 1) + (oc != 1);
+                    if (nz <= 1) continue;
+                    const T xv = x[nb[0][oa] + sy * jj + sz * kk];
+                    T cf;
+                    if (nz == 3) {
+                        cf = -v[oc >> 1][ob >> 1][oa >> 1];
+                    } else if (oc == 1) {
+                        cf = (T)-2 * ((v[0][ob >> 1][oa >> 1] + v[1][ob >> 1][oa >> 1]) / (T)2);
+                    } else if (ob == 1) {
+                        cf = (T)-2 * ((v[oc >> 1][0][oa >> 1] + v[oc >> 1][1][oa >> 1]) / (T)2);
+                    } else {
+                        cf = (T)-2 * ((v[oc >> 1][ob >> 1][0] + v[oc >> 1][ob >> 1][1]) / (T)2);
+                    }
+                    s += cf * xv;
+                }
+            }
+        }
+        T c8 = 0;
+        for (int a = 0; a < 2; a++)
+            for (int b = 0; b < 2; b++)
+                for (int e = 0; e < 2; e++) c8 += v[a][b][e];
+        diag = (T)32 * (c8 / (T)8);
+        return s;
+    }
     T s = 0;
     for (int oc = 0; oc < 3; oc++) {
         const int kk = nb[2][oc];
@@ -233,6 +268,8 @@ struct pmg_level {
     int prd[3];
     double *x, *r, *res;
     float *xs, *rs, *ress;
+    const double *ri;  // variable density: 1/rho per cell (null: constant)
+    const float *ris;
 };
 
 struct pmg_args {
@@ -249,7 +286,7 @@ __device__ __forceinline__ lvl_dev ldev(const pmg_level &L) {
 
 // ---- one phase over a level, for the points [t0, total) with stride ts ----
 template <typename T>
-__device__ void ph_smooth_colour(int kind, const lvl_dev L, T *x, const T *r, int colour, int t0, int ts) {
+__device__ void ph_smooth_colour(int kind, const lvl_dev L, T *x, const T *r, const T *ri, int colour, int t0, int ts) {
     if (kind == 0) {
         const int h = (L.n0 + 1) / 2;
         const int tot = h * L.n1 * L.n2;
@@ -258,7 +295,7 @@ __device__ void ph_smooth_colour(int kind, const lvl_dev L, T *x, const T *r, in
             int i = 2 * hi + ((j + k + colour) & 1);
             if (i >= L.n0) continue;
             T diag;
-            T s = mac_offdiag(L, x, i, j, k, diag);
+            T s = op_offdiag<T>(0, L, x, ri, i, j, k, diag);
             int id = i + L.n0 * (j + L.n1 * k);
             x[id] = (r[id] - s) / diag;
         }
@@ -270,7 +307,7 @@ __device__ void ph_smooth_colour(int kind, const lvl_dev L, T *x, const T *r, in
             int i = 2 * a + (colour & 1), j = 2 * b + ((colour >> 1) & 1);
             if (i >= L.n0 || j >= L.n1) continue;
             T diag;
-            T s = fem_offdiag(L, x, i, j, k, diag);
+            T s = op_offdiag<T>(1, L, x, ri, i, j, k, diag);
             int id = i + L.n0 * (j + L.n1 * k);
             x[id] = (r[id] - s) / diag;
         }
@@ -278,13 +315,13 @@ __device__ void ph_smooth_colour(int kind, const lvl_dev L, T *x, const T *r, in
 }
 
 template <typename T>
-__device__ double ph_resid(int kind, const lvl_dev L, const T *x, const T *r, T *res, int t0, int ts) {
+__device__ double ph_resid(int kind, const lvl_dev L, const T *x, const T *r, T *res, const T *ri, int t0, int ts) {
     const int tot = L.n0 * L.n1 * L.n2;
     double mx = 0;
     for (int t = t0; t < tot; t += ts) {
         int i = t % L.n0, j = (t / L.n0) % L.n1, k = t / (L.n0 * L.n1);
         T diag;
-        T s = (kind == 0) ? mac_offdiag(L, x, i, j, k, diag) : fem_offdiag(L, x, i, j, k, diag);
+        T s = op_offdiag<T>(kind, L, x, ri, i, j, k, diag);
         T v = r[t] - s - diag * x[t];
         if (res) res[t] = v;
         double a = fabs((double)v);
@@ -389,6 +426,12 @@ __device__ __forceinline__ void set_level_ptrs(pmg_level &L, T *x, T *r, T *res)
 }
 
 template <typename T>
+__device__ __forceinline__ const T *LRI(const pmg_level &L) {
+    if constexpr (sizeof(T) == 8) return (const T *)L.ri;
+    else return (const T *)L.ris;
+}
+
+template <typename T>
 __device__ __forceinline__ T *LX(const pmg_level &L) {
     if constexpr (sizeof(T) == 8) return (T *)L.x;
     else return (T *)L.xs;
@@ -413,10 +456,10 @@ __device__ void coarse_cycle(const pmg_args &A, int cf) {
         const pmg_level &F = A.lv[l];
         for (int s = 0; s < A.v_down; s++)
             for (int c = 0; c < nc; c++) {
-                ph_smooth_colour<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), c, t0, ts);
+                ph_smooth_colour<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), LRI<T>(F), c, t0, ts);
                 __syncthreads();
             }
-        ph_resid<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), LS<T>(F), t0, ts);
+        ph_resid<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), LS<T>(F), LRI<T>(F), t0, ts);
         __syncthreads();
         const pmg_level &C = A.lv[l + 1];
         ph_restrict<T>(A.kind, ldev(F), ldev(C), LS<T>(F), LR<T>(C), LX<T>(C), t0, ts);
@@ -443,7 +486,7 @@ __device__ void coarse_cycle(const pmg_args &A, int cf) {
             __syncthreads();
             for (int s = 0; s < 80; s++)
                 for (int c = 0; c < nc; c++) {
-                    ph_smooth_colour<T>(A.kind, ldev(L), x, r, c, t0, ts);
+                    ph_smooth_colour<T>(A.kind, ldev(L), x, r, LRI<T>(L), c, t0, ts);
                     __syncthreads();
                 }
         }
@@ -455,7 +498,7 @@ __device__ void coarse_cycle(const pmg_args &A, int cf) {
         __syncthreads();
         for (int s = 0; s < A.v_up; s++)
             for (int c = 0; c < nc; c++) {
-                ph_smooth_colour<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), c, t0, ts);
+                ph_smooth_colour<T>(A.kind, ldev(F), LX<T>(F), LR<T>(F), LRI<T>(F), c, t0, ts);
                 __syncthreads();
             }
     }

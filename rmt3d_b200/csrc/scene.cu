@@ -132,6 +132,8 @@ struct rmt3d_scene {
     bool capturing = false;
     bool use_graph = true;
     long long graph_fixed = 0;  // kernels per step outside the multigrid loops
+    double *d_diag = nullptr;  // solid diagnostics: [0..7] totals, then per-block partials
+    unsigned *diag_ticket = nullptr;
     double *d_mean = nullptr;  // [0] mean, [1..] per-block partial sums
     unsigned *mean_ticket = nullptr;
     double *h_scalar = nullptr;
@@ -142,9 +144,12 @@ struct rmt3d_scene {
     std::vector<double *> rinv;
     std::vector<float *> rinvs;
 
+    // stream-ordered allocation from the device's memory pool (no device-wide
+    // synchronisation when scenes are created or destroyed)
     template <typename T>
     int alloc(T **p, size_t n) {
-        if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) return fail(RMT3D_ERR_OOM, "device allocation failed");
+        if (cudaMallocAsync((void **)p, n * sizeof(T), st) != cudaSuccess)
+            return fail(RMT3D_ERR_OOM, "device allocation failed");
         allocs.push_back(*p);
         dev_bytes += n * sizeof(T);
         cudaMemsetAsync(*p, 0, n * sizeof(T), st);
@@ -369,11 +374,130 @@ static void cfl_recheck(rmt3d_scene *s) {
     s->g.K_stiff = s->K_stiff;
 }
 
+static int read_ctl(rmt3d_scene *s);
+static bool graph_mode(rmt3d_scene *s);
+static int build_step_graph(rmt3d_scene *s);
+
+// ---- initial conditions on the device (the objects simulation) ------------
+struct vel_profile_dev {
+    int n;
+    double e[2 * RMT3D_MAX_VEL_PROF];
+};
+
+// sim_manager::velocity (sim_manager.cc:102-131) at every cell of the ghosted
+// box, with the running maximum of |u| for the CFL recheck (as ordered bits)
+__global__ void k_init_velocity(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                                const double *lz, vel_profile_dev prof, unsigned long long *vmax_bits) {
+    const int ind = blockIdx.x * blockDim.x + threadIdx.x;
+    double tmp = 0;
+    if (ind < g.ncell) {
+        const int i = ind % g.sm4, j = (ind / g.sm4) % g.sn4, k = ind / g.smn4;
+        const double coords[3] = {lx[i], ly[j], lz[k]};
+        double u = 0, v = 0, w = 0;
+        for (int q = 0; q < prof.n; q++) {
+            const int vt = static_cast<int>(prof.e[2 * q]);
+            const double amp = prof.e[2 * q + 1];
+            if (vt == 1) u += amp;
+            else if (vt == 2) v += amp;
+            else if (vt == 3) w += amp;
+        }
+        for (int o = 0; o < g.n_obj; o++) {
+            const obj_dev &ob = g.obj[o];
+            double rx[3];
+            for (int a = 0; a < 3; a++)
+                rx[a] = (ob.type == RMT3D_OBJ_SPHERE) ? (coords[a] - ob.c[a]) * ob.eig[a] + ob.c[a] : coords[a];
+            if (obj_phi(g, o, rx[0], rx[1], rx[2]) < 0.) {
+                double L[3];
+                for (int a = 0; a < 3; a++) L[a] = rx[a] - ob.c[a];
+                u += ob.omega[1] * L[2] - ob.omega[2] * L[1];
+                v -= ob.omega[0] * L[2] - ob.omega[2] * L[0];
+                w += ob.omega[0] * L[1] - ob.omega[1] * L[0];
+            }
+        }
+        F->vel[0][ind] = u;
+        F->vel[1][ind] = v;
+        F->vel[2][ind] = w;
+        tmp = sqrt(u * u + v * v + w * w);
+        if (F->rho) F->rho[ind] = g.frho;
+    }
+    unsigned long long b = (unsigned long long)__double_as_longlong(tmp);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
+        b = t > b ? t : b;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(vmax_bits, b);
+}
+
+// fluid_3d::init_refmap (fluid_3d.cc:348-400) on the device: every map reset;
+// each interior cell takes the initial map of each object in turn (the last
+// one stays in x, as the reference's loop leaves it) and belongs to the first
+// object whose level set is negative there
+__global__ void k_init_refmap(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                              const double *lz, int *err) {
+    const int ind = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ind >= g.ncell) return;
+    const int i = ind % g.sm4, j = (ind / g.sm4) % g.sn4, k = ind / g.smn4;
+    const bool interior = i >= 2 && i < g.sm4 - 2 && j >= 2 && j < g.sn4 - 2 && k >= 2 && k < g.so4 - 2;
+    double X[3] = {0, 0, 0};
+    int owner = -1;
+    if (interior) {
+        const double tx[3] = {lx[i], ly[j], lz[k]};
+        for (int o = 0; o < g.n_obj; o++) {
+            const obj_dev &ob = g.obj[o];
+            for (int a = 0; a < 3; a++)
+                X[a] = (ob.type == RMT3D_OBJ_SPHERE) ? (tx[a] - ob.c[a]) * ob.eig[a] + ob.c[a] : tx[a];
+            if (obj_phi(g, o, X[0], X[1], X[2]) < 0) {
+                if (owner < 0) owner = o;
+                else atomicAdd(err, 1);
+            }
+        }
+    }
+    for (int o = 0; o < g.n_obj; o++) {
+        const objmap_dev &m = F->om[o];
+        m.code[ind] = (owner == o) ? 0 : -1;
+        for (int a = 0; a < 3; a++) {
+            m.x[a][ind] = X[a];
+            m.xp[a][ind] = X[a];
+        }
+        for (int a = 0; a < 9; a++) m.gp[a][ind] = -kBig;
+        for (int a = 0; a < 18; a++) m.fx[a][ind] = 0;
+    }
+}
+
+// the objects simulation's initial state is computed on the device; the
+// manufactured-solution and shear-test cases keep the host path (trigonometric
+// initial fields evaluated with the host's libm, as the reference does)
+static bool device_init(const rmt3d_scene *s) {
+    return s->d.sim_type == RMT3D_SIM_OBJECTS && !s->d.has_exact;
+}
+
 // init_fluid (fluid_3d.cc:292-320): every cell reset (p kept), velocities from
 // the initial condition, periodic exchange, CFL recheck, dt = dt_reg
 static int init_fluid(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     const size_t n = g.ncell;
+    if (device_init(s)) {
+        CK(cudaMemsetAsync(s->d_red, 0, sizeof(double), s->st));
+        vel_profile_dev prof;
+        memset(&prof, 0, sizeof(prof));
+        prof.n = s->d.vel_prof_num;
+        for (int q = 0; q < 2 * RMT3D_MAX_VEL_PROF; q++) prof.e[q] = s->d.vel_profile[q];
+        k_init_velocity<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, prof,
+                                                                 (unsigned long long *)s->d_red);
+        s->count();
+        CK(cudaMemsetAsync(s->hF.q, 0, n * 8, s->st));
+        CK(cudaMemsetAsync(s->hF.dp, 0, n * 8, s->st));
+        for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(s->hF.dvel[c], 0, n * 8, s->st));
+        for (int c = 0; c < 18; c++) CK(cudaMemsetAsync(s->hF.fvel[c], 0, n * 8, s->st));
+        for (int c = 0; c < 9; c++) CK(cudaMemsetAsync(s->hF.sigma[c], 0, n * 8, s->st));
+        CK(cudaMemcpyAsync(s->h_scalar, s->d_red, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+        CK(cudaStreamSynchronize(s->st));
+        if (*s->h_scalar > s->vmax) s->vmax = *s->h_scalar;
+        periodic(s, {s->hF.vel[0], s->hF.vel[1], s->hF.vel[2]}, {}, 0);
+        cfl_recheck(s);
+        rmt3d_set_dt(s, s->dt_reg);
+        return 0;
+    }
     std::vector<double> u(n), v(n), w(n);
     for (int k = 0; k < g.so4; k++)
         for (int j = 0; j < g.sn4; j++)
@@ -406,10 +530,26 @@ static int init_fluid(rmt3d_scene *s) {
     return 0;
 }
 
+__global__ void k_zero_pres(grid_dev g, double *p) {
+    const int ind = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ind >= g.ncell) return;
+    const int i = ind % g.sm4, j = (ind / g.sm4) % g.sn4, k = ind / g.smn4;
+    if (i >= 2 && i < g.sm4 - 1 && j >= 2 && j < g.sn4 - 1 && k >= 2 && k < g.so4 - 1) p[ind] = 0;
+}
+
 // init_pres (fluid_3d.cc:326-343)
 static int init_pres(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     const size_t n = g.ncell;
+    if (device_init(s)) {
+        // sim_manager::pressure is 0 for the objects simulation; the reference
+        // writes it to the nodes 2..s+2 and keeps the rest of p
+        k_zero_pres<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->hF.p);
+        s->count();
+        CK(cudaMemsetAsync(s->hF.q, 0, n * 8, s->st));
+        comm_pressure(s);
+        return 0;
+    }
     std::vector<double> p(n);
     CK(cudaMemcpyAsync(p.data(), s->hF.p, n * 8, cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -430,43 +570,13 @@ static int init_pres(rmt3d_scene *s) {
 // level set is negative there
 static int init_refmap(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    const size_t n = g.ncell;
     if (g.n_obj == 0) return 0;
-    std::vector<int> code(n);
-    std::vector<double> X[3], init_gp(n, -kBig);
-    for (int c = 0; c < 3; c++) X[c].assign(n, 0.0);
-    std::vector<int> owner(n, -1);
-    for (int k = 2; k < g.so4 - 2; k++)
-        for (int j = 2; j < g.sn4 - 2; j++)
-            for (int i = 2; i < g.sm4 - 2; i++) {
-                size_t id = gidx(g, i, j, k);
-                double tx[3] = {s->hlx[i], s->hly[j], s->hlz[k]};
-                double xi[3];
-                bool found = false;
-                for (int o = 0; o < g.n_obj; o++) {
-                    s->obj[o].rm0(tx, xi);
-                    for (int c = 0; c < 3; c++) X[c][id] = xi[c];
-                    if (s->obj[o].phi(xi) < 0) {
-                        if (!found) {
-                            owner[id] = o;
-                            found = true;
-                        } else {
-                            return fail(RMT3D_ERR_INVALID, "init_refmap: overlapping primary points");
-                        }
-                    }
-                }
-            }
-    for (int o = 0; o < g.n_obj; o++) {
-        objmap_dev &m = s->hF.om[o];
-        for (size_t id = 0; id < n; id++) code[id] = (owner[id] == o) ? 0 : -1;
-        CK(copy_sync(s, m.code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-        for (int c = 0; c < 3; c++) {
-            CK(copy_sync(s, m.x[c], X[c].data(), n * 8, cudaMemcpyHostToDevice));
-            CK(copy_sync(s, m.xp[c], X[c].data(), n * 8, cudaMemcpyHostToDevice));
-        }
-        for (int c = 0; c < 9; c++) CK(copy_sync(s, m.gp[c], init_gp.data(), n * 8, cudaMemcpyHostToDevice));
-        for (int c = 0; c < 18; c++) CK(cudaMemsetAsync(m.fx[c], 0, n * 8, s->st));
-    }
+    CK(cudaMemsetAsync(s->counters + 6, 0, sizeof(int), s->st));
+    k_init_refmap<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->counters + 6);
+    s->count();
+    int e = read_ctl(s);
+    if (e) return e;
+    if (s->h_counters[6] > 0) return fail(RMT3D_ERR_INVALID, "init_refmap: overlapping primary points");
     comm_primary(s);
     return 0;
 }
@@ -669,6 +779,7 @@ static void ph_ustar(rmt3d_scene *s) {
 // result does not depend on scheduling (scenes give the same answer alone
 // and when they share the device with others).
 constexpr int kMeanBlocks = 148;
+constexpr int kDiagVals = 8;
 
 __global__ void k_mean(const double *x, size_t n, double scale, double *out, unsigned *ticket) {
     double sum = 0;
@@ -1034,6 +1145,24 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
         }
         s->own_stream = true;
     }
+    {
+        // keep up to 16 GB of freed scene memory in the device's pool, so that
+        // scenes created after others were destroyed reuse it without a trip
+        // to the driver's allocator
+        static std::mutex mu;
+        static bool done[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev >= 0 && dev < 64 && !done[dev]) {
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                uint64_t thr = 16ull << 30;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+            }
+            done[dev] = true;
+        }
+    }
     grid_dev &g = s->g;
     memset(&g, 0, sizeof(g));
     g.sm = d.sys_size[0];
@@ -1207,7 +1336,8 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
         e |= s->alloc(&s->lay, n) | s->alloc(&s->inl, n) | s->alloc(&s->front[0], n) | s->alloc(&s->front[1], n);
     }
     e |= s->alloc(&s->ctl, 1) | s->alloc(&s->d_mean, 1 + kMeanBlocks) | s->alloc(&s->d_red, 4) |
-         s->alloc(&s->mean_ticket, 1);
+         s->alloc(&s->mean_ticket, 1) | s->alloc(&s->d_diag, kDiagVals * (1 + kMeanBlocks)) |
+         s->alloc(&s->diag_ticket, 1);
     if (e || cudaMallocHost(&s->h_ctl, sizeof(scene_ctl)) != cudaSuccess ||
         cudaMallocHost(&s->h_scalar, sizeof(double)) != cudaSuccess) {
         rmt3d_scene_destroy(s);
@@ -1355,6 +1485,8 @@ extern "C" int rmt3d_prepare(rmt3d_scene *s) {
     rmt3d_set_dt(s, dt);
     if ((e = rmt3d_init_iter(s))) return e;
     rmt3d_set_dt(s, dt);  // stepper::run re-links dt (stepper.hh:336)
+    // build the step graph now, so that the first step's latency is a step's
+    if (graph_mode(s) && (s->graph_dirty || !s->step_exec) && (e = build_step_graph(s))) return e;
     return RMT3D_OK;
 }
 
@@ -1638,10 +1770,94 @@ extern "C" int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *ref
     return RMT3D_OK;
 }
 
+// Solid diagnostics over the interior cells, reduced in a fixed order (block
+// partials, summed by the last block in block order):
+//  [0] sum H(phi) and [1..3] sum x H(phi), y H(phi), z H(phi) over the primary
+//      maps (compute_centroid, fluid_3d_utils.cc:1348-1379);
+//  [4] sum of squared mean |det F - 1| over the six faces of each primary
+//      map's cell, [5] its maximum (total_dev_in_detF, :1032-1084).
+__global__ void k_solid_diag(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                             const double *lz, double *out, unsigned *ticket) {
+    double v[kDiagVals] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int ncell = g.sm * g.sn * g.so;
+    const int strides[3] = {1, g.sm4, g.smn4};
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += gridDim.x * blockDim.x) {
+        const int i = t % g.sm + 2, j = (t / g.sm) % g.sn + 2, k = t / (g.sm * g.sn) + 2;
+        const int ind = gidx(g, i, j, k);
+        for (int o = 0; o < g.n_obj; o++) {
+            const objmap_dev &m = F->om[o];
+            if (m.code[ind] != 0) continue;
+            const double sf = heaviside(g, obj_phi(g, o, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
+            v[0] += sf;
+            v[1] += lx[i] * sf;
+            v[2] += ly[j] * sf;
+            v[3] += lz[k] * sf;
+            double dev = 0;
+            for (int a = 0; a < 3; a++) {
+                dev += fabs(m.det[a][ind] - 1);
+                const int nb = ind + strides[a];
+                if (m.code[nb] >= 0) dev += fabs(m.det[a][nb] - 1);
+            }
+            dev /= 6.;
+            v[4] += dev * dev;
+            v[5] = fmax(v[5], dev * dev);
+        }
+    }
+    __shared__ double sh[kDiagVals][32];
+    __shared__ bool last;
+    for (int c = 0; c < kDiagVals; c++) {
+        double a = v[c];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double b = __shfl_xor_sync(0xffffffffu, a, o);
+            a = (c == 5) ? fmax(a, b) : a + b;
+        }
+        if ((threadIdx.x & 31) == 0) sh[c][threadIdx.x >> 5] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < kDiagVals; c++) {
+            double a = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) a = (c == 5) ? fmax(a, sh[c][w]) : a + sh[c][w];
+            out[kDiagVals * (1 + blockIdx.x) + c] = a;
+        }
+        __threadfence();
+        last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x < kDiagVals) {
+        __threadfence();
+        const int c = threadIdx.x;
+        const volatile double *part = out + kDiagVals;
+        double a = 0;
+        for (unsigned b = 0; b < gridDim.x; b++) a = (c == 5) ? fmax(a, part[kDiagVals * b + c]) : a + part[kDiagVals * b + c];
+        out[c] = a;
+        if (c == 0) *ticket = 0;
+    }
+}
+
+static int solid_diag(rmt3d_scene *s, double out[kDiagVals]) {
+    k_solid_diag<<<kMeanBlocks, 256, 0, s->st>>>(s->g, s->dF, s->lx, s->ly, s->lz, s->d_diag, s->diag_ticket);
+    s->count();
+    CK(cudaMemcpyAsync(out, s->d_diag, kDiagVals * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return 0;
+}
+
 extern "C" int rmt3d_diag(rmt3d_scene *s, int kind, double *value) {
     if (!s || !value) return fail(RMT3D_ERR_INVALID, "null argument");
     if (kind == 0) return div_u(s, value);
-    return fail(RMT3D_ERR_INVALID, "unknown diagnostic");
+    if (kind < 1 || kind > 6) return fail(RMT3D_ERR_INVALID, "unknown diagnostic");
+    double v[kDiagVals];
+    int e = solid_diag(s, v);
+    if (e) return e;
+    const double dv = s->g.dx * s->g.dy * s->g.dz;
+    switch (kind) {
+        case 1: *value = v[0] * dv; break;                 // compute_centroid's vol
+        case 2: case 3: case 4: *value = v[kind - 1] / v[0]; break;  // centroid x, y, z
+        case 5: *value = sqrt(v[4] * dv); break;           // total_dev_in_detF
+        case 6: *value = sqrt(v[5]); break;                // its max_dev
+    }
+    return RMT3D_OK;
 }
 
 extern "C" int rmt3d_sync(rmt3d_scene *s) {
@@ -1653,6 +1869,17 @@ extern "C" int rmt3d_sync(rmt3d_scene *s) {
 extern "C" int rmt3d_launch_count(rmt3d_scene *s, long long *count) {
     if (!s || !count) return fail(RMT3D_ERR_INVALID, "null argument");
     *count = s->launches;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_scene_set_mg_launch(rmt3d_scene *s, int cluster) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (cluster && (!s->mac.cluster_size || !s->fem.cluster_size))
+        return fail(RMT3D_ERR_UNSUPPORTED, "thread-block clusters of 8 or more CTAs are not available");
+    s->mac.use_cluster = s->fem.use_cluster = cluster != 0;
+    s->mac.invalidate();
+    s->fem.invalidate();
+    s->graph_dirty = true;
     return RMT3D_OK;
 }
 
@@ -1679,6 +1906,7 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     if (d->n_obj > 0) b += n * (2 * sizeof(uint8_t) + 2 * sizeof(int));
     b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);
     b += sizeof(fields_dev) + sizeof(scene_ctl) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);
+    b += kDiagVals * (1 + kMeanBlocks) * sizeof(double) + sizeof(unsigned);
     int prd[3], nm[3], nf[3];
     for (int a = 0; a < 3; a++) {
         prd[a] = d->periodic[a] != 0;
@@ -1761,7 +1989,10 @@ extern "C" int rmt3d_scene_destroy(rmt3d_scene *s) {
     for (cudaEvent_t e : s->prof.ev) cudaEventDestroy(e);
     if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
     s->gb.release();
-    for (void *p : s->allocs) cudaFree(p);
+    for (void *p : s->allocs) cudaFreeAsync(p, s->st);
+    s->mac.release();
+    s->fem.release();
+    cudaStreamSynchronize(s->st);
     if (s->h_ctl) cudaFreeHost(s->h_ctl);
     if (s->h_scalar) cudaFreeHost(s->h_scalar);
     if (s->own_stream) cudaStreamDestroy(s->st);

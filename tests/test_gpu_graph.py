@@ -85,3 +85,29 @@ def test_graph_run_stops_at_failing_step(tmp_path):
         assert sc.scalar(4) == nt0 + 1  # the later steps did not run
     finally:
         sc.close()
+
+
+@pytest.mark.parametrize("kind", ["sphere", "mixed", "varden"])
+def test_cluster_solve_matches_phase_launches(tmp_path, kind):
+    """The whole-solve cluster kernel and the per-phase launches apply the
+    same operators and control; solved to round-off they agree closely."""
+    text = scenes.cavity_sphere(24, steps=4, radius=0.25, rho=1.4 if kind == "varden" else 1.0)
+    desc = R.desc_from_cfg(scenes.write(str(tmp_path / "c.cfg"), text))
+    desc.mg_exact = 1
+    if kind == "mixed":
+        desc.precision = R.MIXED
+    if kind == "varden":
+        desc.var_den = 1
+    out = []
+    for cluster in (1, 0):
+        sc = R.Scene(desc)
+        try:
+            sc.set_mg_launch(cluster)
+            sc.prepare()
+            assert sc.run(4) == R.NORMAL_EXIT
+            out.append({f: sc.field(f)[H.INTERIOR] for f in ("u", "v", "w", "p")})
+        finally:
+            sc.close()
+    for f in out[0]:
+        e = H.rel_l2(out[0][f], out[1][f])
+        assert e < 1e-10, (f, e)
