@@ -94,6 +94,11 @@ typedef struct {
                       mg_probs.hh:483-518); 1: additionally iterate every
                       Poisson solve until its residual stops shrinking, so
                       results are free of tolerance-level noise */
+    double mixed_rtol; /* mixed form only: a solve also ends once its max-norm
+                          residual is below mixed_rtol times the max-norm of
+                          its right-hand side, and skips the two insurance
+                          cycles (the form's accuracy target is 1e-5 rel-L2);
+                          0 keeps the reference's control.  Default 1e-9. */
 } rmt3d_scene_desc;
 
 typedef struct rmt3d_scene rmt3d_scene;

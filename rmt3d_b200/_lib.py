@@ -78,6 +78,7 @@ class SceneDesc(ctypes.Structure):
         ("var_den", ctypes.c_int),
         ("precision", ctypes.c_int),
         ("mg_exact", ctypes.c_int),
+        ("mixed_rtol", ctypes.c_double),
     ]
 
 

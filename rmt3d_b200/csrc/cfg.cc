@@ -64,6 +64,7 @@ extern "C" int rmt3d_desc_defaults(rmt3d_scene_desc *d) {
     d->sys_size[0] = d->sys_size[1] = d->sys_size[2] = 96;
     d->sim_type = RMT3D_SIM_FTEST;
     d->precision = RMT3D_FP64;
+    d->mixed_rtol = 1e-9;
     return RMT3D_OK;
 }
 
@@ -233,6 +234,9 @@ extern "C" int rmt3d_desc_from_cfg(const char *path, rmt3d_scene_desc *d) {
         } else if (k == "precision") {
             // extension keyword: 0 FP64, 1 FP32 V-cycles inside FP64 refinement
             d->precision = t.next_int();
+        } else if (k == "mixed_rtol") {
+            // extension keyword: relative solve tolerance of the mixed form
+            d->mixed_rtol = t.next_double();
         } else {
             fclose(f);
             return rmt3d::fail(RMT3D_ERR_INVALID, "Unrecognized keyword '" + k + "' at line " + std::to_string(t.line));

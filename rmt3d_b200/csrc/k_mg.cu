@@ -529,7 +529,7 @@ size_t mg_solver::footprint(mg_kind k, const int n[3], const int prd[3], bool mi
     for (auto &l : v) b += l.npts() * (3 * sizeof(double) + (mixed_form ? 3 * sizeof(float) : 0));
     // the coarsest-level inverse is shared by all solvers with that level
     // (one copy per distinct level shape in the process) and not counted here
-    return b + sizeof(double);
+    return b + 2 * sizeof(double);
 }
 
 int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_form, cudaStream_t st) {
@@ -568,10 +568,10 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
         const char *e = getenv("RMT3D_MG_CLUSTER");
         if (e && e[0] == '1') use_cluster = true;
     }
-    if (cudaMallocAsync((void **)&d_max, sizeof(unsigned long long), st) != cudaSuccess)
+    if (cudaMallocAsync((void **)&d_max, 2 * sizeof(unsigned long long), st) != cudaSuccess)
         return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
-    bytes_alloc += sizeof(unsigned long long);
-    cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st);
+    bytes_alloc += 2 * sizeof(unsigned long long);
+    cudaMemsetAsync(d_max, 0, 2 * sizeof(unsigned long long), st);
     return 0;
 }
 
@@ -759,24 +759,46 @@ __global__ void k_mg_begin(mg_ctl *c, unsigned long long *mx, cudaGraphCondition
     c->it = 0;
     c->count = 0;
     c->active = 1;
-    *mx = 0;
+    mx[0] = 0;
+    mx[1] = 0;
     if (armed) cudaGraphSetConditional(h, 1u);
 }
 
-__global__ void k_mg_ctl(mg_ctl *c, unsigned long long *mx, double tol, int exact, cudaGraphConditionalHandle h,
-                         int armed) {
-    const double r = __longlong_as_double((long long)*mx);
-    *mx = 0;
+// max |r| of the right-hand side into mx[1] (ordered bits), for the mixed
+// form's relative tolerance
+__global__ void k_absmax(const double *__restrict__ r, size_t n, unsigned long long *mx) {
+    double a = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = fabs(r[i]);
+        if (v != v || v > a) a = (v != v) ? __longlong_as_double(0x7ff8000000000000LL) : v;
+    }
+    unsigned long long b = (unsigned long long)__double_as_longlong(a);
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
+        b = t > b ? t : b;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(mx + 1, b);
+}
+
+__global__ void k_mg_ctl(mg_ctl *c, unsigned long long *mx, double tol, double rtol, int exact,
+                         cudaGraphConditionalHandle h, int armed) {
+    const double r = __longlong_as_double((long long)mx[0]);
+    mx[0] = 0;
+    // the mixed form's relative tolerance (mixed_rtol x max |rhs|)
+    const double rhs = __longlong_as_double((long long)mx[1]);
+    const double tol_eff = (rtol > 0 && rtol * rhs > tol) ? rtol * rhs : tol;
     c->count++;
     c->cycles_total++;
     bool done = false;
     if (c->phase <= 1) {
         if (--c->todo <= 0) {
             c->res_out = r;
-            if (r > tol && c->extra < 20) {
+            if (r > tol_eff && c->extra < 20) {
                 c->extra++;
                 c->todo = c->extra;
                 c->phase = 1;
+            } else if (rtol > 0 && !exact) {
+                done = true;  // the relaxed form skips the insurance cycles
             } else {
                 c->phase = 2;
                 c->todo = 2;
@@ -827,7 +849,7 @@ void mg_solver::launch_body(cudaStream_t st, bool armed, unsigned long long h) {
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]);
     if (kind == MG_MAC) LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, d_max, F.ri)));
     else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, d_max, F.ri)));
-    LAUNCH(k_mg_ctl<<<1, 1, 0, st>>>(ctl, d_max, max_norm_tol, exact ? 1 : 0, h, armed ? 1 : 0));
+    LAUNCH(k_mg_ctl<<<1, 1, 0, st>>>(ctl, d_max, max_norm_tol, rtol, exact ? 1 : 0, h, armed ? 1 : 0));
 }
 
 int mg_solver::capture_solve(cudaStream_t cur, graph_builder &gb) {
@@ -835,11 +857,14 @@ int mg_solver::capture_solve(cudaStream_t cur, graph_builder &gb) {
         // the whole solve is one kernel node
         gb.note(launch_cluster(cur));
         body_kernels = 0;
+        outside_kernels = 1;
         return gb.err == cudaSuccess ? 0 : -1;
     }
+    outside_kernels = rtol > 0 ? 2 : 1;
     cudaGraphConditionalHandle h = gb.handle(cur);
     if (gb.err != cudaSuccess) return -1;
     k_mg_begin<<<1, 1, 0, cur>>>(ctl, d_max, h, 1);
+    if (rtol > 0) k_absmax<<<148, 256, 0, cur>>>(lv[0].r, lv[0].npts(), d_max);
     cudaStream_t body = gb.open(cur, h, cudaGraphCondTypeWhile);
     if (!body) return -1;
     long long n = 0, *saved = launches;
@@ -897,6 +922,10 @@ double mg_solver::run(cudaStream_t st) {
         // launch by launch, so that the profiler's events bracket single kernels
         k_mg_begin<<<1, 1, 0, st>>>(ctl, d_max, 0, 0);
         if (launches) (*launches)++;
+        if (rtol > 0) {
+            k_absmax<<<148, 256, 0, st>>>(lv[0].r, lv[0].npts(), d_max);
+            if (launches) (*launches)++;
+        }
         for (int guard = 0; guard < kMgMaxCycles; guard++) {
             launch_body(st, false, 0);
             cudaMemcpyAsync(h_ctl, ctl, sizeof(mg_ctl), cudaMemcpyDeviceToHost, st);

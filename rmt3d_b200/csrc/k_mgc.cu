@@ -32,7 +32,7 @@ constexpr int kClThreads = 512;
 
 struct cmg_args {
     pmg_args A;
-    double tol;
+    double tol, rtol;
     int exact, mixed;
     mg_ctl *ctl;
 };
@@ -155,6 +155,18 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(cmg_args P) {
     if (todo < 1) todo = 1;
     double prev = 0, res_out = 0;
     bool done = false;
+    double tol = P.tol;
+    if (P.rtol > 0) {
+        // the mixed form's relative tolerance: mixed_rtol x max |rhs|
+        double a = 0;
+        const int n0 = L0.n[0] * L0.n[1] * L0.n[2];
+        for (int t = t0; t < n0; t += ts) {
+            const double v = fabs(L0.r[t]);
+            if (v != v || v > a) a = v;
+        }
+        const double rhs = cl_max(cl, a);
+        if (P.rtol * rhs > tol) tol = P.rtol * rhs;
+    }
     while (!done) {
         cl_iterate(P, cl, t0, ts);
         const double r = cl_max(cl, ph_resid<double>(P.A.kind, ldev(L0), L0.x, L0.r, nullptr, L0.ri, t0, ts));
@@ -162,10 +174,12 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(cmg_args P) {
         if (phase <= 1) {
             if (--todo <= 0) {
                 res_out = r;
-                if (r > P.tol && extra < 20) {
+                if (r > tol && extra < 20) {
                     extra++;
                     todo = extra;
                     phase = 1;
+                } else if (P.rtol > 0 && !P.exact) {
+                    done = true;  // the relaxed form skips the insurance cycles
                 } else {
                     phase = 2;
                     todo = 2;
@@ -276,6 +290,7 @@ cudaError_t mg_solver::launch_cluster(cudaStream_t st) {
     memset(&P, 0, sizeof(P));
     P.A = level_args(*this);
     P.tol = max_norm_tol;
+    P.rtol = rtol;
     P.exact = exact ? 1 : 0;
     P.mixed = mixed ? 1 : 0;
     P.ctl = ctl;

@@ -84,6 +84,7 @@ class mg_solver {
     int last_cycles = 0;
     bool mixed = false;  // FP32 cycles inside FP64 iterative refinement
     bool exact = false;  // iterate each solve until the residual stagnates
+    double rtol = 0;     // mixed form: relative tolerance (x max |rhs|), no insurance cycles
     long long *launches = nullptr;
     kernel_profiler *prof = nullptr;
     mg_ctl *ctl = nullptr;       // device control block (owned by the scene)
@@ -126,7 +127,7 @@ class mg_solver {
     // WHILE node whose body is one iteration, the residual norm and the
     // control kernel.  Returns the kernels per loop iteration.
     int capture_solve(cudaStream_t cur, graph_builder &gb);
-    int outside_kernels = 1;   // kernels of a solve outside its loop body
+    int outside_kernels = 1;   // kernels of a solve outside its loop body (set by capture_solve)
     int body_kernels = 0;      // kernels per loop iteration (set by capture_solve)
     void invalidate();         // drop the solver's own graph (schedule changed)
     void release();            // free the device memory (stream-ordered, on the set-up stream)

@@ -1378,6 +1378,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     int nm[3] = {g.sm, g.sn, g.so}, nf[3] = {g.fm, g.fn, g.fo};
     bool mixed = d.precision == RMT3D_MIXED;
     s->mac.exact = s->fem.exact = d.mg_exact != 0;
+    s->mac.rtol = s->fem.rtol = (mixed && d.mixed_rtol > 0) ? d.mixed_rtol : 0;
     s->mac.vd = s->fem.vd = d.var_den != 0;
     if ((e = s->mac.setup(MG_MAC, nm, g.prd, mixed, s->st)) != 0 || (e = s->fem.setup(MG_FEM, nf, g.prd, mixed, s->st)) != 0) {
         rmt3d_scene_destroy(s);
