@@ -160,6 +160,23 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def reduce_max(dist, x, device="cuda"):
+    """Max over ranks of a per-rank scalar (the replicas' timing rule); the
+    identity without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, cells, steps, ms_max):
+    """Whole-job throughput of `world` independent replicas, each stepping a
+    scene of `cells` cells `steps` times, timed as the slowest rank."""
+    return world * cells * steps / (ms_max / 1e3) / 1e6
+
+
 def percentiles(xs):
     import numpy as np
     if not xs:
@@ -202,6 +219,41 @@ def form_batched(R, args):
             "prepare_s": prep, "schedules": {str(k): list(v) for k, v in tuned.items()},
             "workload": "seeded cavities, n in {32,48,64,96}, 1-8 spheres R~U(0.08,0.15), G log-U[0.1,10], "
                         "lid U(0.5,1.5), solid density U(0.8,1.2) (variable-density projection), mixed precision"}
+
+
+def form_stretched(R, args):
+    """The pre-stretched sphere relaxing in a periodic box (128^3, radius 0.3,
+    1.3x volume-preserving stretch, viscosity 0.005): FP64 and mixed forms,
+    solid volume drift and the mixed form's error against FP64."""
+    import numpy as np
+    import torch
+    wd = tempfile.mkdtemp(prefix="rmt3d_str_")
+    n, steps = args.stretch_size, args.stretch_steps
+    cfg = scenes.write(os.path.join(wd, "s.cfg"), scenes.stretched_sphere(n, steps, radius=0.3))
+    out, fields = {}, {}
+    for name, prec in (("fp64", R.FP64), ("mixed", R.MIXED)):
+        sc = R.Scene.from_cfg(cfg, precision=prec)
+        sc.prepare()
+        v0 = sc.diag(1)
+        sc.sync()
+        t0 = time.perf_counter()
+        if sc.run(steps) != R.NORMAL_EXIT:
+            raise RuntimeError("stretched-sphere step failed")
+        sc.sync()
+        wall = time.perf_counter() - t0
+        out[name] = {"value": n ** 3 * steps / wall / 1e6, "ms_per_step": 1e3 * wall / steps,
+                     "volume_drift": sc.diag(1) / v0 - 1, "detF_dev": sc.diag(5)}
+        sl = (slice(2, -2),) * 3
+        fields[name] = {f: sc.field(f)[sl] for f in ("u", "v", "w", "p")}
+        sc.close()
+        torch.cuda.synchronize()
+    a, b = fields["fp64"], fields["mixed"]
+    va, vb = np.stack([a[f] for f in "uvw"]), np.stack([b[f] for f in "uvw"])
+    out["mixed"]["rel_l2_vs_fp64"] = {"velocity": float(np.linalg.norm(vb - va) / np.linalg.norm(va)),
+                                      "p": float(np.linalg.norm(b["p"] - a["p"]) / np.linalg.norm(a["p"]))}
+    out["workload"] = "periodic %d^3 box, pre-stretched sphere R=0.3 (1.3x along x), G=1, mu=0.005, %d steps, " \
+                      "wall-clock timed" % (n, steps)
+    return out
 
 
 def serve_stream(R, wd, seconds, rate, steps, seed, precision):
@@ -280,17 +332,21 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(dist, x)
 
     def make(precision):
         d = R.desc_from_cfg(cfg)
         d.precision = precision
+        # the multigrid schedule chosen by the project's autotuner (timing
+        # candidates on a probe copy of the scene)
+        b = R.Batch([d], host_threads=1)
+        tuned = list(b.autotune(probe_steps=3).values())[0]
+        b.close()
         sc = R.Scene(d, stream=stream.cuda_stream)
+        sc.set_schedule(tuned[0], tuned[1], 0)
+        sc.set_mg_launch(tuned[2])
         sc.prepare()
+        sc.schedule = tuned
         return sc
 
     def timed(sc, k):
@@ -350,12 +406,12 @@ def run_ours(args):
     with ClockSampler(local) as clk:
         ms64, launches64 = timed(s64, args.steps)
     clocks = clk.summary()
-    v64 = world * cells * args.steps / (ms64 / 1e3) / 1e6
+    v64 = replica_value(world, cells, args.steps, ms64)
     lat64 = step_latency(s64, max(5, args.steps // 2))
     # mixed form (FP32 V-cycles inside FP64 iterative refinement)
     smx = make(R.MIXED)
     msmx, launchesmx = timed(smx, args.steps)
-    vmx = world * cells * args.steps / (msmx / 1e3) / 1e6
+    vmx = replica_value(world, cells, args.steps, msmx)
     latmx = step_latency(smx, max(5, args.steps // 2))
     # both scenes have now run the same number of steps from the same state
     sl = (slice(2, -2),) * 3
@@ -377,14 +433,16 @@ def run_ours(args):
     bufs = [torch.empty(shp, dtype=torch.float64, pin_memory=True) for _ in range(4)]
     sce = smx if head_form == "mixed" else s64
     mse = e2e(sce, args.steps, bufs)
-    ve = world * cells * args.steps / (mse / 1e3) / 1e6
+    ve = replica_value(world, cells, args.steps, mse)
     d2h = 4 * s64.ncell * 8
     roof = roofline(R, sce, args)
     for s_ in (s64, smx):
         s_.close()
-    batched = served = None
+    batched = served = stretched = None
     if world == 1 and not args.no_batched:
         batched = form_batched(R, args)
+    if world == 1 and not args.no_stretched:
+        stretched = form_stretched(R, args)
     if world == 1 and not args.no_served:
         served = form_served(R, args)
     cpu = None
@@ -403,11 +461,11 @@ def run_ours(args):
             "config": dict(config_block(n, "state %.0f MB per scene > 126 MB L2" % (state_mb_desc(R, cfg))),
                            headline_form=head_form),
             "forms": {"fp64": {"value": v64, "ms_per_step": ms64 / args.steps, "gpu_launches": launches64,
-                               "step_latency_ms": lat64},
+                               "step_latency_ms": lat64, "schedule": list(s64.schedule)},
                       "mixed": {"value": vmx, "ms_per_step": msmx / args.steps, "gpu_launches": launchesmx,
-                                "step_latency_ms": latmx, "rel_l2_vs_fp64": errs,
+                                "step_latency_ms": latmx, "rel_l2_vs_fp64": errs, "schedule": list(smx.schedule),
                                 "steps_compared": 2 * args.warmup + args.steps + max(5, args.steps // 2)},
-                      "batched": batched, "served": served},
+                      "batched": batched, "served": served, "stretched": stretched},
             "e2e": {"value": ve, "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": roof,
@@ -467,6 +525,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-stretched", action="store_true")
+    ap.add_argument("--stretch-size", type=int, default=128)
+    ap.add_argument("--stretch-steps", type=int, default=20)
     ap.add_argument("--batch-scenes", type=int, default=32)
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--serve-steps", type=int, default=20)
