@@ -10,6 +10,7 @@
 // candidates on a probe scene.
 #include <algorithm>
 #include <array>
+#include <cstdlib>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -35,7 +36,53 @@ struct rmt3d_batch {
     std::vector<int> status;
     std::map<int, std::array<int, 3>> tuned;  // grid cells -> (v_down, v_up, cluster launch)
     int nthreads = 1;
+    // equally sized scenes stepped together: one graph per group, each
+    // multigrid solve batched over the group's scenes
+    std::vector<rmt3d::scene_group *> sg;
+    std::vector<std::vector<int>> sg_members;
+    bool sg_dirty = true;
+    bool use_groups = true;
 };
+
+namespace {
+void drop_groups(rmt3d_batch *b) {
+    for (auto *g : b->sg) rmt3d::group_destroy(g);
+    b->sg.clear();
+    b->sg_members.clear();
+    b->sg_dirty = true;
+}
+
+// partition the scenes into groups that can share batched solves: same grid,
+// periodicity, form and multigrid schedule
+int build_groups(rmt3d_batch *b) {
+    drop_groups(b);
+    std::map<std::vector<double>, std::vector<int>> part;
+    for (size_t i = 0; i < b->scenes.size(); i++) {
+        const rmt3d_scene_desc &d = b->descs[i];
+        auto it = b->tuned.find((int)((long long)d.sys_size[0] * d.sys_size[1] * d.sys_size[2]));
+        const int vd = it != b->tuned.end() ? it->second[0] : 2, vu = it != b->tuned.end() ? it->second[1] : 2;
+        std::vector<double> key = {(double)d.sys_size[0], (double)d.sys_size[1], (double)d.sys_size[2],
+                                   (double)d.periodic[0], (double)d.periodic[1], (double)d.periodic[2],
+                                   (double)d.precision, (double)d.var_den, (double)d.mg_exact, d.mixed_rtol,
+                                   (double)vd, (double)vu};
+        part[key].push_back((int)i);
+    }
+    for (auto &kv : part) {
+        std::vector<rmt3d_scene *> sc;
+        for (int i : kv.second) sc.push_back(b->scenes[i]);
+        rmt3d::scene_group *g = nullptr;
+        int e = rmt3d::group_create(sc.data(), (int)sc.size(), &g);
+        if (e) {
+            drop_groups(b);
+            return e;
+        }
+        b->sg.push_back(g);
+        b->sg_members.push_back(kv.second);
+    }
+    b->sg_dirty = false;
+    return 0;
+}
+}  // namespace
 
 namespace {
 
@@ -108,6 +155,7 @@ extern "C" int rmt3d_batch_create(const rmt3d_scene_desc *descs, int nscenes, in
 
 extern "C" int rmt3d_batch_prepare(rmt3d_batch *b) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
+    drop_groups(b);
     return for_all(b, [&](int i) { return rmt3d_prepare(b->scenes[i]); });
 }
 
@@ -116,6 +164,38 @@ extern "C" int rmt3d_batch_prepare(rmt3d_batch *b) {
 // scene of the batch is in flight on the device at once.
 extern "C" int rmt3d_batch_step(rmt3d_batch *b, int nsteps, int *status) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
+    {
+        const char *e = getenv("RMT3D_GRAPH");
+        if ((e && e[0] == '0') || (getenv("RMT3D_BATCH_GROUPS") && getenv("RMT3D_BATCH_GROUPS")[0] == '0'))
+            b->use_groups = false;
+    }
+    if (b->use_groups) {
+        if (b->sg_dirty) {
+            int e = build_groups(b);
+            if (e) return e;
+        }
+        int err = 0;
+        std::string msg;
+        for (auto *g : b->sg) {
+            int e = rmt3d::group_launch(g, nsteps);
+            if (e && !err) {
+                err = e;
+                msg = rmt3d_last_error();
+            }
+        }
+        for (size_t k = 0; k < b->sg.size(); k++) {
+            std::vector<int> st(b->sg_members[k].size(), 0);
+            int e = rmt3d::group_finish(b->sg[k], st.data());
+            if (e && !err) {
+                err = e;
+                msg = rmt3d_last_error();
+            }
+            for (size_t j = 0; j < st.size(); j++) b->status[b->sg_members[k][j]] = st[j];
+        }
+        if (status)
+            for (size_t i = 0; i < b->status.size(); i++) status[i] = b->status[i];
+        return err ? rmt3d::fail(err, msg) : RMT3D_OK;
+    }
     std::vector<int> err(b->groups.size(), 0);
     std::vector<std::string> msg(b->groups.size());
     std::vector<std::thread> th;
@@ -166,6 +246,7 @@ extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
 extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
+    drop_groups(b);
     static const int smooth[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
     std::map<long long, int> first;
     for (size_t i = 0; i < b->descs.size(); i++)
@@ -223,6 +304,7 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
 
 extern "C" int rmt3d_batch_destroy(rmt3d_batch *b) {
     if (!b) return RMT3D_OK;
+    drop_groups(b);
     for (auto *s : b->scenes) rmt3d_scene_destroy(s);
     delete b;
     return RMT3D_OK;

@@ -14,4 +14,15 @@ int fail(int code, const std::string &msg);
 // steps_launch and steps_finish only reports.
 int steps_launch(rmt3d_scene *s, int nsteps);
 int steps_finish(rmt3d_scene *s, int *status);
+
+// Equally sized scenes (same grid, form and multigrid schedule, all prepared)
+// stepped together by one graph: per-scene phases as parallel branches, each
+// multigrid solve one batched solve over the group.  group_finish fills one
+// status per scene.
+struct scene_group;
+int group_create(rmt3d_scene *const *scenes, int n, scene_group **out);
+int group_launch(scene_group *g, int nsteps);
+int group_finish(scene_group *g, int *status);
+void group_destroy(scene_group *g);
+long long group_mg_launches(const scene_group *g);
 }

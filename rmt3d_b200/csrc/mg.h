@@ -132,6 +132,7 @@ class mg_solver {
     void invalidate();         // drop the solver's own graph (schedule changed)
     void release();            // free the device memory (stream-ordered, on the set-up stream)
     void sync_host_mirror();   // cycles from the pinned control mirror
+    unsigned long long *max_slots() const { return d_max; }
 
   private:
     cudaStream_t alloc_stream = nullptr;
@@ -148,6 +149,46 @@ class mg_solver {
     void smooth(int l, int sweeps, cudaStream_t st);
     void smooth_f32(int l, int sweeps, cudaStream_t st);
     void refine_step(cudaStream_t st);
+};
+
+// One multigrid solve for every scene of a group of equally sized scenes
+// with the same form and schedule, each phase one launch over all of them
+// (k_mgb.cu).  The scenes' own solvers keep the level arrays and control
+// state; the group holds device tables of their pointers.
+struct mgb_level_tab {
+    double **x, **r, **res;
+    float **xs, **rs, **ress;
+    const double **ri;
+    const float **ris;
+};
+
+class mg_group {
+  public:
+    int B = 0;
+    mg_kind kind = MG_MAC;
+    std::vector<mg_level> lv;
+    bool mixed = false, exact = false, vd = false;
+    double tol = 0, rtol = 0;
+    int v_down = 2, v_up = 2;
+    const double *dense = nullptr;
+    std::vector<mgb_level_tab> tab;  // device tables per level
+    mg_ctl **ctls = nullptr;         // device table of the scenes' control blocks
+    unsigned long long **mx = nullptr;  // device table of the scenes' residual slots
+    int *part = nullptr;             // device flags: scene b takes part in the next solve
+    int *run = nullptr;              // device flags: scene b's solve is still running
+    int body_kernels = 0, outside_kernels = 1;
+
+    mg_group() = default;
+    mg_group(const mg_group &) = delete;
+    mg_group &operator=(const mg_group &) = delete;
+    ~mg_group();
+    int setup(const std::vector<mg_solver *> &solvers);
+    // append the group's solve (arming kernel + WHILE loop) to the capture
+    int capture(cudaStream_t cur, graph_builder &gb);
+
+  private:
+    void *dev_tables = nullptr;
+    void iterate(cudaStream_t st);
 };
 
 }  // namespace rmt3d

@@ -91,7 +91,7 @@ struct scene_ctl {
     int halted;  // a step of the step graph failed: its later launches do nothing
     int steps;   // steps the step graph has executed
     int status;  // status of the failing step
-    int pad;
+    int run_flag;  // the current step of a group graph runs for this scene
     int counters[8];  // [0..1] frontier sizes, [2] extrapolation errors, [3] corrector problems,
                       // [4] redraw fatal, [5] refmap-derivative errors
     mg_ctl mac, fem;
@@ -132,6 +132,7 @@ struct rmt3d_scene {
     bool capturing = false;
     bool use_graph = true;
     long long graph_fixed = 0;  // kernels per step outside the multigrid loops
+    long long param_version = 0;  // bumped whenever captured step parameters change
     double *d_diag = nullptr;  // solid diagnostics: [0..7] totals, then per-block partials
     unsigned *diag_ticket = nullptr;
     double *d_mean = nullptr;  // [0] mean, [1..] per-block partial sums
@@ -157,6 +158,13 @@ struct rmt3d_scene {
     }
     void count(int n = 1) { launches += n; }
 };
+
+// the step's captured parameters (dt, FEM basis, multigrid schedule) changed:
+// graphs that hold this scene's step must be captured again
+static void mark_dirty(rmt3d_scene *s) {
+    s->graph_dirty = true;
+    s->param_version++;
+}
 
 // A blocking copy ordered on the scene's (non-blocking) stream: plain
 // cudaMemcpy runs on the legacy stream, which does not wait for it.
@@ -1027,6 +1035,328 @@ static int build_step_graph(rmt3d_scene *s) {
     return 0;
 }
 
+struct pending_steps_g {
+    long long c0 = 0, f0 = 0;
+    int steps0 = 0;
+};
+
+// ---- groups: equally sized scenes stepped by one graph ---------------------
+// The per-scene phases run as parallel branches of one graph (one branch per
+// scene, forked and joined around the solves); each of the two multigrid
+// solves is one batched solve over the group (k_mgb.cu), each phase one
+// launch over all scenes.  A scene's gates are device flags: a halted scene
+// skips its branches and sits out the solves; a scene whose MAC solve gave
+// NaN or whose reference-map update must be reverted sits out the FEM solve.
+
+// step start: run only while not halted; per-step counters to zero; the
+// scene takes part in the MAC solve when it runs
+__global__ void k_gstep_gate(scene_ctl *c, int *mac_part, cudaGraphConditionalHandle h) {
+    const int run = c->halted == 0;
+    if (run)
+        for (int i = 2; i < 8; i++) c->counters[i] = 0;
+    c->run_flag = run;
+    *mac_part = run;
+    cudaGraphSetConditional(h, run ? 1u : 0u);
+}
+
+// after the MAC solve: continue when the step runs and the solve is finite;
+// the FEM solve flag starts cleared and is set by the branch that reaches it
+__global__ void k_gstep_seg2(scene_ctl *c, int *fem_part, cudaGraphConditionalHandle h) {
+    *fem_part = 0;
+    cudaGraphSetConditional(h, (c->run_flag && !c->mac.nan) ? 1u : 0u);
+}
+
+// after update_reference_map (objects): continue or revert, and take part in
+// the FEM solve only when continuing
+__global__ void k_gstep_branch(scene_ctl *c, int *fem_part, cudaGraphConditionalHandle h_rest,
+                               cudaGraphConditionalHandle h_rev) {
+    const bool err = c->mac.nan || c->counters[2] > 0 || c->counters[5] > 0;
+    const bool rest = !err && c->counters[3] == 0;
+    *fem_part = rest;
+    cudaGraphSetConditional(h_rest, rest ? 1u : 0u);
+    cudaGraphSetConditional(h_rev, (!err && c->counters[3] != 0) ? 1u : 0u);
+}
+
+__global__ void k_set_flag(int *f, int v) { *f = v; }
+
+// after the FEM solve: the rest of the step for the scenes that took part
+__global__ void k_gstep_seg3(const int *fem_part, cudaGraphConditionalHandle h) {
+    cudaGraphSetConditional(h, *fem_part ? 1u : 0u);
+}
+
+__global__ void k_gstep_end(scene_ctl *c, int with_objects) {
+    if (!c->run_flag) return;
+    int st = 0;
+    if (c->mac.nan) st = RMT3D_ERR_NAN;
+    else if (with_objects && (c->counters[2] > 0 || c->counters[5] > 0)) st = RMT3D_ERR_EXTRAP;
+    else if (with_objects && c->counters[3] != 0) st = RMT3D_REFMAP_UPDATE_ERR;
+    else if (c->fem.nan) st = RMT3D_PROJECTION_ERR;
+    else if (with_objects && c->counters[4] > 0) st = RMT3D_ERR_INVALID;
+    c->status = st;
+    c->halted = st != 0;
+    c->steps++;
+}
+
+namespace rmt3d {
+struct scene_group {
+    std::vector<rmt3d_scene *> sc;
+    mg_group mac, fem;
+    graph_builder gb;
+    cudaStream_t st = nullptr;
+    std::vector<cudaStream_t> br;
+    cudaEvent_t ev_fork = nullptr;
+    std::vector<cudaEvent_t> ev_join;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<long long> fixed;     // per scene: its own kernels per step
+    std::vector<long long> version;   // the scenes' parameter versions at capture
+    long long mg_launches = 0;        // batched multigrid kernels issued so far
+    std::vector<pending_steps_g> pend;
+    ~scene_group() {
+        if (exec) cudaGraphExecDestroy(exec);
+        gb.release();
+        for (cudaStream_t b : br) cudaStreamDestroy(b);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        for (cudaEvent_t e : ev_join) cudaEventDestroy(e);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+}  // namespace rmt3d
+
+// fork the capture of `main` into the scenes' branch streams
+static int g_fork(scene_group &G, cudaStream_t main) {
+    CK(cudaEventRecord(G.ev_fork, main));
+    for (cudaStream_t b : G.br) CK(cudaStreamWaitEvent(b, G.ev_fork, 0));
+    return 0;
+}
+static int g_join(scene_group &G, cudaStream_t main) {
+    for (size_t b = 0; b < G.br.size(); b++) {
+        CK(cudaEventRecord(G.ev_join[b], G.br[b]));
+        CK(cudaStreamWaitEvent(main, G.ev_join[b], 0));
+    }
+    return 0;
+}
+
+// capture work of scene b on its branch stream, counting its kernels
+template <typename F>
+static void g_on(scene_group &G, size_t b, F fn) {
+    rmt3d_scene *s = G.sc[b];
+    const cudaStream_t saved = s->st;
+    const long long l0 = s->launches;
+    s->st = G.br[b];
+    s->capturing = true;
+    fn(s);
+    s->capturing = false;
+    G.fixed[b] += s->launches - l0;
+    s->launches = l0;
+    s->st = saved;
+}
+
+// an IF node on scene b's current stream whose handle a kernel has just set
+template <typename F>
+static void g_if(scene_group &G, rmt3d_scene *s, cudaGraphConditionalHandle h, F body) {
+    const cudaStream_t cur = s->st;
+    cudaStream_t bs = G.gb.open(cur, h, cudaGraphCondTypeIf);
+    if (!bs) return;
+    s->st = bs;
+    body();
+    s->st = cur;
+    G.gb.close(bs);
+}
+
+static int build_group_graph(scene_group &G) {
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    G.exec = nullptr;
+    if (G.gb.init()) return fail(RMT3D_ERR_CUDA, "stream creation failed");
+    G.gb.err = cudaSuccess;
+    G.gb.depth = 0;
+    const size_t B = G.sc.size();
+    G.fixed.assign(B, 0);
+    G.version.clear();
+    for (rmt3d_scene *s : G.sc) G.version.push_back(s->param_version);
+    const cudaStream_t main = G.st;
+    CK(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+    // phases 1-4 up to the MAC solve
+    g_fork(G, main);
+    for (size_t b = 0; b < B; b++)
+        g_on(G, b, [&](rmt3d_scene *s) {
+            cudaGraphConditionalHandle h = G.gb.handle(s->st);
+            k_gstep_gate<<<1, 1, 0, s->st>>>(s->ctl, G.mac.part + b, h);
+            s->count();
+            g_if(G, s, h, [&]() {
+                compute_stress(s);
+                ph_edges(s);
+                ph_upwind(s);
+                ph_mac_pre(s, s->dt);
+            });
+        });
+    g_join(G, main);
+    if (G.mac.capture(main, G.gb)) G.gb.note(cudaErrorUnknown);
+    // phases 4-7 up to the FEM solve
+    g_fork(G, main);
+    for (size_t b = 0; b < B; b++)
+        g_on(G, b, [&](rmt3d_scene *s) {
+            int *fp = G.fem.part + b;
+            cudaGraphConditionalHandle h2 = G.gb.handle(s->st);
+            k_gstep_seg2<<<1, 1, 0, s->st>>>(s->ctl, fp, h2);
+            s->count();
+            g_if(G, s, h2, [&]() {
+                ph_mac_post(s, s->dt);
+                auto rest = [&]() {
+                    compute_stress(s);
+                    ph_ustar(s);
+                    ph_pp_pre(s);
+                };
+                if (s->g.n_obj > 0) {
+                    ph_refmap(s, s->dt);
+                    cudaGraphConditionalHandle h_rev = G.gb.handle(s->st), h_rest = G.gb.handle(s->st);
+                    k_gstep_branch<<<1, 1, 0, s->st>>>(s->ctl, fp, h_rest, h_rev);
+                    s->count();
+                    g_if(G, s, h_rev, [&]() {
+                        const long long l0 = s->launches;
+                        ph_revert(s);
+                        s->launches = l0;  // not part of a normal step
+                    });
+                    g_if(G, s, h_rest, rest);
+                } else {
+                    rest();
+                    k_set_flag<<<1, 1, 0, s->st>>>(fp, 1);
+                    s->count();
+                }
+            });
+        });
+    g_join(G, main);
+    if (G.fem.capture(main, G.gb)) G.gb.note(cudaErrorUnknown);
+    // phases 8-9 and the step's status
+    g_fork(G, main);
+    for (size_t b = 0; b < B; b++)
+        g_on(G, b, [&](rmt3d_scene *s) {
+            cudaGraphConditionalHandle h3 = G.gb.handle(s->st);
+            k_gstep_seg3<<<1, 1, 0, s->st>>>(G.fem.part + b, h3);
+            s->count();
+            g_if(G, s, h3, [&]() {
+                ph_pp_post(s);
+                ph_final(s);
+            });
+            k_gstep_end<<<1, 1, 0, s->st>>>(s->ctl, s->g.n_obj > 0);
+            s->count();
+            cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(scene_ctl), cudaMemcpyDeviceToHost, s->st);
+        });
+    g_join(G, main);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(main, &graph);
+    if (e != cudaSuccess || G.gb.err != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return fail(RMT3D_ERR_CUDA, std::string("group graph capture failed: ") +
+                                        cudaGetErrorString(e != cudaSuccess ? e : G.gb.err));
+    }
+    e = cudaGraphInstantiate(&G.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(RMT3D_ERR_CUDA, std::string("group graph instantiation: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+namespace rmt3d {
+int group_create(rmt3d_scene *const *scenes, int n, scene_group **out) {
+    *out = nullptr;
+    scene_group *G = new scene_group();
+    G->sc.assign(scenes, scenes + n);
+    std::vector<mg_solver *> ms, fs;
+    for (rmt3d_scene *s : G->sc) {
+        ms.push_back(&s->mac);
+        fs.push_back(&s->fem);
+        const rmt3d_scene *s0 = G->sc[0];
+        if (s->g.sm != s0->g.sm || s->g.sn != s0->g.sn || s->g.so != s0->g.so || s->g.prd[0] != s0->g.prd[0] ||
+            s->g.prd[1] != s0->g.prd[1] || s->g.prd[2] != s0->g.prd[2]) {
+            delete G;
+            return fail(RMT3D_ERR_INVALID, "scenes of a group must have the same grid");
+        }
+    }
+    int e = G->mac.setup(ms);
+    if (!e) e = G->fem.setup(fs);
+    if (!e && cudaStreamCreateWithFlags(&G->st, cudaStreamNonBlocking) != cudaSuccess) e = RMT3D_ERR_CUDA;
+    if (!e && cudaEventCreateWithFlags(&G->ev_fork, cudaEventDisableTiming) != cudaSuccess) e = RMT3D_ERR_CUDA;
+    for (int b = 0; b < n && !e; b++) {
+        cudaStream_t bs;
+        cudaEvent_t ev;
+        if (cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            e = RMT3D_ERR_CUDA;
+            break;
+        }
+        G->br.push_back(bs);
+        G->ev_join.push_back(ev);
+    }
+    // the group's launches must follow each scene's outstanding work
+    for (rmt3d_scene *s : G->sc)
+        if (!e && cudaStreamSynchronize(s->st) != cudaSuccess) e = RMT3D_ERR_CUDA;
+    if (!e) e = build_group_graph(*G);
+    if (e) {
+        delete G;
+        return e < 0 ? e : fail(RMT3D_ERR_CUDA, "group set-up failed");
+    }
+    *out = G;
+    return 0;
+}
+
+void group_destroy(scene_group *G) {
+    if (!G) return;
+    cudaStreamSynchronize(G->st);
+    delete G;
+}
+
+int group_launch(scene_group *G, int nsteps) {
+    G->pend.assign(G->sc.size(), pending_steps_g{});
+    for (size_t b = 0; b < G->sc.size(); b++) {
+        rmt3d_scene *s = G->sc[b];
+        if (s->param_version != G->version[b]) {
+            // dt, basis or schedule of a scene changed since the capture
+            int e = build_group_graph(*G);
+            if (e) return e;
+        }
+        G->pend[b].c0 = s->mac.cycles_total;
+        G->pend[b].f0 = s->fem.cycles_total;
+        G->pend[b].steps0 = s->h_ctl->steps;
+        CK(cudaMemsetAsync(&s->ctl->halted, 0, sizeof(int), G->st));
+        CK(cudaMemsetAsync(&s->ctl->status, 0, sizeof(int), G->st));
+    }
+    for (int i = 0; i < nsteps; i++) CK(cudaGraphLaunch(G->exec, G->st));
+    G->mg_launches += (long long)nsteps * (G->mac.outside_kernels + G->fem.outside_kernels);
+    return 0;
+}
+
+int group_finish(scene_group *G, int *status) {
+    CK(cudaStreamSynchronize(G->st));
+    CK(cudaGetLastError());
+    int first_err = 0;
+    std::string msg;
+    long long cmax = 0, fmax = 0;
+    for (size_t b = 0; b < G->sc.size(); b++) {
+        rmt3d_scene *s = G->sc[b];
+        const scene_ctl &h = *s->h_ctl;
+        const int done = h.steps - G->pend[b].steps0;
+        s->nt += done;
+        s->time = h.time;
+        s->mac.sync_host_mirror();
+        s->fem.sync_host_mirror();
+        cmax = std::max(cmax, s->mac.cycles_total - G->pend[b].c0);
+        fmax = std::max(fmax, s->fem.cycles_total - G->pend[b].f0);
+        s->launches += (long long)done * G->fixed[b];
+        status[b] = h.status;
+        if (h.status < 0 && !first_err) {
+            first_err = h.status;
+            msg = "scene " + std::to_string(b) + ": step status " + std::to_string(h.status);
+        }
+    }
+    // the batched loops ran as many iterations as the slowest scene needed
+    G->mg_launches += cmax * G->mac.body_kernels + fmax * G->fem.body_kernels;
+    if (first_err) return fail(first_err, msg);
+    return 0;
+}
+
+long long group_mg_launches(const scene_group *G) { return G->mg_launches; }
+}  // namespace rmt3d
+
 struct pending_steps {
     long long c0, f0;
     int steps0;
@@ -1426,7 +1756,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
 extern "C" int rmt3d_initialize(rmt3d_scene *s) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     set_time(s, 0);
-    s->graph_dirty = true;
+    mark_dirty(s);
     int e;
     if ((e = init_fluid(s))) return e;
     if ((e = init_pres(s))) return e;
@@ -1444,7 +1774,7 @@ extern "C" int rmt3d_initialize(rmt3d_scene *s) {
 
 extern "C" int rmt3d_set_dt(rmt3d_scene *s, double dt) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
-    if (dt != s->dt) s->graph_dirty = true;
+    if (dt != s->dt) mark_dirty(s);
     s->dt = dt;
     return RMT3D_OK;
 }
@@ -1707,7 +2037,7 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
     rmt3d_set_dt(s, dt);
     set_time(s, time);
     update_rho(s);  // the density the reference derives from the imported maps
-    s->graph_dirty = true;
+    mark_dirty(s);
     CK(cudaStreamSynchronize(s->st));
     return RMT3D_OK;
 }
@@ -1880,7 +2210,7 @@ extern "C" int rmt3d_scene_set_mg_launch(rmt3d_scene *s, int cluster) {
     s->mac.use_cluster = s->fem.use_cluster = cluster != 0;
     s->mac.invalidate();
     s->fem.invalidate();
-    s->graph_dirty = true;
+    mark_dirty(s);
     return RMT3D_OK;
 }
 
@@ -1892,7 +2222,7 @@ extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, in
     s->mac.v_up = s->fem.v_up = v_up;
     s->mac.invalidate();
     s->fem.invalidate();
-    s->graph_dirty = true;
+    mark_dirty(s);
     if (coarse_pts >= 0 && (s->mac.set_coarse(coarse_pts) || s->fem.set_coarse(coarse_pts)))
         return fail(RMT3D_ERR_CUDA, "coarse multigrid kernel configuration failed");
     return RMT3D_OK;

@@ -8,6 +8,7 @@ depend on what else runs, so the only differences allowed are those of the
 floating-point atomics of the checksum reduction, far below the tolerance
 used here (the step's own reductions sum in a fixed order).
 """
+import numpy as np
 import pytest
 
 import helpers as H
@@ -144,3 +145,80 @@ def test_serve_admission_by_budget(tmp_path):
     with pytest.raises(_lib.RMT3DError) as ei:
         R.serve(reqs, big // 2, max_slots=2)
     assert ei.value.code == _lib.ERR_TOO_LARGE
+
+
+def _group_descs(tmp_path, precision=R.FP64, var_den=0):
+    """Three 24^3 scenes that differ in their objects and lid speed (one group)
+    and one 16^3 scene (a group of its own)."""
+    cfgs = [
+        scenes.cavity_sphere(24, steps=4, radius=0.25, rho=1.3),
+        scenes.multi_sphere(24, 4, spheres=[((0.3, 0.3, 0.35), 0.15, 0.5, 0.8), ((0.7, 0.65, 0.4), 0.15, 2.0, 1.2)],
+                            lid=0.7),
+        scenes.cavity(24, steps=4, lid=1.3),
+        scenes.cavity_sphere(16, steps=4, radius=0.3),
+    ]
+    out = []
+    for i, c in enumerate(cfgs):
+        d = R.desc_from_cfg(scenes.write(str(tmp_path / ("g%d.cfg" % i)), c))
+        d.precision = precision
+        d.var_den = var_den
+        out.append(d)
+    return out
+
+
+@pytest.mark.parametrize("form", ["fp64", "mixed_vd"])
+def test_group_matches_alone_bitwise(tmp_path, form):
+    """Equally sized scenes step as one group (batched multigrid over the
+    group); each scene's result is bit for bit its solo result."""
+    descs = _group_descs(tmp_path, R.MIXED if form == "mixed_vd" else R.FP64, 1 if form == "mixed_vd" else 0)
+    b = R.Batch(descs, host_threads=2)
+    try:
+        b.prepare()
+        assert b.step(2) == [R.NORMAL_EXIT] * len(descs)
+        assert b.step(3) == [R.NORMAL_EXIT] * len(descs)
+        for i, d in enumerate(descs):
+            ref, _ = _alone(d, 5)
+            for f in ("u", "v", "w", "p"):
+                got = b.field(i, f)
+                assert np.array_equal(got[H.INTERIOR], ref[f][H.INTERIOR]), (i, f)
+    finally:
+        b.close()
+
+
+def test_group_failure_is_isolated(tmp_path):
+    """A scene of a group that fails stops at its failing step; the others of
+    the group keep stepping and stay bit-identical to their solo runs."""
+    import ctypes
+
+    descs = _group_descs(tmp_path)[:3]
+    b = R.Batch(descs, host_threads=1)
+    try:
+        b.prepare()
+        # plant a NaN in an interior cell of scene 2's velocity
+        h = b.scene_handle(2)
+        L = R.lib()
+        dims = (ctypes.c_int * 6)()
+        L.rmt3d_get_dims(h, dims)
+        sm4, sn4, so4 = dims[0], dims[1], dims[2]
+        from oracle.refdump import FIELD_DT, REFMAP_DT
+        fa = np.zeros(sm4 * sn4 * so4, dtype=FIELD_DT)
+        ra = np.zeros(sm4 * sn4 * so4, dtype=REFMAP_DT)
+        cnt = ctypes.c_int()
+        L.rmt3d_export_reference(h, fa.ctypes.data_as(ctypes.c_void_p), ra.ctypes.data_as(ctypes.c_void_p), None,
+                                 None, 0, ctypes.byref(cnt))
+        fa["vel"][10 + sm4 * (10 + sn4 * 10), 0] = np.nan
+        dt = ctypes.c_double()
+        L.rmt3d_get_scalar(h, 0, ctypes.byref(dt))
+        ei = np.zeros(1, dtype=np.int32)
+        em = np.zeros(1, dtype=REFMAP_DT)
+        assert L.rmt3d_import_reference(h, fa.ctypes.data_as(ctypes.c_void_p), ra.ctypes.data_as(ctypes.c_void_p),
+                                        ei.ctypes.data_as(ctypes.c_void_p), em.ctypes.data_as(ctypes.c_void_p), 0,
+                                        dt.value, 0.0) == 0
+        st = b.step(3)
+        assert st[2] == R.PROJECTION_ERR and st[:2] == [R.NORMAL_EXIT] * 2
+        for i in range(2):
+            ref, _ = _alone(descs[i], 3)
+            for f in ("u", "v", "w", "p"):
+                assert np.array_equal(b.field(i, f)[H.INTERIOR], ref[f][H.INTERIOR]), (i, f)
+    finally:
+        b.close()
