@@ -44,6 +44,10 @@ CASES = {
     "multi24": (scenes.multi_sphere(24, 4, spheres=[((0.3, 0.3, 0.35), 0.15, 0.5, 0.8),
                                                   ((0.7, 0.65, 0.4), 0.15, 2.0, 1.2),
                                                   ((0.45, 0.6, 0.72), 0.15, 1.0, 1.0)]), [0, 1, 4], True),
+    # two spheres 0.02 apart: their transition bands overlap, so the collision
+    # stress between the two solids is active from the first step
+    "collide24": (scenes.multi_sphere(24, 4, spheres=[((0.29, 0.5, 0.5), 0.2, 1.0, 1.0),
+                                                    ((0.71, 0.5, 0.5), 0.2, 2.0, 1.0)]), [0, 1, 4]),
 }
 # longer runs stored as interior (u, v, w, p) only
 LONG = {

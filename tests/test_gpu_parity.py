@@ -8,6 +8,8 @@ reference's residual tolerance.
 * varden24 (one sphere of density 1.5) and multi24 (three spheres of
   densities 0.8, 1.2, 1.0) are states of the reference's VAR_DEN build and
   run the variable-density form (1/rho-weighted MAC and FEM operators).
+* collide24 holds two spheres 0.02 apart, whose transition bands overlap:
+  the collision stress between solids (fluid_3d.cc:1465-1773) is active.
 * Over several steps the reference is not reproducible even by itself below
   a rounding envelope: rebuilt without FMA contraction, or with its own
   tolerance-based multigrid control, it moves by the amount stored in each
@@ -68,7 +70,7 @@ def make_scene(tmp_path, name, exact=1, prepare=True):
 
 
 @pytest.mark.parametrize("name,steps", [("cavity16", [1, 8]), ("sphere24", [1, 4]), ("stretch24", [1, 4]),
-                                        ("varden24", [1, 4]), ("multi24", [1, 4])])
+                                        ("varden24", [1, 4]), ("multi24", [1, 4]), ("collide24", [1, 4])])
 def test_full_path_matches_reference(tmp_path, name, steps):
     """run_sim's set-up (initialize, dt fit, 5 pressure pre-iterations) and
     the first steps, against the reference's states."""
@@ -97,7 +99,7 @@ def test_full_path_matches_reference(tmp_path, name, steps):
         sc.close()
 
 
-@pytest.mark.parametrize("name", ["cavity16", "sphere24", "stretch24", "varden24", "multi24"])
+@pytest.mark.parametrize("name", ["cavity16", "sphere24", "stretch24", "varden24", "multi24", "collide24"])
 def test_single_step_from_reference_state(tmp_path, name):
     """One step from the reference's own state (imported in its AoS layout)."""
     fx, sc = make_scene(tmp_path, name)

@@ -18,7 +18,7 @@ needs_ref = pytest.mark.skipif(not (os.path.exists(DRIVER) and os.path.exists(DR
 
 @needs_ref
 @pytest.mark.parametrize("name,k", [("cavity16", 1), ("sphere24", 1), ("stretch24", 0), ("varden24", 1),
-                                    ("multi24", 1)])
+                                    ("multi24", 1), ("collide24", 1)])
 def test_fixture_reproduces_from_reference(tmp_path, name, k):
     fx = H.load_fixture(name)
     cfg = H.fixture_cfg(fx, str(tmp_path / "case.cfg"))
@@ -36,7 +36,7 @@ def test_fixture_reproduces_from_reference(tmp_path, name, k):
 
 
 def test_fixture_invariants():
-    for name in ("cavity16", "sphere24", "stretch24", "varden24", "multi24"):
+    for name in ("cavity16", "sphere24", "stretch24", "varden24", "multi24", "collide24"):
         fx = H.load_fixture(name)
         for k in (0, 1):
             st = H.state(fx, k)
@@ -45,8 +45,12 @@ def test_fixture_invariants():
             # at most one map per object per cell
             keys = st["ext_index"].astype(np.int64) * 1024 + (st["ext_c"] & 1023)
             assert len(np.unique(keys)) == len(keys)
-            assert not set(st["prim_index"][st["prim_c"] != 0]) & set(st["ext_index"][(st["ext_c"] & 1023) == 1]) \
-                or name == "cavity16"
+            # an object never has both its primary map and an extrapolated
+            # map in one cell (other objects' maps may share the cell)
+            for oid in set((st["prim_c"] & 1023).tolist()) - {0}:
+                prim = set(st["prim_index"][(st["prim_c"] & 1023) == oid].tolist())
+                ext = set(st["ext_index"][(st["ext_c"] & 1023) == oid].tolist())
+                assert not prim & ext, (name, oid)
         # lid-driven cavity: walls hold the Dirichlet values through the ghost mirror
     fx = H.load_fixture("cavity16")
     st = H.state(fx, 8)
