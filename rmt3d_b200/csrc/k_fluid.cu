@@ -343,15 +343,45 @@ __device__ void face_stress(const grid_dev &g, const fields_dev *__restrict__ F,
     for (int s = 0; s < 3; s++) F->sigma[3 * FF + s][ind] = out[s];
 }
 
+// Cells that hold any reference map: the full stress (solid, fluid blend,
+// collision).  Cells without maps are left to k_stress_fluid.
 __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.sm + 3 || j > g.sn + 3 || k > g.so + 3) return;
     const int ind = gidx(g, i, j, k);
+    bool any = false;
+    for (int o = 0; o < g.n_obj; o++) any = any || F->om[o].code[ind] >= 0;
+    if (!any) return;
     face_stress<0>(g, F, i, j, k, ind, true);
     face_stress<1>(g, F, i, j, k, ind, true);
     face_stress<2>(g, F, i, j, k, ind, true);
+}
+
+// Cells without reference maps (most of the box): the pure fluid stress of
+// the three lower faces, the nmaps = 0 path of face_stress written with the
+// same expression ((1 - sfrac) * fs + ss with sfrac = ss = 0), in a small
+// kernel that keeps many more threads resident than the full one.
+__global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.sm + 3 || j > g.sn + 3 || k > g.so + 3) return;
+    const int ind = gidx(g, i, j, k);
+    for (int o = 0; o < g.n_obj; o++)
+        if (F->om[o].code[ind] >= 0) return;
+    const int strides[3] = {1, g.sm4, g.smn4};
+    const double facs[3] = {g.dxsp, g.dysp, g.dzsp};
+    const double sfrac = 0, ss = 0;
+#pragma unroll
+    for (int FF = 0; FF < 3; FF++) {
+        const int strd = strides[FF];
+        for (int nn = 0; nn < 3; nn++) {
+            const double fs = g.mu * facs[FF] * (F->vel[nn][ind] - F->vel[nn][ind - strd]);
+            F->sigma[3 * FF + nn][ind] = (1 - sfrac) * fs + ss;
+        }
+    }
 }
 
 // -------------------------------------------------------------------------

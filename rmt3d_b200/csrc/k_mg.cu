@@ -51,6 +51,14 @@ __global__ void k_resid(lvl_dev L, const T *__restrict__ x, const T *__restrict_
     const double a = body_resid<T, KIND>(L, x, r, res, ri, blockIdx.x, blockIdx.y, blockIdx.z);
     if (mx) warp_max_into(a, mx);
 }
+// the control's max-norm residual, computed only when the control will read it
+template <int KIND>
+__global__ void k_resid_ctl(lvl_dev L, const double *__restrict__ x, const double *__restrict__ r,
+                            unsigned long long *mx, const double *__restrict__ ri, const mg_ctl *c) {
+    if (!c->need_res) return;
+    const double a = body_resid<double, KIND>(L, x, r, nullptr, ri, blockIdx.x, blockIdx.y, blockIdx.z);
+    warp_max_into(a, mx);
+}
 template <typename T>
 __global__ void k_mac_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, T *__restrict__ rc,
                                T *__restrict__ xc0) {
@@ -615,8 +623,8 @@ void mg_solver::launch_body(cudaStream_t st, bool armed, unsigned long long h) {
     mg_level &F = lv[0];
     lvl_dev fd = dev_of(F);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]);
-    if (kind == MG_MAC) LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, d_max, F.ri)));
-    else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, nullptr, d_max, F.ri)));
+    if (kind == MG_MAC) LAUNCH((k_resid_ctl<0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, d_max, F.ri, ctl)));
+    else LAUNCH((k_resid_ctl<1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, d_max, F.ri, ctl)));
     LAUNCH(k_mg_ctl<<<1, 1, 0, st>>>(ctl, d_max, max_norm_tol, rtol, exact ? 1 : 0, h, armed ? 1 : 0));
 }
 

@@ -48,6 +48,16 @@ __global__ void k_resid_b(lvl_dev L, T *const *x, T *const *r, T *const *res, co
                                          blockIdx.x, blockIdx.y, bz_);
     if (mx) warp_max_into(a, mx[b_]);
 }
+// the control's residual: only for scenes whose control will read it
+template <int KIND>
+__global__ void k_resid_ctl_b(lvl_dev L, double *const *x, double *const *r, const double *const *ri,
+                              unsigned long long *const *mx, mg_ctl *const *ctl, const int *run, int zb) {
+    MGB_SCENE(zb)
+    if (!ctl[b_]->need_res) return;
+    const double a = body_resid<double, KIND>(L, x[b_], r[b_], nullptr, ri ? ri[b_] : nullptr, blockIdx.x,
+                                              blockIdx.y, bz_);
+    warp_max_into(a, mx[b_]);
+}
 template <typename T>
 __global__ void k_mac_restrict_b(lvl_dev F, lvl_dev C, T *const *res, T *const *rc, T *const *xc, const int *run,
                                  int zb) {
@@ -326,9 +336,9 @@ int mg_group::capture(cudaStream_t cur, graph_builder &gb) {
     int zbf;
     const dim3 gf = ggrid(F.n[0], F.n[1], F.n[2], B, zbf);
     if (kind == MG_MAC)
-        k_resid_b<double, 0><<<gf, gblk(), 0, body>>>(ldv(F), tab[0].x, tab[0].r, nullptr, tab[0].ri, mx, run, zbf);
+        k_resid_ctl_b<0><<<gf, gblk(), 0, body>>>(ldv(F), tab[0].x, tab[0].r, tab[0].ri, mx, ctls, run, zbf);
     else
-        k_resid_b<double, 1><<<gf, gblk(), 0, body>>>(ldv(F), tab[0].x, tab[0].r, nullptr, tab[0].ri, mx, run, zbf);
+        k_resid_ctl_b<1><<<gf, gblk(), 0, body>>>(ldv(F), tab[0].x, tab[0].r, tab[0].ri, mx, ctls, run, zbf);
     k_mgb_ctl<<<1, 1024, 0, body>>>(ctls, mx, run, B, tol, rtol, exact ? 1 : 0, h);
     body_kernels += 2;
     gb.close(body);

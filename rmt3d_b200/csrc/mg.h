@@ -63,7 +63,7 @@ struct mg_ctl {
     int last_cycles;   // cycles of the last finished solve
     int active;        // the current solve continues
     int nan;           // the last solve ended with a NaN residual
-    int pad;
+    int need_res;      // the next iteration ends at a point where the control reads the residual
     long long cycles_total;
     double V_avg, V_var;
     double prev, res_out;  // previous / reported max-norm residual

@@ -249,6 +249,7 @@ __device__ __forceinline__ void mg_begin_state(mg_ctl *c, unsigned long long *mx
     c->it = 0;
     c->count = 0;
     c->active = 1;
+    c->need_res = c->todo == 1;
     mx[0] = 0;
     mx[1] = 0;
 }
@@ -312,6 +313,9 @@ __device__ __forceinline__ bool mg_ctl_step(mg_ctl *c, unsigned long long *mx, d
         c->active = 0;
         c->nan = (c->res_out != c->res_out);
     }
+    // the residual is read only where a phase ends (and every cycle of the
+    // stagnation loop): the next iteration computes it only then
+    c->need_res = (c->phase <= 1 && c->todo == 1) || (c->phase == 2 && c->todo == 1 && exact) || c->phase == 3;
     return done;
 }
 

@@ -686,8 +686,12 @@ static void compute_grad_basis(rmt3d_scene *s) {
 // ---------------------------------------------------------------------------
 static void compute_stress(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    k_stress<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF);
+    k_stress_fluid<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF);
     s->count();
+    if (g.n_obj > 0) {
+        k_stress<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF);
+        s->count();
+    }
 }
 
 // ---- simulation time, kept on the device (read by the kernels) -----------
