@@ -504,10 +504,12 @@ def roofline(R, sc, args):
     achieved = (byts / n) / (ms / n * 1e-3) / 1e9 if n else None
     traffic = None
     try:
-        traffic = json.load(open(TRAFFIC_FILE)).get("fem_gs_fine_%d" % args.size)
+        traffic = json.load(open(TRAFFIC_FILE)).get(
+            "fem_gs_fine_%d_%s" % (args.size, "f32" if sc.desc.precision == R.MIXED else "fp64"))
     except (OSError, ValueError):
         pass
-    return {"bound": "hbm", "kernel": "k_fem_gs (finest level colour pass)", "achieved": achieved, "peak": peak,
+    kname = "k_fem_gs<%s> (finest level colour pass)" % ("float" if sc.desc.precision == R.MIXED else "double")
+    return {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
             "peak_source": src, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
             "traffic": traffic, "launches_timed": n, "avg_launch_us": (1e3 * ms / n) if n else None,
             "algorithmic_bytes_per_launch": (byts / n) if n else None}
