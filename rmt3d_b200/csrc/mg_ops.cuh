@@ -109,11 +109,27 @@ __device__ __forceinline__ T fem_offdiag(const lvl_dev L, const T *__restrict__ 
 template <typename T>
 __device__ __forceinline__ T mac_offdiag_vd(const lvl_dev L, const T *__restrict__ x, const T *__restrict__ ri, int i,
                                             int j, int k, T &diag) {
+    const int base = i + L.n0 * (j + L.n1 * k);
+    const T rc = ri[base];
+    if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
+        // interior cell: all six faces, the same operations in the same order
+        const int sy = L.n0, sz = L.n0 * L.n1;
+        const T ax1 = (T)0.5 * (ri[base - 1] + rc), ax2 = (T)0.5 * (rc + ri[base + 1]);
+        const T ay1 = (T)0.5 * (ri[base - sy] + rc), ay2 = (T)0.5 * (rc + ri[base + sy]);
+        const T az1 = (T)0.5 * (ri[base - sz] + rc), az2 = (T)0.5 * (rc + ri[base + sz]);
+        T s = 0, csum = 0;
+        s += ax1 * x[base - 1] + ax2 * x[base + 1];
+        csum += ax1 + ax2;
+        s += ay1 * x[base - sy] + ay2 * x[base + sy];
+        csum += ay1 + ay2;
+        s += az1 * x[base - sz] + az2 * x[base + sz];
+        csum += az1 + az2;
+        diag = (T)(-6) * (csum / (T)6);
+        return s;
+    }
     const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
     const int c[3] = {i, j, k};
     const int st[3] = {1, L.n0, L.n0 * L.n1};
-    const int base = i + L.n0 * (j + L.n1 * k);
-    const T rc = ri[base];
     T s = 0, csum = 0;
     int cnt = 0;
     for (int d = 0; d < 3; d++) {

@@ -135,3 +135,24 @@ def test_mixed_form_accuracy(tmp_path):
     assert H.rel_l2(b["p"], a["p"]) < 1e-5
     # the relaxed solves need fewer V-cycles
     assert out[R.MIXED][1] < out[R.FP64][1]
+
+
+def test_graph_rebuilt_after_dt_change(tmp_path):
+    """dt is a captured parameter of the step graph: after set_dt the graph is
+    captured again, and the run matches the eager form through the change."""
+    path = scenes.write(str(tmp_path / "d.cfg"), scenes.cavity_sphere(24, steps=8, radius=0.25))
+    desc = R.desc_from_cfg(path)
+    res = []
+    for graph in (False, True):
+        sc = _scene(desc, graph)
+        try:
+            sc.prepare()
+            assert sc.run(2) == R.NORMAL_EXIT
+            sc.set_dt(sc.dt * 0.7)
+            assert sc.run(3) == R.NORMAL_EXIT
+            res.append(({f: sc.field(f) for f in ("u", "v", "w", "p")}, sc.time, sc.dt))
+        finally:
+            sc.close()
+    for f in res[0][0]:
+        assert np.array_equal(res[0][0][f], res[1][0][f]), f
+    assert res[0][1] == res[1][1] and res[0][2] == res[1][2]
