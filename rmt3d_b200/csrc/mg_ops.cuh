@@ -164,6 +164,56 @@ __device__ __forceinline__ T mac_offdiag_vd(const lvl_dev L, const T *__restrict
 template <typename T>
 __device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict__ x, const T *__restrict__ ri, int i,
                                             int j, int k, T &diag) {
+    if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
+        // interior node (all 8 cells exist, no halving): corners take one
+        // cell, edges the mean of two (lower index first), the centre the
+        // mean of all eight in (z, y, x) order
+        const int sy = L.n0, sz = L.n0 * L.n1;
+        const int ncx = L.p0 ? L.n0 : L.n0 - 1, ncy = L.p1 ? L.n1 : L.n1 - 1;
+        const int c0 = (i - 1) + ncx * ((j - 1) + ncy * (k - 1));  // cell below-left-front
+        const int cy = ncx, cz = ncx * ncy;
+        T v[2][2][2];
+        v[0][0][0] = ri[c0];
+        v[0][0][1] = ri[c0 + 1];
+        v[0][1][0] = ri[c0 + cy];
+        v[0][1][1] = ri[c0 + cy + 1];
+        v[1][0][0] = ri[c0 + cz];
+        v[1][0][1] = ri[c0 + cz + 1];
+        v[1][1][0] = ri[c0 + cz + cy];
+        v[1][1][1] = ri[c0 + cz + cy + 1];
+        const T *xc = x + i + sy * j + sz * k;
+        T s = 0;
+#pragma unroll
+        for (int oc = 0; oc < 3; oc++)
+#pragma unroll
+            for (int ob = 0; ob < 3; ob++)
+#pragma unroll
+                for (int oa = 0; oa < 3; oa++) {
+                    const int nz = (oa != 1) + (ob != 1) + (oc != 1);
+                    if (nz <= 1) continue;
+                    const T xv = xc[(oa - 1) + sy * (ob - 1) + sz * (oc - 1)];
+                    T cf;
+                    if (nz == 3) {
+                        cf = -v[oc >> 1][ob >> 1][oa >> 1];
+                    } else if (oc == 1) {
+                        cf = (T)-2 * ((v[0][ob >> 1][oa >> 1] + v[1][ob >> 1][oa >> 1]) / (T)2);
+                    } else if (ob == 1) {
+                        cf = (T)-2 * ((v[oc >> 1][0][oa >> 1] + v[oc >> 1][1][oa >> 1]) / (T)2);
+                    } else {
+                        cf = (T)-2 * ((v[oc >> 1][ob >> 1][0] + v[oc >> 1][ob >> 1][1]) / (T)2);
+                    }
+                    s += cf * xv;
+                }
+        T c8 = 0;
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) c8 += v[a][b][e];
+        diag = (T)32 * (c8 / (T)8);
+        return s;
+    }
     const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
     const int nc[3] = {p[0] ? n[0] : n[0] - 1, p[1] ? n[1] : n[1] - 1, p[2] ? n[2] : n[2] - 1};
     const int c[3] = {i, j, k};
@@ -184,41 +234,6 @@ __device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict
                 const bool ok = cell[0][e] >= 0 && cell[1][b] >= 0 && cell[2][a] >= 0;
                 v[a][b][e] = ok ? ri[cell[0][e] + nc[0] * (cell[1][b] + nc[1] * cell[2][a])] : (T)0;
             }
-    if (!bd[0] && !bd[1] && !bd[2]) {
-        // interior node (all 8 cells exist, no halving): the same entries in
-        // closed form -- corners take one cell, edges the mean of two (lower
-        // index first), the centre the mean of all eight in (z, y, x) order
-        const int sy = L.n0, sz = L.n0 * L.n1;
-        T s = 0;
-        for (int oc = 0; oc < 3; oc++) {
-            const int kk = nb[2][oc];
-            for (int ob = 0; ob < 3; ob++) {
-                const int jj = nb[1][ob];
-                for (int oa = 0; oa < 3; oa++) {
-                    const int nz = (oa != 1) + (ob != 1) + (oc != 1);
-                    if (nz <= 1) continue;
-                    const T xv = x[nb[0][oa] + sy * jj + sz * kk];
-                    T cf;
-                    if (nz == 3) {
-                        cf = -v[oc >> 1][ob >> 1][oa >> 1];
-                    } else if (oc == 1) {
-                        cf = (T)-2 * ((v[0][ob >> 1][oa >> 1] + v[1][ob >> 1][oa >> 1]) / (T)2);
-                    } else if (ob == 1) {
-                        cf = (T)-2 * ((v[oc >> 1][0][oa >> 1] + v[oc >> 1][1][oa >> 1]) / (T)2);
-                    } else {
-                        cf = (T)-2 * ((v[oc >> 1][ob >> 1][0] + v[oc >> 1][ob >> 1][1]) / (T)2);
-                    }
-                    s += cf * xv;
-                }
-            }
-        }
-        T c8 = 0;
-        for (int a = 0; a < 2; a++)
-            for (int b = 0; b < 2; b++)
-                for (int e = 0; e < 2; e++) c8 += v[a][b][e];
-        diag = (T)32 * (c8 / (T)8);
-        return s;
-    }
     T s = 0;
     for (int oc = 0; oc < 3; oc++) {
         const int kk = nb[2][oc];

@@ -1,6 +1,6 @@
 """Profiling driver: set up the bench workload, step once, then run N steps.
 
-    RMT3D_GRAPH=0 python -m rmt3d_b200.prof_step [n=64] [steps=2] [precision=0]
+    RMT3D_GRAPH=0 python -m rmt3d_b200.prof_step [n=64] [steps=2] [precision=0] [var_den=0] [objects=1]
 
 Prints PREP_LAUNCHES (kernel launches before the profiled steps, for ncu -s)
 and STEP_LAUNCHES (launches of the profiled steps, for ncu -c).  ncu cannot
@@ -14,9 +14,12 @@ from rmt3d_b200 import scenes
 n = int(sys.argv[1]) if len(sys.argv) > 1 else 64
 steps = int(sys.argv[2]) if len(sys.argv) > 2 else 2
 prec = int(sys.argv[3]) if len(sys.argv) > 3 else 0
+vd = int(sys.argv[4]) if len(sys.argv) > 4 else 0
+nobj = int(sys.argv[5]) if len(sys.argv) > 5 else 1
 wd = tempfile.mkdtemp()
-cfg = scenes.write(os.path.join(wd, 'w.cfg'), scenes.cavity_sphere(n, 100000, radius=0.2))
-d = R.desc_from_cfg(cfg); d.precision = prec
+text = scenes.cavity_sphere(n, 100000, radius=0.2, rho=1.2 if vd else 1.0) if nobj else scenes.cavity(n, 100000)
+cfg = scenes.write(os.path.join(wd, 'w.cfg'), text)
+d = R.desc_from_cfg(cfg); d.precision = prec; d.var_den = vd
 sc = R.Scene(d)
 sc.prepare()
 sc.step_forward(0)
