@@ -60,6 +60,23 @@ typedef struct {
     double G;
 } rmt3d_object_desc;
 
+/* Run controls of sim_params that the step does not read: output and
+ * checkpoint settings of run_sim/stepper (Sim/sim_params.cc:10-22, 86-160)
+ * and the restart point.  A checkpoint's recover.cfg carries them
+ * (sim_params.cc:489-600). */
+typedef struct {
+    int suppress, display;
+    int chk_num;  /* > 0: initialize restarts from recover_dirname/chk.<chk_num> */
+    int chk_step; /* total step count at that checkpoint */
+    int chkpt_freq;
+    int omp_num_thr, debug_flag, debug_obj_id, obj_body, data_fmt, out_flag, output_dim, output_ind;
+    unsigned int dump_code; /* bit 8: checkpoints (stepper.hh:603-609) */
+    int ntracers;
+    double current_time; /* simulation time at the checkpoint */
+    char dirname[256];   /* output directory: the .cfg path with ".cfg" -> ".out" */
+    char recover_dirname[256];
+} rmt3d_run_desc;
+
 /* Everything the reference reads from sim_params and sim_manager for this
  * path (Sim/sim_params.cc:10-410, Sim/sim_manager.hh:164-188). */
 typedef struct {
@@ -101,6 +118,7 @@ typedef struct {
                           0 keeps the reference's control.  Default 1e-7
                           (64^3 cavity + sphere, 100 steps: velocity 2e-8
                           and pressure 4e-8 rel-L2 from the FP64 form). */
+    rmt3d_run_desc run;
 } rmt3d_scene_desc;
 
 typedef struct rmt3d_scene rmt3d_scene;
@@ -123,8 +141,13 @@ int rmt3d_desc_defaults(rmt3d_scene_desc *out);
  * stream may be 0 (the legacy default stream) or a cudaStream_t cast to void*. */
 int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rmt3d_scene **out);
 
-/* fluid_3d::initialize (fluid_3d.cc:192-233): fields from the initial
- * conditions, first extrapolation, dt_reg from the CFL recheck. */
+/* fluid_3d::initialize (fluid_3d.cc:192-233).  With run.chk_num > 0 the
+ * state comes from the checkpoint run.recover_dirname/chk.<chk_num>
+ * (rmt3d_read_chk_pt); otherwise, or when a checkpoint file is missing or
+ * empty, from the initial conditions with a first extrapolation and dt_reg
+ * from the CFL recheck, and run.chk_num is reset to 0.  The reference's
+ * return value init_err (0 restarted, 1 started from scratch) is scalar 13
+ * of rmt3d_get_scalar. */
 int rmt3d_initialize(rmt3d_scene *s);
 
 /* fluid_3d::set_dt (fluid_3d.hh:454-457). */
@@ -135,9 +158,38 @@ int rmt3d_set_dt(rmt3d_scene *s, double dt);
  * the number of steps per frame.  Pure host arithmetic. */
 int rmt3d_stepper_dt(const rmt3d_scene_desc *desc, double dt_reg, double *dt_out, int *steps_per_frame);
 
-/* fluid_3d::init_iter (fluid_3d.cc:235-287): up to num_iters pressure
- * pre-iterations, then the t=0 stress. */
+/* fluid_3d::init_iter(init_err) (fluid_3d.cc:235-287) with the init_err of
+ * the last rmt3d_initialize: up to num_iters pressure pre-iterations (time
+ * and step count reset to 0) when it started from scratch, then in either
+ * case the stress of the current state. */
 int rmt3d_init_iter(rmt3d_scene *s);
+
+/* fluid_3d::write_chk_pt (F3D_Source/fluid_3d_chk_pt.cc:3-72): writes the
+ * checkpoint files vx vy vz p X Y Z OID and recover.cfg into chk_dirname
+ * (created if missing).  Each field file holds the o z-slices of the
+ * domain, each a (m+1)(n+1) double buffer filled as the reference's slice
+ * gather does: cell fields at i + m*j, pressure on the nodal grid at
+ * i + fem_m*j; X/Y/Z/OID take the map of least level set at each cell
+ * (fluid_3d_io.cc:420-434), 100 / 0 where a cell has none.  recover.cfg is
+ * sim_params::write_params (Sim/sim_params.cc:489-600) with chk_num = fnum,
+ * chk_step = snum and current_time = the scene's time; the scene's run
+ * block takes those values too.  compress != 0 compresses each field file
+ * with xz as the reference does (fluid_3d_chk_pt.cc:54-59); a failed
+ * compression leaves the file uncompressed, which the reader accepts. */
+int rmt3d_write_chk_pt(rmt3d_scene *s, int snum, int fnum, const char *chk_dirname, int compress);
+
+/* fluid_3d::initialize_from_chk_point (fluid_3d_chk_pt.cc:74-163) followed
+ * by the rest of initialize: reads the eight field files (an X.xz file is
+ * decompressed in memory when X itself is absent), resets the scene to a
+ * fresh state, loads velocities, pressure, primary maps (x = xpred = X,
+ * owner = OID), exchanges periodic images, extrapolates the maps and fills
+ * the velocity boundary.  time and the step count come from the scene's
+ * run block (current_time, chk_step).  The pressure slices are read with
+ * the reference's stride m on the nodal grid (fluid_3d_chk_pt.cc:303-316),
+ * so a restart reproduces the reference's restart.  *status is the
+ * reference's code: 0 read, 1 a file is missing, 2 a file is empty; the
+ * scene is unchanged unless it is 0. */
+int rmt3d_read_chk_pt(rmt3d_scene *s, const char *chk_dirname, int *status);
 
 /* run_sim's whole set-up sequence: initialize, stepper dt fit, set_dt,
  * init_iter (run_sim.cc:94-106). */
@@ -161,7 +213,8 @@ int rmt3d_run(rmt3d_scene *s, int nsteps, int *status);
 
 /* Scalars: 0 dt, 1 time, 2 dt_reg, 3 eps (transition width), 4 nt (steps
  * taken), 5 last MAC V-cycles, 6 last FEM V-cycles, 7 total MAC V-cycles,
- * 8 total FEM V-cycles, 9 extrapolated maps, 10 K_stiff, 11 vmax. */
+ * 8 total FEM V-cycles, 9 extrapolated maps, 10 K_stiff, 11 vmax,
+ * 12 device bytes held, 13 init_err of the last rmt3d_initialize. */
 int rmt3d_get_scalar(rmt3d_scene *s, int which, double *value);
 
 /* Grid extents of the ghosted arrays: sm+4, sn+4, so+4 and the FEM node

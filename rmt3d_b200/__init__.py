@@ -13,6 +13,7 @@ All work runs in the CUDA library ``librmt3d_gpu.so`` through the C ABI of
 include/rmt3d_gpu.h; there is no CPU path.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -82,15 +83,33 @@ class Scene:
 
     # -- the fluid_3d members the stepper and run_sim use -------------------
     def initialize(self):
+        """Returns init_err: 0 restarted from the descriptor's checkpoint
+        (run.chk_num > 0), 1 started from scratch (fluid_3d.cc:192-233)."""
         _lib.check(lib().rmt3d_initialize(self._h))
-        return 1  # init_err: started from scratch (fluid_3d.cc:193-196)
+        return int(self.scalar(13))
 
     def set_dt(self, dt):
         _lib.check(lib().rmt3d_set_dt(self._h, dt))
 
-    def init_iter(self, init_err=1):
-        if init_err > 0:
-            _lib.check(lib().rmt3d_init_iter(self._h))
+    def init_iter(self, init_err=None):
+        """Pressure pre-iterations when the last initialize started from
+        scratch, then the stress of the current state; init_err, when given,
+        must be that initialize's result."""
+        if init_err is not None and int(init_err) != int(self.scalar(13)):
+            raise ValueError("init_err differs from the last initialize's result")
+        _lib.check(lib().rmt3d_init_iter(self._h))
+
+    def write_chk_pt(self, snum, fnum, chk_dirname, compress=True):
+        """Checkpoint in the reference's format (fluid_3d_chk_pt.cc:3-72)."""
+        _lib.check(lib().rmt3d_write_chk_pt(self._h, int(snum), int(fnum), str(chk_dirname).encode(),
+                                            int(bool(compress))))
+
+    def read_chk_pt(self, chk_dirname):
+        """Restart from a checkpoint directory (fluid_3d_chk_pt.cc:74-163);
+        returns the reference's status: 0 read, 1 file missing, 2 file empty."""
+        st = ctypes.c_int()
+        _lib.check(lib().rmt3d_read_chk_pt(self._h, str(chk_dirname).encode(), ctypes.byref(st)))
+        return st.value
 
     def prepare(self):
         _lib.check(lib().rmt3d_prepare(self._h))
@@ -231,22 +250,38 @@ class Scene:
 
 
 class Stepper:
-    """Frame/step loop of the reference's stepper (Sim/stepper.hh:211-376)."""
+    """Frame/step loop of the reference's stepper (Sim/stepper.hh:211-376):
+    dt fit to frames, a restart's initial step and frame (chk_step,
+    chk_num), stop_short counted from the initial step, and checkpoints
+    every chkpt_freq frames when dump_code has bit 8 (stepper.hh:583-610)."""
 
     def __init__(self, desc, scene):
         self.dt, self.steps = stepper_dt(desc, desc.dt)
+        run = desc.run
+        self.init_step = run.chk_step
+        self.init_frame = run.chk_num
+        self.curr_tot_step = self.init_step
         self.frames = desc.frames
         self.total = (self.frames - 1) * self.steps
-        self.stop_short = desc.stop_short if desc.stop_short > 0 else self.total + 1
-        self.curr_tot_step = 0
+        self.stop_short = desc.stop_short + self.init_step if desc.stop_short > 0 else self.total + 1
+        if self.frames - 1 > self.total:
+            self.frames = self.total + 1
+        self.dump_code = run.dump_code
+        self.chkpt_freq = run.chkpt_freq
+        self.dirname = run.dirname.decode()
         scene.set_dt(self.dt)
+
+    def write_files(self, scene, snum, fnum):
+        if (self.dump_code & 8) and fnum % self.chkpt_freq == 0:
+            os.makedirs(self.dirname, exist_ok=True)
+            scene.write_chk_pt(snum, fnum, os.path.join(self.dirname, "chk.%05d" % fnum))
 
     def run(self, scene):
         scene.set_dt(self.dt)
+        self.write_files(scene, self.init_step, self.init_frame)
         err = 0
-        for _frame in range(1, self.frames):
-            if self.curr_tot_step >= self.stop_short:
-                break
+        frame = self.init_frame + 1
+        while frame <= self.frames - 1 and self.curr_tot_step < self.stop_short:
             for _s in range(self.steps):
                 if self.curr_tot_step >= self.stop_short:
                     break
@@ -254,11 +289,18 @@ class Stepper:
                 err = scene.step_forward(0)
                 if err not in (NORMAL_EXIT, STEADY_SOLN_EXIT):
                     raise RMT3DError(err, "Stepper: Something went wrong, sorry.")
+                if err == STEADY_SOLN_EXIT:
+                    break
+            self.write_files(scene, self.curr_tot_step, frame)
+            if err == STEADY_SOLN_EXIT:
+                break
+            frame += 1
         return err
 
 
 def run_sim(cfg_path, **overrides):
-    """The run_sim driver sequence (Execs/run_sim.cc:64-141); returns the scene."""
+    """The run_sim driver sequence (Execs/run_sim.cc:64-141); returns the scene.
+    A .cfg with chk_num > 0 (a checkpoint's recover.cfg) restarts from it."""
     desc = desc_from_cfg(cfg_path)
     for k, v in overrides.items():
         setattr(desc, k, v)

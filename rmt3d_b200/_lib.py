@@ -40,6 +40,20 @@ class ObjectDesc(ctypes.Structure):
     ]
 
 
+class RunDesc(ctypes.Structure):
+    """rmt3d_run_desc: run controls and the restart point."""
+    _fields_ = [
+        ("suppress", ctypes.c_int), ("display", ctypes.c_int),
+        ("chk_num", ctypes.c_int), ("chk_step", ctypes.c_int), ("chkpt_freq", ctypes.c_int),
+        ("omp_num_thr", ctypes.c_int), ("debug_flag", ctypes.c_int), ("debug_obj_id", ctypes.c_int),
+        ("obj_body", ctypes.c_int), ("data_fmt", ctypes.c_int), ("out_flag", ctypes.c_int),
+        ("output_dim", ctypes.c_int), ("output_ind", ctypes.c_int),
+        ("dump_code", ctypes.c_uint), ("ntracers", ctypes.c_int),
+        ("current_time", ctypes.c_double),
+        ("dirname", ctypes.c_char * 256), ("recover_dirname", ctypes.c_char * 256),
+    ]
+
+
 class SceneDesc(ctypes.Structure):
     _fields_ = [
         ("sys_size", ctypes.c_int * 3),
@@ -79,6 +93,7 @@ class SceneDesc(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("mg_exact", ctypes.c_int),
         ("mixed_rtol", ctypes.c_double),
+        ("run", RunDesc),
     ]
 
 
@@ -118,6 +133,8 @@ SIGNATURES = {
     "rmt3d_set_dt": (_I, [_P, _D]),
     "rmt3d_stepper_dt": (_I, [ctypes.POINTER(SceneDesc), _D, _DP, _IP]),
     "rmt3d_init_iter": (_I, [_P]),
+    "rmt3d_write_chk_pt": (_I, [_P, _I, _I, ctypes.c_char_p, _I]),
+    "rmt3d_read_chk_pt": (_I, [_P, ctypes.c_char_p, _IP]),
     "rmt3d_prepare": (_I, [_P]),
     "rmt3d_step": (_I, [_P, _I, _IP]),
     "rmt3d_run": (_I, [_P, _I, _IP]),

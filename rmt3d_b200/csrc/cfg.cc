@@ -65,6 +65,17 @@ extern "C" int rmt3d_desc_defaults(rmt3d_scene_desc *d) {
     d->sim_type = RMT3D_SIM_FTEST;
     d->precision = RMT3D_FP64;
     d->mixed_rtol = 1e-7;
+    // run controls, sim_params.cc:12-22
+    rmt3d_run_desc &r = d->run;
+    r.chkpt_freq = 1;
+    r.omp_num_thr = 1;
+    r.debug_obj_id = -1;
+    r.obj_body = -1;
+    r.out_flag = 1 | 2 | 4 | 128;
+    r.output_dim = 2;
+    r.output_ind = -1;
+    r.dump_code = 1 | 2;
+    r.ntracers = 1000;
     return RMT3D_OK;
 }
 
@@ -75,6 +86,16 @@ extern "C" int rmt3d_desc_from_cfg(const char *path, rmt3d_scene_desc *d) {
         return rmt3d::fail(RMT3D_ERR_INVALID, "Filename must end in '.cfg'");
     FILE *f = fopen(path, "r");
     if (!f) return rmt3d::fail(RMT3D_ERR_IO, std::string("cannot open ") + path);
+    // the output directory is the .cfg path with ".cfg" -> ".out", and the
+    // recovery directory defaults to it (sim_params.cc:53-61)
+    rmt3d_run_desc &r = d->run;
+    if (len - 4 + 5 > sizeof(r.dirname)) {
+        fclose(f);
+        return rmt3d::fail(RMT3D_ERR_TOO_LARGE, "cfg path longer than 250 characters");
+    }
+    memcpy(r.dirname, path, len - 4);
+    memcpy(r.dirname + len - 4, ".out", 5);
+    memcpy(r.recover_dirname, r.dirname, sizeof(r.dirname));
     char buf[1024];
     int ln = 1;
     bool var_den = false;
@@ -100,11 +121,45 @@ extern "C" int rmt3d_desc_from_cfg(const char *path, rmt3d_scene_desc *d) {
                 d->bcv[i][face] = va[i];
             }
         };
-        if (k == "suppress" || k == "display" || k == "chk_num" || k == "chk_step" || k == "chkpt_freq" ||
-            k == "omp_num_thr" || k == "debug_flag" || k == "debug_obj_id" || k == "out_flag" || k == "obj_body" ||
-            k == "data_fmt" || k == "output_dim" || k == "output_ind" || k == "dump_code" || k == "ntracers" ||
-            k == "current_time" || k == "recover_dirname") {
-            t.next();  // output / checkpoint / tracer controls: outside this path
+        if (k == "suppress") {
+            r.suppress = t.next_int();
+        } else if (k == "display") {
+            r.display = t.next_int();
+        } else if (k == "recover_dirname") {
+            const std::string &v = t.next();
+            snprintf(r.recover_dirname, sizeof(r.recover_dirname), "%s", v.c_str());
+        } else if (k == "chk_num") {
+            r.chk_num = t.next_int();
+        } else if (k == "chk_step") {
+            r.chk_step = t.next_int();
+        } else if (k == "chkpt_freq") {
+            r.chkpt_freq = t.next_int();
+        } else if (k == "omp_num_thr") {
+            int v = t.next_int();
+            if (v > 0) r.omp_num_thr = v;
+        } else if (k == "debug_flag") {
+            r.debug_flag = t.next_int();
+        } else if (k == "debug_obj_id") {
+            r.debug_obj_id = t.next_int();
+        } else if (k == "out_flag") {
+            r.out_flag = t.next_int();
+        } else if (k == "obj_body") {
+            r.obj_body = t.next_int();
+        } else if (k == "data_fmt") {
+            r.data_fmt = t.next_int();
+        } else if (k == "output_dim") {
+            r.output_dim = t.next_int();
+            if (r.output_dim < 0 || r.output_dim > 2) r.output_dim = -1;
+        } else if (k == "output_ind") {
+            r.output_ind = t.next_int();
+            if (r.output_ind < 0 || r.output_dim < 0 || r.output_ind >= d->sys_size[r.output_dim]) r.output_ind = -1;
+        } else if (k == "dump_code") {
+            r.dump_code = (unsigned int)atol(t.next().c_str());
+        } else if (k == "ntracers") {
+            r.ntracers = t.next_int();
+        } else if (k == "current_time") {
+            double v = t.next_double();
+            if (v > 0) r.current_time = v;
         } else if (k == "implicit") {
             d->implicit_visc = t.next_int();
         } else if (k == "godunov") {
@@ -267,6 +322,16 @@ extern "C" int rmt3d_desc_from_cfg(const char *path, rmt3d_scene_desc *d) {
     double mdh = dx < dy ? dx : dy;
     mdh = mdh < dz ? mdh : dz;
     d->wall_dist = mdh > d->wall_dist ? mdh : d->wall_dist;
+    if (r.output_ind == -1 && r.output_dim >= 0) r.output_ind = d->sys_size[r.output_dim] / 2;
+    // a restart needs recover_dirname/chk.<chk_num>/recover.cfg, else it is
+    // dropped (sim_params.cc:374-397)
+    if (r.chk_num > 0) {
+        char probe[600];
+        snprintf(probe, sizeof(probe), "%s/chk.%05d/recover.cfg", r.recover_dirname, r.chk_num);
+        FILE *fh = fopen(probe, "rb");
+        if (fh) fclose(fh);
+        else r.chk_num = r.chk_step = 0;
+    }
     if (d->sim_type != RMT3D_SIM_OBJECTS) d->n_obj = 0;
     return RMT3D_OK;
 }

@@ -1,6 +1,9 @@
 // Shared host-side helpers: thread-local error message and status plumbing.
 #pragma once
+#include <cstddef>
 #include <string>
+
+#include "rmt3d_gpu.h"
 
 struct rmt3d_scene;
 
@@ -25,4 +28,14 @@ int group_launch(scene_group *g, int nsteps);
 int group_finish(scene_group *g, int *status);
 void group_destroy(scene_group *g);
 long long group_mg_launches(const scene_group *g);
+
+// Checkpoint files (chk_io.cc).  A packed checkpoint holds kChkFields
+// fields in kChkNames order, each nslices slices of slice_len doubles.
+constexpr int kChkFields = 8;
+extern const char *const kChkNames[kChkFields];
+int chk_make_dir(const char *dir);
+int chk_write_files(const char *dir, const double *buf, size_t slice_len, int nslices, int compress);
+// *status: 0 read, 1 a file missing, 2 a file empty (the reference's codes)
+int chk_read_files(const char *dir, double *buf, size_t slice_len, int nslices, int *status);
+int chk_write_recover_cfg(const char *dir, const rmt3d_scene_desc &d, double dt);
 }

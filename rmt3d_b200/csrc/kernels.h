@@ -40,5 +40,7 @@ __global__ void k_ustar(grid_dev g, const fields_dev *__restrict__ F, const doub
 __global__ void k_fem_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, gradphi_t gp);
 __global__ void k_fem_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x, const double *mean);
 __global__ void k_sub_pgrad(grid_dev g, const fields_dev *__restrict__ F, double dt, int var_den);
+__global__ void k_chk_pack(grid_dev g, const fields_dev *__restrict__ F, double *__restrict__ buf);
+__global__ void k_chk_unpack(grid_dev g, const fields_dev *__restrict__ F, const double *__restrict__ buf, int *bad);
 
 }  // namespace rmt3d

@@ -114,6 +114,10 @@ struct rmt3d_scene {
     bool wall[6];
     double dt = 0, time = 0, dt_reg = 0, eps = 0, vmax = 1, K_stiff = 0;
     double min_wall_acc = 0, wall_acc_mult = 0;
+    // dt_reg, K_stiff and vmax as sim_manager leaves them at construction,
+    // before init_fluid's CFL recheck (a checkpoint restart skips it)
+    double dt_reg0 = 0, K_stiff0 = 0, vmax0 = 1;
+    int init_err = 1;  // fluid_3d::initialize's result: 0 restarted, 1 from scratch
     int nt = 0;
     long long launches = 0;
     kernel_profiler prof;
@@ -1753,20 +1757,70 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
         rmt3d_scene_destroy(s);
         return fail(RMT3D_ERR_CUDA, "scene set-up failed");
     }
+    s->dt_reg0 = s->dt_reg;
+    s->K_stiff0 = s->K_stiff;
+    s->vmax0 = s->vmax;
     *out = s;
     return RMT3D_OK;
 }
 
-extern "C" int rmt3d_initialize(rmt3d_scene *s) {
-    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
-    set_time(s, 0);
-    mark_dirty(s);
-    int e;
-    if ((e = init_fluid(s))) return e;
-    if ((e = init_pres(s))) return e;
-    if ((e = init_refmap(s))) return e;
+// ---------------------------------------------------------------------------
+// checkpoints (F3D_Source/fluid_3d_chk_pt.cc)
+// ---------------------------------------------------------------------------
+// doubles per slice of a checkpoint field file: (m+1)(n+1), the reference's
+// u_global (fluid_3d_chk_pt.cc:16, :91)
+static size_t chk_slice_len(const rmt3d_scene *s) { return (size_t)(s->g.sm + 1) * (s->g.sn + 1); }
+
+// fluid_3d::initialize_from_chk_point (fluid_3d_chk_pt.cc:74-163).  All eight
+// files are read before the device state is touched, so a missing or empty
+// file (*status 1 or 2) leaves the scene as it was.
+static int read_chk_pt(rmt3d_scene *s, const char *dir, int *status) {
+    const grid_dev &g = s->g;
+    const size_t n = g.ncell;
+    const size_t L = chk_slice_len(s), total = L * g.so * kChkFields;
+    std::vector<double> h(total);
+    int e = chk_read_files(dir, h.data(), L, g.so, status);
+    if (e || *status) return e;
+    double *dbuf = nullptr;
+    CK(cudaMallocAsync((void **)&dbuf, total * sizeof(double) + sizeof(double), s->st));
+    int *bad = (int *)(dbuf + total);
+    cudaError_t ce = cudaMemcpyAsync(dbuf, h.data(), total * sizeof(double), cudaMemcpyHostToDevice, s->st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(bad, 0, sizeof(int), s->st);
+    // the values of a freshly constructed fluid_3d that the files do not set
+    const fields_dev &F = s->hF;
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(F.dp, 0, n * 8, s->st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(F.q, 0, n * 8, s->st);
+    for (int c = 0; c < 3 && ce == cudaSuccess; c++) ce = cudaMemsetAsync(F.dvel[c], 0, n * 8, s->st);
+    for (int c = 0; c < 18 && ce == cudaSuccess; c++) ce = cudaMemsetAsync(F.fvel[c], 0, n * 8, s->st);
+    for (int c = 0; c < 9 && ce == cudaSuccess; c++) ce = cudaMemsetAsync(F.sigma[c], 0, n * 8, s->st);
+    int hbad = 0;
+    if (ce == cudaSuccess) {
+        k_chk_unpack<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, dbuf, bad);
+        s->count();
+        ce = cudaMemcpyAsync(s->h_scalar, bad, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->st);
+    if (ce == cudaSuccess) memcpy(&hbad, s->h_scalar, sizeof(int));
+    cudaFreeAsync(dbuf, s->st);
+    CK(ce);
+    if (hbad) return fail(RMT3D_ERR_INVALID, std::string("checkpoint ") + dir + ": OID names no object");
+    // communicate<1>, <2>, <8>, <16|32>; init_extrapolate; update_rho
+    periodic(s, {F.vel[0], F.vel[1], F.vel[2]}, {}, 0);
+    comm_pressure(s);
+    comm_primary(s);
     init_extrapolate(s);
     update_rho(s);
+    set_time(s, s->d.run.current_time);
+    s->nt = s->d.run.chk_step;
+    s->dt_reg = s->dt_reg0;
+    s->K_stiff = s->K_stiff0;
+    s->g.K_stiff = s->K_stiff0;
+    s->vmax = s->vmax0;
+    return 0;
+}
+
+// the end of fluid_3d::initialize shared by both starts (fluid_3d.cc:212-232)
+static int init_finish(rmt3d_scene *s) {
     fill_boundary_cc(s);
     compute_grad_basis(s);
     int re = read_ctl(s);
@@ -1774,6 +1828,63 @@ extern "C" int rmt3d_initialize(rmt3d_scene *s) {
     if (s->h_counters[2] > 0) return fail(RMT3D_ERR_EXTRAP, "Extrapolation failed: no eligible points or degenerate matrix");
     CK(cudaGetLastError());
     return RMT3D_OK;
+}
+
+extern "C" int rmt3d_initialize(rmt3d_scene *s) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    mark_dirty(s);
+    int e;
+    rmt3d_run_desc &r = s->d.run;
+    s->init_err = 1;
+    if (r.chk_num > 0) {
+        char dir[600];
+        snprintf(dir, sizeof(dir), "%s/chk.%05d", r.recover_dirname, r.chk_num);
+        if ((e = read_chk_pt(s, dir, &s->init_err))) return e;
+    }
+    if (s->init_err > 0) {
+        r.chk_num = 0;
+        set_time(s, 0);
+        if ((e = init_fluid(s))) return e;
+        if ((e = init_pres(s))) return e;
+        if ((e = init_refmap(s))) return e;
+        init_extrapolate(s);
+        update_rho(s);
+    }
+    return init_finish(s);
+}
+
+extern "C" int rmt3d_read_chk_pt(rmt3d_scene *s, const char *chk_dirname, int *status) {
+    if (!s || !chk_dirname || !status) return fail(RMT3D_ERR_INVALID, "null argument");
+    int e = read_chk_pt(s, chk_dirname, status);
+    if (e || *status) return e;
+    mark_dirty(s);
+    s->init_err = 0;
+    return init_finish(s);
+}
+
+extern "C" int rmt3d_write_chk_pt(rmt3d_scene *s, int snum, int fnum, const char *chk_dirname, int compress) {
+    if (!s || !chk_dirname) return fail(RMT3D_ERR_INVALID, "null argument");
+    CK(cudaStreamSynchronize(s->st));
+    const grid_dev &g = s->g;
+    const size_t L = chk_slice_len(s), per = L * g.so, total = per * kChkFields;
+    std::vector<double> h(total);
+    double *dbuf = nullptr;
+    CK(cudaMallocAsync((void **)&dbuf, total * sizeof(double), s->st));
+    const int blocks = (int)std::min<size_t>((per + 255) / 256, 148 * 16);
+    k_chk_pack<<<blocks, 256, 0, s->st>>>(g, s->dF, dbuf);
+    s->count();
+    cudaError_t ce = cudaMemcpyAsync(h.data(), dbuf, total * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->st);
+    cudaFreeAsync(dbuf, s->st);
+    CK(ce);
+    int e = chk_make_dir(chk_dirname);
+    if (!e) e = chk_write_files(chk_dirname, h.data(), L, g.so, compress);
+    if (e) return e;
+    // set_current_chk_num / _chk_step / _time, then write_params
+    s->d.run.chk_num = fnum;
+    s->d.run.chk_step = snum;
+    s->d.run.current_time = s->time;
+    return chk_write_recover_cfg(chk_dirname, s->d, s->dt);
 }
 
 extern "C" int rmt3d_set_dt(rmt3d_scene *s, double dt) {
@@ -1786,7 +1897,7 @@ extern "C" int rmt3d_set_dt(rmt3d_scene *s, double dt) {
 extern "C" int rmt3d_init_iter(rmt3d_scene *s) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     const double tol = 1e-4;
-    for (int i = 0; i < s->d.num_iters; i++) {
+    for (int i = 0; s->init_err > 0 && i < s->d.num_iters; i++) {
         set_time(s, 0);
         fill_boundary_cc(s);
         int e = step_forward(s, 0);
@@ -1803,8 +1914,10 @@ extern "C" int rmt3d_init_iter(rmt3d_scene *s) {
         update_rho(s);
         if (divu < tol) break;
     }
-    s->nt = 0;
-    set_time(s, 0.0);
+    if (s->init_err > 0) {
+        s->nt = 0;
+        set_time(s, 0.0);
+    }
     compute_stress(s);
     CK(cudaStreamSynchronize(s->st));
     CK(cudaGetLastError());
@@ -1919,6 +2032,7 @@ extern "C" int rmt3d_get_scalar(rmt3d_scene *s, int which, double *v) {
         case 10: *v = s->K_stiff; break;
         case 11: *v = s->vmax; break;
         case 12: *v = (double)(s->dev_bytes + s->mac.bytes_alloc + s->fem.bytes_alloc); break;
+        case 13: *v = s->init_err; break;
         default: return fail(RMT3D_ERR_INVALID, "unknown scalar");
     }
     return RMT3D_OK;

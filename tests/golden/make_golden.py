@@ -11,8 +11,16 @@ is present):
 
     make -C oracle all nofma && make -C oracle VARDEN=1 all nofma
     python tests/golden/make_golden.py [case ...]
+
+The checkpoint case chk16 (16^3 cavity + sphere of radius 0.3, 2 steps per
+frame) holds the reference's checkpoint after frame 1 (write_chk_pt: the
+eight slice files, decompressed, and recover.cfg), the reference's state at
+that point (s2_*), and its state after restarting from the checkpoint with
+run_sim's sequence and stepping CHK_RESTART_STEPS more steps (s4_*).
 """
+import lzma
 import os
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -53,6 +61,90 @@ CASES = {
 LONG = {
     "cavity32_64": (scenes.cavity(32, 64), 64),
 }
+
+
+CHK_NAMES = ["vx", "vy", "vz", "p", "X", "Y", "Z", "OID"]
+CHK_RESTART_STEPS = 2
+
+
+def chk_cfg():
+    """16^3 cavity + sphere writing a checkpoint every frame of 2 steps."""
+    txt = scenes.cavity_sphere(16, 1000, radius=0.3)
+    for a, b in (("dump_code 0", "dump_code 8"), ("frames 100000", "frames 4"), ("T 100000", "T 0.05")):
+        assert a in txt
+        txt = txt.replace(a, b)
+    return txt
+
+
+def read_chk_dir(d):
+    """The eight field files of a checkpoint directory (raw or .xz) as float64."""
+    out = {}
+    for n in CHK_NAMES:
+        raw = os.path.join(d, n)
+        if os.path.exists(raw):
+            with open(raw, "rb") as fh:
+                data = fh.read()
+        else:
+            with lzma.open(raw + ".xz") as fh:
+                data = fh.read()
+        out[n] = np.frombuffer(data, dtype=np.float64).copy()
+    return out
+
+
+def restart(chk_src, steps, workdir, driver, exact):
+    """The reference restarted from a copy of checkpoint directory chk_src
+    (c.out/chk.00001 relative to workdir, as its recover.cfg names it)."""
+    dst = os.path.join(workdir, "c.out", "chk.00001")
+    if os.path.exists(dst):
+        shutil.rmtree(dst)
+    shutil.copytree(chk_src, dst)
+    out = os.path.join(workdir, "restart.bin")
+    env = dict(os.environ, RMT3D_SHIM_EXACT=exact)
+    subprocess.run([driver, "c.out/chk.00001/recover.cfg", str(steps), out], check=True, capture_output=True,
+                   cwd=workdir, env=env)
+    return refdump.read(out)
+
+
+def make_chk(workdir):
+    txt = chk_cfg()
+    with open(os.path.join(workdir, "c.cfg"), "w") as fh:
+        fh.write(txt)
+    env = dict(os.environ, RMT3D_SHIM_EXACT="1")
+    subprocess.run([DRIVER, "c.cfg", "2", "s2.bin"], check=True, capture_output=True, cwd=workdir, env=env)
+    saved = os.path.join(workdir, "saved_chk1")
+    shutil.copytree(os.path.join(workdir, "c.out", "chk.00001"), saved)
+    arrays = {"cfg": np.frombuffer(txt.encode(), dtype=np.uint8),
+              "restart_steps": np.array(CHK_RESTART_STEPS)}
+    with open(os.path.join(saved, "recover.cfg"), "rb") as fh:
+        arrays["recover_cfg"] = np.frombuffer(fh.read(), dtype=np.uint8)
+    for n, v in read_chk_dir(saved).items():
+        arrays["chk_" + n] = v
+    d2 = refdump.read(os.path.join(workdir, "s2.bin"))
+    for key, val in compact(d2).items():
+        arrays["s2_" + key] = val
+    arrays["s2_env"] = envelope(txt, 2, d2, os.path.join(workdir, "env"))
+    k = 2 + CHK_RESTART_STEPS
+    dr = restart(saved, CHK_RESTART_STEPS, workdir, DRIVER, "1")
+    for key, val in compact(dr).items():
+        arrays["s%d_%s" % (k, key)] = val
+    # rounding envelope of the restart, as envelope() does for a run
+    shp = dr["shape"]
+    sl = (slice(2, -2),) * 3
+    vb = dr["fields"]["vel"].reshape(shp + (3,))[sl]
+    pb = dr["fields"]["p"].reshape(shp)[sl]
+    xb = dr["refmaps"]["x"][dr["refmaps"]["c"] != 0]
+    e = np.zeros(3)
+    for drv, ex in ((DRIVER_NOFMA, "1"), (DRIVER, "0")):
+        dd = restart(saved, CHK_RESTART_STEPS, workdir, drv, ex)
+        v = dd["fields"]["vel"].reshape(shp + (3,))[sl]
+        p = dd["fields"]["p"].reshape(shp)[sl]
+        xd = dd["refmaps"]["x"][dd["refmaps"]["c"] != 0]
+        xe = _rel(xd, xb) if xd.shape == xb.shape and xb.size else 0.0
+        e = np.maximum(e, [_rel(v, vb), _rel(p, pb), xe])
+    arrays["s%d_env" % k] = e
+    print("chk16 envelopes", arrays["s2_env"], e)
+    np.savez_compressed(os.path.join(HERE, "chk16.npz"), **arrays)
+    print("wrote chk16")
 
 
 def compact(d):
@@ -134,6 +226,9 @@ def main():
                 print(name, k, "envelope", arrays["s%d_env" % k])
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
             print("wrote", name)
+        if not only or "chk16" in only:
+            os.makedirs(os.path.join(wd, "chk", "env"))
+            make_chk(os.path.join(wd, "chk"))
         for name, (txt, k) in LONG.items():
             if only and name not in only:
                 continue
