@@ -250,6 +250,43 @@ int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *refmap_aos,
  * and 6 its maximum (total_dev_in_detF, :1032-1084). */
 int rmt3d_diag(rmt3d_scene *s, int kind, double *value);
 
+/* One frame's diagnostics, the values the reference's stepper writes to
+ * macro.dat and centroid.dat (Sim/stepper.hh:378-474). */
+typedef struct {
+    double time;
+    double div_u_max, div_u_min; /* extremes of the face-velocity divergence over the cells */
+    double div_u_l2;             /* weighted L2 norm of the FEM rhs (div_u, fluid_3d_utils.cc:507-653) */
+    double momentum[3];          /* total_momentum (:783-800) */
+    double energy, kinetic, elastic, potential, power; /* total_energy (:806-872); energy is
+                                    elastic + kinetic + potential; power is 0 (no object type of
+                                    this path has active stress) */
+    double max_dev_detF, dev_detF; /* total_dev_in_detF (:1032-1084) */
+    int n_obj;
+    double centroid[RMT3D_MAX_OBJ][3]; /* compute_v_centroid (:1290-1346): heaviside-weighted mean */
+    double velocity[RMT3D_MAX_OBJ][3]; /* position and velocity of each object's primary cells */
+} rmt3d_macro_data;
+
+/* All of rmt3d_macro_data in device reductions of fixed order. */
+int rmt3d_macro(rmt3d_scene *s, rmt3d_macro_data *out);
+
+/* fluid_3d::slice (F3D_Source/fluid_3d_io.cc:98-434): output type `type`
+ * (write_params numbering 0-21: vx vy vz wx wy wz |u| p phi X Y Z OID LID
+ * pr_phi pr_X pr_Y pr_Z div_u div_eu rho J) on the plane `point` of axis
+ * `dim`, as the reference's global slice array out[a + d1 b], the two other
+ * axes in increasing order.  Types 3, 4, 5, 7 and 18 live on the nodal grid
+ * (m+1 points on a non-periodic axis), the rest on the cells.  obj_id -1
+ * picks the map of least level set at each cell, obj_id >= 1 that object's
+ * map.  A point outside the cell range gives zeros, as the reference's
+ * bounds check does (:260-264).  out may be NULL to query d1 and d2. */
+int rmt3d_slice(rmt3d_scene *s, int type, int dim, int point, int obj_id, double *out, int *d1, int *d2);
+
+/* fluid_3d::write_slice (fluid_3d_io.cc:3-91): the slice written to
+ * filename as a text matrix (format 0, "%17.14g "), coordinate text lines
+ * (1) or gnuplot binary floats (2).  Coordinates are cell centres; the
+ * last node of a nodal axis takes the next centre position, where the
+ * reference reads one past its coordinate array. */
+int rmt3d_write_slice(rmt3d_scene *s, int type, int dim, int point, int obj_id, int format, const char *filename);
+
 /* Allocation-free divergence diagnostic (no counterpart in the reference; it
  * is an addition of this library).  Same value as rmt3d_diag(s, 0, ...) for
  * a scene with the given grid, computed from caller-owned device arrays, for

@@ -22,6 +22,10 @@ from ._lib import FP64, MIXED, PROJECTION_ERR, REFMAP_UPDATE_ERR, STEADY_SOLN_EX
 from ._lib import OK as NORMAL_EXIT
 from ._lib import RMT3DError, SceneDesc
 
+# write_params::default_names (IO/write_params.cc:3): slice output types 0-21
+OUTPUT_NAMES = ["vx", "vy", "vz", "wx", "wy", "wz", "w", "p", "phi", "X", "Y", "Z", "OID", "LID", "pr_phi",
+                "pr_X", "pr_Y", "pr_Z", "div_u", "div_eu", "rho", "J"]
+
 FIELD_INDEX = {"u": 0, "v": 1, "w": 2, "p": 3, "dp": 4, "q": 5, "du": 6, "dv": 7, "dw": 8}
 for _f in range(6):
     for _c in range(3):
@@ -124,6 +128,25 @@ class Scene:
         st = ctypes.c_int()
         _lib.check(lib().rmt3d_step_phases(self._h, last_phase, ctypes.byref(st)))
         return st.value
+
+    def macro(self):
+        """The frame diagnostics of macro.dat / centroid.dat (MacroData)."""
+        m = _lib.MacroData()
+        _lib.check(lib().rmt3d_macro(self._h, ctypes.byref(m)))
+        return m
+
+    def slice(self, otype, dim, point, obj_id=-1):
+        """fluid_3d::slice: the global slice array, shape (d2, d1)."""
+        d1, d2 = ctypes.c_int(), ctypes.c_int()
+        _lib.check(lib().rmt3d_slice(self._h, otype, dim, point, obj_id, None, ctypes.byref(d1), ctypes.byref(d2)))
+        out = np.empty(d1.value * d2.value, dtype=np.float64)
+        _lib.check(lib().rmt3d_slice(self._h, otype, dim, point, obj_id, out.ctypes.data_as(ctypes.c_void_p),
+                                     ctypes.byref(d1), ctypes.byref(d2)))
+        return out.reshape(d2.value, d1.value)
+
+    def write_slice(self, otype, dim, point, obj_id, fmt, filename):
+        """fluid_3d::write_slice in format 0 (matrix), 1 (text) or 2 (gnuplot)."""
+        _lib.check(lib().rmt3d_write_slice(self._h, otype, dim, point, obj_id, fmt, str(filename).encode()))
 
     def export_reference(self):
         """State in the reference's AoS layout: (fields, refmaps, ext_index, ext_maps)."""
@@ -252,8 +275,11 @@ class Scene:
 class Stepper:
     """Frame/step loop of the reference's stepper (Sim/stepper.hh:211-376):
     dt fit to frames, a restart's initial step and frame (chk_step,
-    chk_num), stop_short counted from the initial step, and checkpoints
-    every chkpt_freq frames when dump_code has bit 8 (stepper.hh:583-610)."""
+    chk_num), stop_short counted from the initial step, and per frame the
+    outputs of write_files and collect_macro_data (stepper.hh:378-474,
+    583-610) that this path covers: slices of every out_flag type when
+    dump_code has bit 4, checkpoints every chkpt_freq frames with bit 8,
+    macro.dat and centroid.dat with bit 32."""
 
     def __init__(self, desc, scene):
         self.dt, self.steps = stepper_dt(desc, desc.dt)
@@ -269,16 +295,64 @@ class Stepper:
         self.dump_code = run.dump_code
         self.chkpt_freq = run.chkpt_freq
         self.dirname = run.dirname.decode()
+        self.slices = []
+        if self.dump_code & 4:
+            self.slices = [(run.output_dim, run.output_ind, t, run.obj_body, run.data_fmt)
+                           for t in range(len(OUTPUT_NAMES)) if (1 << t) & run.out_flag]
         scene.set_dt(self.dt)
 
     def write_files(self, scene, snum, fnum):
-        if (self.dump_code & 8) and fnum % self.chkpt_freq == 0:
+        if self.slices or (self.dump_code & 8):
             os.makedirs(self.dirname, exist_ok=True)
+        for dim, point, otype, obj_id, fmt in self.slices:
+            scene.write_slice(otype, dim, point, obj_id, fmt,
+                              os.path.join(self.dirname, "%s.%05d" % (OUTPUT_NAMES[otype], fnum)))
+        if (self.dump_code & 8) and fnum % self.chkpt_freq == 0:
             scene.write_chk_pt(snum, fnum, os.path.join(self.dirname, "chk.%05d" % fnum))
+
+    def collect_macro_data(self, scene, frame):
+        """macro.dat and, with objects, centroid.dat, in the reference's
+        layout (stepper.hh:378-474): a header when the file is new or at the
+        initial step, then one record per frame (macro.dat's records carry
+        no newline, as the reference writes them)."""
+        if not self.dump_code & 32:
+            return
+        os.makedirs(self.dirname, exist_ok=True)
+        fn = os.path.join(self.dirname, "macro.dat")
+        if not os.path.exists(fn) or self.curr_tot_step == self.init_step:
+            with open(fn, "w") as fh:
+                fh.write("%10s %6s %6s %10s %6s %10s %6s %10s %10s %10s %10s %10s %10s %10s %10s %10s "
+                         "%10s %10s %16s %16s %10s\n" % (
+                             "#Time", "frame", "steps", "div_u_max", "rank", "div_u_min", "rank", "divu_L2",
+                             "tot_mmt_x", "tot_mmt_y", "tot_mmt_z", "tot_energy", "kinetic", "elastic",
+                             "potential", "power", "max_dev_detF", "dev_detF_L2", "sing. obj. cent.", "volume",
+                             "change in u"))
+        m = scene.macro()
+        e = "%.15e"
+        rec = ("%s %06d %06d %s %06d %s %06d " % (e % m.time, frame, self.curr_tot_step, e % m.div_u_max, 0,
+                                                 e % m.div_u_min, 0))
+        rec += e % m.div_u_l2 + " "
+        rec += " ".join(e % v for v in (m.momentum[0], m.momentum[1], m.momentum[2], m.energy)) + " "
+        rec += " ".join(e % v for v in (m.kinetic, m.elastic, m.potential, m.power)) + " "
+        rec += " ".join(e % v for v in (m.max_dev_detF, m.dev_detF)) + " "
+        with open(fn, "a") as fh:
+            fh.write(rec)
+        if m.n_obj > 0:
+            fc = os.path.join(self.dirname, "centroid.dat")
+            if not os.path.exists(fc) or self.curr_tot_step == self.init_step:
+                with open(fc, "w") as fh:
+                    fh.write("%10s %6s %6s %6s %6s %6s %6s %6s %6s->\n" % ("#Time", "frame", "steps", "x", "y", "z",
+                                                                         "vx", "vy", "vz"))
+            line = "%s %d %d " % (e % m.time, frame, self.curr_tot_step)
+            for o in range(m.n_obj):
+                line += " ".join(e % v for v in tuple(m.centroid[o]) + tuple(m.velocity[o])) + " "
+            with open(fc, "a") as fh:
+                fh.write(line + "\n")
 
     def run(self, scene):
         scene.set_dt(self.dt)
         self.write_files(scene, self.init_step, self.init_frame)
+        self.collect_macro_data(scene, self.init_frame)
         err = 0
         frame = self.init_frame + 1
         while frame <= self.frames - 1 and self.curr_tot_step < self.stop_short:
@@ -292,6 +366,7 @@ class Stepper:
                 if err == STEADY_SOLN_EXIT:
                     break
             self.write_files(scene, self.curr_tot_step, frame)
+            self.collect_macro_data(scene, frame)
             if err == STEADY_SOLN_EXIT:
                 break
             frame += 1

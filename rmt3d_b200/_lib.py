@@ -97,6 +97,19 @@ class SceneDesc(ctypes.Structure):
     ]
 
 
+class MacroData(ctypes.Structure):
+    """rmt3d_macro_data: one frame's macro.dat / centroid.dat values."""
+    _fields_ = [
+        ("time", ctypes.c_double), ("div_u_max", ctypes.c_double), ("div_u_min", ctypes.c_double),
+        ("div_u_l2", ctypes.c_double), ("momentum", ctypes.c_double * 3),
+        ("energy", ctypes.c_double), ("kinetic", ctypes.c_double), ("elastic", ctypes.c_double),
+        ("potential", ctypes.c_double), ("power", ctypes.c_double),
+        ("max_dev_detF", ctypes.c_double), ("dev_detF", ctypes.c_double),
+        ("n_obj", ctypes.c_int),
+        ("centroid", (ctypes.c_double * 3) * MAX_OBJ), ("velocity", (ctypes.c_double * 3) * MAX_OBJ),
+    ]
+
+
 class Request(ctypes.Structure):
     _fields_ = [("arrival_s", ctypes.c_double), ("steps", ctypes.c_int), ("desc", SceneDesc)]
 
@@ -135,6 +148,9 @@ SIGNATURES = {
     "rmt3d_init_iter": (_I, [_P]),
     "rmt3d_write_chk_pt": (_I, [_P, _I, _I, ctypes.c_char_p, _I]),
     "rmt3d_read_chk_pt": (_I, [_P, ctypes.c_char_p, _IP]),
+    "rmt3d_macro": (_I, [_P, ctypes.POINTER(MacroData)]),
+    "rmt3d_slice": (_I, [_P, _I, _I, _I, _I, _P, _IP, _IP]),
+    "rmt3d_write_slice": (_I, [_P, _I, _I, _I, _I, _I, ctypes.c_char_p]),
     "rmt3d_prepare": (_I, [_P]),
     "rmt3d_step": (_I, [_P, _I, _IP]),
     "rmt3d_run": (_I, [_P, _I, _IP]),

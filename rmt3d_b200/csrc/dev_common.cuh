@@ -115,6 +115,7 @@ struct objmap_dev {
     double *fx[18];  // face states fx[f][c] (fields.hh:296)
     double *gp[9];   // grad_phi[F][c] (fields.hh:310)
     double *det[3];  // detF per lower face (fields.hh:308)
+    double *el[3];   // elastic energy density per lower face (fields.hh:307)
     // snapshot of the previous extrapolated maps (temp_extraps, fluid_3d.hh:122)
     int *code_prev;
     double *x_prev[3];

@@ -1,7 +1,10 @@
-// Checkpoint files of the reference (F3D_Source/fluid_3d_chk_pt.cc:3-163):
-// eight raw double files of o z-slices each, optionally xz-compressed, and
-// the recover.cfg parameter file (Sim/sim_params.cc:489-600).  Host side
-// only; the slices are packed and unpacked on the device.
+// Output files in the reference's formats, host side only (the values are
+// computed on the device):
+//  * checkpoints (F3D_Source/fluid_3d_chk_pt.cc:3-163): eight raw double
+//    files of o z-slices each, optionally xz-compressed, and the
+//    recover.cfg parameter file (Sim/sim_params.cc:489-600);
+//  * slice files (fluid_3d_io.cc:3-91): text matrix, coordinate text or
+//    gnuplot binary.
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
@@ -230,6 +233,39 @@ int chk_write_recover_cfg(const char *dir, const rmt3d_scene_desc &d, double dt)
     fprintf(fh, "wall_pos                  %g %g %g %g %g %g\n", d.wall_pos[0], d.wall_pos[1], d.wall_pos[2],
             d.wall_pos[3], d.wall_pos[4], d.wall_pos[5]);
     fprintf(fh, "wall_dist                 %g\n", d.wall_dist);
+    fclose(fh);
+    return 0;
+}
+
+int slice_write_file(const char *filename, const double *u, int d1, int d2, int format, const double *c1,
+                     const double *c2, int m) {
+    FILE *fh = fopen(filename, "w");
+    if (!fh) return fail(RMT3D_ERR_IO, std::string("cannot write ") + filename);
+    if (format == 0) {
+        // save_matrix (fluid_3d_io.cc:58-63)
+        for (int j = 0; j < d2; j++) {
+            for (int i = 0; i < d1; i++) fprintf(fh, "%17.14g ", u[i + j * d1]);
+            fputc('\n', fh);
+        }
+    } else if (format == 1) {
+        // save_text (:65-71)
+        for (int j = 0; j < d2; j++) {
+            for (int i = 0; i < d1; i++) fprintf(fh, "%17.14f %17.14f %17.14f\n", c1[i], c2[j], u[i + j * d1]);
+            fputc('\n', fh);
+        }
+    } else {
+        // save_gnuplot (:73-91): a row of (m, x coordinates), then per line
+        // (y coordinate, values), all as floats
+        std::vector<float> buf(d1 + 1);
+        buf[0] = (float)m;
+        for (int i = 0; i < d1; i++) buf[i + 1] = (float)c1[i];
+        fwrite(buf.data(), sizeof(float), d1 + 1, fh);
+        for (int j = 0; j < d2; j++) {
+            buf[0] = (float)c2[j];
+            for (int i = 0; i < d1; i++) buf[i + 1] = (float)u[i + j * d1];
+            fwrite(buf.data(), sizeof(float), d1 + 1, fh);
+        }
+    }
     fclose(fh);
     return 0;
 }

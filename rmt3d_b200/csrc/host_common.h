@@ -29,7 +29,7 @@ int group_finish(scene_group *g, int *status);
 void group_destroy(scene_group *g);
 long long group_mg_launches(const scene_group *g);
 
-// Checkpoint files (chk_io.cc).  A packed checkpoint holds kChkFields
+// Checkpoint files (files.cc).  A packed checkpoint holds kChkFields
 // fields in kChkNames order, each nslices slices of slice_len doubles.
 constexpr int kChkFields = 8;
 extern const char *const kChkNames[kChkFields];
@@ -38,4 +38,8 @@ int chk_write_files(const char *dir, const double *buf, size_t slice_len, int ns
 // *status: 0 read, 1 a file missing, 2 a file empty (the reference's codes)
 int chk_read_files(const char *dir, double *buf, size_t slice_len, int nslices, int *status);
 int chk_write_recover_cfg(const char *dir, const rmt3d_scene_desc &d, double dt);
+// a slice u[a + d1 b] in write_slice's format 0, 1 or 2; c1, c2 are the
+// coordinates of the two axes, m the x extent written in the gnuplot header
+int slice_write_file(const char *filename, const double *u, int d1, int d2, int format, const double *c1,
+                     const double *c2, int m);
 }

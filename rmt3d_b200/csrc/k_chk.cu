@@ -105,6 +105,7 @@ __global__ void k_chk_unpack(grid_dev g, const fields_dev *__restrict__ F, const
             mm.x[a][ind] = X[a];
             mm.xp[a][ind] = X[a];
             mm.det[a][ind] = 0.;
+            mm.el[a][ind] = 0.;
         }
         for (int a = 0; a < 9; a++) mm.gp[a][ind] = -kBig;
         for (int a = 0; a < 18; a++) mm.fx[a][ind] = 0.;

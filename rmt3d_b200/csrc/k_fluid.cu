@@ -246,6 +246,7 @@ __device__ void face_stress(const grid_dev &g, const fields_dev *__restrict__ F,
         const objmap_dev &m = F->om[o];
         for (int c = 0; c < 3; c++) m.gp[3 * FF + c][ind] = -kBig;
         m.det[FF][ind] = -kBig;
+        m.el[FF][ind] = -kBig;
         // neighbour inside the local box (get_refmap with a position check)
         auto nb = [&](int da, int sa, int db, int sb) -> int {
             int p[3] = {pos[0], pos[1], pos[2]};
@@ -302,8 +303,18 @@ __device__ void face_stress(const grid_dev &g, const fields_dev *__restrict__ F,
                              v[3 * ((ii + 1) % 3) + (jj + 2) % 3] * v[3 * ((ii + 2) % 3) + (jj + 1) % 3];
                 Fm[3 * jj + ii] = cof / d;
             }
-        m.det[FF][ind] = Fm[0] * (Fm[4] * Fm[8] - Fm[5] * Fm[7]) + Fm[3] * (Fm[2] * Fm[7] - Fm[1] * Fm[8]) +
-                         Fm[6] * (Fm[1] * Fm[5] - Fm[2] * Fm[4]);
+        const double detF = Fm[0] * (Fm[4] * Fm[8] - Fm[5] * Fm[7]) + Fm[3] * (Fm[2] * Fm[7] - Fm[1] * Fm[8]) +
+                            Fm[6] * (Fm[1] * Fm[5] - Fm[2] * Fm[4]);
+        m.det[FF][ind] = detF;
+        {  // strain energy 0.5 G (tr(F^T F) - 3 - 2 log det F) (fluid_3d.cc:1933-1938)
+            double tr = 0;
+            for (int a = 0; a < 3; a++) {
+                double d = 0;
+                for (int kk = 0; kk < 3; kk++) d += Fm[3 * kk + a] * Fm[3 * kk + a];
+                tr += d;
+            }
+            m.el[FF][ind] = 0.5 * G * (tr - 3 - 2 * log(detF));
+        }
         // left Cauchy-Green F F^T as a symmetric matrix (matlib.hh:214-229)
         double sg[3][3];
         for (int a = 0; a < 3; a++)

@@ -41,6 +41,13 @@ __global__ void k_fem_rhs(grid_dev g, const fields_dev *__restrict__ F, double *
 __global__ void k_fem_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x, const double *mean);
 __global__ void k_sub_pgrad(grid_dev g, const fields_dev *__restrict__ F, double dt, int var_den);
 __global__ void k_chk_pack(grid_dev g, const fields_dev *__restrict__ F, double *__restrict__ buf);
+__global__ void k_macro_cells(grid_dev g, const fields_dev *__restrict__ F, const double *lz, int var_den,
+                              double *out, unsigned *ticket);
+__global__ void k_macro_obj(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+                            const double *lz, int o, double *out, unsigned *ticket);
+__global__ void k_divu_l2(grid_dev g, const double *r, double *out, unsigned *ticket);
+__global__ void k_slice(grid_dev g, const fields_dev *__restrict__ F, const double *r, int type, int dim, int point,
+                        int obj_id, int var_den, int d1, int d2, double *out);
 __global__ void k_chk_unpack(grid_dev g, const fields_dev *__restrict__ F, const double *__restrict__ buf, int *bad);
 
 }  // namespace rmt3d

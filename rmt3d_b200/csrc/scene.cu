@@ -1422,33 +1422,14 @@ static int run_graph(rmt3d_scene *s, int nsteps, int *status) {
     return graph_finish(s, p, status);
 }
 
-// div_u (fluid_3d_utils.cc:507-560): weighted L2 norm of the FEM rhs
-__global__ void k_divu(grid_dev g, const double *r, double *out) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    int b = blockIdx.y * blockDim.y + threadIdx.y;
-    int c = blockIdx.z * blockDim.z + threadIdx.z;
-    double v = 0;
-    if (a < g.fm && b < g.fn && c < g.fo) {
-        double nk = (c == 0 || c == g.fo - 1) ? 0.5 : 1.0;
-        if (g.prd[2]) nk = 1.0;
-        double nj = (b == 0 || b == g.fn - 1) ? 0.5 : 1.0;
-        if (g.prd[1]) nj = 1.0;
-        double ni = (a == 0 || a == g.fm - 1) ? 0.5 : 1.0;
-        if (g.prd[0]) ni = 1.0;
-        double rr = r[a + g.fm * (b + g.fn * c)];
-        v = ni * nj * nk * rr * rr;
-    }
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) % 32 == 0) atomicAdd(out, v);
-}
-
+// div_u (fluid_3d_utils.cc:507-560): weighted L2 norm of the FEM rhs, reduced
+// in a fixed order
 static int div_u(rmt3d_scene *s, double *out) {
     const grid_dev &g = s->g;
     k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
-    CK(cudaMemsetAsync(s->d_red, 0, sizeof(double), s->st));
-    k_divu<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->fem.rhs(), s->d_red);
+    k_divu_l2<<<kMeanBlocks, 256, 0, s->st>>>(g, s->fem.rhs(), s->d_diag, s->diag_ticket);
     s->count(2);
-    CK(cudaMemcpyAsync(s->h_scalar, s->d_red, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(s->h_scalar, s->d_diag, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     *out = sqrt(*s->h_scalar / ((double)g.fm * g.fn * g.fo));
     return 0;
@@ -1662,7 +1643,8 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     for (int o = 0; o < d.n_obj && !e; o++) {
         objmap_dev &m = F.om[o];
         e |= s->alloc(&m.code, n) | s->alloc(&m.code_prev, n);
-        for (int c = 0; c < 3; c++) e |= s->alloc(&m.x[c], n) | s->alloc(&m.xp[c], n) | s->alloc(&m.x_prev[c], n) | s->alloc(&m.det[c], n);
+        for (int c = 0; c < 3; c++) e |= s->alloc(&m.x[c], n) | s->alloc(&m.xp[c], n) | s->alloc(&m.x_prev[c], n) | s->alloc(&m.det[c], n) |
+                                         s->alloc(&m.el[c], n);
         for (int c = 0; c < 18; c++) e |= s->alloc(&m.fx[c], n);
         for (int c = 0; c < 9; c++) e |= s->alloc(&m.gp[c], n) | s->alloc(&m.gp_prev[c], n);
         cudaMemsetAsync(m.code, 0xff, n * sizeof(int), s->st);
@@ -2090,7 +2072,7 @@ namespace {
 constexpr int F_VEL = 0, F_P = 3, F_DP = 4, F_Q = 5, F_DVEL = 6, F_FVEL = 18, F_SIGMA = 36, F_N = 45;
 // ref_map (in doubles after the 8-byte id word): x[3], xpred[3], nv_der[3][3],
 // fx[6][3], sigma[3][3], elastic_energy[3], detF[3], grad_phi[3][3], act_power[3]
-constexpr int R_X = 1, R_XP = 4, R_FX = 16, R_DET = 46, R_GP = 49;
+constexpr int R_X = 1, R_XP = 4, R_FX = 16, R_EL = 43, R_DET = 46, R_GP = 49;
 }  // namespace
 
 extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, const void *refmap_aos,
@@ -2114,7 +2096,7 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
     const int no = s->g.n_obj;
     if (no > 0 && refmap_aos) {
         std::vector<int> code(n);
-        std::vector<double> X(n * 3), XP(n * 3), FX(n * 18), GP(n * 9), DT(n * 3);
+        std::vector<double> X(n * 3), XP(n * 3), FX(n * 18), GP(n * 9), DT(n * 3), EL(n * 3);
         auto rd = [&](const unsigned char *rec, int off) { return ((const double *)rec)[off]; };
         for (int o = 0; o < no; o++) {
             std::fill(code.begin(), code.end(), -1);
@@ -2126,6 +2108,7 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
                     X[c * n + cell] = rd(rec, R_X + c);
                     XP[c * n + cell] = rd(rec, R_XP + c);
                     DT[c * n + cell] = rd(rec, R_DET + c);
+                    EL[c * n + cell] = rd(rec, R_EL + c);
                 }
                 for (int c = 0; c < 18; c++) FX[c * n + cell] = rd(rec, R_FX + c);
                 for (int c = 0; c < 9; c++) GP[c * n + cell] = rd(rec, R_GP + c);
@@ -2147,6 +2130,7 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
                 CK(copy_sync(s, m.x[c], X.data() + c * n, n * 8, cudaMemcpyHostToDevice));
                 CK(copy_sync(s, m.xp[c], XP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
                 CK(copy_sync(s, m.det[c], DT.data() + c * n, n * 8, cudaMemcpyHostToDevice));
+                CK(copy_sync(s, m.el[c], EL.data() + c * n, n * 8, cudaMemcpyHostToDevice));
             }
             for (int c = 0; c < 18; c++) CK(copy_sync(s, m.fx[c], FX.data() + c * n, n * 8, cudaMemcpyHostToDevice));
             for (int c = 0; c < 9; c++) CK(copy_sync(s, m.gp[c], GP.data() + c * n, n * 8, cudaMemcpyHostToDevice));
@@ -2184,13 +2168,15 @@ extern "C" int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *ref
     int ne = 0;
     if (refmap_aos) memset(refmap_aos, 0, n * 488);
     std::vector<int> code(n);
-    std::vector<double> X(3 * n), XP(3 * n), FX(18 * n), GP(9 * n);
+    std::vector<double> X(3 * n), XP(3 * n), FX(18 * n), GP(9 * n), DT(3 * n), EL(3 * n);
     for (int o = 0; o < s->g.n_obj; o++) {
         objmap_dev &m = s->hF.om[o];
         CK(copy_sync(s, code.data(), m.code, n * sizeof(int), cudaMemcpyDeviceToHost));
         for (int c = 0; c < 3; c++) {
             CK(copy_sync(s, X.data() + c * n, m.x[c], n * 8, cudaMemcpyDeviceToHost));
             CK(copy_sync(s, XP.data() + c * n, m.xp[c], n * 8, cudaMemcpyDeviceToHost));
+            CK(copy_sync(s, DT.data() + c * n, m.det[c], n * 8, cudaMemcpyDeviceToHost));
+            CK(copy_sync(s, EL.data() + c * n, m.el[c], n * 8, cudaMemcpyDeviceToHost));
         }
         for (int c = 0; c < 18; c++) CK(copy_sync(s, FX.data() + c * n, m.fx[c], n * 8, cudaMemcpyDeviceToHost));
         for (int c = 0; c < 9; c++) CK(copy_sync(s, GP.data() + c * n, m.gp[c], n * 8, cudaMemcpyDeviceToHost));
@@ -2200,6 +2186,8 @@ extern "C" int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *ref
             for (int c = 0; c < 3; c++) {
                 r[R_X + c] = X[c * n + cell];
                 r[R_XP + c] = XP[c * n + cell];
+                r[R_DET + c] = DT[c * n + cell];
+                r[R_EL + c] = EL[c * n + cell];
             }
             for (int c = 0; c < 18; c++) r[R_FX + c] = FX[c * n + cell];
             for (int c = 0; c < 9; c++) r[R_GP + c] = GP[c * n + cell];
@@ -2309,6 +2297,116 @@ extern "C" int rmt3d_diag(rmt3d_scene *s, int kind, double *value) {
     return RMT3D_OK;
 }
 
+// ---------------------------------------------------------------------------
+// frame diagnostics and slices (Sim/stepper.hh:378-474, fluid_3d_io.cc:3-434)
+// ---------------------------------------------------------------------------
+extern "C" int rmt3d_macro(rmt3d_scene *s, rmt3d_macro_data *out) {
+    if (!s || !out) return fail(RMT3D_ERR_INVALID, "null argument");
+    memset(out, 0, sizeof(*out));
+    const grid_dev &g = s->g;
+    out->time = s->time;
+    out->n_obj = g.n_obj;
+    int e = div_u(s, &out->div_u_l2);
+    if (e) return e;
+    double v[8];
+    k_macro_cells<<<kMeanBlocks, 256, 0, s->st>>>(g, s->dF, s->lz, s->d.var_den, s->d_diag, s->diag_ticket);
+    s->count();
+    CK(copy_sync(s, v, s->d_diag, 8 * sizeof(double), cudaMemcpyDeviceToHost));
+    // total_momentum: sum * dx * dy * dz; total_energy: each sum * (dx dy dz)
+    for (int c = 0; c < 3; c++) out->momentum[c] = v[c] * g.dx * g.dy * g.dz;
+    const double dv = g.dx * g.dy * g.dz;
+    out->elastic = v[5] * dv;
+    out->kinetic = v[3] * dv;
+    out->potential = v[4] * dv;
+    out->power = 0;
+    out->energy = out->elastic + out->kinetic + out->potential;
+    out->div_u_max = v[6];
+    out->div_u_min = -v[7];
+    for (int o = 0; o < g.n_obj; o++) {
+        double w[7];
+        k_macro_obj<<<kMeanBlocks, 256, 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, o, s->d_diag, s->diag_ticket);
+        s->count();
+        CK(copy_sync(s, w, s->d_diag, 7 * sizeof(double), cudaMemcpyDeviceToHost));
+        // sim_manager::compute_avgs: means, 0 for an object without weight
+        for (int c = 0; c < 3; c++) {
+            out->velocity[o][c] = w[0] != 0. ? w[4 + c] / w[0] : 0.;
+            out->centroid[o][c] = w[0] != 0. ? w[1 + c] / w[0] : 0.;
+        }
+    }
+    if (g.n_obj > 0) {
+        double d[kDiagVals];
+        if ((e = solid_diag(s, d))) return e;
+        out->dev_detF = sqrt(d[4] * dv);
+        out->max_dev_detF = sqrt(d[5]);
+    }
+    return RMT3D_OK;
+}
+
+// extents of a slice: the two axes other than dim, in increasing order, over
+// the cells or (types 3, 4, 5, 7, 18) the nodes
+static void slice_dims(const rmt3d_scene *s, int type, int dim, int *d1, int *d2) {
+    const bool corner = (type >= 3 && type < 6) || type == 7 || type == 18;
+    int ext[3] = {s->g.sm, s->g.sn, s->g.so};
+    if (corner) {
+        ext[0] = s->g.fm;
+        ext[1] = s->g.fn;
+        ext[2] = s->g.fo;
+    }
+    *d1 = ext[dim == 0 ? 1 : 0];
+    *d2 = ext[dim == 2 ? 1 : 2];
+}
+
+extern "C" int rmt3d_slice(rmt3d_scene *s, int type, int dim, int point, int obj_id, double *out, int *d1,
+                           int *d2) {
+    if (!s || !d1 || !d2) return fail(RMT3D_ERR_INVALID, "null argument");
+    if (type < 0 || type > 21) return fail(RMT3D_ERR_INVALID, "output type outside 0..21");
+    if (dim < 0 || dim > 2) return fail(RMT3D_ERR_INVALID, "slice axis outside 0..2");
+    if (obj_id != -1 && (obj_id < 1 || obj_id > s->g.n_obj)) return fail(RMT3D_ERR_INVALID, "object id outside -1, 1..n_obj");
+    slice_dims(s, type, dim, d1, d2);
+    if (!out) return RMT3D_OK;
+    const size_t n = (size_t)*d1 * *d2;
+    const int cells[3] = {s->g.sm, s->g.sn, s->g.so};
+    if (point < 0 || point >= cells[dim]) {
+        memset(out, 0, n * sizeof(double));
+        return RMT3D_OK;
+    }
+    const grid_dev &g = s->g;
+    if (type == 18) {  // fill_pp_rhs first (fluid_3d_io.cc:162-164)
+        k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
+        s->count();
+    }
+    double *d = nullptr;
+    CK(cudaMallocAsync((void **)&d, n * sizeof(double), s->st));
+    k_slice<<<lin_blocks((int)n), 256, 0, s->st>>>(g, s->dF, s->fem.rhs(), type, dim, point, obj_id, s->d.var_den,
+                                                  *d1, *d2, d);
+    s->count();
+    cudaError_t ce = cudaMemcpyAsync(out, d, n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->st);
+    cudaFreeAsync(d, s->st);
+    CK(ce);
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_write_slice(rmt3d_scene *s, int type, int dim, int point, int obj_id, int format,
+                                 const char *filename) {
+    if (!s || !filename) return fail(RMT3D_ERR_INVALID, "null argument");
+    if (format < 0 || format > 2) return fail(RMT3D_ERR_INVALID, "slice format outside 0..2");
+    int d1, d2;
+    int e = rmt3d_slice(s, type, dim, point, obj_id, nullptr, &d1, &d2);
+    if (e) return e;
+    std::vector<double> u((size_t)d1 * d2);
+    if ((e = rmt3d_slice(s, type, dim, point, obj_id, u.data(), &d1, &d2))) return e;
+    // the coordinates of the two axes: cell centres (gx, gy, gz of
+    // fluid_3d.cc:132-134), continued by the ghost centre for the last node
+    // of a nodal axis
+    const std::vector<double> *ax[3] = {&s->hlx, &s->hly, &s->hlz};
+    const int a1 = dim == 0 ? 1 : 0, a2 = dim == 2 ? 1 : 2;
+    std::vector<double> c1(d1), c2(d2);
+    for (int i = 0; i < d1; i++) c1[i] = (*ax[a1])[i + 2];
+    for (int j = 0; j < d2; j++) c2[j] = (*ax[a2])[j + 2];
+    return slice_write_file(filename, u.data(), d1, d2, format, c1.data(), c2.data(), s->g.sm);
+}
+
 extern "C" int rmt3d_sync(rmt3d_scene *s) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     CK(cudaStreamSynchronize(s->st));
@@ -2351,7 +2449,7 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     if (!d || d->sys_size[0] < 1 || d->sys_size[1] < 1 || d->sys_size[2] < 1) return 0;
     const size_t n = (size_t)(d->sys_size[0] + 4) * (d->sys_size[1] + 4) * (d->sys_size[2] + 4);
     size_t b = n * sizeof(double) * (36 + (d->var_den ? 1 : 0));
-    b += (size_t)d->n_obj * n * (2 * sizeof(int) + 48 * sizeof(double));
+    b += (size_t)d->n_obj * n * (2 * sizeof(int) + 51 * sizeof(double));
     if (d->n_obj > 0) b += n * (2 * sizeof(uint8_t) + 2 * sizeof(int));
     b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);
     b += sizeof(fields_dev) + sizeof(scene_ctl) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);
@@ -2470,7 +2568,10 @@ namespace {
 constexpr size_t kNoallocMaxNodes = 65 * 65 * 65;
 constexpr size_t kNoallocHeader = 16384;  // accumulator + argument block, 256-aligned
 constexpr size_t kNoallocBytes = kNoallocHeader + kNoallocMaxNodes * sizeof(double);
-static_assert(sizeof(fields_dev) + 256 <= kNoallocHeader, "argument block does not fit");
+// [0, 256): reduction ticket; [256, kNoallocRed): argument block;
+// [kNoallocRed, ...): fixed-order reduction partials of k_divu_l2
+constexpr size_t kNoallocRed = 256 + (sizeof(fields_dev) + 255) / 256 * 256;
+static_assert(kNoallocRed + (1 + kMeanBlocks) * sizeof(double) <= kNoallocHeader, "argument block does not fit");
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
@@ -2549,15 +2650,16 @@ extern "C" int rmt3d_div_u_noalloc(const int sys_size[3], const int periodic[3],
     int e = noalloc_scratch(&base);
     if (e) return e;
     cudaStream_t st = (cudaStream_t)stream;
-    double *acc = (double *)base;
+    unsigned *ticket = (unsigned *)base;
     fields_dev *dF = (fields_dev *)(base + 256);
+    double *red = (double *)(base + kNoallocRed);
     double *rhs = (double *)(base + kNoallocHeader);
-    CK(cudaMemsetAsync(acc, 0, sizeof(double), st));
+    CK(cudaMemsetAsync(ticket, 0, sizeof(unsigned), st));
     CK(cudaMemcpyAsync(dF, &hf, sizeof(hf), cudaMemcpyHostToDevice, st));
     k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, st>>>(g, dF, rhs, gp);
-    k_divu<<<grd(g.fm, g.fn, g.fo), blk(), 0, st>>>(g, rhs, acc);
+    k_divu_l2<<<kMeanBlocks, 256, 0, st>>>(g, rhs, red, ticket);
     double sum = 0;
-    CK(cudaMemcpyAsync(&sum, acc, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&sum, red, sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     CK(cudaGetLastError());
     *norm_out = sqrt(sum / ((double)g.fm * g.fn * g.fo));

@@ -12,6 +12,12 @@ is present):
     make -C oracle all nofma && make -C oracle VARDEN=1 all nofma
     python tests/golden/make_golden.py [case ...]
 
+The output case out16 holds the files the reference's stepper writes for the
+same workload with slice output and frame diagnostics switched on (dump_code
+4 | 32): slices of all 22 output types along y (text matrices), a subset
+along x (gnuplot binary) and along z (coordinate text), and macro.dat /
+centroid.dat, at frames 0 and 1.
+
 The checkpoint case chk16 (16^3 cavity + sphere of radius 0.3, 2 steps per
 frame) holds the reference's checkpoint after frame 1 (write_chk_pt: the
 eight slice files, decompressed, and recover.cfg), the reference's state at
@@ -147,6 +153,40 @@ def make_chk(workdir):
     print("wrote chk16")
 
 
+# name -> extra .cfg lines of the output case (same workload as chk16)
+OUT_RUNS = {
+    "y_matrix": "dump_code 36\nout_flag %d\noutput_dim 1\noutput_ind 8\ndata_fmt 0\n" % ((1 << 22) - 1),
+    "x_gnuplot": "dump_code 4\nout_flag %d\noutput_dim 0\noutput_ind 5\ndata_fmt 2\n" % (
+        (1 << 0) | (1 << 6) | (1 << 8) | (1 << 12) | (1 << 19)),
+    "z_text": "dump_code 4\nout_flag %d\noutput_dim 2\noutput_ind 3\ndata_fmt 1\n" % (
+        (1 << 1) | (1 << 9) | (1 << 13) | (1 << 20)),
+}
+
+
+def out_cfg(extra):
+    txt = chk_cfg().replace("dump_code 8", "")
+    return txt + extra
+
+
+def make_out(workdir):
+    arrays = {}
+    for name, extra in OUT_RUNS.items():
+        wd = os.path.join(workdir, name)
+        os.makedirs(wd)
+        txt = out_cfg(extra)
+        with open(os.path.join(wd, "c.cfg"), "w") as fh:
+            fh.write(txt)
+        env = dict(os.environ, RMT3D_SHIM_EXACT="1")
+        subprocess.run([DRIVER, "c.cfg", "2", "s2.bin"], check=True, capture_output=True, cwd=wd, env=env)
+        arrays["cfg_" + name] = np.frombuffer(txt.encode(), dtype=np.uint8)
+        outdir = os.path.join(wd, "c.out")
+        for fn in sorted(os.listdir(outdir)):
+            with open(os.path.join(outdir, fn), "rb") as fh:
+                arrays["file_%s/%s" % (name, fn)] = np.frombuffer(fh.read(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "out16.npz"), **arrays)
+    print("wrote out16", len(arrays), "arrays")
+
+
 def compact(d):
     """Reduce a dump to the state the step reads and writes."""
     f, rm = d["fields"], d["refmaps"]
@@ -226,6 +266,9 @@ def main():
                 print(name, k, "envelope", arrays["s%d_env" % k])
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
             print("wrote", name)
+        if not only or "out16" in only:
+            os.makedirs(os.path.join(wd, "out"))
+            make_out(os.path.join(wd, "out"))
         if not only or "chk16" in only:
             os.makedirs(os.path.join(wd, "chk", "env"))
             make_chk(os.path.join(wd, "chk"))
