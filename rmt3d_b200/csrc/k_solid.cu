@@ -134,54 +134,72 @@ __device__ inline bool inner_ghost(const grid_dev &g, int i, int j, int k) {
     return i >= 1 && i <= g.sm4 - 2 && j >= 1 && j <= g.sn4 - 2 && k >= 1 && k <= g.so4 - 2;
 }
 
+// The frontier state of every object side by side: lay[o * ncell + cell]
+// holds, for object o, 0 on primary cells, L on cells listed for layer L and
+// 255 on free cells (the reference's mask values relative to cur_mask);
+// front[o * ncell + t] lists object o's current frontier, cnt[o] its length.
+// Objects are extrapolated independently of one another (each reads and
+// writes only its own maps), so all of them advance one layer per launch.
+
 // first_layer + mark_primary (fluid_3d_ex.cc:52-70): reset the layer tags
-__global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, int o, uint8_t *lay, uint8_t *inl) {
+__global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t *lay, uint8_t *inl) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
-    lay[ind] = (F->om[o].code[ind] == 0) ? 0 : 255;
-    inl[ind] = 0;
+    for (int o = 0; o < g.n_obj; o++) {
+        lay[(size_t)o * g.ncell + ind] = (F->om[o].code[ind] == 0) ? 0 : 255;
+        inl[(size_t)o * g.ncell + ind] = 0;
+    }
 }
 
-// neighbours of the current frontier join the next layer
-// (add_to_next_list with the orthogonal rule, extrap_helper.hh:166-255)
-__global__ void k_lay_push(grid_dev g, const int *front, const int *nfront, int from_primary, uint8_t *lay,
-                           uint8_t *inl, int next) {
+// mark the free orthogonal neighbours of cell ind for layer `next`
+__device__ inline void push_from(const grid_dev &g, int ind, uint8_t *lay, uint8_t *inl, int next) {
     const int strides[3] = {1, g.sm4, g.smn4};
+    int k = ind / g.smn4, j = (ind % g.smn4) / g.sm4, i = ind % g.sm4;
+    if (!inner_ghost(g, i, j, k)) return;
+    for (int d = 0; d < 3; d++)
+        for (int sg = -1; sg <= 1; sg += 2) {
+            int c = ind + sg * strides[d];
+            if (lay[c] == 255) {
+                lay[c] = (uint8_t)next;
+                inl[c] = 1;
+            }
+        }
+}
+
+// (object, index) of entry t of the concatenated frontiers; false past the end
+__device__ inline bool front_entry(int n_obj, const int *cnt, int &t, int &o) {
+    for (o = 0; o < n_obj; o++) {
+        if (t < cnt[o]) return true;
+        t -= cnt[o];
+    }
+    return false;
+}
+
+// neighbours of the primary cells (from_primary) or of the current
+// frontiers join the next layer (add_to_next_list with the orthogonal rule,
+// extrap_helper.hh:166-255)
+__global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int from_primary, uint8_t *lay,
+                           uint8_t *inl, int next) {
     if (from_primary) {
         int ind = blockIdx.x * blockDim.x + threadIdx.x;
         if (ind >= g.ncell) return;
-        if (lay[ind] != 0) return;
-        int k = ind / g.smn4, j = (ind % g.smn4) / g.sm4, i = ind % g.sm4;
-        if (!inner_ghost(g, i, j, k)) return;
-        for (int d = 0; d < 3; d++)
-            for (int sg = -1; sg <= 1; sg += 2) {
-                int c = ind + sg * strides[d];
-                if (lay[c] == 255) {
-                    lay[c] = (uint8_t)next;
-                    inl[c] = 1;
-                }
-            }
+        for (int o = 0; o < g.n_obj; o++) {
+            uint8_t *lo = lay + (size_t)o * g.ncell;
+            if (lo[ind] == 0) push_from(g, ind, lo, inl + (size_t)o * g.ncell, next);
+        }
         return;
     }
-    const int nf = *nfront;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nf; t += gridDim.x * blockDim.x) {
-        int ind = front[t];
-        int k = ind / g.smn4, j = (ind % g.smn4) / g.sm4, i = ind % g.sm4;
-        if (!inner_ghost(g, i, j, k)) continue;
-        for (int d = 0; d < 3; d++)
-            for (int sg = -1; sg <= 1; sg += 2) {
-                int c = ind + sg * strides[d];
-                if (lay[c] == 255) {
-                    lay[c] = (uint8_t)next;
-                    inl[c] = 1;
-                }
-            }
+    int total = 0;
+    for (int o = 0; o < g.n_obj; o++) total += cnt[o];
+    for (int t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < total; t0 += gridDim.x * blockDim.x) {
+        int t = t0, o;
+        if (!front_entry(g.n_obj, cnt, t, o)) break;
+        const size_t off = (size_t)o * g.ncell;
+        push_from(g, front[off + t], lay + off, inl + off, next);
     }
 }
 
-// comm_mask on one rank: image-backed ghosts take the mask of their image
-// (extrap_helper.cc:261-300); then scan_ghost_region (:304-327) lists ghosts
-// that received the newest tag.
+// image-backed ghost cells take their image's tag (periodic domains only)
 __global__ void k_lay_ghost(grid_dev g, uint8_t *lay, uint8_t *inl, int next) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
@@ -193,19 +211,26 @@ __global__ void k_lay_ghost(grid_dev g, uint8_t *lay, uint8_t *inl, int next) {
         if (c[d] < 2) c[d] += s[d];
         else if (c[d] >= 2 + s[d]) c[d] -= s[d];
     }
-    uint8_t v = lay[gidx(g, c[0], c[1], c[2])];
-    lay[ind] = v;
-    if (v == next) inl[ind] = 1;
+    const int src = gidx(g, c[0], c[1], c[2]);
+    for (int o = 0; o < g.n_obj; o++) {
+        const size_t off = (size_t)o * g.ncell;
+        uint8_t v = lay[off + src];
+        lay[off + ind] = v;
+        if (v == next) inl[off + ind] = 1;
+    }
 }
 
-// compaction of the listed cells into the next frontier (update_list)
-__global__ void k_lay_compact(grid_dev g, uint8_t *inl, int *front, int *nfront) {
+// compaction of the listed cells into the next frontiers (update_list)
+__global__ void k_lay_compact(grid_dev g, uint8_t *inl, int *front, int *cnt) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
-    if (!inl[ind]) return;
-    inl[ind] = 0;
-    int p = atomicAdd(nfront, 1);
-    front[p] = ind;
+    for (int o = 0; o < g.n_obj; o++) {
+        const size_t off = (size_t)o * g.ncell;
+        if (!inl[off + ind]) continue;
+        inl[off + ind] = 0;
+        int p = atomicAdd(cnt + o, 1);
+        front[off + p] = ind;
+    }
 }
 
 __device__ inline double warp_sum(double v) {
@@ -219,16 +244,28 @@ __device__ inline double warp_sum(double v) {
 // (extrap_helper.cc:34-103) with lin_sys (:129-146), mat3::inverse
 // (Utilities/mat3.hh:61-67) and transfer (fluid_3d_ex.cc:293-328).
 // -------------------------------------------------------------------------
-__global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, int o, const int *front,
-                               const int *nfront, int L, int max_rs, double wt, const double *lx, const double *ly,
-                               const double *lz, int *err) {
+// Every object's frontier in one launch: warp w takes entry w of the
+// concatenated frontiers.  The weights wt^n (n = |p|+|q|+|r|) come from a
+// per-block table of the same pow() values.
+constexpr int kPowTab = 64;
+__global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, const int *front, const int *cnt, int L,
+                               int max_rs, double wt, const double *lx, const double *ly, const double *lz,
+                               int *err) {
+    __shared__ double wpow[kPowTab];
+    const int npow = 3 * max_rs + 1;
+    for (int q = threadIdx.x; q < kPowTab && q < npow; q += blockDim.x) wpow[q] = pow(wt, (double)q);
+    __syncthreads();
+    auto wpw = [&](int e) { return e < kPowTab ? wpow[e] : pow(wt, (double)e); };
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const objmap_dev &m = F->om[o];
-    const int nf = *nfront;
-    for (int t = warp; t < nf; t += nwarps) {
-        const int ind = front[t];
+    int total = 0;
+    for (int o = 0; o < g.n_obj; o++) total += cnt[o];
+    for (int t0 = warp; t0 < total; t0 += nwarps) {
+        int t = t0, o;
+        if (!front_entry(g.n_obj, cnt, t, o)) break;
+        const objmap_dev &m = F->om[o];
+        const int ind = front[(size_t)o * g.ncell + t];
         const int kk = ind / g.smn4, jj = (ind % g.smn4) / g.sm4, ii = ind % g.sm4;
         if (image_backed(g, ii, jj, kk)) continue;  // within_extrapolation_domain
         // average of the previous step's interface normals over the six faces
@@ -289,7 +326,7 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, int
                 int cd = m.code[qi];
                 if (cd < 0 || cd >= L) continue;
                 double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
-                double wgt = pow(wt, (double)(abs(p) + abs(q) + abs(r)));
+                double wgt = wpw(abs(p) + abs(q) + abs(r));
                 if (directional) {
                     double ev[3] = {cx - d[0], cy - d[1], cz - d[2]};
                     double dw = 0, en = 0;
@@ -333,7 +370,7 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, int
                 int cd = m.code[qi];
                 if (cd < 0 || cd >= L) continue;
                 double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
-                double Q = pow(wt, (double)(abs(p) + abs(q) + abs(r)));
+                double Q = wpw(abs(p) + abs(q) + abs(r));
                 if (directional) {
                     double ev[3] = {cx - d[0], cy - d[1], cz - d[2]};
                     double dw = 0, en = 0;
@@ -400,8 +437,9 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, int
 }
 
 // communicate_a_layer on one rank (fluid_3d_comm.cc:203-280): image-backed
-// ghosts receive the maps of the layer just made at their image.
-__global__ void k_layer_ghost_copy(grid_dev g, const fields_dev *__restrict__ F, int o, int L) {
+// ghosts receive the maps of the layer just made at their image (periodic
+// domains only).
+__global__ void k_layer_ghost_copy(grid_dev g, const fields_dev *__restrict__ F, int L) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
     int k = ind / g.smn4, j = (ind % g.smn4) / g.sm4, i = ind % g.sm4;
@@ -412,13 +450,15 @@ __global__ void k_layer_ghost_copy(grid_dev g, const fields_dev *__restrict__ F,
         if (c[d] < 2) c[d] += s[d];
         else if (c[d] >= 2 + s[d]) c[d] -= s[d];
     }
-    const objmap_dev &m = F->om[o];
-    int src = gidx(g, c[0], c[1], c[2]);
-    if (m.code[src] != L) return;
-    m.code[ind] = L;
-    for (int a = 0; a < 3; a++) {
-        m.x[a][ind] = m.xp[a][src];
-        m.xp[a][ind] = m.xp[a][src];
+    const int src = gidx(g, c[0], c[1], c[2]);
+    for (int o = 0; o < g.n_obj; o++) {
+        const objmap_dev &m = F->om[o];
+        if (m.code[src] != L) continue;
+        m.code[ind] = L;
+        for (int a = 0; a < 3; a++) {
+            m.x[a][ind] = m.xp[a][src];
+            m.xp[a][ind] = m.xp[a][src];
+        }
     }
 }
 

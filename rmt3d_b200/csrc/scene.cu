@@ -123,7 +123,8 @@ struct rmt3d_scene {
     kernel_profiler prof;
     // extrapolation scratch
     uint8_t *lay = nullptr, *inl = nullptr;
-    int *front[2] = {nullptr, nullptr};
+    int *front[2] = {nullptr, nullptr};  // per object: ncell entries each
+    int *fcnt = nullptr;                  // frontier lengths, [2][kMaxObj]
     scene_ctl *ctl = nullptr;    // device control block
     scene_ctl *h_ctl = nullptr;  // pinned mirror
     int *counters = nullptr;     // = ctl->counters
@@ -271,32 +272,44 @@ static void comm_primary(rmt3d_scene *s) {
 // ---------------------------------------------------------------------------
 static void extrapolate(rmt3d_scene *s) {
     const grid_dev &g = s->g;
+    if (g.n_obj == 0) return;
     const int nb = lin_blocks(g.ncell);
     const int per_warp_blocks = 148 * 8;
-    for (int o = 0; o < g.n_obj; o++) {
-        k_lay_init<<<nb, 256, 0, s->st>>>(g, s->dF, o, s->lay, s->inl);
-        cudaMemsetAsync(s->counters, 0, 2 * sizeof(int), s->st);
-        k_lay_push<<<nb, 256, 0, s->st>>>(g, nullptr, nullptr, 1, s->lay, s->inl, 1);
+    // without a periodic axis no ghost cell is the image of an interior
+    // cell, and the two ghost-copy kernels would find nothing to do
+    const bool prd = g.prd[0] || g.prd[1] || g.prd[2];
+    int *cnt[2] = {s->fcnt, s->fcnt + kMaxObj};
+    k_lay_init<<<nb, 256, 0, s->st>>>(g, s->dF, s->lay, s->inl);
+    cudaMemsetAsync(s->fcnt, 0, 2 * kMaxObj * sizeof(int), s->st);
+    k_lay_push<<<nb, 256, 0, s->st>>>(g, nullptr, nullptr, 1, s->lay, s->inl, 1);
+    s->count(2);
+    if (prd) {
         k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, 1);
-        k_lay_compact<<<nb, 256, 0, s->st>>>(g, s->inl, s->front[0], s->counters + 0);
-        s->count(4);
-        int cur = 0;
-        for (int L = 1; L <= s->d.nlayers; L++) {
-            k_extrap_layer<<<per_warp_blocks, 128, 0, s->st>>>(g, s->dF, o, s->front[cur], s->counters + cur, L,
-                                                               s->d.max_extrap_rs, s->d.weight_fac, s->lx, s->ly,
-                                                               s->lz, s->counters + 2);
-            k_layer_ghost_copy<<<nb, 256, 0, s->st>>>(g, s->dF, o, L);
-            s->count(2);
-            if (L < s->d.nlayers) {
-                int nxt = cur ^ 1;
-                cudaMemsetAsync(s->counters + nxt, 0, sizeof(int), s->st);
-                k_lay_push<<<per_warp_blocks, 256, 0, s->st>>>(g, s->front[cur], s->counters + cur, 0, s->lay, s->inl,
-                                                               L + 1);
+        s->count();
+    }
+    k_lay_compact<<<nb, 256, 0, s->st>>>(g, s->inl, s->front[0], cnt[0]);
+    s->count();
+    int cur = 0;
+    for (int L = 1; L <= s->d.nlayers; L++) {
+        k_extrap_layer<<<per_warp_blocks, 128, 0, s->st>>>(g, s->dF, s->front[cur], cnt[cur], L, s->d.max_extrap_rs,
+                                                           s->d.weight_fac, s->lx, s->ly, s->lz, s->counters + 2);
+        s->count();
+        if (prd) {
+            k_layer_ghost_copy<<<nb, 256, 0, s->st>>>(g, s->dF, L);
+            s->count();
+        }
+        if (L < s->d.nlayers) {
+            int nxt = cur ^ 1;
+            cudaMemsetAsync(cnt[nxt], 0, kMaxObj * sizeof(int), s->st);
+            k_lay_push<<<per_warp_blocks, 256, 0, s->st>>>(g, s->front[cur], cnt[cur], 0, s->lay, s->inl, L + 1);
+            s->count();
+            if (prd) {
                 k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, L + 1);
-                k_lay_compact<<<nb, 256, 0, s->st>>>(g, s->inl, s->front[nxt], s->counters + nxt);
-                s->count(3);
-                cur = nxt;
+                s->count();
             }
+            k_lay_compact<<<nb, 256, 0, s->st>>>(g, s->inl, s->front[nxt], cnt[nxt]);
+            s->count();
+            cur = nxt;
         }
     }
 }
@@ -1653,7 +1666,9 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     e |= s->alloc(&s->lx, g.sm4) | s->alloc(&s->ly, g.sn4) | s->alloc(&s->lz, g.so4);
     e |= s->alloc(&s->dF, 1);
     if (d.n_obj > 0) {
-        e |= s->alloc(&s->lay, n) | s->alloc(&s->inl, n) | s->alloc(&s->front[0], n) | s->alloc(&s->front[1], n);
+        const size_t no = (size_t)d.n_obj * n;
+        e |= s->alloc(&s->lay, no) | s->alloc(&s->inl, no) | s->alloc(&s->front[0], no) | s->alloc(&s->front[1], no) |
+             s->alloc(&s->fcnt, 2 * kMaxObj);
     }
     e |= s->alloc(&s->ctl, 1) | s->alloc(&s->d_mean, 1 + kMeanBlocks) | s->alloc(&s->d_red, 4) |
          s->alloc(&s->mean_ticket, 1) | s->alloc(&s->d_diag, kDiagVals * (1 + kMeanBlocks)) |
@@ -2450,7 +2465,7 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     const size_t n = (size_t)(d->sys_size[0] + 4) * (d->sys_size[1] + 4) * (d->sys_size[2] + 4);
     size_t b = n * sizeof(double) * (36 + (d->var_den ? 1 : 0));
     b += (size_t)d->n_obj * n * (2 * sizeof(int) + 51 * sizeof(double));
-    if (d->n_obj > 0) b += n * (2 * sizeof(uint8_t) + 2 * sizeof(int));
+    if (d->n_obj > 0) b += (size_t)d->n_obj * n * (2 * sizeof(uint8_t) + 2 * sizeof(int)) + 2 * kMaxObj * sizeof(int);
     b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);
     b += sizeof(fields_dev) + sizeof(scene_ctl) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);
     b += kDiagVals * (1 + kMeanBlocks) * sizeof(double) + sizeof(unsigned);

@@ -27,8 +27,9 @@ def test_objects_precision_and_size_order(tmp_path):
     base = _desc(tmp_path, scenes.cavity(64), "c64.cfg")
     sph = _desc(tmp_path, scenes.cavity_sphere(64), "s64.cfg")
     n = 68 ** 3
-    # one object: 51 doubles + 2 ints of map state, plus frontier scratch
-    assert R.footprint(sph) - R.footprint(base) == n * (51 * 8 + 8) + n * 10
+    # one object: 51 doubles + 2 ints of map state, frontier scratch of
+    # 10 bytes per cell and object, and the frontier lengths
+    assert R.footprint(sph) - R.footprint(base) == n * (51 * 8 + 8) + n * 10 + 2 * 16 * 4
     mixed = _desc(tmp_path, scenes.cavity_sphere(64), "m64.cfg")
     mixed.precision = R.MIXED
     assert R.footprint(mixed) > R.footprint(sph)
