@@ -115,9 +115,11 @@ typedef struct {
                           residual is below mixed_rtol times the max-norm of
                           its right-hand side, and skips the two insurance
                           cycles (the form's accuracy target is 1e-5 rel-L2);
-                          0 keeps the reference's control.  Default 1e-7
-                          (64^3 cavity + sphere, 100 steps: velocity 2e-8
-                          and pressure 4e-8 rel-L2 from the FP64 form). */
+                          0 keeps the reference's control.  Default 1e-5
+                          (64^3 cavity + sphere, 100 steps: velocity 3e-8
+                          and pressure 6e-8 rel-L2 from the FP64 form, the
+                          same as at 1e-7 with 2.8 + 2.3 V-cycles per step
+                          instead of 4.9 + 3.3). */
     rmt3d_run_desc run;
 } rmt3d_scene_desc;
 

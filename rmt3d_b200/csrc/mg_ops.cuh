@@ -19,6 +19,13 @@ __host__ __device__ __forceinline__ int wrapi(int v, int n, int prd) {
     return v;
 }
 
+// v / num for num in {1, 2, 4, 8} as an exact power-of-two scaling (the same
+// bits as the division, without its instruction sequence)
+template <typename T>
+__device__ __forceinline__ T div_pow2(T v, int num) {
+    return num == 1 ? v : num == 2 ? v * (T)0.5 : num == 4 ? v * (T)0.25 : num == 8 ? v * (T)0.125 : v / (T)num;
+}
+
 // ---- operator application -------------------------------------------------
 template <typename T>
 __device__ __forceinline__ T mac_offdiag(const lvl_dev L, const T *__restrict__ x, int i, int j, int k, T &diag) {
@@ -214,38 +221,43 @@ __device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict
         diag = (T)32 * (c8 / (T)8);
         return s;
     }
+    // boundary or wrapped node; every loop below unrolls to constant indices
     const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
     const int nc[3] = {p[0] ? n[0] : n[0] - 1, p[1] ? n[1] : n[1] - 1, p[2] ? n[2] : n[2] - 1};
     const int c[3] = {i, j, k};
     int cell[3][2];  // cells below / above the node on each axis (-1: none)
     bool bd[3];
     int nb[3][3];
+#pragma unroll
     for (int d = 0; d < 3; d++) {
         bd[d] = !p[d] && (c[d] == 0 || c[d] == n[d] - 1);
         cell[d][0] = (c[d] - 1 >= 0) ? c[d] - 1 : (p[d] ? c[d] - 1 + nc[d] : -1);
         cell[d][1] = (c[d] < nc[d]) ? c[d] : (p[d] ? c[d] - nc[d] : -1);
+#pragma unroll
         for (int o = -1; o <= 1; o++) nb[d][o + 1] = wrapi(c[d] + o, n[d], p[d]);
     }
     // the up to 8 adjacent cells' 1/rho, [cz][cy][cx]
     T v[2][2][2];
+#pragma unroll
     for (int a = 0; a < 2; a++)
+#pragma unroll
         for (int b = 0; b < 2; b++)
+#pragma unroll
             for (int e = 0; e < 2; e++) {
                 const bool ok = cell[0][e] >= 0 && cell[1][b] >= 0 && cell[2][a] >= 0;
                 v[a][b][e] = ok ? ri[cell[0][e] + nc[0] * (cell[1][b] + nc[1] * cell[2][a])] : (T)0;
             }
     T s = 0;
+#pragma unroll
     for (int oc = 0; oc < 3; oc++) {
-        const int kk = nb[2][oc];
-        if (kk < 0) continue;
+#pragma unroll
         for (int ob = 0; ob < 3; ob++) {
-            const int jj = nb[1][ob];
-            if (jj < 0) continue;
+#pragma unroll
             for (int oa = 0; oa < 3; oa++) {
-                const int ii = nb[0][oa];
-                if (ii < 0) continue;
                 const int nz = (oa != 1) + (ob != 1) + (oc != 1);
                 if (nz <= 1) continue;  // centre handled below, faces are 0
+                const int kk = nb[2][oc], jj = nb[1][ob], ii = nb[0][oa];
+                if (kk < 0 || jj < 0 || ii < 0) continue;
                 T co = (nz == 2) ? (T)-2 : (T)-1;
                 const int halve = (bd[0] && oa == 1) + (bd[1] && ob == 1) + (bd[2] && oc == 1);
                 if (halve == 1) co *= (T)0.5;
@@ -253,32 +265,34 @@ __device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict
                 // cells shared by the node and this neighbour, in (z, y, x) order
                 T sum = 0;
                 int num = 0;
-                for (int a = (oc == 2 ? 1 : 0); a <= (oc == 0 ? 0 : 1); a++) {
-                    if (cell[2][a] < 0) continue;
-                    for (int b = (ob == 2 ? 1 : 0); b <= (ob == 0 ? 0 : 1); b++) {
-                        if (cell[1][b] < 0) continue;
-                        for (int e = (oa == 2 ? 1 : 0); e <= (oa == 0 ? 0 : 1); e++) {
-                            if (cell[0][e] < 0) continue;
-                            sum += v[a][b][e];
-                            num++;
-                        }
-                    }
-                }
-                s += co * (sum / (T)num) * x[ii + L.n0 * (jj + L.n1 * kk)];
+#pragma unroll
+                for (int a = (oc == 2 ? 1 : 0); a <= (oc == 0 ? 0 : 1); a++)
+#pragma unroll
+                    for (int b = (ob == 2 ? 1 : 0); b <= (ob == 0 ? 0 : 1); b++)
+#pragma unroll
+                        for (int e = (oa == 2 ? 1 : 0); e <= (oa == 0 ? 0 : 1); e++)
+                            if (cell[2][a] >= 0 && cell[1][b] >= 0 && cell[0][e] >= 0) {
+                                sum += v[a][b][e];
+                                num++;
+                            }
+                s += co * div_pow2(sum, num) * x[ii + L.n0 * (jj + L.n1 * kk)];
             }
         }
     }
     T sum = 0;
     int num = 0;
+#pragma unroll
     for (int a = 0; a < 2; a++)
+#pragma unroll
         for (int b = 0; b < 2; b++)
+#pragma unroll
             for (int e = 0; e < 2; e++)
                 if (cell[2][a] >= 0 && cell[1][b] >= 0 && cell[0][e] >= 0) {
                     sum += v[a][b][e];
                     num++;
                 }
     const int hc = bd[0] + bd[1] + bd[2];
-    diag = ((T)32 / (T)(1 << hc)) * (sum / (T)num);
+    diag = ((T)32 / (T)(1 << hc)) * div_pow2(sum, num);
     return s;
 }
 
