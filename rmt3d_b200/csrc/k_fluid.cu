@@ -356,7 +356,9 @@ __device__ void face_stress(const grid_dev &g, const fields_dev *__restrict__ F,
 
 // Cells that hold any reference map: the full stress (solid, fluid blend,
 // collision).  Cells without maps are left to k_stress_fluid.
-__global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F) {
+// Cells that hold any reference map, listed for the full stress kernel (the
+// box range of the stress faces: absolute indices 1..s+3 on every axis).
+__global__ void k_map_cells(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
@@ -364,10 +366,26 @@ __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F) {
     const int ind = gidx(g, i, j, k);
     bool any = false;
     for (int o = 0; o < g.n_obj; o++) any = any || F->om[o].code[ind] >= 0;
-    if (!any) return;
-    face_stress<0>(g, F, i, j, k, ind, true);
-    face_stress<1>(g, F, i, j, k, ind, true);
-    face_stress<2>(g, F, i, j, k, ind, true);
+    if (any) list[atomicAdd(cnt, 1)] = ind;
+}
+
+// The full stress of the listed cells, one thread per (cell, face): work
+// item t is face t / n of cell list[t % n].  The three faces of a cell write
+// disjoint outputs and read only what no face writes, so they run in any
+// order; a thread holds one face's state instead of three, and every lane of
+// a warp has a map cell to work on.
+__global__ void __launch_bounds__(128) k_stress(grid_dev g, const fields_dev *__restrict__ F, const int *list,
+                                                const int *cnt) {
+    const int n = *cnt;
+    const long total = 3L * n;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const int FF = (int)(t / n), e = (int)(t - (long)FF * n);
+        const int ind = list[e];
+        const int i = ind % g.sm4, j = (ind / g.sm4) % g.sn4, k = ind / g.smn4;
+        if (FF == 0) face_stress<0>(g, F, i, j, k, ind, true);
+        else if (FF == 1) face_stress<1>(g, F, i, j, k, ind, true);
+        else face_stress<2>(g, F, i, j, k, ind, true);
+    }
 }
 
 // Cells without reference maps (most of the box): the pure fluid stress of

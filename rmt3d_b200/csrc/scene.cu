@@ -125,6 +125,7 @@ struct rmt3d_scene {
     uint8_t *lay = nullptr, *inl = nullptr;
     int *front[2] = {nullptr, nullptr};  // per object: ncell entries each
     int *fcnt = nullptr;                  // frontier lengths, [2][kMaxObj]
+    int *mlist = nullptr, *mcnt = nullptr;  // cells holding a map, for the stress kernel
     scene_ctl *ctl = nullptr;    // device control block
     scene_ctl *h_ctl = nullptr;  // pinned mirror
     int *counters = nullptr;     // = ctl->counters
@@ -706,8 +707,10 @@ static void compute_stress(rmt3d_scene *s) {
     k_stress_fluid<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF);
     s->count();
     if (g.n_obj > 0) {
-        k_stress<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF);
-        s->count();
+        cudaMemsetAsync(s->mcnt, 0, sizeof(int), s->st);
+        k_map_cells<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF, s->mlist, s->mcnt);
+        k_stress<<<148 * 8, 128, 0, s->st>>>(g, s->dF, s->mlist, s->mcnt);
+        s->count(2);
     }
 }
 
@@ -1668,7 +1671,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     if (d.n_obj > 0) {
         const size_t no = (size_t)d.n_obj * n;
         e |= s->alloc(&s->lay, no) | s->alloc(&s->inl, no) | s->alloc(&s->front[0], no) | s->alloc(&s->front[1], no) |
-             s->alloc(&s->fcnt, 2 * kMaxObj);
+             s->alloc(&s->fcnt, 2 * kMaxObj) | s->alloc(&s->mlist, n) | s->alloc(&s->mcnt, 1);
     }
     e |= s->alloc(&s->ctl, 1) | s->alloc(&s->d_mean, 1 + kMeanBlocks) | s->alloc(&s->d_red, 4) |
          s->alloc(&s->mean_ticket, 1) | s->alloc(&s->d_diag, kDiagVals * (1 + kMeanBlocks)) |
@@ -2465,7 +2468,9 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     const size_t n = (size_t)(d->sys_size[0] + 4) * (d->sys_size[1] + 4) * (d->sys_size[2] + 4);
     size_t b = n * sizeof(double) * (36 + (d->var_den ? 1 : 0));
     b += (size_t)d->n_obj * n * (2 * sizeof(int) + 51 * sizeof(double));
-    if (d->n_obj > 0) b += (size_t)d->n_obj * n * (2 * sizeof(uint8_t) + 2 * sizeof(int)) + 2 * kMaxObj * sizeof(int);
+    if (d->n_obj > 0)
+        b += (size_t)d->n_obj * n * (2 * sizeof(uint8_t) + 2 * sizeof(int)) + 2 * kMaxObj * sizeof(int) +
+             n * sizeof(int) + sizeof(int);
     b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);
     b += sizeof(fields_dev) + sizeof(scene_ctl) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);
     b += kDiagVals * (1 + kMeanBlocks) * sizeof(double) + sizeof(unsigned);
