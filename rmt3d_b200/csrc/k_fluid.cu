@@ -45,16 +45,22 @@ __global__ void k_periodic_copy(grid_dev g, ptr_list pl, int corner) {
 // Physical BC ghost fill of one face, face_gm::set_ghost_cc
 // (fields.hh:765-800): both ghost layers, the whole tangential extent.
 // -------------------------------------------------------------------------
-__global__ void k_bc_cc(grid_dev g, int face, bc_face bc, double *u, double *v, double *w) {
-    const int n = face / 2;
-    const int lower = (face % 2 == 0);
+__global__ void k_bc_cc(grid_dev g, int n, bc_face lo, bc_face hi, double *u, double *v, double *w) {
+    // both faces of axis n in one launch: blockIdx.z = 2 * side + layer - 1.
+    // The two faces write disjoint ghost layers and read only cells of their
+    // own side, so they run together; the axes still run in order, x, y, z,
+    // since a later axis reads the earlier axes' ghost values at edges.
+    const int lower = (blockIdx.z < 2);
+    const int face = 2 * n + (lower ? 0 : 1);
+    const bc_face &bc = lower ? lo : hi;
     const int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
     const int ext[3] = {g.sm4, g.sn4, g.so4};
     const int len[3] = {g.sm, g.sn, g.so};
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     int b = blockIdx.y * blockDim.y + threadIdx.y;
-    int layer = blockIdx.z + 1;  // 1 or 2
+    int layer = (blockIdx.z & 1) + 1;  // 1 or 2
     if (a >= ext[t0] || b >= ext[t1]) return;
+    (void)face;
     int gc[3], mc[3];
     gc[t0] = mc[t0] = a;
     gc[t1] = mc[t1] = b;
@@ -81,7 +87,13 @@ __global__ void k_bc_cc(grid_dev g, int face, bc_face bc, double *u, double *v, 
 // (fields.hh:804-849): the boundary face of the outermost interior layer and
 // the matching face of the inner ghost layer.
 // -------------------------------------------------------------------------
-__global__ void k_bc_cf(grid_dev g, int face, bc_face bc, const fields_dev *F) {
+// All wall faces in one launch (blockIdx.z = face; bit f of walls marks a
+// wall): each face reads velocities only and writes its own face-velocity
+// components, so the faces are independent.
+__global__ void k_bc_cf(grid_dev g, int walls, bc_faces bcs, const fields_dev *F) {
+    const int face = blockIdx.z;
+    if (!((walls >> face) & 1)) return;
+    const bc_face &bc = bcs.f[face];
     const int n = face / 2;
     const int lower = (face % 2 == 0);
     const int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;

@@ -244,10 +244,131 @@ __device__ inline double warp_sum(double v) {
 // (extrap_helper.cc:34-103) with lin_sys (:129-146), mat3::inverse
 // (Utilities/mat3.hh:61-67) and transfer (fluid_3d_ex.cc:293-328).
 // -------------------------------------------------------------------------
+constexpr int kPowTab = 64;
+
+// One radius R of the least-squares fit for the frontier cell (ii, jj, kk)
+// of map m: false when no candidate is eligible or the normal matrix is
+// singular (the caller then widens R).  W = 2R + 1 as a compile-time
+// constant for the common radii, 0 for the general case.
+template <int W>
+__device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, int lane, int ii, int jj, int kk,
+                          int ind, bool directional, const double (&gph)[3], double cx, double cy, double cz,
+                          const double *lx, const double *ly, const double *lz, const double *wpow, double wt,
+                          double (&val)[3]) {
+    const int w = W ? W : 2 * R + 1, nc = w * w * w;
+    auto wpw = [&](int e) { return e < kPowTab ? wpow[e] : pow(wt, (double)e); };
+    // pass 1: weights and weighted sums of positions and values
+    double sw = 0, sd[3] = {0, 0, 0}, sr[3] = {0, 0, 0};
+    int cnt = 0;
+    for (int s = lane; s < nc; s += 32) {
+        int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
+        if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
+        if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
+        if (kk + r > g.so4 - 1 || kk + r < 0) continue;
+        int qi = ind + p + g.sm4 * q + g.smn4 * r;
+        int cd = m.code[qi];
+        if (cd < 0 || cd >= L) continue;
+        double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
+        double wgt = wpw(abs(p) + abs(q) + abs(r));
+        if (directional) {
+            double ev[3] = {cx - d[0], cy - d[1], cz - d[2]};
+            double dw = 0, en = 0;
+            for (int pp = 0; pp < 3; pp++) {
+                dw += ev[pp] * gph[pp];
+                en += ev[pp] * ev[pp];
+            }
+            en = sqrt(en);
+            dw /= en;
+            dw *= wgt;
+            if (!(dw > 0)) continue;
+            wgt = dw;
+        }
+        sw += wgt;
+        cnt++;
+        for (int c = 0; c < 3; c++) {
+            sd[c] += d[c] * wgt;
+            sr[c] += m.xp[c][qi] * wgt;
+        }
+    }
+    sw = warp_sum(sw);
+    for (int c = 0; c < 3; c++) {
+        sd[c] = warp_sum(sd[c]);
+        sr[c] = warp_sum(sr[c]);
+    }
+    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    if (cnt == 0) return false;
+    double davg[3], ravg[3];
+    for (int c = 0; c < 3; c++) {
+        ravg[c] = sr[c] / sw;
+        davg[c] = sd[c] / sw;
+    }
+    // pass 2: weighted normal equations about the averages
+    double a[6] = {0, 0, 0, 0, 0, 0}, rhs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int s = lane; s < nc; s += 32) {
+        int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
+        if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
+        if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
+        if (kk + r > g.so4 - 1 || kk + r < 0) continue;
+        int qi = ind + p + g.sm4 * q + g.smn4 * r;
+        int cd = m.code[qi];
+        if (cd < 0 || cd >= L) continue;
+        double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
+        double Q = wpw(abs(p) + abs(q) + abs(r));
+        if (directional) {
+            double ev[3] = {cx - d[0], cy - d[1], cz - d[2]};
+            double dw = 0, en = 0;
+            for (int pp = 0; pp < 3; pp++) {
+                dw += ev[pp] * gph[pp];
+                en += ev[pp] * ev[pp];
+            }
+            en = sqrt(en);
+            dw /= en;
+            dw *= Q;
+            if (!(dw > 0)) continue;
+            Q = dw;
+        }
+        double e0 = d[0] - davg[0], e1 = d[1] - davg[1], e2 = d[2] - davg[2];
+        a[0] += Q * e0 * e0;
+        a[1] += Q * e1 * e1;
+        a[2] += Q * e2 * e2;
+        a[3] += Q * e0 * e1;
+        a[4] += Q * e0 * e2;
+        a[5] += Q * e1 * e2;
+        for (int c = 0; c < 3; c++) {
+            double lr = Q * (m.xp[c][qi] - ravg[c]);
+            rhs[3 * c + 0] += e0 * lr;
+            rhs[3 * c + 1] += e1 * lr;
+            rhs[3 * c + 2] += e2 * lr;
+        }
+    }
+    for (int c = 0; c < 6; c++) a[c] = warp_sum(a[c]);
+    for (int c = 0; c < 9; c++) rhs[c] = warp_sum(rhs[c]);
+    // mat3 A(XX, XY, XZ, XY, YY, YZ, XZ, YZ, ZZ) and its inverse
+    const double a11 = a[0], a12 = a[3], a13 = a[4], a21 = a[3], a22 = a[1], a23 = a[5], a31 = a[4],
+                 a32 = a[5], a33 = a[2];
+    double det = a11 * (a22 * a33 - a23 * a32) + a21 * (a13 * a32 - a12 * a33) + a31 * (a12 * a23 - a13 * a22);
+    if (fabs(det) < 1e-17) return false;
+    double id = 1 / det;
+    double inv[9] = {(a22 * a33 - a23 * a32) * id, (a13 * a32 - a12 * a33) * id, (a12 * a23 - a13 * a22) * id,
+                     (a23 * a31 - a21 * a33) * id, (a11 * a33 - a13 * a31) * id, (a13 * a21 - a11 * a23) * id,
+                     (a21 * a32 - a22 * a31) * id, (a12 * a31 - a11 * a32) * id, (a11 * a22 - a12 * a21) * id};
+    double ps[3] = {cx - davg[0], cy - davg[1], cz - davg[2]};
+    for (int c = 0; c < 3; c++) {
+        double co0 = inv[0] * rhs[3 * c] + inv[1] * rhs[3 * c + 1] + inv[2] * rhs[3 * c + 2];
+        double co1 = inv[3] * rhs[3 * c] + inv[4] * rhs[3 * c + 1] + inv[5] * rhs[3 * c + 2];
+        double co2 = inv[6] * rhs[3 * c] + inv[7] * rhs[3 * c + 1] + inv[8] * rhs[3 * c + 2];
+        double v = ravg[c];
+        v += co0 * ps[0];
+        v += co1 * ps[1];
+        v += co2 * ps[2];
+        val[c] = v;
+    }
+    return true;
+}
+
 // Every object's frontier in one launch: warp w takes entry w of the
 // concatenated frontiers.  The weights wt^n (n = |p|+|q|+|r|) come from a
 // per-block table of the same pow() values.
-constexpr int kPowTab = 64;
 __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, const int *front, const int *cnt, int L,
                                int max_rs, double wt, const double *lx, const double *ly, const double *lz,
                                int *err) {
@@ -255,7 +376,6 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
     const int npow = 3 * max_rs + 1;
     for (int q = threadIdx.x; q < kPowTab && q < npow; q += blockDim.x) wpow[q] = pow(wt, (double)q);
     __syncthreads();
-    auto wpw = [&](int e) { return e < kPowTab ? wpow[e] : pow(wt, (double)e); };
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -313,114 +433,13 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
         bool success = false;
         double val[3] = {0, 0, 0};
         for (int R = 2; R <= max_rs && !success; R++) {
-            const int w = 2 * R + 1, nc = w * w * w;
-            // pass 1: weights and weighted sums of positions and values
-            double sw = 0, sd[3] = {0, 0, 0}, sr[3] = {0, 0, 0};
-            int cnt = 0;
-            for (int s = lane; s < nc; s += 32) {
-                int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
-                if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
-                if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
-                if (kk + r > g.so4 - 1 || kk + r < 0) continue;
-                int qi = ind + p + g.sm4 * q + g.smn4 * r;
-                int cd = m.code[qi];
-                if (cd < 0 || cd >= L) continue;
-                double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
-                double wgt = wpw(abs(p) + abs(q) + abs(r));
-                if (directional) {
-                    double ev[3] = {cx - d[0], cy - d[1], cz - d[2]};
-                    double dw = 0, en = 0;
-                    for (int pp = 0; pp < 3; pp++) {
-                        dw += ev[pp] * gph[pp];
-                        en += ev[pp] * ev[pp];
-                    }
-                    en = sqrt(en);
-                    dw /= en;
-                    dw *= wgt;
-                    if (!(dw > 0)) continue;
-                    wgt = dw;
-                }
-                sw += wgt;
-                cnt++;
-                for (int c = 0; c < 3; c++) {
-                    sd[c] += d[c] * wgt;
-                    sr[c] += m.xp[c][qi] * wgt;
-                }
+            switch (R) {
+                case 2: success = ls_radius<5>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                case 3: success = ls_radius<7>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                case 4: success = ls_radius<9>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                case 5: success = ls_radius<11>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                default: success = ls_radius<0>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
             }
-            sw = warp_sum(sw);
-            for (int c = 0; c < 3; c++) {
-                sd[c] = warp_sum(sd[c]);
-                sr[c] = warp_sum(sr[c]);
-            }
-            for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-            if (cnt == 0) continue;
-            double davg[3], ravg[3];
-            for (int c = 0; c < 3; c++) {
-                ravg[c] = sr[c] / sw;
-                davg[c] = sd[c] / sw;
-            }
-            // pass 2: weighted normal equations about the averages
-            double a[6] = {0, 0, 0, 0, 0, 0}, rhs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-            for (int s = lane; s < nc; s += 32) {
-                int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
-                if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
-                if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
-                if (kk + r > g.so4 - 1 || kk + r < 0) continue;
-                int qi = ind + p + g.sm4 * q + g.smn4 * r;
-                int cd = m.code[qi];
-                if (cd < 0 || cd >= L) continue;
-                double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
-                double Q = wpw(abs(p) + abs(q) + abs(r));
-                if (directional) {
-                    double ev[3] = {cx - d[0], cy - d[1], cz - d[2]};
-                    double dw = 0, en = 0;
-                    for (int pp = 0; pp < 3; pp++) {
-                        dw += ev[pp] * gph[pp];
-                        en += ev[pp] * ev[pp];
-                    }
-                    en = sqrt(en);
-                    dw /= en;
-                    dw *= Q;
-                    if (!(dw > 0)) continue;
-                    Q = dw;
-                }
-                double e0 = d[0] - davg[0], e1 = d[1] - davg[1], e2 = d[2] - davg[2];
-                a[0] += Q * e0 * e0;
-                a[1] += Q * e1 * e1;
-                a[2] += Q * e2 * e2;
-                a[3] += Q * e0 * e1;
-                a[4] += Q * e0 * e2;
-                a[5] += Q * e1 * e2;
-                for (int c = 0; c < 3; c++) {
-                    double lr = Q * (m.xp[c][qi] - ravg[c]);
-                    rhs[3 * c + 0] += e0 * lr;
-                    rhs[3 * c + 1] += e1 * lr;
-                    rhs[3 * c + 2] += e2 * lr;
-                }
-            }
-            for (int c = 0; c < 6; c++) a[c] = warp_sum(a[c]);
-            for (int c = 0; c < 9; c++) rhs[c] = warp_sum(rhs[c]);
-            // mat3 A(XX, XY, XZ, XY, YY, YZ, XZ, YZ, ZZ) and its inverse
-            const double a11 = a[0], a12 = a[3], a13 = a[4], a21 = a[3], a22 = a[1], a23 = a[5], a31 = a[4],
-                         a32 = a[5], a33 = a[2];
-            double det = a11 * (a22 * a33 - a23 * a32) + a21 * (a13 * a32 - a12 * a33) + a31 * (a12 * a23 - a13 * a22);
-            if (fabs(det) < 1e-17) continue;
-            double id = 1 / det;
-            double inv[9] = {(a22 * a33 - a23 * a32) * id, (a13 * a32 - a12 * a33) * id, (a12 * a23 - a13 * a22) * id,
-                             (a23 * a31 - a21 * a33) * id, (a11 * a33 - a13 * a31) * id, (a13 * a21 - a11 * a23) * id,
-                             (a21 * a32 - a22 * a31) * id, (a12 * a31 - a11 * a32) * id, (a11 * a22 - a12 * a21) * id};
-            double ps[3] = {cx - davg[0], cy - davg[1], cz - davg[2]};
-            for (int c = 0; c < 3; c++) {
-                double co0 = inv[0] * rhs[3 * c] + inv[1] * rhs[3 * c + 1] + inv[2] * rhs[3 * c + 2];
-                double co1 = inv[3] * rhs[3 * c] + inv[4] * rhs[3 * c + 1] + inv[5] * rhs[3 * c + 2];
-                double co2 = inv[6] * rhs[3 * c] + inv[7] * rhs[3 * c + 1] + inv[8] * rhs[3 * c + 2];
-                double v = ravg[c];
-                v += co0 * ps[0];
-                v += co1 * ps[1];
-                v += co2 * ps[2];
-                val[c] = v;
-            }
-            success = true;
         }
         if (!success) {
             if (lane == 0) atomicAdd(err, 1);

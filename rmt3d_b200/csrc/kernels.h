@@ -18,6 +18,9 @@ struct bc_face {
     double bcv[3];
     double h;
 };
+struct bc_faces {
+    bc_face f[6];
+};
 
 // FEM element-integrated basis gradients (fluid_3d.cc:2506-2517)
 struct gradphi_t {
@@ -25,8 +28,8 @@ struct gradphi_t {
 };
 
 __global__ void k_periodic_copy(grid_dev g, ptr_list pl, int corner);
-__global__ void k_bc_cc(grid_dev g, int face, bc_face bc, double *u, double *v, double *w);
-__global__ void k_bc_cf(grid_dev g, int face, bc_face bc, const fields_dev *F);
+__global__ void k_bc_cc(grid_dev g, int n, bc_face lo, bc_face hi, double *u, double *v, double *w);
+__global__ void k_bc_cf(grid_dev g, int walls, bc_faces bcs, const fields_dev *F);
 __global__ void k_map_cells(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt);
 __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F, const int *list, const int *cnt);
 __global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F);

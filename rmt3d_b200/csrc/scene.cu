@@ -198,13 +198,13 @@ static void periodic(rmt3d_scene *s, std::initializer_list<double *> arrs, std::
 // fill_boundary_cc: set_bc_cc then communicate<1> (fluid_3d.cc:145-152)
 static void fill_boundary_cc(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    for (int f = 0; f < 6; f++) {
-        if (!s->wall[f]) continue;
-        int n = f / 2;
-        int ext[3] = {g.sm4, g.sn4, g.so4};
+    const int ext[3] = {g.sm4, g.sn4, g.so4};
+    for (int n = 0; n < 3; n++) {  // walls come in pairs: both faces of an axis at once
+        if (!s->wall[2 * n]) continue;
         int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
-        dim3 gr((ext[t0] + 31) / 32, (ext[t1] + 7) / 8, 2);
-        k_bc_cc<<<gr, dim3(32, 8, 1), 0, s->st>>>(g, f, s->faces[f], s->hF.vel[0], s->hF.vel[1], s->hF.vel[2]);
+        dim3 gr((ext[t0] + 31) / 32, (ext[t1] + 7) / 8, 4);
+        k_bc_cc<<<gr, dim3(32, 8, 1), 0, s->st>>>(g, n, s->faces[2 * n], s->faces[2 * n + 1], s->hF.vel[0],
+                                                  s->hF.vel[1], s->hF.vel[2]);
         s->count();
     }
     periodic(s, {s->hF.vel[0], s->hF.vel[1], s->hF.vel[2]}, {}, 0);
@@ -213,13 +213,16 @@ static void fill_boundary_cc(rmt3d_scene *s) {
 // fill_boundary_cf: set_bc_cf then communicate<4> (fluid_3d.cc:155-165)
 static void fill_boundary_cf(rmt3d_scene *s) {
     const grid_dev &g = s->g;
+    int walls = 0;
+    bc_faces bcs;
     for (int f = 0; f < 6; f++) {
-        if (!s->wall[f]) continue;
-        int n = f / 2;
-        int ext[3] = {g.sm4, g.sn4, g.so4};
-        int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
-        dim3 gr((ext[t0] + 31) / 32, (ext[t1] + 7) / 8, 1);
-        k_bc_cf<<<gr, dim3(32, 8, 1), 0, s->st>>>(g, f, s->faces[f], s->dF);
+        bcs.f[f] = s->faces[f];
+        if (s->wall[f]) walls |= 1 << f;
+    }
+    if (walls) {
+        const int mx = std::max(g.sm4, std::max(g.sn4, g.so4));
+        dim3 gr((mx + 31) / 32, (mx + 7) / 8, 6);
+        k_bc_cf<<<gr, dim3(32, 8, 1), 0, s->st>>>(g, walls, bcs, s->dF);
         s->count();
     }
     if (g.prd[0] || g.prd[1] || g.prd[2]) {
