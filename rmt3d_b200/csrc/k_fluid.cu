@@ -55,30 +55,27 @@ __global__ void k_bc_cc(grid_dev g, int n, bc_face lo, bc_face hi, double *u, do
     const bc_face &bc = lower ? lo : hi;
     const int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
     const int ext[3] = {g.sm4, g.sn4, g.so4};
-    const int len[3] = {g.sm, g.sn, g.so};
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     int b = blockIdx.y * blockDim.y + threadIdx.y;
     int layer = (blockIdx.z & 1) + 1;  // 1 or 2
     if (a >= ext[t0] || b >= ext[t1]) return;
     (void)face;
-    int gc[3], mc[3];
-    gc[t0] = mc[t0] = a;
-    gc[t1] = mc[t1] = b;
-    if (lower) {
-        gc[n] = 2 - layer;
-        mc[n] = 2 + layer - 1;
-    } else {
-        gc[n] = 2 + len[n] - 1 + layer;
-        mc[n] = 2 + len[n] - layer;
-    }
-    const int gi = gidx(g, gc[0], gc[1], gc[2]);
-    const int mi = gidx(g, mc[0], mc[1], mc[2]);
+    // flat indices from the strides of the three axes (no runtime-indexed
+    // arrays, which would live in local memory)
+    const int sa = t0 == 0 ? 1 : g.sm4, sb = t1 == 1 ? g.sm4 : g.smn4;
+    const int sn_ = n == 0 ? 1 : (n == 1 ? g.sm4 : g.smn4);
+    const int ln = n == 0 ? g.sm : (n == 1 ? g.sn : g.so);
+    const int gn = lower ? 2 - layer : 2 + ln - 1 + layer;
+    const int mn = lower ? 2 + layer - 1 : 2 + ln - layer;
+    const int gi = a * sa + b * sb + gn * sn_;
+    const int mi = a * sa + b * sb + mn * sn_;
     const double sgn = lower ? -1 : 1;
     const double dn = 2 * fabs(0.5 * bc.h * (2 * layer - 1));
-    double *vel[3] = {u, v, w};
+#pragma unroll
     for (int c = 0; c < 3; c++) {
-        if (bc.bct[c] == 1) vel[c][gi] = 2 * bc.bcv[c] - vel[c][mi];
-        else vel[c][gi] = sgn * dn * bc.bcv[c] + vel[c][mi];
+        double *vc = c == 0 ? u : (c == 1 ? v : w);
+        if (bc.bct[c] == 1) vc[gi] = 2 * bc.bcv[c] - vc[mi];
+        else vc[gi] = sgn * dn * bc.bcv[c] + vc[mi];
     }
 }
 
@@ -98,25 +95,16 @@ __global__ void k_bc_cf(grid_dev g, int walls, bc_faces bcs, const fields_dev *F
     const int lower = (face % 2 == 0);
     const int t0 = (n == 0) ? 1 : 0, t1 = (n == 2) ? 1 : 2;
     const int ext[3] = {g.sm4, g.sn4, g.so4};
-    const int len[3] = {g.sm, g.sn, g.so};
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     int b = blockIdx.y * blockDim.y + threadIdx.y;
     if (a >= ext[t0] || b >= ext[t1]) return;
-    int gc[3], y0[3], y1[3];
-    gc[t0] = y0[t0] = y1[t0] = a;
-    gc[t1] = y0[t1] = y1[t1] = b;
-    if (lower) {
-        gc[n] = 1;
-        y0[n] = 2;
-        y1[n] = 3;
-    } else {
-        gc[n] = 2 + len[n];
-        y0[n] = 1 + len[n];
-        y1[n] = len[n];
-    }
-    const int gi = gidx(g, gc[0], gc[1], gc[2]);
-    const int i0 = gidx(g, y0[0], y0[1], y0[2]);
-    const int i1 = gidx(g, y1[0], y1[1], y1[2]);
+    const int sa = t0 == 0 ? 1 : g.sm4, sb = t1 == 1 ? g.sm4 : g.smn4;
+    const int sn_ = n == 0 ? 1 : (n == 1 ? g.sm4 : g.smn4);
+    const int ln = n == 0 ? g.sm : (n == 1 ? g.sn : g.so);
+    const int base = a * sa + b * sb;
+    const int gi = base + (lower ? 1 : 2 + ln) * sn_;
+    const int i0 = base + (lower ? 2 : 1 + ln) * sn_;
+    const int i1 = base + (lower ? 3 : ln) * sn_;
     const double sgn = lower ? -1 : 1;
     const int inner = 2 * n + (lower ? 1 : 0);
     for (int c = 0; c < 3; c++) {
@@ -560,7 +548,7 @@ __device__ void acceleration(const grid_dev &g, const fields_dev *__restrict__ F
 // compute_half_time_edge_velocities (:1038-1066) and field::godunov_extrap
 // (fields.hh:147-177, non-TANG branch).  Interior cells.
 // -------------------------------------------------------------------------
-__global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+__global__ void __launch_bounds__(256, 3) k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
                            const double *lz, double cdt, const double *time_p, int var_den) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
@@ -739,7 +727,7 @@ __global__ void k_sub_qgrad(grid_dev g, const fields_dev *__restrict__ F, double
 // -------------------------------------------------------------------------
 // Explicit momentum update, fluid_3d::compute_ustar (fluid_3d.cc:1309-1352).
 // -------------------------------------------------------------------------
-__global__ void k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
+__global__ void __launch_bounds__(256, 3) k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
                         const double *lz, double cdt, const double *time_p, int var_den) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 2;

@@ -16,7 +16,7 @@ __device__ inline double mphi(const grid_dev &g, const objmap_dev &m, int o, int
 // (fields.hh:572-592, non-TANG): for the primary map of every interior cell
 // and for extrapolated maps that abut a primary map orthogonally.
 // -------------------------------------------------------------------------
-__global__ void k_edge_refmap(grid_dev g, const fields_dev *__restrict__ F, double cdt, int *err) {
+__global__ void __launch_bounds__(256, 3) k_edge_refmap(grid_dev g, const fields_dev *__restrict__ F, double cdt, int *err) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
     int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
