@@ -142,7 +142,7 @@ __device__ inline bool inner_ghost(const grid_dev &g, int i, int j, int k) {
 // writes only its own maps), so all of them advance one layer per launch.
 
 // first_layer + mark_primary (fluid_3d_ex.cc:52-70): reset the layer tags
-__global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t *lay, uint8_t *inl) {
+__global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t *lay, int *inl) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
     for (int o = 0; o < g.n_obj; o++) {
@@ -151,18 +151,25 @@ __global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t
     }
 }
 
-// mark the free orthogonal neighbours of cell ind for layer `next`
-__device__ inline void push_from(const grid_dev &g, int ind, uint8_t *lay, uint8_t *inl, int next) {
+// Cell c joins the frontier of layer `next`: its tag becomes `next`, and the
+// one thread whose claim on inl[c] succeeds appends it to the frontier list
+// (add_to_next_list and update_list in one step; the list order is free,
+// since the cells of one layer do not read one another).
+__device__ inline void join_layer(int c, uint8_t *lay, int *inl, int next, int *front, int *cnt) {
+    lay[c] = (uint8_t)next;
+    if (atomicCAS(inl + c, 0, next) == 0) front[atomicAdd(cnt, 1)] = c;
+}
+
+// the free orthogonal neighbours of cell ind join layer `next`
+__device__ inline void push_from(const grid_dev &g, int ind, uint8_t *lay, int *inl, int next, int *front,
+                                 int *cnt) {
     const int strides[3] = {1, g.sm4, g.smn4};
     int k = ind / g.smn4, j = (ind % g.smn4) / g.sm4, i = ind % g.sm4;
     if (!inner_ghost(g, i, j, k)) return;
     for (int d = 0; d < 3; d++)
         for (int sg = -1; sg <= 1; sg += 2) {
             int c = ind + sg * strides[d];
-            if (lay[c] == 255) {
-                lay[c] = (uint8_t)next;
-                inl[c] = 1;
-            }
+            if (lay[c] == 255) join_layer(c, lay, inl, next, front, cnt);
         }
 }
 
@@ -176,16 +183,16 @@ __device__ inline bool front_entry(int n_obj, const int *cnt, int &t, int &o) {
 }
 
 // neighbours of the primary cells (from_primary) or of the current
-// frontiers join the next layer (add_to_next_list with the orthogonal rule,
-// extrap_helper.hh:166-255)
-__global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int from_primary, uint8_t *lay,
-                           uint8_t *inl, int next) {
+// frontiers (front, cnt) join the next layer, listed in nfront / ncnt
+// (add_to_next_list with the orthogonal rule, extrap_helper.hh:166-255)
+__global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int from_primary, uint8_t *lay, int *inl,
+                           int next, int *nfront, int *ncnt) {
     if (from_primary) {
         int ind = blockIdx.x * blockDim.x + threadIdx.x;
         if (ind >= g.ncell) return;
         for (int o = 0; o < g.n_obj; o++) {
-            uint8_t *lo = lay + (size_t)o * g.ncell;
-            if (lo[ind] == 0) push_from(g, ind, lo, inl + (size_t)o * g.ncell, next);
+            const size_t off = (size_t)o * g.ncell;
+            if (lay[off + ind] == 0) push_from(g, ind, lay + off, inl + off, next, nfront + off, ncnt + o);
         }
         return;
     }
@@ -195,12 +202,13 @@ __global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int fro
         int t = t0, o;
         if (!front_entry(g.n_obj, cnt, t, o)) break;
         const size_t off = (size_t)o * g.ncell;
-        push_from(g, front[off + t], lay + off, inl + off, next);
+        push_from(g, front[off + t], lay + off, inl + off, next, nfront + off, ncnt + o);
     }
 }
 
-// image-backed ghost cells take their image's tag (periodic domains only)
-__global__ void k_lay_ghost(grid_dev g, uint8_t *lay, uint8_t *inl, int next) {
+// image-backed ghost cells take their image's tag and join its layer
+// (periodic domains only)
+__global__ void k_lay_ghost(grid_dev g, uint8_t *lay, int *inl, int next, int *nfront, int *ncnt) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
     int k = ind / g.smn4, j = (ind % g.smn4) / g.sm4, i = ind % g.sm4;
@@ -216,20 +224,7 @@ __global__ void k_lay_ghost(grid_dev g, uint8_t *lay, uint8_t *inl, int next) {
         const size_t off = (size_t)o * g.ncell;
         uint8_t v = lay[off + src];
         lay[off + ind] = v;
-        if (v == next) inl[off + ind] = 1;
-    }
-}
-
-// compaction of the listed cells into the next frontiers (update_list)
-__global__ void k_lay_compact(grid_dev g, uint8_t *inl, int *front, int *cnt) {
-    int ind = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ind >= g.ncell) return;
-    for (int o = 0; o < g.n_obj; o++) {
-        const size_t off = (size_t)o * g.ncell;
-        if (!inl[off + ind]) continue;
-        inl[off + ind] = 0;
-        int p = atomicAdd(cnt + o, 1);
-        front[off + p] = ind;
+        if (v == next && atomicCAS(inl + off + ind, 0, next) == 0) nfront[off + atomicAdd(ncnt + o, 1)] = ind;
     }
 }
 

@@ -122,7 +122,8 @@ struct rmt3d_scene {
     long long launches = 0;
     kernel_profiler prof;
     // extrapolation scratch
-    uint8_t *lay = nullptr, *inl = nullptr;
+    uint8_t *lay = nullptr;  // per object: layer tags
+    int *inl = nullptr;      // per object: layer that claimed the cell (0: none)
     int *front[2] = {nullptr, nullptr};  // per object: ncell entries each
     int *fcnt = nullptr;                  // frontier lengths, [2][kMaxObj]
     int *mlist = nullptr, *mcnt = nullptr;  // cells holding a map, for the stress kernel
@@ -285,14 +286,12 @@ static void extrapolate(rmt3d_scene *s) {
     int *cnt[2] = {s->fcnt, s->fcnt + kMaxObj};
     k_lay_init<<<nb, 256, 0, s->st>>>(g, s->dF, s->lay, s->inl);
     cudaMemsetAsync(s->fcnt, 0, 2 * kMaxObj * sizeof(int), s->st);
-    k_lay_push<<<nb, 256, 0, s->st>>>(g, nullptr, nullptr, 1, s->lay, s->inl, 1);
+    k_lay_push<<<nb, 256, 0, s->st>>>(g, nullptr, nullptr, 1, s->lay, s->inl, 1, s->front[0], cnt[0]);
     s->count(2);
     if (prd) {
-        k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, 1);
+        k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, 1, s->front[0], cnt[0]);
         s->count();
     }
-    k_lay_compact<<<nb, 256, 0, s->st>>>(g, s->inl, s->front[0], cnt[0]);
-    s->count();
     int cur = 0;
     for (int L = 1; L <= s->d.nlayers; L++) {
         k_extrap_layer<<<per_warp_blocks, 128, 0, s->st>>>(g, s->dF, s->front[cur], cnt[cur], L, s->d.max_extrap_rs,
@@ -305,14 +304,13 @@ static void extrapolate(rmt3d_scene *s) {
         if (L < s->d.nlayers) {
             int nxt = cur ^ 1;
             cudaMemsetAsync(cnt[nxt], 0, kMaxObj * sizeof(int), s->st);
-            k_lay_push<<<per_warp_blocks, 256, 0, s->st>>>(g, s->front[cur], cnt[cur], 0, s->lay, s->inl, L + 1);
+            k_lay_push<<<per_warp_blocks, 256, 0, s->st>>>(g, s->front[cur], cnt[cur], 0, s->lay, s->inl, L + 1,
+                                                           s->front[nxt], cnt[nxt]);
             s->count();
             if (prd) {
-                k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, L + 1);
+                k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, L + 1, s->front[nxt], cnt[nxt]);
                 s->count();
             }
-            k_lay_compact<<<nb, 256, 0, s->st>>>(g, s->inl, s->front[nxt], cnt[nxt]);
-            s->count();
             cur = nxt;
         }
     }
@@ -848,7 +846,8 @@ __global__ void k_mean(const double *x, size_t n, double scale, double *out, uns
 // pp_solve (fluid_3d.cc:2653-2681) before and after the multigrid solve
 static void ph_pp_pre(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    update_rho(s);
+    // the density is already that of the current maps: update_rho ran after
+    // the reference-map update, and nothing since has moved a map
     update_rinv(s);
     k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
     s->count();
@@ -2472,7 +2471,7 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     size_t b = n * sizeof(double) * (36 + (d->var_den ? 1 : 0));
     b += (size_t)d->n_obj * n * (2 * sizeof(int) + 51 * sizeof(double));
     if (d->n_obj > 0)
-        b += (size_t)d->n_obj * n * (2 * sizeof(uint8_t) + 2 * sizeof(int)) + 2 * kMaxObj * sizeof(int) +
+        b += (size_t)d->n_obj * n * (sizeof(uint8_t) + 3 * sizeof(int)) + 2 * kMaxObj * sizeof(int) +
              n * sizeof(int) + sizeof(int);
     b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);
     b += sizeof(fields_dev) + sizeof(scene_ctl) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);

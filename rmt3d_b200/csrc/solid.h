@@ -9,11 +9,10 @@ __global__ void k_edge_refmap(grid_dev g, const fields_dev *__restrict__ F, doub
 __global__ void k_refmap_predict(grid_dev g, const fields_dev *__restrict__ F, double cdt);
 __global__ void k_snapshot_reset(grid_dev g, const fields_dev *__restrict__ F);
 __global__ void k_reset_extraps(grid_dev g, const fields_dev *__restrict__ F);
-__global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t *lay, uint8_t *inl);
-__global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int from_primary, uint8_t *lay,
-                           uint8_t *inl, int next);
-__global__ void k_lay_ghost(grid_dev g, uint8_t *lay, uint8_t *inl, int next);
-__global__ void k_lay_compact(grid_dev g, uint8_t *inl, int *front, int *cnt);
+__global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t *lay, int *inl);
+__global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int from_primary, uint8_t *lay, int *inl,
+                           int next, int *nfront, int *ncnt);
+__global__ void k_lay_ghost(grid_dev g, uint8_t *lay, int *inl, int next, int *nfront, int *ncnt);
 __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, const int *front, const int *cnt, int L,
                                int max_rs, double wt, const double *lx, const double *ly, const double *lz,
                                int *err);

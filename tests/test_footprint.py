@@ -28,9 +28,9 @@ def test_objects_precision_and_size_order(tmp_path):
     sph = _desc(tmp_path, scenes.cavity_sphere(64), "s64.cfg")
     n = 68 ** 3
     # one object: 51 doubles + 2 ints of map state, frontier scratch of
-    # 10 bytes per cell and object, the frontier lengths, and the list of
+    # 13 bytes per cell and object, the frontier lengths, and the list of
     # cells holding a map with its length
-    assert R.footprint(sph) - R.footprint(base) == n * (51 * 8 + 8) + n * 10 + 2 * 16 * 4 + n * 4 + 4
+    assert R.footprint(sph) - R.footprint(base) == n * (51 * 8 + 8) + n * 13 + 2 * 16 * 4 + n * 4 + 4
     mixed = _desc(tmp_path, scenes.cavity_sphere(64), "m64.cfg")
     mixed.precision = R.MIXED
     assert R.footprint(mixed) > R.footprint(sph)
