@@ -530,7 +530,7 @@ def main():
     ap.add_argument("--no-stretched", action="store_true")
     ap.add_argument("--stretch-size", type=int, default=128)
     ap.add_argument("--stretch-steps", type=int, default=20)
-    ap.add_argument("--batch-scenes", type=int, default=32)
+    ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--serve-steps", type=int, default=20)
     ap.add_argument("--serve-slots", type=int, default=16)
