@@ -70,7 +70,7 @@ typedef struct {
     int chk_step; /* total step count at that checkpoint */
     int chkpt_freq;
     int omp_num_thr, debug_flag, debug_obj_id, obj_body, data_fmt, out_flag, output_dim, output_ind;
-    unsigned int dump_code; /* bit 8: checkpoints (stepper.hh:603-609) */
+    unsigned int dump_code; /* bit 1: tracers, 4: slices, 8: checkpoints, 32: macro.dat (stepper.hh:378-610) */
     int ntracers;
     double current_time; /* simulation time at the checkpoint */
     char dirname[256];   /* output directory: the .cfg path with ".cfg" -> ".out" */
@@ -251,6 +251,33 @@ int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *refmap_aos,
  * x, y, z (compute_centroid, :1348-1379); 5 total deviation of det F from 1
  * and 6 its maximum (total_dev_in_detF, :1032-1084). */
 int rmt3d_diag(rmt3d_scene *s, int kind, double *value);
+
+/* Passive tracers (Utilities/tracers.{hh,cc}), present when the run block
+ * has dump_code bit 1 and ntracers > 0 (fluid_3d.cc:217-219).  Each step
+ * moves them by the reference's improved Euler scheme: a predictor with the
+ * velocity at the start of the step and a corrector with the velocity at
+ * its end, both interpolated tricubically from the 4x4x4 cell centres
+ * around the tracer (tracers.hh:222-318, tracers.cc:395-457), slowed near
+ * homogeneous Dirichlet walls as tracers::dx does.  A tracer that crosses a
+ * periodic face re-enters on the other side; one that crosses a wall is
+ * lost.  rmt3d_initialize places them: from the checkpoint's tr.<chk_num>
+ * file on a restart, else uniformly at random (SplitMix64, seed 1 -- not
+ * the reference's GSL stream, so fresh placements differ from its own). */
+
+/* tracers::print's coordinates: x y z of every tracer by id (3 * ntracers
+ * floats, 0 0 0 for a lost tracer) into xyz, at most max_tracers of them;
+ * *n receives ntracers (0 when the scene has none). */
+int rmt3d_tracer_positions(rmt3d_scene *s, float *xyz, int max_tracers, int *n);
+
+/* tracers::set for every tracer (the restart path of
+ * tracers::init_from_chkpt_files, tracers.cc:140-168): n must be ntracers;
+ * a position outside the domain leaves that tracer out. */
+int rmt3d_tracer_place(rmt3d_scene *s, const double *xyz, int n);
+
+/* tracers::print (tracers.cc:105-133): binary (int count, then float x y z
+ * per tracer) or text ("%g %g %g" lines).  rmt3d_write_chk_pt also writes
+ * the frame's tr.<fnum> into the checkpoint directory. */
+int rmt3d_write_tracers(rmt3d_scene *s, const char *filename, int binary);
 
 /* One frame's diagnostics, the values the reference's stepper writes to
  * macro.dat and centroid.dat (Sim/stepper.hh:378-474). */

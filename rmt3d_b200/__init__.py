@@ -135,6 +135,26 @@ class Scene:
         _lib.check(lib().rmt3d_macro(self._h, ctypes.byref(m)))
         return m
 
+    def tracers(self):
+        """Tracer coordinates by id as an (ntracers, 3) float32 array
+        (0 0 0 for a lost tracer); empty when the scene has none."""
+        n = ctypes.c_int()
+        _lib.check(lib().rmt3d_tracer_positions(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 3), dtype=np.float32)
+        if n.value:
+            _lib.check(lib().rmt3d_tracer_positions(self._h, out.ctypes.data_as(ctypes.c_void_p), n.value,
+                                                    ctypes.byref(n)))
+        return out
+
+    def place_tracers(self, xyz):
+        """Place every tracer at the given coordinates ((ntracers, 3))."""
+        a = np.ascontiguousarray(xyz, dtype=np.float64)
+        _lib.check(lib().rmt3d_tracer_place(self._h, a.ctypes.data_as(ctypes.c_void_p), a.shape[0]))
+
+    def write_tracers(self, filename, binary=True):
+        """tracers::print: binary or text tracer file."""
+        _lib.check(lib().rmt3d_write_tracers(self._h, str(filename).encode(), int(bool(binary))))
+
     def slice(self, otype, dim, point, obj_id=-1):
         """fluid_3d::slice: the global slice array, shape (d2, d1)."""
         d1, d2 = ctypes.c_int(), ctypes.c_int()
@@ -277,8 +297,8 @@ class Stepper:
     dt fit to frames, a restart's initial step and frame (chk_step,
     chk_num), stop_short counted from the initial step, and per frame the
     outputs of write_files and collect_macro_data (stepper.hh:378-474,
-    583-610) that this path covers: slices of every out_flag type when
-    dump_code has bit 4, checkpoints every chkpt_freq frames with bit 8,
+    578-610) that this path covers: tracer files with bit 1, slices of every
+    out_flag type with bit 4, checkpoints every chkpt_freq frames with bit 8,
     macro.dat and centroid.dat with bit 32."""
 
     def __init__(self, desc, scene):
@@ -293,6 +313,7 @@ class Stepper:
         if self.frames - 1 > self.total:
             self.frames = self.total + 1
         self.dump_code = run.dump_code
+        self.trace = run.ntracers > 0
         self.chkpt_freq = run.chkpt_freq
         self.dirname = run.dirname.decode()
         self.slices = []
@@ -302,8 +323,11 @@ class Stepper:
         scene.set_dt(self.dt)
 
     def write_files(self, scene, snum, fnum):
-        if self.slices or (self.dump_code & 8):
+        if self.slices or (self.dump_code & 9):
             os.makedirs(self.dirname, exist_ok=True)
+        if self.trace and (self.dump_code & 1):
+            scene.write_tracers(os.path.join(self.dirname, "tr.%05d" % fnum), True)
+            scene.write_tracers(os.path.join(self.dirname, "tr_st.%05d" % fnum), False)
         for dim, point, otype, obj_id, fmt in self.slices:
             scene.write_slice(otype, dim, point, obj_id, fmt,
                               os.path.join(self.dirname, "%s.%05d" % (OUTPUT_NAMES[otype], fnum)))

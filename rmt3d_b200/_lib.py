@@ -149,6 +149,9 @@ SIGNATURES = {
     "rmt3d_write_chk_pt": (_I, [_P, _I, _I, ctypes.c_char_p, _I]),
     "rmt3d_read_chk_pt": (_I, [_P, ctypes.c_char_p, _IP]),
     "rmt3d_macro": (_I, [_P, ctypes.POINTER(MacroData)]),
+    "rmt3d_tracer_positions": (_I, [_P, _P, _I, _IP]),
+    "rmt3d_tracer_place": (_I, [_P, _P, _I]),
+    "rmt3d_write_tracers": (_I, [_P, ctypes.c_char_p, _I]),
     "rmt3d_slice": (_I, [_P, _I, _I, _I, _I, _P, _IP, _IP]),
     "rmt3d_write_slice": (_I, [_P, _I, _I, _I, _I, _I, ctypes.c_char_p]),
     "rmt3d_prepare": (_I, [_P]),

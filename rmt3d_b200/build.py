@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "--fmad=false",
                    "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
                    "-I" + INCLUDE, "-I" + CSRC]
-CU_SOURCES = ["k_fluid.cu", "k_mg.cu", "k_mgb.cu", "k_mgc.cu", "k_solid.cu", "k_chk.cu", "k_diag.cu", "scene.cu", "batch.cu"]
+CU_SOURCES = ["k_fluid.cu", "k_mg.cu", "k_mgb.cu", "k_mgc.cu", "k_solid.cu", "k_chk.cu", "k_diag.cu", "k_tracer.cu", "scene.cu", "batch.cu"]
 PER_FILE = {}
 CC_SOURCES = ["cfg.cc", "files.cc"]
 

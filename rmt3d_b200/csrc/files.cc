@@ -4,7 +4,9 @@
 //    files of o z-slices each, optionally xz-compressed, and the
 //    recover.cfg parameter file (Sim/sim_params.cc:489-600);
 //  * slice files (fluid_3d_io.cc:3-91): text matrix, coordinate text or
-//    gnuplot binary.
+//    gnuplot binary;
+//  * tracer files (Utilities/tracers.cc:105-170): the count and float
+//    coordinates in binary, or coordinate text.
 #include <cerrno>
 #include <cstdio>
 #include <cstring>
@@ -267,6 +269,37 @@ int slice_write_file(const char *filename, const double *u, int d1, int d2, int 
         }
     }
     fclose(fh);
+    return 0;
+}
+
+int tracer_write_file(const char *filename, const float *pos, int n, int binary) {
+    FILE *fh = fopen(filename, binary ? "wb" : "w");
+    if (!fh) return fail(RMT3D_ERR_IO, std::string("cannot write ") + filename);
+    if (binary) {
+        fwrite(&n, sizeof(int), 1, fh);
+        fwrite(pos, sizeof(float), 3 * (size_t)n, fh);
+    } else {
+        for (int t = 0; t < n; t++) fprintf(fh, "%g %g %g\n", pos[3 * t], pos[3 * t + 1], pos[3 * t + 2]);
+    }
+    fclose(fh);
+    return 0;
+}
+
+int tracer_read_file(const char *filename, int n, std::vector<float> &pos) {
+    FILE *fh = fopen(filename, "rb");
+    if (!fh) return fail(RMT3D_ERR_IO, std::string("cannot read tracer file ") + filename);
+    int lnum = 0;
+    size_t got = fread(&lnum, sizeof(int), 1, fh);
+    if (got == 1 && lnum == n) {
+        pos.assign(3 * (size_t)n, 0.f);
+        got = fread(pos.data(), sizeof(float), 3 * (size_t)n, fh);
+    } else {
+        got = 0;
+    }
+    fclose(fh);
+    if (lnum != n || got != 3 * (size_t)n)
+        return fail(RMT3D_ERR_IO, std::string("tracer file ") + filename +
+                                      ": reading failed, or its count differs from ntracers");
     return 0;
 }
 

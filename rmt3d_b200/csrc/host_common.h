@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <string>
+#include <vector>
 
 #include "rmt3d_gpu.h"
 
@@ -42,4 +43,7 @@ int chk_write_recover_cfg(const char *dir, const rmt3d_scene_desc &d, double dt)
 // coordinates of the two axes, m the x extent written in the gnuplot header
 int slice_write_file(const char *filename, const double *u, int d1, int d2, int format, const double *c1,
                      const double *c2, int m);
+// tracer files: binary (count, then float x y z per tracer) or text lines
+int tracer_write_file(const char *filename, const float *pos, int n, int binary);
+int tracer_read_file(const char *filename, int n, std::vector<float> &pos);
 }

@@ -1,6 +1,8 @@
 // Kernel declarations and small by-value argument structs shared between the
 // kernel translation units and the host orchestration (scene.cu).
 #pragma once
+#include <stdint.h>
+
 #include "dev_common.cuh"
 
 namespace rmt3d {
@@ -18,6 +20,18 @@ struct bc_face {
     double bcv[3];
     double h;
 };
+// the tracers of a scene and the constants their kernels read
+struct tracer_args {
+    int *pc;         // [3][n] corner cell of each tracer's 4x4x4 cube
+    double *rp;      // [6][n] rp0 (x, y, z) then rpf (x, y, z), in cell units
+    uint8_t *alive;  // [n] 0 for a tracer that left through a wall
+    double low[3];   // coordinate of ghost cell 0 on each axis (tracers.cc:18-20)
+    double h[3];
+    double lo[3], hi[3];  // the domain's walls (tracers.hh:370-375)
+    double dt;
+    int homog[3][2];  // [axis][low/high face]: homogeneous Dirichlet wall for that velocity component
+};
+
 struct bc_faces {
     bc_face f[6];
 };
@@ -52,6 +66,10 @@ __global__ void k_macro_obj(grid_dev g, const fields_dev *__restrict__ F, const 
 __global__ void k_divu_l2(grid_dev g, const double *r, double *out, unsigned *ticket);
 __global__ void k_slice(grid_dev g, const fields_dev *__restrict__ F, const double *r, int type, int dim, int point,
                         int obj_id, int var_den, int d1, int d2, double *out);
+__global__ void k_tracer_predict(grid_dev g, const fields_dev *__restrict__ F, tracer_args A, int n);
+__global__ void k_tracer_advect(grid_dev g, const fields_dev *__restrict__ F, tracer_args A, int n);
+__global__ void k_tracer_place(grid_dev g, tracer_args A, int n, const double *xyz);
+__global__ void k_tracer_positions(tracer_args A, int n, float *out);
 __global__ void k_chk_unpack(grid_dev g, const fields_dev *__restrict__ F, const double *__restrict__ buf, int *bad);
 
 }  // namespace rmt3d

@@ -127,6 +127,11 @@ struct rmt3d_scene {
     int *front[2] = {nullptr, nullptr};  // per object: ncell entries each
     int *fcnt = nullptr;                  // frontier lengths, [2][kMaxObj]
     int *mlist = nullptr, *mcnt = nullptr;  // cells holding a map, for the stress kernel
+    // passive tracers (dump_code bit 1 and ntracers > 0, fluid_3d.cc:217-219)
+    int ntr = 0;
+    int *tr_pc = nullptr;
+    double *tr_rp = nullptr;
+    uint8_t *tr_alive = nullptr;
     scene_ctl *ctl = nullptr;    // device control block
     scene_ctl *h_ctl = nullptr;  // pinned mirror
     int *counters = nullptr;     // = ctl->counters
@@ -879,6 +884,96 @@ static void ph_final(rmt3d_scene *s) {
     comm_dvel(s);
 }
 
+// ---------------------------------------------------------------------------
+// passive tracers (Utilities/tracers.{hh,cc}); kernels in k_tracer.cu
+// ---------------------------------------------------------------------------
+static tracer_args tr_args(const rmt3d_scene *s) {
+    tracer_args A;
+    memset(&A, 0, sizeof(A));
+    A.pc = s->tr_pc;
+    A.rp = s->tr_rp;
+    A.alive = s->tr_alive;
+    const double h[3] = {s->g.dx, s->g.dy, s->g.dz};
+    const double ax[3] = {s->g.ax, s->g.ay, s->g.az};
+    const int cells[3] = {s->g.sm, s->g.sn, s->g.so};
+    for (int f = 0; f < 3; f++) {
+        A.h[f] = h[f];
+        A.low[f] = ax[f] + (0 + 0 - 2 + 0.5) * h[f];  // lx[0] (fluid_3d.cc:136-138)
+        const double g0 = ax[f] + (0 + 0.5) * h[f];  // gx[0] (fluid_3d.cc:132-134)
+        A.lo[f] = g0 - 0.5 * h[f];
+        A.hi[f] = A.lo[f] + cells[f] * h[f];
+        for (int lr = 0; lr < 2; lr++)
+            A.homog[f][lr] = s->d.bct[f][2 * f + lr] == 1 && s->d.bcv[f][2 * f + lr] == 0;
+    }
+    A.dt = s->dt;
+    return A;
+}
+
+// tracers::predict at the start of a step, tracers::advect at its end
+// (fluid_3d.cc:459-461, 570-572)
+static void tracer_predict(rmt3d_scene *s) {
+    if (!s->ntr) return;
+    k_tracer_predict<<<(s->ntr + 127) / 128, 128, 0, s->st>>>(s->g, s->dF, tr_args(s), s->ntr);
+    s->count();
+}
+static void tracer_advect(rmt3d_scene *s) {
+    if (!s->ntr) return;
+    k_tracer_advect<<<(s->ntr + 127) / 128, 128, 0, s->st>>>(s->g, s->dF, tr_args(s), s->ntr);
+    s->count();
+}
+
+// tracers::set for every tracer, from host coordinates xyz[3 * ntr]
+static int tracers_place(rmt3d_scene *s, const double *xyz) {
+    double *d = nullptr;
+    const size_t bytes = 3 * (size_t)s->ntr * sizeof(double);
+    CK(cudaMallocAsync((void **)&d, bytes, s->st));
+    cudaError_t ce = cudaMemcpyAsync(d, xyz, bytes, cudaMemcpyHostToDevice, s->st);
+    if (ce == cudaSuccess) {
+        k_tracer_place<<<(s->ntr + 127) / 128, 128, 0, s->st>>>(s->g, tr_args(s), s->ntr, d);
+        s->count();
+        ce = cudaStreamSynchronize(s->st);
+    }
+    cudaFreeAsync(d, s->st);
+    CK(ce);
+    return 0;
+}
+
+// The tracers constructor (tracers.cc:7-70): a fresh start scatters them
+// uniformly over the domain; a restart reads the checkpoint's tr.<chk_num>
+// file.  The uniform draws are SplitMix64 (Steele, Lea and Flood 2014,
+// seed 1), not GSL's taus generator, so a fresh start places the tracers
+// elsewhere than the reference does; a restart places them identically.
+static int alloc_tracers(rmt3d_scene *s, const char *chk_dir) {
+    if (!s->ntr) return 0;
+    std::vector<double> xyz(3 * (size_t)s->ntr);
+    if (chk_dir) {
+        char fn[700];
+        snprintf(fn, sizeof(fn), "%s/tr.%05d", chk_dir, s->d.run.chk_num);
+        std::vector<float> pos;
+        int e = tracer_read_file(fn, s->ntr, pos);
+        if (e) return e;
+        for (size_t i = 0; i < xyz.size(); i++) xyz[i] = pos[i];
+    } else {
+        uint64_t state = 1;
+        auto uniform = [&]() {
+            uint64_t z = (state += 0x9e3779b97f4a7c15ULL);
+            z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+            z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+            z ^= z >> 31;
+            return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+        };
+        const double h[3] = {s->g.dx, s->g.dy, s->g.dz};
+        const double ax[3] = {s->g.ax, s->g.ay, s->g.az};
+        const int cells[3] = {s->g.sm, s->g.sn, s->g.so};
+        for (int t = 0; t < s->ntr; t++)
+            for (int f = 0; f < 3; f++) {
+                const double lo = (ax[f] + 0.5 * h[f]) - 0.5 * h[f];
+                xyz[3 * t + f] = lo + cells[f] * h[f] * uniform();
+            }
+    }
+    return tracers_place(s, xyz.data());
+}
+
 static int read_ctl(rmt3d_scene *s) {
     CK(cudaMemcpyAsync(s->h_ctl, s->ctl, sizeof(scene_ctl), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -901,6 +996,7 @@ static int step_forward(rmt3d_scene *s, int debug, int stop = 99) {
     (void)debug;
     s->nt++;
     CK(cudaMemsetAsync(s->counters + 2, 0, 6 * sizeof(int), s->st));
+    tracer_predict(s);
     compute_stress(s);
     if (stop <= 1) return RMT3D_OK;
     ph_edges(s);
@@ -936,6 +1032,7 @@ static int step_forward(rmt3d_scene *s, int debug, int stop = 99) {
     ph_pp_post(s);
     if (stop <= 8) return RMT3D_OK;
     ph_final(s);
+    tracer_advect(s);
     if (g.n_obj > 0) {
         int e = read_ctl(s);
         if (e) return e;
@@ -986,6 +1083,7 @@ static int capture_rest(rmt3d_scene *s) {
     s->launches += s->fem.outside_kernels;
     ph_pp_post(s);
     ph_final(s);
+    tracer_advect(s);
     return 0;
 }
 
@@ -1007,6 +1105,7 @@ static int build_step_graph(rmt3d_scene *s) {
     cudaStream_t b1 = s->gb.open(main, h_step, cudaGraphCondTypeIf);
     if (b1) {
         s->st = b1;
+        tracer_predict(s);
         compute_stress(s);
         ph_edges(s);
         ph_upwind(s);
@@ -1209,6 +1308,7 @@ static int build_group_graph(scene_group &G) {
             k_gstep_gate<<<1, 1, 0, s->st>>>(s->ctl, G.mac.part + b, h);
             s->count();
             g_if(G, s, h, [&]() {
+                tracer_predict(s);
                 compute_stress(s);
                 ph_edges(s);
                 ph_upwind(s);
@@ -1262,6 +1362,7 @@ static int build_group_graph(scene_group &G) {
             g_if(G, s, h3, [&]() {
                 ph_pp_post(s);
                 ph_final(s);
+                tracer_advect(s);
             });
             k_gstep_end<<<1, 1, 0, s->st>>>(s->ctl, s->g.n_obj > 0);
             s->count();
@@ -1675,6 +1776,11 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
         e |= s->alloc(&s->lay, no) | s->alloc(&s->inl, no) | s->alloc(&s->front[0], no) | s->alloc(&s->front[1], no) |
              s->alloc(&s->fcnt, 2 * kMaxObj) | s->alloc(&s->mlist, n) | s->alloc(&s->mcnt, 1);
     }
+    if ((d.run.dump_code & 1) && d.run.ntracers > 0) {
+        s->ntr = d.run.ntracers;
+        e |= s->alloc(&s->tr_pc, 3 * (size_t)s->ntr) | s->alloc(&s->tr_rp, 6 * (size_t)s->ntr) |
+             s->alloc(&s->tr_alive, (size_t)s->ntr);
+    }
     e |= s->alloc(&s->ctl, 1) | s->alloc(&s->d_mean, 1 + kMeanBlocks) | s->alloc(&s->d_red, 4) |
          s->alloc(&s->mean_ticket, 1) | s->alloc(&s->d_diag, kDiagVals * (1 + kMeanBlocks)) |
          s->alloc(&s->diag_ticket, 1);
@@ -1852,6 +1958,13 @@ extern "C" int rmt3d_initialize(rmt3d_scene *s) {
         init_extrapolate(s);
         update_rho(s);
     }
+    // alloc_tracers (fluid_3d.cc:217-219): from the checkpoint's tracer file
+    // on a restart, scattered afresh otherwise
+    if (s->ntr) {
+        char dir[600];
+        snprintf(dir, sizeof(dir), "%s/chk.%05d", r.recover_dirname, r.chk_num);
+        if ((e = alloc_tracers(s, r.chk_num > 0 ? dir : nullptr))) return e;
+    }
     return init_finish(s);
 }
 
@@ -1882,6 +1995,13 @@ extern "C" int rmt3d_write_chk_pt(rmt3d_scene *s, int snum, int fnum, const char
     int e = chk_make_dir(chk_dirname);
     if (!e) e = chk_write_files(chk_dirname, h.data(), L, g.so, compress);
     if (e) return e;
+    // the tracer file of this frame (the reference copies the stepper's
+    // tr.<fnum>, fluid_3d_chk_pt.cc:22-33)
+    if (s->ntr) {
+        char fn[700];
+        snprintf(fn, sizeof(fn), "%s/tr.%05d", chk_dirname, fnum);
+        if ((e = rmt3d_write_tracers(s, fn, 1))) return e;
+    }
     // set_current_chk_num / _chk_step / _time, then write_params
     s->d.run.chk_num = fnum;
     s->d.run.chk_step = snum;
@@ -2427,6 +2547,42 @@ extern "C" int rmt3d_write_slice(rmt3d_scene *s, int type, int dim, int point, i
     return slice_write_file(filename, u.data(), d1, d2, format, c1.data(), c2.data(), s->g.sm);
 }
 
+extern "C" int rmt3d_tracer_positions(rmt3d_scene *s, float *xyz, int max_tracers, int *n) {
+    if (!s || !n) return fail(RMT3D_ERR_INVALID, "null argument");
+    *n = s->ntr;
+    if (!s->ntr || !xyz) return RMT3D_OK;
+    float *d = nullptr;
+    const size_t bytes = 3 * (size_t)s->ntr * sizeof(float);
+    CK(cudaMallocAsync((void **)&d, bytes, s->st));
+    k_tracer_positions<<<(s->ntr + 127) / 128, 128, 0, s->st>>>(tr_args(s), s->ntr, d);
+    s->count();
+    std::vector<float> h(3 * (size_t)s->ntr);
+    cudaError_t ce = cudaMemcpyAsync(h.data(), d, bytes, cudaMemcpyDeviceToHost, s->st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s->st);
+    cudaFreeAsync(d, s->st);
+    CK(ce);
+    const int m = max_tracers < s->ntr ? max_tracers : s->ntr;
+    memcpy(xyz, h.data(), 3 * (size_t)(m > 0 ? m : 0) * sizeof(float));
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_tracer_place(rmt3d_scene *s, const double *xyz, int n) {
+    if (!s || !xyz) return fail(RMT3D_ERR_INVALID, "null argument");
+    if (n != s->ntr) return fail(RMT3D_ERR_INVALID, "tracer count differs from the scene's ntracers");
+    if (!s->ntr) return RMT3D_OK;
+    return tracers_place(s, xyz);
+}
+
+extern "C" int rmt3d_write_tracers(rmt3d_scene *s, const char *filename, int binary) {
+    if (!s || !filename) return fail(RMT3D_ERR_INVALID, "null argument");
+    if (!s->ntr) return fail(RMT3D_ERR_INVALID, "the scene has no tracers (dump_code bit 1, ntracers)");
+    std::vector<float> pos(3 * (size_t)s->ntr);
+    int n = 0;
+    int e = rmt3d_tracer_positions(s, pos.data(), s->ntr, &n);
+    if (e) return e;
+    return tracer_write_file(filename, pos.data(), n, binary);
+}
+
 extern "C" int rmt3d_sync(rmt3d_scene *s) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     CK(cudaStreamSynchronize(s->st));
@@ -2473,6 +2629,8 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     if (d->n_obj > 0)
         b += (size_t)d->n_obj * n * (sizeof(uint8_t) + 3 * sizeof(int)) + 2 * kMaxObj * sizeof(int) +
              n * sizeof(int) + sizeof(int);
+    if ((d->run.dump_code & 1) && d->run.ntracers > 0)
+        b += (size_t)d->run.ntracers * (3 * sizeof(int) + 6 * sizeof(double) + sizeof(uint8_t));
     b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);
     b += sizeof(fields_dev) + sizeof(scene_ctl) + (1 + kMeanBlocks + 4) * sizeof(double) + sizeof(unsigned);
     b += kDiagVals * (1 + kMeanBlocks) * sizeof(double) + sizeof(unsigned);

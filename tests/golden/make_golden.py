@@ -18,6 +18,11 @@ same workload with slice output and frame diagnostics switched on (dump_code
 along x (gnuplot binary) and along z (coordinate text), and macro.dat /
 centroid.dat, at frames 0 and 1.
 
+The tracer case tr16 runs the same workload with 200 passive tracers
+(dump_code 1 | 8): the tracer files of frames 0 and 1, the checkpoint of
+frame 1 (with its tracer file), and the tracer file after restarting from
+that checkpoint and stepping 2 more steps.
+
 The checkpoint case chk16 (16^3 cavity + sphere of radius 0.3, 2 steps per
 frame) holds the reference's checkpoint after frame 1 (write_chk_pt: the
 eight slice files, decompressed, and recover.cfg), the reference's state at
@@ -187,6 +192,33 @@ def make_out(workdir):
     print("wrote out16", len(arrays), "arrays")
 
 
+def make_tr(workdir):
+    txt = chk_cfg().replace("dump_code 8", "dump_code 9") + "ntracers 200\n"
+    with open(os.path.join(workdir, "c.cfg"), "w") as fh:
+        fh.write(txt)
+    env = dict(os.environ, RMT3D_SHIM_EXACT="1")
+    subprocess.run([DRIVER, "c.cfg", "2", "s2.bin"], check=True, capture_output=True, cwd=workdir, env=env)
+    arrays = {"cfg": np.frombuffer(txt.encode(), dtype=np.uint8)}
+    out = os.path.join(workdir, "c.out")
+    for fn in ("tr.00000", "tr.00001"):
+        with open(os.path.join(out, fn), "rb") as fh:
+            arrays["file_" + fn] = np.frombuffer(fh.read(), dtype=np.uint8)
+    chk = os.path.join(out, "chk.00001")
+    saved = os.path.join(workdir, "saved_chk1")
+    shutil.copytree(chk, saved)
+    for n, v in read_chk_dir(saved).items():
+        arrays["chk_" + n] = v
+    for fn in ("recover.cfg", "tr.00001"):
+        with open(os.path.join(saved, fn), "rb") as fh:
+            arrays["chkfile_" + fn] = np.frombuffer(fh.read(), dtype=np.uint8)
+    subprocess.run([DRIVER, "c.out/chk.00001/recover.cfg", "2", "r.bin"], check=True, capture_output=True,
+                   cwd=workdir, env=env)
+    with open(os.path.join(chk, "recover.out", "tr.00002"), "rb") as fh:
+        arrays["file_restart_tr.00002"] = np.frombuffer(fh.read(), dtype=np.uint8)
+    np.savez_compressed(os.path.join(HERE, "tr16.npz"), **arrays)
+    print("wrote tr16")
+
+
 def compact(d):
     """Reduce a dump to the state the step reads and writes."""
     f, rm = d["fields"], d["refmaps"]
@@ -269,6 +301,9 @@ def main():
         if not only or "out16" in only:
             os.makedirs(os.path.join(wd, "out"))
             make_out(os.path.join(wd, "out"))
+        if not only or "tr16" in only:
+            os.makedirs(os.path.join(wd, "tr"))
+            make_tr(os.path.join(wd, "tr"))
         if not only or "chk16" in only:
             os.makedirs(os.path.join(wd, "chk", "env"))
             make_chk(os.path.join(wd, "chk"))
