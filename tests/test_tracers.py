@@ -131,7 +131,7 @@ def test_tracers_stay_inside(tmp_path):
     finally:
         sc.close()
     q = tmp_path / "p.cfg"
-    q.write_text(scenes.stretched_sphere(16, 100, radius=0.3) + "ntracers 300\n")
+    q.write_text(scenes.stretched_sphere(24, 100, radius=0.2) + "ntracers 300\n")
     dd = R.desc_from_cfg(str(q))
     dd.run.dump_code = 1
     sc = R.Scene(dd)
