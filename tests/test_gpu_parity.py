@@ -49,6 +49,7 @@ def vec_errors(scene, st):
     ref = np.stack([st["vel"][c].reshape(shp)[H.INTERIOR] for c in range(3)])
     got = np.stack([scene.field(n)[H.INTERIOR] for n in "uvw"])
     scale = np.linalg.norm(ref)
+    scale = scale if scale > 0 else 1.0  # the initial state is at rest
     out = {n: float(np.linalg.norm(got[c] - ref[c]) / scale) for c, n in enumerate("uvw")}
     out["p"] = H.rel_l2(scene.field("p")[H.INTERIOR], st["p"].reshape(shp)[H.INTERIOR])
     return out
