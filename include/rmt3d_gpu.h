@@ -381,8 +381,9 @@ int rmt3d_scene_set_mg_launch(rmt3d_scene *s, int cluster);
 /* Device bytes a scene with this descriptor allocates (admission control). */
 size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d);
 
-/* Sums of u^2, v^2, w^2, p^2 over the interior cells: a compact fingerprint of
- * a scene's state. */
+/* Sums of u^2, v^2, w^2, p^2 over the interior cells, added in a fixed order
+ * (the same bits for the same state on every run): a compact fingerprint of a
+ * scene's state. */
 int rmt3d_scene_checksum(rmt3d_scene *s, double out[4]);
 
 /* ---- serving loop ------------------------------------------------------ */

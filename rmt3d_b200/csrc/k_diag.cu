@@ -48,6 +48,19 @@ __device__ void fixed_order_reduce(double (&v)[NV], unsigned max_mask, double *o
     }
 }
 
+// Sums of u^2, v^2, w^2 and p^2 over the interior cells, in a fixed order
+// (the same bits on every run)
+__global__ void k_checksum(grid_dev g, const fields_dev *__restrict__ F, double *out, unsigned *ticket) {
+    double v[4] = {0, 0, 0, 0};
+    const int ncell = g.sm * g.sn * g.so;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ncell; t += gridDim.x * blockDim.x) {
+        const int ind = gidx(g, t % g.sm + 2, (t / g.sm) % g.sn + 2, t / (g.sm * g.sn) + 2);
+        for (int c = 0; c < 3; c++) v[c] += F->vel[c][ind] * F->vel[c][ind];
+        v[3] += F->p[ind] * F->p[ind];
+    }
+    fixed_order_reduce<4>(v, 0u, out, ticket);
+}
+
 // Interior-cell sums and extremes of one frame:
 //  [0..2] sum of velocity (times density in the variable-density form)
 //         (total_momentum, fluid_3d_utils.cc:783-800);

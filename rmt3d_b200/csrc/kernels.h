@@ -64,6 +64,7 @@ __global__ void k_macro_cells(grid_dev g, const fields_dev *__restrict__ F, cons
 __global__ void k_macro_obj(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
                             const double *lz, int o, double *out, unsigned *ticket);
 __global__ void k_divu_l2(grid_dev g, const double *r, double *out, unsigned *ticket);
+__global__ void k_checksum(grid_dev g, const fields_dev *__restrict__ F, double *out, unsigned *ticket);
 __global__ void k_slice(grid_dev g, const fields_dev *__restrict__ F, const double *r, int type, int dim, int point,
                         int obj_id, int var_den, int d1, int d2, double *out);
 __global__ void k_tracer_predict(grid_dev g, const fields_dev *__restrict__ F, tracer_args A, int n);

@@ -2651,30 +2651,13 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     return b + mac + fem;
 }
 
-__global__ void k_checksum(grid_dev g, const fields_dev *__restrict__ F, double *out) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
-    int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-    int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
-    double v[4] = {0, 0, 0, 0};
-    if (i < g.sm + 2 && j < g.sn + 2 && k < g.so + 2) {
-        int ind = gidx(g, i, j, k);
-        for (int c = 0; c < 3; c++) v[c] = F->vel[c][ind] * F->vel[c][ind];
-        v[3] = F->p[ind] * F->p[ind];
-    }
-    for (int c = 0; c < 4; c++) {
-        double a = v[c];
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-        if ((threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z)) % 32 == 0) atomicAdd(out + c, a);
-    }
-}
-
 extern "C" int rmt3d_scene_checksum(rmt3d_scene *s, double out[4]) {
     if (!s || !out) return fail(RMT3D_ERR_INVALID, "null argument");
     const grid_dev &g = s->g;
-    CK(cudaMemsetAsync(s->d_red, 0, 4 * sizeof(double), s->st));
-    k_checksum<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->d_red);
+    static_assert(4 <= kDiagVals, "checksum partials exceed the diagnostics area");
+    k_checksum<<<kMeanBlocks, 256, 0, s->st>>>(g, s->dF, s->d_diag, s->diag_ticket);
     s->count();
-    CK(cudaMemcpyAsync(out, s->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(out, s->d_diag, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     return RMT3D_OK;
 }

@@ -3,10 +3,9 @@
 A batch steps independent scenes of uneven grid sizes together (each on its
 own stream, kernels overlapping on the device); the serving loop admits
 requests over time under an HBM budget.  Each scene's result must be the same
-as when the scene runs alone: the kernels and their order per scene do not
-depend on what else runs, so the only differences allowed are those of the
-floating-point atomics of the checksum reduction, far below the tolerance
-used here (the step's own reductions sum in a fixed order).
+as when the scene runs alone, bit for bit: the kernels and their order per
+scene do not depend on what else runs, and every reduction (the step's and
+the checksum's) sums in a fixed order.
 """
 import numpy as np
 import pytest
@@ -17,8 +16,6 @@ from rmt3d_b200 import _lib, scenes
 
 pytestmark = pytest.mark.gpu
 
-SAME_TOL = 1e-11      # batch / mix versus alone, rel-L2 per field
-CHECK_TOL = 1e-11     # checksums, relative
 
 
 def _descs(tmp_path):
@@ -51,6 +48,7 @@ def test_alone_is_deterministic(tmp_path):
     b, cb = _alone(d, 3)
     for f in a:
         assert (a[f] == b[f]).all(), f
+    assert list(ca) == list(cb)
 
 
 def test_batch_matches_alone(tmp_path):
@@ -61,11 +59,11 @@ def test_batch_matches_alone(tmp_path):
         st = b.step(3)
         assert st == [R.NORMAL_EXIT] * len(descs)
         for i, d in enumerate(descs):
-            ref, _ = _alone(d, 3)
+            ref, rc = _alone(d, 3)
             for f in ("u", "v", "w", "p"):
                 got = b.field(i, f)
-                e = H.rel_l2(got[H.INTERIOR], ref[f][H.INTERIOR])
-                assert e < SAME_TOL, (i, f, e)
+                assert np.array_equal(got[H.INTERIOR], ref[f][H.INTERIOR]), (i, f)
+            assert list(b.checksum(i)) == list(rc), i
     finally:
         b.close()
 
@@ -122,8 +120,7 @@ def test_serve_same_alone_and_in_mix(tmp_path):
         assert r["status"] == R.NORMAL_EXIT and r["steps_done"] == n
         assert r["admit_s"] >= arr - 1e-6
         _, alone = _alone(d, n)
-        for a, b in zip(r["checksum"], alone):
-            assert abs(a - b) <= CHECK_TOL * max(abs(b), 1e-300), (a, b)
+        assert list(r["checksum"]) == list(alone), (r["checksum"], alone)
 
 
 def test_serve_admission_by_budget(tmp_path):
