@@ -134,4 +134,29 @@ struct fields_dev {
     unsigned int *flags;  // scratch per-cell flags (extrapolation frontier)
 };
 
+// update_rho at one cell (fluid_3d.cc:1104-1143, VAR_DEN): the solid fractions of the
+// primary map, then of every extrapolated map, blended with the fluid density
+__device__ inline double cell_rho(const grid_dev &g, const fields_dev *__restrict__ F, int ind) {
+    double sfrac = 0, srho = 0;
+    int prim = -1;
+    for (int o = 0; o < g.n_obj; o++)
+        if (F->om[o].code[ind] == 0) prim = o;
+    if (prim >= 0) {
+        const objmap_dev &m = F->om[prim];
+        double t = heaviside(g, obj_phi(g, prim, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
+        srho += t * g.obj[prim].rho;
+        sfrac += t;
+    }
+    for (int o = 0; o < g.n_obj; o++) {
+        const objmap_dev &m = F->om[o];
+        if (m.code[ind] <= 0) continue;
+        double t = heaviside(g, obj_phi(g, o, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
+        srho += t * g.obj[o].rho;
+        sfrac += t;
+    }
+    if (sfrac > 1.) srho /= sfrac;
+    else srho += (1 - sfrac) * g.frho;
+    return srho;
+}
+
 }  // namespace rmt3d

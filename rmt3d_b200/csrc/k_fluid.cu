@@ -356,19 +356,6 @@ __device__ void face_stress(const grid_dev &g, const fields_dev *__restrict__ F,
 
 // Cells that hold any reference map: the full stress (solid, fluid blend,
 // collision).  Cells without maps are left to k_stress_fluid.
-// Cells that hold any reference map, listed for the full stress kernel (the
-// box range of the stress faces: absolute indices 1..s+3 on every axis).
-__global__ void k_map_cells(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (i > g.sm + 3 || j > g.sn + 3 || k > g.so + 3) return;
-    const int ind = gidx(g, i, j, k);
-    bool any = false;
-    for (int o = 0; o < g.n_obj; o++) any = any || F->om[o].code[ind] >= 0;
-    if (any) list[atomicAdd(cnt, 1)] = ind;
-}
-
 // The full stress of the listed cells, one thread per (cell, face): work
 // item t is face t / n of cell list[t % n].  The three faces of a cell write
 // disjoint outputs and read only what no face writes, so they run in any
@@ -388,18 +375,34 @@ __global__ void __launch_bounds__(128) k_stress(grid_dev g, const fields_dev *__
     }
 }
 
-// Cells without reference maps (most of the box): the pure fluid stress of
-// the three lower faces, the nmaps = 0 path of face_stress written with the
-// same expression ((1 - sfrac) * fs + ss with sfrac = ss = 0), in a small
-// kernel that keeps many more threads resident than the full one.
-__global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F) {
+// One pass over the box range of the stress faces (absolute indices 1..s+3
+// on every axis).  Cells without reference maps (most of the box) get the
+// pure fluid stress of their three lower faces: the nmaps = 0 path of
+// face_stress written with the same expression ((1 - sfrac) * fs + ss with
+// sfrac = ss = 0), in a small kernel that keeps many more threads resident
+// than the full one.  Cells that hold any map are appended to list (when
+// given) for the full stress kernel, one atomic per warp.
+__global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.sm + 3 || j > g.sn + 3 || k > g.so + 3) return;
     const int ind = gidx(g, i, j, k);
-    for (int o = 0; o < g.n_obj; o++)
-        if (F->om[o].code[ind] >= 0) return;
+    bool any = false;
+    for (int o = 0; o < g.n_obj; o++) any = any || F->om[o].code[ind] >= 0;
+    if (list) {
+        const unsigned act = __activemask();
+        const unsigned maps = __ballot_sync(act, any);
+        if (maps) {
+            const int lane = threadIdx.x & 31;  // blockDim.x is a multiple of 32
+            const int leader = __ffs(maps) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(cnt, __popc(maps));
+            base = __shfl_sync(act, base, leader);
+            if (any) list[base + __popc(maps & ((1u << lane) - 1))] = ind;
+        }
+    }
+    if (any) return;
     const int strides[3] = {1, g.sm4, g.smn4};
     const double facs[3] = {g.dxsp, g.dysp, g.dzsp};
     const double sfrac = 0, ss = 0;

@@ -481,7 +481,7 @@ __global__ void k_layer_ghost_copy(grid_dev g, const fields_dev *__restrict__ F,
 // primary x = (x + xpred)/2; extrapolated maps average with the previous
 // extrapolation of the same object, or take xpred where none existed.
 // -------------------------------------------------------------------------
-__global__ void k_refmap_correct(grid_dev g, const fields_dev *__restrict__ F, int *prob) {
+__global__ void k_refmap_correct(grid_dev g, const fields_dev *__restrict__ F, int *prob, int var_den) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
     for (int o = 0; o < g.n_obj; o++) {
@@ -499,6 +499,8 @@ __global__ void k_refmap_correct(grid_dev g, const fields_dev *__restrict__ F, i
                 for (int c = 0; c < 3; c++) m.x[c][ind] = m.xp[c][ind];
         }
     }
+    // update_rho (fluid_3d.cc:1252) from this cell's corrected maps
+    if (var_den) F->rho[ind] = cell_rho(g, F, ind);
 }
 
 // revert_reference_map_update (fluid_3d.cc:1257-1283)
@@ -516,8 +518,9 @@ __global__ void k_refmap_revert(grid_dev g, const fields_dev *__restrict__ F) {
     }
 }
 
-// update_reference_map_full (fluid_3d.cc:1285-1306): x = xpred everywhere
-__global__ void k_refmap_full(grid_dev g, const fields_dev *__restrict__ F) {
+// update_reference_map_full (fluid_3d.cc:1285-1306): x = xpred everywhere,
+// then its update_rho (:1304) from this cell's maps
+__global__ void k_refmap_full(grid_dev g, const fields_dev *__restrict__ F, int var_den) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
     for (int o = 0; o < g.n_obj; o++) {
@@ -525,6 +528,7 @@ __global__ void k_refmap_full(grid_dev g, const fields_dev *__restrict__ F) {
         if (m.code[ind] < 0) continue;
         for (int c = 0; c < 3; c++) m.x[c][ind] = m.xp[c][ind];
     }
+    if (var_den) F->rho[ind] = cell_rho(g, F, ind);
 }
 
 // x = xpred for the maps of one extrapolation (init_extrapolate,

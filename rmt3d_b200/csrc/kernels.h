@@ -44,9 +44,8 @@ struct gradphi_t {
 __global__ void k_periodic_copy(grid_dev g, ptr_list pl, int corner);
 __global__ void k_bc_cc(grid_dev g, int n, bc_face lo, bc_face hi, double *u, double *v, double *w);
 __global__ void k_bc_cf(grid_dev g, int walls, bc_faces bcs, const fields_dev *F);
-__global__ void k_map_cells(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt);
 __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F, const int *list, const int *cnt);
-__global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F);
+__global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt);
 __global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
                            const double *lz, double cdt, const double *time_p, int var_den);
 __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F);

@@ -617,26 +617,7 @@ static int init_refmap(rmt3d_scene *s) {
 __global__ void k_update_rho(grid_dev g, const fields_dev *__restrict__ F) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
-    double sfrac = 0, srho = 0;
-    int prim = -1;
-    for (int o = 0; o < g.n_obj; o++)
-        if (F->om[o].code[ind] == 0) prim = o;
-    if (prim >= 0) {
-        const objmap_dev &m = F->om[prim];
-        double t = heaviside(g, obj_phi(g, prim, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
-        srho += t * g.obj[prim].rho;
-        sfrac += t;
-    }
-    for (int o = 0; o < g.n_obj; o++) {
-        const objmap_dev &m = F->om[o];
-        if (m.code[ind] <= 0) continue;
-        double t = heaviside(g, obj_phi(g, o, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
-        srho += t * g.obj[o].rho;
-        sfrac += t;
-    }
-    if (sfrac > 1.) srho /= sfrac;
-    else srho += (1 - sfrac) * g.frho;
-    F->rho[ind] = srho;
+    F->rho[ind] = cell_rho(g, F, ind);
 }
 
 static void update_rho(rmt3d_scene *s) {
@@ -710,13 +691,14 @@ static void compute_grad_basis(rmt3d_scene *s) {
 // ---------------------------------------------------------------------------
 static void compute_stress(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    k_stress_fluid<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF);
+    const bool maps = g.n_obj > 0;
+    if (maps) cudaMemsetAsync(s->mcnt, 0, sizeof(int), s->st);
+    k_stress_fluid<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF, maps ? s->mlist : nullptr,
+                                                                          s->mcnt);
     s->count();
-    if (g.n_obj > 0) {
-        cudaMemsetAsync(s->mcnt, 0, sizeof(int), s->st);
-        k_map_cells<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF, s->mlist, s->mcnt);
+    if (maps) {
         k_stress<<<148 * 8, 128, 0, s->st>>>(g, s->dF, s->mlist, s->mcnt);
-        s->count(2);
+        s->count();
     }
 }
 
@@ -791,9 +773,9 @@ static void ph_refmap(rmt3d_scene *s, double cdt) {
     s->count(2);
     comm_primary(s);
     extrapolate(s);
-    k_refmap_correct<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->counters + 3);
+    // update_rho follows in the same pass (var_den)
+    k_refmap_correct<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->counters + 3, s->d.var_den);
     s->count();
-    update_rho(s);
 }
 
 static void ph_revert(rmt3d_scene *s) {
@@ -874,9 +856,9 @@ static void ph_pp_post(rmt3d_scene *s) {
 static void ph_final(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     if (g.n_obj > 0) {
-        k_refmap_full<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
+        // update_rho follows in the same pass (var_den)
+        k_refmap_full<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->d.var_den);
         s->count();
-        update_rho(s);
         k_redraw<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->d.nlayers, s->counters + 4);
         s->count();
     }

@@ -17,9 +17,9 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
                                int max_rs, double wt, const double *lx, const double *ly, const double *lz,
                                int *err);
 __global__ void k_layer_ghost_copy(grid_dev g, const fields_dev *__restrict__ F, int L);
-__global__ void k_refmap_correct(grid_dev g, const fields_dev *__restrict__ F, int *prob);
+__global__ void k_refmap_correct(grid_dev g, const fields_dev *__restrict__ F, int *prob, int var_den);
 __global__ void k_refmap_revert(grid_dev g, const fields_dev *__restrict__ F);
-__global__ void k_refmap_full(grid_dev g, const fields_dev *__restrict__ F);
+__global__ void k_refmap_full(grid_dev g, const fields_dev *__restrict__ F, int var_den);
 __global__ void k_extraps_full(grid_dev g, const fields_dev *__restrict__ F);
 __global__ void k_redraw(grid_dev g, const fields_dev *__restrict__ F, int nlayers, int *fatal);
 
