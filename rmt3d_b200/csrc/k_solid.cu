@@ -228,13 +228,25 @@ __global__ void k_lay_ghost(grid_dev g, uint8_t *lay, int *inl, int next, int *n
     }
 }
 
-__device__ inline double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+// Lanes that work on one frontier cell: an aligned group of a warp.  Fewer
+// lanes per cell put more cells in flight at once (a layer's frontier is a
+// few thousand cells, each a chain of dependent loads and reductions).
+constexpr int kExtrapLanes = 8;
+static_assert(kExtrapLanes == 8 || kExtrapLanes == 16 || kExtrapLanes == 32, "lanes per frontier cell");
+
+// the lanes of this thread's group
+__device__ inline unsigned group_mask() {
+    if (kExtrapLanes == 32) return 0xffffffffu;
+    return ((1u << kExtrapLanes) - 1) << ((threadIdx.x & 31) & ~(kExtrapLanes - 1));
+}
+
+__device__ inline double group_sum(double v, unsigned mask) {
+    for (int o = kExtrapLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
     return v;
 }
 
 // -------------------------------------------------------------------------
-// One layer of least-squares extrapolation, one warp per frontier cell:
+// One layer of least-squares extrapolation, one lane group per frontier cell:
 // gather_and_list (fluid_3d_ex.cc:86-272), extrap_helper::least_square
 // (extrap_helper.cc:34-103) with lin_sys (:129-146), mat3::inverse
 // (Utilities/mat3.hh:61-67) and transfer (fluid_3d_ex.cc:293-328).
@@ -255,7 +267,7 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
     // pass 1: weights and weighted sums of positions and values
     double sw = 0, sd[3] = {0, 0, 0}, sr[3] = {0, 0, 0};
     int cnt = 0;
-    for (int s = lane; s < nc; s += 32) {
+    for (int s = lane; s < nc; s += kExtrapLanes) {
         int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
         if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
         if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
@@ -285,12 +297,13 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
             sr[c] += m.xp[c][qi] * wgt;
         }
     }
-    sw = warp_sum(sw);
+    const unsigned gm = group_mask();
+    sw = group_sum(sw, gm);
     for (int c = 0; c < 3; c++) {
-        sd[c] = warp_sum(sd[c]);
-        sr[c] = warp_sum(sr[c]);
+        sd[c] = group_sum(sd[c], gm);
+        sr[c] = group_sum(sr[c], gm);
     }
-    for (int off = 16; off > 0; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    for (int off = kExtrapLanes / 2; off > 0; off >>= 1) cnt += __shfl_xor_sync(gm, cnt, off);
     if (cnt == 0) return false;
     double davg[3], ravg[3];
     for (int c = 0; c < 3; c++) {
@@ -299,7 +312,7 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
     }
     // pass 2: weighted normal equations about the averages
     double a[6] = {0, 0, 0, 0, 0, 0}, rhs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int s = lane; s < nc; s += 32) {
+    for (int s = lane; s < nc; s += kExtrapLanes) {
         int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
         if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
         if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
@@ -336,8 +349,8 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
             rhs[3 * c + 2] += e2 * lr;
         }
     }
-    for (int c = 0; c < 6; c++) a[c] = warp_sum(a[c]);
-    for (int c = 0; c < 9; c++) rhs[c] = warp_sum(rhs[c]);
+    for (int c = 0; c < 6; c++) a[c] = group_sum(a[c], gm);
+    for (int c = 0; c < 9; c++) rhs[c] = group_sum(rhs[c], gm);
     // mat3 A(XX, XY, XZ, XY, YY, YZ, XZ, YZ, ZZ) and its inverse
     const double a11 = a[0], a12 = a[3], a13 = a[4], a21 = a[3], a22 = a[1], a23 = a[5], a31 = a[4],
                  a32 = a[5], a33 = a[2];
@@ -361,8 +374,8 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
     return true;
 }
 
-// Every object's frontier in one launch: warp w takes entry w of the
-// concatenated frontiers.  The weights wt^n (n = |p|+|q|+|r|) come from a
+// Every object's frontier in one launch: lane group w (kExtrapLanes lanes)
+// takes entry w of the concatenated frontiers.  The weights wt^n (n = |p|+|q|+|r|) come from a
 // per-block table of the same pow() values.
 __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, const int *front, const int *cnt, int L,
                                int max_rs, double wt, const double *lx, const double *ly, const double *lz,
@@ -371,9 +384,9 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
     const int npow = 3 * max_rs + 1;
     for (int q = threadIdx.x; q < kPowTab && q < npow; q += blockDim.x) wpow[q] = pow(wt, (double)q);
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & (kExtrapLanes - 1);
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / kExtrapLanes;
+    const int nwarps = (gridDim.x * blockDim.x) / kExtrapLanes;
     int total = 0;
     for (int o = 0; o < g.n_obj; o++) total += cnt[o];
     for (int t0 = warp; t0 < total; t0 += nwarps) {
