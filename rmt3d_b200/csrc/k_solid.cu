@@ -155,9 +155,23 @@ __global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t
 // one thread whose claim on inl[c] succeeds appends it to the frontier list
 // (add_to_next_list and update_list in one step; the list order is free,
 // since the cells of one layer do not read one another).
+// A slot at the end of list cnt for each calling thread: one atomic per
+// group of converged threads that append to the same list (the threads of a
+// warp may serve different objects' lists).  Blocks are one-dimensional.
+__device__ inline int list_slot(int *cnt) {
+    const unsigned act = __activemask();
+    const unsigned same = __match_any_sync(act, (unsigned long long)cnt);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(same) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(cnt, __popc(same));
+    base = __shfl_sync(same, base, leader);
+    return base + __popc(same & ((1u << lane) - 1));
+}
+
 __device__ inline void join_layer(int c, uint8_t *lay, int *inl, int next, int *front, int *cnt) {
     lay[c] = (uint8_t)next;
-    if (atomicCAS(inl + c, 0, next) == 0) front[atomicAdd(cnt, 1)] = c;
+    if (atomicCAS(inl + c, 0, next) == 0) front[list_slot(cnt)] = c;
 }
 
 // the free orthogonal neighbours of cell ind join layer `next`
@@ -224,15 +238,15 @@ __global__ void k_lay_ghost(grid_dev g, uint8_t *lay, int *inl, int next, int *n
         const size_t off = (size_t)o * g.ncell;
         uint8_t v = lay[off + src];
         lay[off + ind] = v;
-        if (v == next && atomicCAS(inl + off + ind, 0, next) == 0) nfront[off + atomicAdd(ncnt + o, 1)] = ind;
+        if (v == next && atomicCAS(inl + off + ind, 0, next) == 0) nfront[off + list_slot(ncnt + o)] = ind;
     }
 }
 
 // Lanes that work on one frontier cell: an aligned group of a warp.  Fewer
 // lanes per cell put more cells in flight at once (a layer's frontier is a
 // few thousand cells, each a chain of dependent loads and reductions).
-constexpr int kExtrapLanes = 8;
-static_assert(kExtrapLanes == 8 || kExtrapLanes == 16 || kExtrapLanes == 32, "lanes per frontier cell");
+constexpr int kExtrapLanes = 4;
+static_assert(kExtrapLanes == 4 || kExtrapLanes == 8 || kExtrapLanes == 16 || kExtrapLanes == 32, "lanes per frontier cell");
 
 // the lanes of this thread's group
 __device__ inline unsigned group_mask() {
