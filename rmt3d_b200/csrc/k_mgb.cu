@@ -5,7 +5,7 @@
 // (mg_ctl); the group holds device tables of their pointers.  Every batched
 // kernel maps blockIdx.z (or blockIdx.y) to (scene, block within the scene)
 // and runs the same body as the single-scene kernel (mg_body.cuh), so each
-// scene's arithmetic is bit-identical to its solo solve.  Scenes take part in
+// scene's solve is bit-identical to its solo solve.  Scenes take part in
 // a solve when their flag part[b] is set (a halted or reverted scene sits
 // out); a scene whose own control has finished stops being touched while the
 // others continue (run[b]).  The graph WHILE loop repeats while any scene of

@@ -242,20 +242,21 @@ __global__ void k_lay_ghost(grid_dev g, uint8_t *lay, int *inl, int next, int *n
     }
 }
 
-// Lanes that work on one frontier cell: an aligned group of a warp.  Fewer
-// lanes per cell put more cells in flight at once (a layer's frontier is a
-// few thousand cells, each a chain of dependent loads and reductions).
-constexpr int kExtrapLanes = 4;
-static_assert(kExtrapLanes == 4 || kExtrapLanes == 8 || kExtrapLanes == 16 || kExtrapLanes == 32, "lanes per frontier cell");
-
-// the lanes of this thread's group
+// LANES lanes work on one frontier cell: an aligned group of a warp.  Fewer
+// lanes per cell put more cells in flight at once but make each cell a
+// longer chain; a layer's frontier is a few thousand cells per scene, which
+// a warp per cell covers in about one round when the scene has the GPU to
+// itself, while concurrent scenes fill the GPU better with 4 lanes per cell.
+template <int LANES>
 __device__ inline unsigned group_mask() {
-    if (kExtrapLanes == 32) return 0xffffffffu;
-    return ((1u << kExtrapLanes) - 1) << ((threadIdx.x & 31) & ~(kExtrapLanes - 1));
+    static_assert(LANES == 4 || LANES == 8 || LANES == 16 || LANES == 32, "lanes per frontier cell");
+    if (LANES == 32) return 0xffffffffu;
+    return ((1u << (LANES & 31)) - 1) << ((threadIdx.x & 31) & ~(LANES - 1));
 }
 
+template <int LANES>
 __device__ inline double group_sum(double v, unsigned mask) {
-    for (int o = kExtrapLanes / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+    for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
     return v;
 }
 
@@ -271,7 +272,7 @@ constexpr int kPowTab = 64;
 // of map m: false when no candidate is eligible or the normal matrix is
 // singular (the caller then widens R).  W = 2R + 1 as a compile-time
 // constant for the common radii, 0 for the general case.
-template <int W>
+template <int W, int LANES>
 __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, int lane, int ii, int jj, int kk,
                           int ind, bool directional, const double (&gph)[3], double cx, double cy, double cz,
                           const double *lx, const double *ly, const double *lz, const double *wpow, double wt,
@@ -281,7 +282,7 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
     // pass 1: weights and weighted sums of positions and values
     double sw = 0, sd[3] = {0, 0, 0}, sr[3] = {0, 0, 0};
     int cnt = 0;
-    for (int s = lane; s < nc; s += kExtrapLanes) {
+    for (int s = lane; s < nc; s += LANES) {
         int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
         if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
         if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
@@ -311,13 +312,13 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
             sr[c] += m.xp[c][qi] * wgt;
         }
     }
-    const unsigned gm = group_mask();
-    sw = group_sum(sw, gm);
+    const unsigned gm = group_mask<LANES>();
+    sw = group_sum<LANES>(sw, gm);
     for (int c = 0; c < 3; c++) {
-        sd[c] = group_sum(sd[c], gm);
-        sr[c] = group_sum(sr[c], gm);
+        sd[c] = group_sum<LANES>(sd[c], gm);
+        sr[c] = group_sum<LANES>(sr[c], gm);
     }
-    for (int off = kExtrapLanes / 2; off > 0; off >>= 1) cnt += __shfl_xor_sync(gm, cnt, off);
+    for (int off = LANES / 2; off > 0; off >>= 1) cnt += __shfl_xor_sync(gm, cnt, off);
     if (cnt == 0) return false;
     double davg[3], ravg[3];
     for (int c = 0; c < 3; c++) {
@@ -326,7 +327,7 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
     }
     // pass 2: weighted normal equations about the averages
     double a[6] = {0, 0, 0, 0, 0, 0}, rhs[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int s = lane; s < nc; s += kExtrapLanes) {
+    for (int s = lane; s < nc; s += LANES) {
         int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
         if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
         if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
@@ -363,8 +364,8 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
             rhs[3 * c + 2] += e2 * lr;
         }
     }
-    for (int c = 0; c < 6; c++) a[c] = group_sum(a[c], gm);
-    for (int c = 0; c < 9; c++) rhs[c] = group_sum(rhs[c], gm);
+    for (int c = 0; c < 6; c++) a[c] = group_sum<LANES>(a[c], gm);
+    for (int c = 0; c < 9; c++) rhs[c] = group_sum<LANES>(rhs[c], gm);
     // mat3 A(XX, XY, XZ, XY, YY, YZ, XZ, YZ, ZZ) and its inverse
     const double a11 = a[0], a12 = a[3], a13 = a[4], a21 = a[3], a22 = a[1], a23 = a[5], a31 = a[4],
                  a32 = a[5], a33 = a[2];
@@ -388,9 +389,10 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
     return true;
 }
 
-// Every object's frontier in one launch: lane group w (kExtrapLanes lanes)
+// Every object's frontier in one launch: lane group w (LANES lanes)
 // takes entry w of the concatenated frontiers.  The weights wt^n (n = |p|+|q|+|r|) come from a
 // per-block table of the same pow() values.
+template <int LANES>
 __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, const int *front, const int *cnt, int L,
                                int max_rs, double wt, const double *lx, const double *ly, const double *lz,
                                int *err) {
@@ -398,9 +400,9 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
     const int npow = 3 * max_rs + 1;
     for (int q = threadIdx.x; q < kPowTab && q < npow; q += blockDim.x) wpow[q] = pow(wt, (double)q);
     __syncthreads();
-    const int lane = threadIdx.x & (kExtrapLanes - 1);
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / kExtrapLanes;
-    const int nwarps = (gridDim.x * blockDim.x) / kExtrapLanes;
+    const int lane = threadIdx.x & (LANES - 1);
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / LANES;
+    const int nwarps = (gridDim.x * blockDim.x) / LANES;
     int total = 0;
     for (int o = 0; o < g.n_obj; o++) total += cnt[o];
     for (int t0 = warp; t0 < total; t0 += nwarps) {
@@ -456,11 +458,11 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
         double val[3] = {0, 0, 0};
         for (int R = 2; R <= max_rs && !success; R++) {
             switch (R) {
-                case 2: success = ls_radius<5>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
-                case 3: success = ls_radius<7>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
-                case 4: success = ls_radius<9>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
-                case 5: success = ls_radius<11>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
-                default: success = ls_radius<0>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                case 2: success = ls_radius<5, LANES>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                case 3: success = ls_radius<7, LANES>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                case 4: success = ls_radius<9, LANES>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                case 5: success = ls_radius<11, LANES>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
+                default: success = ls_radius<0, LANES>(g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val); break;
             }
         }
         if (!success) {
@@ -476,6 +478,11 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
         }
     }
 }
+
+template __global__ void k_extrap_layer<4>(grid_dev, const fields_dev *__restrict__, const int *, const int *, int,
+                                            int, double, const double *, const double *, const double *, int *);
+template __global__ void k_extrap_layer<32>(grid_dev, const fields_dev *__restrict__, const int *, const int *, int,
+                                             int, double, const double *, const double *, const double *, int *);
 
 // communicate_a_layer on one rank (fluid_3d_comm.cc:203-280): image-backed
 // ghosts receive the maps of the layer just made at their image (periodic

@@ -1,7 +1,7 @@
 // Bodies of the multigrid phase kernels, with the block coordinates passed
 // in: the single-scene kernels (k_mg.cu) and the batched kernels that run a
 // phase for every scene of a group in one launch (k_mgb.cu) call the same
-// code, so a scene gives the same bits alone and in a group.
+// code, so a scene's solve gives the same bits alone and in a group.
 #pragma once
 #include <cuda_runtime.h>
 

@@ -126,6 +126,9 @@ struct rmt3d_scene {
     int *inl = nullptr;      // per object: layer that claimed the cell (0: none)
     int *front[2] = {nullptr, nullptr};  // per object: ncell entries each
     int *fcnt = nullptr;                  // frontier lengths, [2][kMaxObj]
+    // lanes per frontier cell of the least-squares extrapolation: a warp when
+    // the scene steps on its own, 4 when it steps inside a group with others
+    int extrap_lanes = 32;
     int *mlist = nullptr, *mcnt = nullptr;  // cells holding a map, for the stress kernel
     // passive tracers (dump_code bit 1 and ntracers > 0, fluid_3d.cc:217-219)
     int ntr = 0;
@@ -173,6 +176,16 @@ struct rmt3d_scene {
 
 // the step's captured parameters (dt, FEM basis, multigrid schedule) changed:
 // graphs that hold this scene's step must be captured again
+static void mark_dirty(rmt3d_scene *s);
+
+// the extrapolation's lanes per frontier cell; a change re-captures the
+// scene's own step graph
+static void set_extrap_lanes(rmt3d_scene *s, int lanes) {
+    if (s->extrap_lanes == lanes) return;
+    s->extrap_lanes = lanes;
+    mark_dirty(s);
+}
+
 static void mark_dirty(rmt3d_scene *s) {
     s->graph_dirty = true;
     s->param_version++;
@@ -299,7 +312,7 @@ static void extrapolate(rmt3d_scene *s) {
     }
     int cur = 0;
     for (int L = 1; L <= s->d.nlayers; L++) {
-        k_extrap_layer<<<per_warp_blocks, 128, 0, s->st>>>(g, s->dF, s->front[cur], cnt[cur], L, s->d.max_extrap_rs,
+        (s->extrap_lanes == 4 ? k_extrap_layer<4> : k_extrap_layer<32>)<<<per_warp_blocks, 128, 0, s->st>>>(g, s->dF, s->front[cur], cnt[cur], L, s->d.max_extrap_rs,
                                                            s->d.weight_fac, s->lx, s->ly, s->lz, s->counters + 2);
         s->count();
         if (prd) {
@@ -1399,6 +1412,10 @@ int group_create(rmt3d_scene *const *scenes, int n, scene_group **out) {
     // the group's launches must follow each scene's outstanding work
     for (rmt3d_scene *s : G->sc)
         if (!e && cudaStreamSynchronize(s->st) != cudaSuccess) e = RMT3D_ERR_CUDA;
+    // scenes that share the GPU with the rest of their group extrapolate with
+    // 4 lanes per frontier cell (more cells in flight)
+    if (!e)
+        for (rmt3d_scene *s : G->sc) set_extrap_lanes(s, n > 1 ? 4 : 32);
     if (!e) e = build_group_graph(*G);
     if (e) {
         delete G;
@@ -1411,6 +1428,7 @@ int group_create(rmt3d_scene *const *scenes, int n, scene_group **out) {
 void group_destroy(scene_group *G) {
     if (!G) return;
     cudaStreamSynchronize(G->st);
+    for (rmt3d_scene *s : G->sc) set_extrap_lanes(s, 32);
     delete G;
 }
 
