@@ -758,10 +758,12 @@ static void ph_upwind(rmt3d_scene *s) {
     fill_boundary_cf(s);
 }
 
-// mac_solve (fluid_3d.cc:2209-2241) before and after the multigrid solve
+// mac_solve (fluid_3d.cc:2209-2241) before and after the multigrid solve.
+// The solve uses the density of the end of the previous step (or of the
+// set-up), as mac.set_rhoinv(lrho) does: update_rho last ran with the full
+// map update (:1304), before redraw_boundary.
 static void ph_mac_pre(rmt3d_scene *s, double cdt) {
     const grid_dev &g = s->g;
-    update_rho(s);
     update_rinv(s);
     k_mac_rhs<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.rhs(), cdt);
     s->count();
