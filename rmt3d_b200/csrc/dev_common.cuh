@@ -134,22 +134,43 @@ struct fields_dev {
     unsigned int *flags;  // scratch per-cell flags (extrapolation frontier)
 };
 
+// Bit o set when object o holds a map (code >= 0) at cell ind.  The codes are
+// loaded four objects at a time, so a cell costs one memory round trip per
+// four objects instead of one per object; loops over the set bits visit the
+// objects in increasing order, as loops over o do.
+__device__ inline unsigned map_mask(const grid_dev &g, const fields_dev *__restrict__ F, int ind) {
+    unsigned m = 0;
+    for (int base = 0; base < g.n_obj; base += 4) {
+        int c[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) c[u] = base + u < g.n_obj ? F->om[base + u].code[ind] : -1;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (c[u] >= 0) m |= 1u << (base + u);
+    }
+    return m;
+}
+
 // update_rho at one cell (fluid_3d.cc:1104-1143, VAR_DEN): the solid fractions of the
 // primary map, then of every extrapolated map, blended with the fluid density
 __device__ inline double cell_rho(const grid_dev &g, const fields_dev *__restrict__ F, int ind) {
     double sfrac = 0, srho = 0;
     int prim = -1;
-    for (int o = 0; o < g.n_obj; o++)
+    unsigned ext = 0;  // objects with an extrapolated map here
+    for (unsigned mk = map_mask(g, F, ind); mk; mk &= mk - 1) {
+        const int o = __ffs(mk) - 1;
         if (F->om[o].code[ind] == 0) prim = o;
+        else ext |= 1u << o;
+    }
     if (prim >= 0) {
         const objmap_dev &m = F->om[prim];
         double t = heaviside(g, obj_phi(g, prim, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
         srho += t * g.obj[prim].rho;
         sfrac += t;
     }
-    for (int o = 0; o < g.n_obj; o++) {
+    for (; ext; ext &= ext - 1) {
+        const int o = __ffs(ext) - 1;
         const objmap_dev &m = F->om[o];
-        if (m.code[ind] <= 0) continue;
         double t = heaviside(g, obj_phi(g, o, m.x[0][ind], m.x[1][ind], m.x[2][ind]));
         srho += t * g.obj[o].rho;
         sfrac += t;

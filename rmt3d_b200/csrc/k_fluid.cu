@@ -388,8 +388,7 @@ __global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F, int
     int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.sm + 3 || j > g.sn + 3 || k > g.so + 3) return;
     const int ind = gidx(g, i, j, k);
-    bool any = false;
-    for (int o = 0; o < g.n_obj; o++) any = any || F->om[o].code[ind] >= 0;
+    const bool any = map_mask(g, F, ind) != 0;
     if (list) {
         const unsigned act = __activemask();
         const unsigned maps = __ballot_sync(act, any);
@@ -621,11 +620,10 @@ __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F) {
     if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
     const int ind = gidx(g, i, j, k);
     const int strides[3] = {1, g.sm4, g.smn4};
-    for (int o = 0; o < g.n_obj; o++) {
+    for (unsigned mk = map_mask(g, F, ind); mk; mk &= mk - 1) {
+        const int o = __ffs(mk) - 1;
         const objmap_dev &m = F->om[o];
-        int cd = m.code[ind];
-        if (cd < 0) continue;
-        bool go = (cd == 0);
+        bool go = (m.code[ind] == 0);
         if (!go) {  // an extrapolated map with a primary neighbour on its upper side (neigh_inside)
             for (int d = 0; d < 3 && !go; d++)
                 if (m.code[ind + strides[d]] == 0) go = true;
@@ -635,8 +633,7 @@ __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F) {
             const int nb = ind + strides[dir];
             const int ff = 2 * dir + 1, nf = ff ^ 1;
             const int a1 = (dir + 1) % 3, a2 = (dir + 2) % 3;
-            double norml = F->fvel[3 * ff + dir][ind];
-            double normr = F->fvel[3 * nf + dir][nb];
+            const double norml = F->fvel[3 * ff + dir][ind], normr = F->fvel[3 * nf + dir][nb];
             double ml = m.fx[3 * ff + dir][ind], vl = m.fx[3 * ff + a1][ind], wl = m.fx[3 * ff + a2][ind];
             double mr = m.fx[3 * nf + dir][nb], vr = m.fx[3 * nf + a1][nb], wr = m.fx[3 * nf + a2][nb];
             set_refmap(norml, normr, ml, vl, wl, mr, vr, wr);
