@@ -482,8 +482,8 @@ __device__ inline void fluid_accel(const grid_dev &g, double x, double y, double
                   sin(2 * PI * x) +
               PI * cos(2 * PI * t) * cos(2 * PI * t) * (2 + cos(4 * PI * y) + cos(4 * PI * z)) * sin(4 * PI * x)) /
              4;
-        fy = -(PI * cos(2 * PI * t) * cos(2 * PI * t) * (-1 + cos(4 * PI * x) - 2 * cos(4 * PI * z)) * sin(4 * PI * y)) / 8;
-        fz = -(PI * cos(2 * PI * t) * cos(2 * PI * t) * (-1 + cos(4 * PI * x) - 2 * cos(4 * PI * y)) * sin(4 * PI * z)) / 8;
+        fy = -(PI * cos(2 * PI * t) * cos(2 * PI * t) * (-1 + cos(4 * PI * x) - 2 * cos(4 * PI * z)) * sin(4 * PI * y)) * 0.125;
+        fz = -(PI * cos(2 * PI * t) * cos(2 * PI * t) * (-1 + cos(4 * PI * x) - 2 * cos(4 * PI * y)) * sin(4 * PI * z)) * 0.125;
     } else if (g.sim_type == 2) {  // sim_objects: gravity (sim_manager.hh:400-404)
         fx = fy = 0;
         fz = 0;
@@ -572,8 +572,9 @@ __global__ void __launch_bounds__(256, 3) k_edge_vel(grid_dev g, const fields_de
     }
     double acc[3] = {0, 0, 0};
     acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
-    const double dh2[3] = {g.dx / 2, g.dy / 2, g.dz / 2};
-    const double dt2 = cdt / 2.0;
+    // halves as products (the same bits as the divisions, far fewer instructions)
+    const double dh2[3] = {g.dx * 0.5, g.dy * 0.5, g.dz * 0.5};
+    const double dt2 = cdt * 0.5;
     double adv[3] = {0, 0, 0};
     for (int a = 0; a < 3; a++) {
         for (int b = 0; b < 3; b++) adv[a] -= vel[b] * nv[b][a];

@@ -34,8 +34,10 @@ __global__ void k_mac_rb_b(lvl_dev L, T *const *x, T *const *r, const T *const *
     MGB_SCENE(zb)
     body_mac_rb<T>(L, x[b_], r[b_], colour, ri ? ri[b_] : nullptr, blockIdx.x, blockIdx.y, bz_);
 }
+// FP32: at most 51 registers, five 256-thread blocks per SM; FP64 keeps
+// four (64 registers; its stencil state spills at 51)
 template <typename T>
-__global__ void k_fem_gs_b(lvl_dev L, T *const *x, T *const *r, const T *const *ri, int colour, const int *run,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 4) k_fem_gs_b(lvl_dev L, T *const *x, T *const *r, const T *const *ri, int colour, const int *run,
                            int zb) {
     MGB_SCENE(zb)
     body_fem_gs<T>(L, x[b_], r[b_], colour, ri ? ri[b_] : nullptr, blockIdx.x, blockIdx.y, bz_);

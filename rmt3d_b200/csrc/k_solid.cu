@@ -24,8 +24,9 @@ __global__ void __launch_bounds__(256, 3) k_edge_refmap(grid_dev g, const fields
     const int ind = gidx(g, i, j, k);
     const int strides[3] = {1, g.sm4, g.smn4};
     const double dhsp[3] = {g.dxsp, g.dysp, g.dzsp};
-    const double dh2[3] = {g.dx / 2, g.dy / 2, g.dz / 2};
-    const double dt2 = cdt / 2.0;
+    // halves as products (the same bits as the divisions, far fewer instructions)
+    const double dh2[3] = {g.dx * 0.5, g.dy * 0.5, g.dz * 0.5};
+    const double dt2 = cdt * 0.5;
     double vel[3];
     for (int c = 0; c < 3; c++) vel[c] = F->vel[c][ind];
     for (int o = 0; o < g.n_obj; o++) {

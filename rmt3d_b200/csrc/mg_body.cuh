@@ -36,9 +36,14 @@ __device__ __forceinline__ void body_fem_gs(lvl_dev L, T *__restrict__ x, const 
     int k = bz_ * blockDim.z + threadIdx.z;
     if (i >= L.n0 || j >= L.n1 || k >= L.n2) return;
     T diag;
-    T s = ri ? fem_offdiag_vd(L, x, ri, i, j, k, diag) : fem_offdiag(L, x, i, j, k, diag);
-    int id = i + L.n0 * (j + L.n1 * k);
-    x[id] = (r[id] - s) / diag;
+    const int id = i + L.n0 * (j + L.n1 * k);
+    if (ri) {
+        const T s = fem_offdiag_vd(L, x, ri, i, j, k, diag);
+        x[id] = (r[id] - s) / diag;
+    } else {
+        const T s = fem_offdiag(L, x, i, j, k, diag);
+        x[id] = (r[id] - s) * fem_inv_diag<T>(L, i, j, k);
+    }
 }
 
 // residual res = r - A x, and max |res| into *mx (as ordered bit pattern)

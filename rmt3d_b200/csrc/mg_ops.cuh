@@ -104,6 +104,17 @@ __device__ __forceinline__ T fem_offdiag(const lvl_dev L, const T *__restrict__ 
 }
 
 
+// 1 / diag of the constant-density FEM stencil at node (i, j, k).  diag is
+// 32 / 2^h, h the number of walled axes on whose end planes the node lies,
+// so the reciprocal 2^h / 32 is exact and (r - s) times it has the same bits
+// as (r - s) / diag, without a division's instruction sequence.
+template <typename T>
+__device__ __forceinline__ T fem_inv_diag(const lvl_dev L, int i, int j, int k) {
+    const int h = (!L.p0 && (i == 0 || i == L.n0 - 1)) + (!L.p1 && (j == 0 || j == L.n1 - 1)) +
+                  (!L.p2 && (k == 0 || k == L.n2 - 1));
+    return (T)(1 << h) * (T)0.03125;
+}
+
 // ---- variable density (VAR_DEN) ---------------------------------------------
 // ri: 1/rho per cell of the level (cell-centred, MAC level dimensions; for a
 // FEM level with n nodes per axis there are n-1 cells on a walled axis and n
@@ -174,7 +185,9 @@ __device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict
     if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
         // interior node (all 8 cells exist, no halving): corners take one
         // cell, edges the mean of two (lower index first), the centre the
-        // mean of all eight in (z, y, x) order
+        // mean of all eight in (z, y, x) order; the means multiply by 1/2 and
+        // 1/8, the same bits as the divisions without their instruction
+        // sequences
         const int sy = L.n0, sz = L.n0 * L.n1;
         const int ncx = L.p0 ? L.n0 : L.n0 - 1, ncy = L.p1 ? L.n1 : L.n1 - 1;
         const int c0 = (i - 1) + ncx * ((j - 1) + ncy * (k - 1));  // cell below-left-front
@@ -203,11 +216,11 @@ __device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict
                     if (nz == 3) {
                         cf = -v[oc >> 1][ob >> 1][oa >> 1];
                     } else if (oc == 1) {
-                        cf = (T)-2 * ((v[0][ob >> 1][oa >> 1] + v[1][ob >> 1][oa >> 1]) / (T)2);
+                        cf = (T)-2 * ((v[0][ob >> 1][oa >> 1] + v[1][ob >> 1][oa >> 1]) * (T)0.5);
                     } else if (ob == 1) {
-                        cf = (T)-2 * ((v[oc >> 1][0][oa >> 1] + v[oc >> 1][1][oa >> 1]) / (T)2);
+                        cf = (T)-2 * ((v[oc >> 1][0][oa >> 1] + v[oc >> 1][1][oa >> 1]) * (T)0.5);
                     } else {
-                        cf = (T)-2 * ((v[oc >> 1][ob >> 1][0] + v[oc >> 1][ob >> 1][1]) / (T)2);
+                        cf = (T)-2 * ((v[oc >> 1][ob >> 1][0] + v[oc >> 1][ob >> 1][1]) * (T)0.5);
                     }
                     s += cf * xv;
                 }
@@ -218,7 +231,7 @@ __device__ __forceinline__ T fem_offdiag_vd(const lvl_dev L, const T *__restrict
             for (int b = 0; b < 2; b++)
 #pragma unroll
                 for (int e = 0; e < 2; e++) c8 += v[a][b][e];
-        diag = (T)32 * (c8 / (T)8);
+        diag = (T)32 * (c8 * (T)0.125);
         return s;
     }
     // boundary or wrapped node; every loop below unrolls to constant indices
