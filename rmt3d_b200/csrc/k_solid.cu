@@ -91,7 +91,11 @@ __global__ void k_refmap_predict(grid_dev g, const fields_dev *__restrict__ F, d
 }
 
 // extraps.copy(temp_extraps); extraps.reset() (fluid_3d.cc:1202-1203)
-__global__ void k_snapshot_reset(grid_dev g, const fields_dev *__restrict__ F) {
+// With lay given (no periodic axis: nothing changes the codes before the
+// extrapolation starts), the pass also sets the extrapolation's layer tags
+// and claims as k_lay_init would from the reset codes: primary cells 0,
+// every other cell free.
+__global__ void k_snapshot_reset(grid_dev g, const fields_dev *__restrict__ F, uint8_t *lay, int *inl) {
     int ind = blockIdx.x * blockDim.x + threadIdx.x;
     if (ind >= g.ncell) return;
     for (int o = 0; o < g.n_obj; o++) {
@@ -102,6 +106,10 @@ __global__ void k_snapshot_reset(grid_dev g, const fields_dev *__restrict__ F) {
             for (int c = 0; c < 3; c++) m.x_prev[c][ind] = m.x[c][ind];
             for (int c = 0; c < 9; c++) m.gp_prev[c][ind] = m.gp[c][ind];
             m.code[ind] = -1;
+        }
+        if (lay) {
+            lay[(size_t)o * g.ncell + ind] = (cd == 0) ? 0 : 255;
+            inl[(size_t)o * g.ncell + ind] = 0;
         }
     }
 }

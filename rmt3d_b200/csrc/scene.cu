@@ -293,7 +293,9 @@ static void comm_primary(rmt3d_scene *s) {
 // ---------------------------------------------------------------------------
 // extrapolation, fluid_3d::extrapolate (fluid_3d_ex.cc:31-47)
 // ---------------------------------------------------------------------------
-static void extrapolate(rmt3d_scene *s) {
+// lay_ready: the layer tags and claims are already initialised (by the
+// snapshot pass of the reference-map update)
+static void extrapolate(rmt3d_scene *s, bool lay_ready = false) {
     const grid_dev &g = s->g;
     if (g.n_obj == 0) return;
     const int nb = lin_blocks(g.ncell);
@@ -302,10 +304,13 @@ static void extrapolate(rmt3d_scene *s) {
     // cell, and the two ghost-copy kernels would find nothing to do
     const bool prd = g.prd[0] || g.prd[1] || g.prd[2];
     int *cnt[2] = {s->fcnt, s->fcnt + kMaxObj};
-    k_lay_init<<<nb, 256, 0, s->st>>>(g, s->dF, s->lay, s->inl);
+    if (!lay_ready) {
+        k_lay_init<<<nb, 256, 0, s->st>>>(g, s->dF, s->lay, s->inl);
+        s->count();
+    }
     cudaMemsetAsync(s->fcnt, 0, 2 * kMaxObj * sizeof(int), s->st);
     k_lay_push<<<nb, 256, 0, s->st>>>(g, nullptr, nullptr, 1, s->lay, s->inl, 1, s->front[0], cnt[0]);
-    s->count(2);
+    s->count();
     if (prd) {
         k_lay_ghost<<<nb, 256, 0, s->st>>>(g, s->lay, s->inl, 1, s->front[0], cnt[0]);
         s->count();
@@ -783,11 +788,14 @@ static void ph_mac_post(rmt3d_scene *s, double cdt) {
 // problem count lands in counters[3]
 static void ph_refmap(rmt3d_scene *s, double cdt) {
     const grid_dev &g = s->g;
+    // without a periodic axis nothing changes the codes between the snapshot
+    // and the extrapolation, so the snapshot pass sets the layer tags too
+    const bool prd = g.prd[0] || g.prd[1] || g.prd[2];
     k_refmap_predict<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, cdt);
-    k_snapshot_reset<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF);
+    k_snapshot_reset<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, prd ? nullptr : s->lay, s->inl);
     s->count(2);
     comm_primary(s);
-    extrapolate(s);
+    extrapolate(s, !prd);
     // update_rho follows in the same pass (var_den)
     k_refmap_correct<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, s->counters + 3, s->d.var_den);
     s->count();

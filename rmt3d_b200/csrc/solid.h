@@ -7,7 +7,7 @@ namespace rmt3d {
 
 __global__ void k_edge_refmap(grid_dev g, const fields_dev *__restrict__ F, double cdt, int *err);
 __global__ void k_refmap_predict(grid_dev g, const fields_dev *__restrict__ F, double cdt);
-__global__ void k_snapshot_reset(grid_dev g, const fields_dev *__restrict__ F);
+__global__ void k_snapshot_reset(grid_dev g, const fields_dev *__restrict__ F, uint8_t *lay, int *inl);
 __global__ void k_reset_extraps(grid_dev g, const fields_dev *__restrict__ F);
 __global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t *lay, int *inl);
 __global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int from_primary, uint8_t *lay, int *inl,
