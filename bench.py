@@ -51,28 +51,58 @@ def config_block(n, l2):
 # ---------------------------------------------------------------------------
 # reference arm: the reference's own run_sim on the host cores
 # ---------------------------------------------------------------------------
-def reference_run(n, steps, procs):
-    """Run `procs` copies of the reference run_sim, `steps` steps each; returns
-    (cell-steps/s aggregate, per-process stepper seconds)."""
-    wd = tempfile.mkdtemp(prefix="rmt3d_ref_")
+def _run_sim_batch(n, steps, procs, wd, tag):
+    """`procs` concurrent copies of the reference run_sim, `steps` steps each:
+    per-process stepper seconds and the phase report of the slowest one."""
     cfgs = []
     for p in range(procs):
-        c = os.path.join(wd, "w%d.cfg" % p)
+        c = os.path.join(wd, "%s%d.cfg" % (tag, p))
         scenes.write(c, workload_cfg(n, steps))
         cfgs.append(c)
-    t0 = time.time()
     ps = [subprocess.Popen([RUN_SIM, c], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True, cwd=wd)
           for c in cfgs]
-    secs = []
+    secs, outs = [], []
     for pr in ps:
         out, _ = pr.communicate()
         m = re.search(r"Stepper: Done with everything, took a total\s+([0-9.eE+-]+) seconds", out)
         if pr.returncode != 0 or not m:
             raise RuntimeError("reference run_sim failed:\n" + out[-2000:])
         secs.append(float(m.group(1)))
-    wall = time.time() - t0
+        outs.append(out)
+    return secs, outs[secs.index(max(secs))]
+
+
+def phase_report(out):
+    """The reference's own phase timers (fluid_3d::watch, printed by run_sim
+    at exit; they include the set-up's pressure pre-iterations), as shares of
+    its tracked compute time."""
+    tot = re.search(r"F3d report:\s*#\s*Total tracked compute time\s+([0-9.eE+-]+) s", out)
+    if not tot:
+        return None
+    total = float(tot.group(1))
+    rep = {"tracked_s": total}
+    for name in ("Extrapolation", "Pressure Poisson", "Communication", "Stresses", "MAC"):
+        m = re.search(r"#\s+%s time\s+([0-9.eE+-]+) s" % name, out)
+        if m:
+            rep[name.lower().replace(" ", "_") + "_share"] = float(m.group(1)) / total if total else None
+    return rep
+
+
+def reference_run(n, steps, procs, warmup=0):
+    """Run `procs` copies of the reference run_sim; returns (cell-steps/s
+    aggregate over steps warmup+1 .. warmup+steps, per-process seconds of that
+    window, the slowest process's phase report).  The window is timed as the
+    difference of a (warmup+steps)-step run and a warmup-step run of the same
+    scene, both with the reference's stepper timer (set-up excluded)."""
+    wd = tempfile.mkdtemp(prefix="rmt3d_ref_")
+    long_s, out = _run_sim_batch(n, warmup + steps, procs, wd, "a")
+    if warmup > 0:
+        short_s, _ = _run_sim_batch(n, warmup, procs, wd, "b")
+        secs = [max(1e-9, a - b) for a, b in zip(sorted(long_s), sorted(short_s))]
+    else:
+        secs = long_s
     cellsteps = procs * steps * n ** 3
-    return cellsteps / max(secs), secs, wall
+    return cellsteps / max(secs), secs, phase_report(out)
 
 
 def host_cores():
@@ -91,16 +121,19 @@ def run_reference(args):
         return
     procs = max(1, min(host_cores(), args.ref_procs))
     steps = max(1, args.ref_steps)
-    rate, secs, wall = reference_run(args.size, steps, procs)
+    warm = max(0, args.warmup)
+    rate, secs, phases = reference_run(args.size, steps, procs, warm)
     value = rate / 1e6
-    sample = "%d processes x %d steps of the %d^3 workload (reference stepper timer; set-up and the 5 pressure pre-iterations excluded)" % (
-        procs, steps, args.size)
+    sample = ("%d processes x steps %d..%d of the %d^3 workload (the reference's stepper timer: a %d-step run "
+              "minus a %d-step run; set-up and the 5 pressure pre-iterations excluded)" % (
+                  procs, warm + 1, warm + steps, args.size, warm + steps, warm))
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * max(secs) / steps,
+        "steps": steps, "warmup": warm, "ms_per_step": 1000 * max(secs) / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_block(args.size, "n/a (CPU)"),
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": procs, "kind": "reference", "sample": sample,
+                         "phases": phases},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -127,6 +160,15 @@ class ClockSampler:
                                       stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+            return self
+        # nvidia-smi takes a moment to start: the timed work begins after its
+        # first sample (at most a few seconds of waiting)
+        t0 = time.time()
+        while time.time() - t0 < 5 and self.p.poll() is None:
+            self.f.flush()
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *a):
@@ -184,22 +226,35 @@ def percentiles(xs):
     return {"p50": float(np.percentile(xs, 50)), "p99": float(np.percentile(xs, 99))}
 
 
-def form_batched(R, args):
-    """Many independent seeded scenes (grid sizes from {32,48,64,96}, 1-8
-    spheres with solid density U(0.8,1.2), lid speed U(0.5,1.5)),
-    variable-density projection, mixed precision, schedules autotuned per
-    grid size; every scene's step graph in flight at once.  Wall time around
-    the synchronous batch step (the scenes run on their own streams)."""
-    import numpy as np
+def _batch_descs(R, args, precision):
     wd = tempfile.mkdtemp(prefix="rmt3d_batch_")
     descs, cells = [], 0
     for seed in range(args.batch_scenes):
         n, text = scenes.random_scene(seed, steps=100000)
         d = R.desc_from_cfg(scenes.write(os.path.join(wd, "s%d.cfg" % seed), text))
-        d.precision = R.MIXED
+        d.precision = precision
         d.var_den = 1  # solid densities U(0.8, 1.2): the variable-density projection
         descs.append(d)
         cells += n ** 3
+    return descs, cells
+
+
+def _batch_fields(b, n):
+    import numpy as np
+    sl = (slice(2, -2),) * 3
+    return [(np.stack([b.field(i, f)[sl] for f in "uvw"]), b.field(i, "p")[sl]) for i in range(n)]
+
+
+def form_batched(R, args):
+    """Many independent seeded scenes (grid sizes from {32,48,64,96}, 1-8
+    spheres with solid density U(0.8,1.2), lid speed U(0.5,1.5)),
+    variable-density projection, mixed precision, schedules autotuned per
+    kind of scene; every group's step graph in flight at once.  Wall time
+    around the synchronous batch step (the scenes run on their own streams).
+    After the timed steps every scene is stepped on to `batch_check_steps`
+    steps and compared with the same batch run in plain FP64."""
+    import numpy as np
+    descs, cells = _batch_descs(R, args, R.MIXED)
     t0 = time.perf_counter()
     b = R.Batch(descs)
     b.prepare()
@@ -213,12 +268,34 @@ def form_batched(R, args):
     wall = time.perf_counter() - t0
     if any(st):
         raise RuntimeError("batched step status %s" % st)
-    b.close()
-    return {"value": cells * args.steps / wall / 1e6, "unit": METRIC, "scenes": len(descs), "cells": cells,
-            "ms_per_batch_step": 1e3 * wall / args.steps, "timing": "wall clock around the synchronous batch step",
-            "prepare_s": prep, "schedules": {str(k): list(v) for k, v in tuned.items()},
-            "workload": "seeded cavities, n in {32,48,64,96}, 1-8 spheres R~U(0.08,0.15), G log-U[0.1,10], "
-                        "lid U(0.5,1.5), solid density U(0.8,1.2) (variable-density projection), mixed precision"}
+    out = {"value": cells * args.steps / wall / 1e6, "unit": METRIC, "scenes": len(descs), "cells": cells,
+           "ms_per_batch_step": 1e3 * wall / args.steps, "timing": "wall clock around the synchronous batch step",
+           "prepare_s": prep, "schedules": {str(k): list(v) for k, v in tuned.items()},
+           "workload": "seeded cavities, n in {32,48,64,96}, 1-8 spheres R~U(0.08,0.15), G log-U[0.1,10], "
+                       "lid U(0.5,1.5), solid density U(0.8,1.2) (variable-density projection), mixed precision"}
+    total = args.batch_check_steps
+    if total > args.warmup + args.steps:
+        st = b.step(total - args.warmup - args.steps)
+        if any(st):
+            raise RuntimeError("batched status %s" % st)
+        mixed = _batch_fields(b, len(descs))
+        b.close()
+        d64, _ = _batch_descs(R, args, R.FP64)
+        b64 = R.Batch(d64)
+        b64.prepare()
+        st = b64.step(total)
+        if any(st):
+            raise RuntimeError("FP64 batch status %s" % st)
+        ref = _batch_fields(b64, len(descs))
+        b64.close()
+        ev = [float(np.linalg.norm(m[0] - r[0]) / np.linalg.norm(r[0])) for m, r in zip(mixed, ref)]
+        ep = [float(np.linalg.norm(m[1] - r[1]) / np.linalg.norm(r[1])) for m, r in zip(mixed, ref)]
+        out["rel_l2_vs_fp64"] = {"steps": total, "velocity_max": max(ev), "p_max": max(ep),
+                                 "velocity_median": float(np.median(ev)), "p_median": float(np.median(ep)),
+                                 "reference": "the same 64 scenes as an FP64 batch (plain form) after the same steps"}
+    else:
+        b.close()
+    return out
 
 
 def form_stretched(R, args):
@@ -301,9 +378,10 @@ def form_served(R, args):
             "serial_fp64": {"value": summ_s["cellsteps_per_s"] / 1e6, "wall_s": summ_s["wall_s"],
                             "step_latency_ms": {"p50": summ_s["step_p50_ms"], "p99": summ_s["step_p99_ms"]}},
             "cellsteps": cells,
-            "workload": "Poisson arrivals 20/s for %g s, n in {32,64,128,192} 4:3:2:1, %d steps each (set-up "
+            "workload": "Poisson arrivals 20/s for %g s (the served workload's 60 s stream cut to its first %g s "
+                        "so that the run ends in minutes), n in {32,64,128,192} 4:3:2:1, %d steps each (set-up "
                         "included in the latency), mixed precision; serial_fp64 = the same stream one request at "
-                        "a time in FP64" % (args.serve_seconds, args.serve_steps)}
+                        "a time in FP64" % (args.serve_seconds, args.serve_seconds, args.serve_steps)}
 
 
 def run_ours(args):
@@ -334,14 +412,15 @@ def run_ours(args):
     def max_over_ranks(x):
         return reduce_max(dist, x)
 
-    def make(precision):
+    def make(precision, tuned=None):
         d = R.desc_from_cfg(cfg)
         d.precision = precision
-        # the multigrid schedule chosen by the project's autotuner (timing
-        # candidates on a probe copy of the scene)
-        b = R.Batch([d], host_threads=1)
-        tuned = list(b.autotune(probe_steps=3).values())[0]
-        b.close()
+        if tuned is None:
+            # the multigrid schedule chosen by the project's autotuner (timing
+            # candidates on a probe copy of the scene)
+            b = R.Batch([d], host_threads=1)
+            tuned = list(b.autotune(probe_steps=3).values())[0]
+            b.close()
         sc = R.Scene(d, stream=stream.cuda_stream)
         sc.set_schedule(tuned[0], tuned[1], 0)
         sc.set_mg_launch(tuned[2])
@@ -401,57 +480,73 @@ def run_ours(args):
         return max_over_ranks(start.elapsed_time(stop))
 
     cells = n ** 3
-    # plain FP64 form
-    s64 = make(R.FP64)
-    with ClockSampler(local) as clk:
+    clk = ClockSampler(local)
+    clk.__enter__()  # sampled over every timed region below
+    try:
+        # plain FP64 form
+        s64 = make(R.FP64)
         ms64, launches64 = timed(s64, args.steps)
+        v64 = replica_value(world, cells, args.steps, ms64)
+        lat64 = step_latency(s64, max(5, args.steps // 2))
+        # mixed form (FP32 V-cycles inside FP64 iterative refinement)
+        smx = make(R.MIXED)
+        msmx, launchesmx = timed(smx, args.steps)
+        vmx = replica_value(world, cells, args.steps, msmx)
+        latmx = step_latency(smx, max(5, args.steps // 2))
+        # both scenes have now run the same number of steps from the same state
+        steps_compared = args.warmup + args.steps + max(5, args.steps // 2)
+        sl = (slice(2, -2),) * 3
+        errs = {}
+        for f in ("u", "v", "w", "p"):
+            a, b = s64.field(f)[sl], smx.field(f)[sl]
+            errs[f] = float(np.linalg.norm(b - a) / np.linalg.norm(a))
+        va = np.stack([s64.field(f)[sl] for f in "uvw"])
+        vb = np.stack([smx.field(f)[sl] for f in "uvw"])
+        errs["velocity"] = float(np.linalg.norm(vb - va) / np.linalg.norm(va))
+        # the 1e-5 budget on the velocity field and the pressure (v alone is a
+        # near-zero cross-flow whose own norm magnifies round-off; reported too)
+        mixed_ok = max(errs["velocity"], errs["p"]) <= 1e-5
+        head_form = "mixed" if (mixed_ok and vmx > v64) else "fp64"
+        value = vmx if head_form == "mixed" else v64
+        ms = msmx if head_form == "mixed" else ms64
+        launches = launchesmx if head_form == "mixed" else launches64
+        shp = (s64.so4, s64.sn4, s64.sm4)
+        bufs = [torch.empty(shp, dtype=torch.float64, pin_memory=True) for _ in range(4)]
+        sce = smx if head_form == "mixed" else s64
+        roof = roofline(R, sce, args)
+        head_schedule = tuple(sce.schedule)
+        for s_ in (s64, smx):
+            s_.close()
+        # end to end on the same step window as `value`: a fresh scene of the
+        # headline form, the same warm-up, then the same K steps through the
+        # public API with host buffers
+        sce = make(R.MIXED if head_form == "mixed" else R.FP64, tuned=head_schedule)
+        if sce.run(args.warmup) != R.NORMAL_EXIT:
+            raise RuntimeError("warm-up step failed")
+        mse = e2e(sce, args.steps, bufs)
+        ve = replica_value(world, cells, args.steps, mse)
+        d2h = 4 * sce.ncell * 8
+        sce.close()
+        batched = served = stretched = None
+        if world == 1 and not args.no_batched:
+            batched = form_batched(R, args)
+        if world == 1 and not args.no_stretched:
+            stretched = form_stretched(R, args)
+        if world == 1 and not args.no_served:
+            served = form_served(R, args)
+    finally:
+        clk.__exit__()
     clocks = clk.summary()
-    v64 = replica_value(world, cells, args.steps, ms64)
-    lat64 = step_latency(s64, max(5, args.steps // 2))
-    # mixed form (FP32 V-cycles inside FP64 iterative refinement)
-    smx = make(R.MIXED)
-    msmx, launchesmx = timed(smx, args.steps)
-    vmx = replica_value(world, cells, args.steps, msmx)
-    latmx = step_latency(smx, max(5, args.steps // 2))
-    # both scenes have now run the same number of steps from the same state
-    sl = (slice(2, -2),) * 3
-    errs = {}
-    for f in ("u", "v", "w", "p"):
-        a, b = s64.field(f)[sl], smx.field(f)[sl]
-        errs[f] = float(np.linalg.norm(b - a) / np.linalg.norm(a))
-    va = np.stack([s64.field(f)[sl] for f in "uvw"])
-    vb = np.stack([smx.field(f)[sl] for f in "uvw"])
-    errs["velocity"] = float(np.linalg.norm(vb - va) / np.linalg.norm(va))
-    # the 1e-5 budget on the velocity field and the pressure (v alone is a
-    # near-zero cross-flow whose own norm magnifies round-off; reported too)
-    mixed_ok = max(errs["velocity"], errs["p"]) <= 1e-5
-    head_form = "mixed" if (mixed_ok and vmx > v64) else "fp64"
-    value = vmx if head_form == "mixed" else v64
-    ms = msmx if head_form == "mixed" else ms64
-    launches = launchesmx if head_form == "mixed" else launches64
-    shp = (s64.so4, s64.sn4, s64.sm4)
-    bufs = [torch.empty(shp, dtype=torch.float64, pin_memory=True) for _ in range(4)]
-    sce = smx if head_form == "mixed" else s64
-    mse = e2e(sce, args.steps, bufs)
-    ve = replica_value(world, cells, args.steps, mse)
-    d2h = 4 * s64.ncell * 8
-    roof = roofline(R, sce, args)
-    for s_ in (s64, smx):
-        s_.close()
-    batched = served = stretched = None
-    if world == 1 and not args.no_batched:
-        batched = form_batched(R, args)
-    if world == 1 and not args.no_stretched:
-        stretched = form_stretched(R, args)
-    if world == 1 and not args.no_served:
-        served = form_served(R, args)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and os.path.exists(RUN_SIM):
         procs = max(1, min(host_cores(), args.ref_procs))
-        rate, secs, wall = reference_run(n, max(1, args.ref_steps), procs)
+        rate, secs, phases = reference_run(n, max(1, args.ref_steps), procs, max(0, args.warmup))
         cpu = {"value": rate / 1e6, "unit": METRIC, "cores": procs, "kind": "reference",
-               "sample": "%d processes x %d steps of the %d^3 workload, reference run_sim stepper timer" % (
-                   procs, args.ref_steps, n)}
+               "sample": "%d processes x steps %d..%d of the %d^3 workload, the reference run_sim's stepper "
+                         "timer (a %d-step run minus a %d-step run)" % (
+                   procs, args.warmup + 1, args.warmup + args.ref_steps, n, args.warmup + args.ref_steps,
+                   args.warmup),
+               "phases": phases}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -464,7 +559,7 @@ def run_ours(args):
                                "step_latency_ms": lat64, "schedule": list(s64.schedule)},
                       "mixed": {"value": vmx, "ms_per_step": msmx / args.steps, "gpu_launches": launchesmx,
                                 "step_latency_ms": latmx, "rel_l2_vs_fp64": errs, "schedule": list(smx.schedule),
-                                "steps_compared": 2 * args.warmup + args.steps + max(5, args.steps // 2)},
+                                "steps_compared": steps_compared},
                       "batched": batched, "served": served, "stretched": stretched},
             "e2e": {"value": ve, "unit": METRIC, "h2d_bytes_per_step": 8, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
@@ -531,8 +626,9 @@ def main():
     ap.add_argument("--stretch-size", type=int, default=128)
     ap.add_argument("--stretch-steps", type=int, default=20)
     ap.add_argument("--batch-scenes", type=int, default=64)
-    ap.add_argument("--serve-seconds", type=float, default=3.0)
-    ap.add_argument("--serve-steps", type=int, default=20)
+    ap.add_argument("--serve-seconds", type=float, default=1.5)
+    ap.add_argument("--serve-steps", type=int, default=100)
+    ap.add_argument("--batch-check-steps", type=int, default=100)
     ap.add_argument("--serve-slots", type=int, default=16)
     args = ap.parse_args()
     if args.impl == "reference":

@@ -324,10 +324,14 @@ int rmt3d_write_slice(rmt3d_scene *s, int type, int dim, int point, int obj_id, 
  * pointers).  The scratch is a fixed array inside the library sized for at
  * most 274,625 FEM nodes (65^3, a 64^3 box with walls); larger grids return
  * RMT3D_ERR_TOO_LARGE.  No cudaMalloc/cudaFree or allocating library call is
- * made.  The first call on a device looks the array's device address up
- * (cudaGetSymbolAddress), so make that first call outside any stream capture.
- * Every call shares the array: calls that overlap on the GPU race.
- *   dvel[3]: du, dv, dw over the ghosted box (sys_size+4 per axis);
+ * made.  Each call looks the array's device address up on the current device
+ * (cudaGetSymbolAddress), copies its argument block from host memory and
+ * waits for `stream` before returning the value: the call is synchronous and
+ * must not be issued on a stream that is capturing.  Every call shares the
+ * array: calls that overlap on the GPU race.
+ *   dvel[3]: du, dv, dw over the ghosted box (sys_size+4 per axis), with the
+ *   two ghost layers filled as the step leaves them (on a periodic axis they
+ *   hold the periodic images, which the FEM right-hand side reads);
  *   face_normal_vel[6]: for each wall face f, fvel[f][f/2] over the same box
  *   (may be NULL for periodic faces); dt_basis: the dt the FEM basis was built
  *   with (dt_reg); stream: cudaStream_t or 0; norm_out: host result. */

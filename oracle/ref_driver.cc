@@ -12,6 +12,14 @@
  *   the nine phase groups of fluid_3d::step_forward (fluid_3d.cc:429-577),
  *   calling the same members in the same order, and writes <prefix>_P<k>.bin
  *   after group k.
+ *        ref_driver <file.cfg> <steps> <prefix> fields <k1,k2,...>
+ *   steps the scene with stepper::step (the body of stepper::run's loop) and
+ *   writes <prefix>_s<k>.f64 after step k for every listed k <= steps: the
+ *   compact form below (velocity components and pressure only), for large
+ *   grids whose full state would be hundreds of MB per dump.
+ *
+ * Compact layout: char[4] "RMTF"; int32 version=1; int32 m,n,o, sm4,sn4,so4,
+ *   steps_done; double dt, time; then u, v, w, p as double[sm4*sn4*so4] each.
  *
  * Output layout (little endian):
  *   char[4] "RMTD"; int32 version=1;
@@ -67,6 +75,27 @@ static void dump(fluid_3d &f3d, int steps_done, const char *fn) {
     fclose(fh);
 }
 
+static void dump_fields(fluid_3d &f3d, int steps_done, const char *fn) {
+    FILE *fh = fopen(fn, "wb");
+    if (!fh) {
+        perror(fn);
+        exit(1);
+    }
+    const int ncell = f3d.sm4 * f3d.sn4 * f3d.so4;
+    fwrite("RMTF", 1, 4, fh);
+    int hdr[8] = {1, f3d.m, f3d.n, f3d.o, f3d.sm4, f3d.sn4, f3d.so4, steps_done};
+    fwrite(hdr, sizeof(int), 8, fh);
+    double sc[2] = {f3d.dt, f3d.time};
+    fwrite(sc, sizeof(double), 2, fh);
+    double *buf = new double[ncell];
+    for (int c = 0; c < 4; c++) {
+        for (int i = 0; i < ncell; i++) buf[i] = c < 3 ? f3d.u_mem[i].vel[c] : f3d.u_mem[i].p;
+        fwrite(buf, sizeof(double), ncell, fh);
+    }
+    delete[] buf;
+    fclose(fh);
+}
+
 int main(int argc, char *argv[]) {
     MPI_Init(&argc, &argv);
     if (argc < 4) {
@@ -87,6 +116,33 @@ int main(int argc, char *argv[]) {
     f3d.dt = sim.dt;
     f3d.init_iter(init_err);
 
+    if (argc > 5 && strcmp(argv[4], "fields") == 0) {
+        // the wanted step counts, ascending
+        bool want[1 << 16] = {false};
+        for (char *t = strtok(argv[5], ","); t; t = strtok(nullptr, ",")) {
+            const int k = atoi(t);
+            if (k >= 0 && k < (1 << 16)) want[k] = true;
+        }
+        char fn[1024];
+        f3d.set_dt(sim.dt);
+        if (want[0]) {
+            snprintf(fn, sizeof(fn), "%s_s0.f64", argv[3]);
+            dump_fields(f3d, 0, fn);
+        }
+        for (int k = 1; k <= nsteps; k++) {
+            const int err = sim.step(f3d);
+            if (err != NORMAL_EXIT) {
+                fprintf(stderr, "ref_driver: step %d returned %d\n", k, err);
+                return 2;
+            }
+            if (want[k]) {
+                snprintf(fn, sizeof(fn), "%s_s%d.f64", argv[3], k);
+                dump_fields(f3d, k, fn);
+            }
+        }
+        printf("# ref_driver: V-cycles fem %ld mac %ld\n", f3d.mg_pres->ncycles, f3d.mg_mac->ncycles);
+        return 0;
+    }
     const bool phases = argc > 4 && strcmp(argv[4], "phases") == 0;
     double t0 = MPI_Wtime();
     if (nsteps > 0) sim.run(f3d);

@@ -3,14 +3,16 @@
 Test infrastructure: returns the reference's AoS arrays (struct field and
 struct ref_map, F3D_Source/fields.hh:34-646) and the extrapolated-map list.
 """
+import os
+import sys
+
 import numpy as np
 
-FIELD_DT = np.dtype([("vel", "<f8", 3), ("p", "<f8"), ("dp", "<f8"), ("q", "<f8"), ("dvel", "<f8", 3),
-                     ("nv_der", "<f8", (3, 3)), ("fvel", "<f8", (6, 3)), ("sigma", "<f8", (3, 3))])
-REFMAP_DT = np.dtype([("c", "<u4"), ("pad", "<u4"), ("x", "<f8", 3), ("xpred", "<f8", 3), ("nv_der", "<f8", (3, 3)),
-                      ("fx", "<f8", (6, 3)), ("sigma", "<f8", (3, 3)), ("elastic_energy", "<f8", 3),
-                      ("detF", "<f8", 3), ("grad_phi", "<f8", (3, 3)), ("act_power", "<f8", 3)])
-assert FIELD_DT.itemsize == 360 and REFMAP_DT.itemsize == 488
+_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if _ROOT not in sys.path:
+    sys.path.insert(0, _ROOT)
+
+from rmt3d_b200.layout import FIELD_DT, REFMAP_DT  # noqa: E402  (the records the dump holds)
 
 
 def read(path):
@@ -32,3 +34,21 @@ def read(path):
     ext = np.frombuffer(raw, rec, n_ext, off).copy()
     return {"m": m, "n": n, "o": o, "shape": (so4, sn4, sm4), "steps": steps, "dt": float(dt), "time": float(time),
             "fields": fields, "refmaps": refmaps, "ext_index": ext["index"].copy(), "ext_maps": ext["map"].copy()}
+
+
+def read_fields(path):
+    """A compact dump (ref_driver ... fields k1,k2,...): dt, time and the
+    velocity components and pressure over the ghosted box, as
+    {"shape": (so4, sn4, sm4), "steps", "dt", "time", "u", "v", "w", "p"}."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    assert raw[:4] == b"RMTF", "not a compact oracle dump"
+    ver, m, n, o, sm4, sn4, so4, steps = [int(v) for v in np.frombuffer(raw, "<i4", 8, 4)]
+    assert ver == 1
+    dt, time = np.frombuffer(raw, "<f8", 2, 36)
+    nc = sm4 * sn4 * so4
+    arr = np.frombuffer(raw, "<f8", 4 * nc, 52).reshape(4, so4, sn4, sm4)
+    out = {"m": m, "n": n, "o": o, "shape": (so4, sn4, sm4), "steps": steps, "dt": float(dt), "time": float(time)}
+    for c, name in enumerate("uvwp"):
+        out[name] = arr[c].copy()
+    return out

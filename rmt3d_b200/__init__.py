@@ -170,7 +170,7 @@ class Scene:
 
     def export_reference(self):
         """State in the reference's AoS layout: (fields, refmaps, ext_index, ext_maps)."""
-        from oracle.refdump import FIELD_DT, REFMAP_DT
+        from .layout import FIELD_DT, REFMAP_DT
         fields = np.zeros(self.ncell, dtype=FIELD_DT)
         rm = np.zeros(self.ncell, dtype=REFMAP_DT)
         n = ctypes.c_int()

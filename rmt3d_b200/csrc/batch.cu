@@ -34,7 +34,8 @@ struct rmt3d_batch {
     std::vector<rmt3d_scene_desc> descs;
     std::vector<std::vector<int>> groups;  // scene indices per host thread
     std::vector<int> status;
-    std::map<int, std::array<int, 3>> tuned;  // grid cells -> (v_down, v_up, cluster launch)
+    // grid shape, periodicity, precision and density form -> (v_down, v_up, cluster launch)
+    std::map<std::array<int, 8>, std::array<int, 3>> tuned;
     int nthreads = 1;
     // equally sized scenes stepped together: one graph per group, each
     // multigrid solve batched over the group's scenes
@@ -45,6 +46,13 @@ struct rmt3d_batch {
 };
 
 namespace {
+// what a tuned schedule is keyed on: the scenes build_groups may put together
+// share it (grid shape, periodicity, precision, density form)
+std::array<int, 8> tune_key(const rmt3d_scene_desc &d) {
+    return {d.sys_size[0], d.sys_size[1], d.sys_size[2], d.periodic[0], d.periodic[1], d.periodic[2],
+            d.precision, d.var_den};
+}
+
 void drop_groups(rmt3d_batch *b) {
     for (auto *g : b->sg) rmt3d::group_destroy(g);
     b->sg.clear();
@@ -59,7 +67,7 @@ int build_groups(rmt3d_batch *b) {
     std::map<std::vector<double>, std::vector<int>> part;
     for (size_t i = 0; i < b->scenes.size(); i++) {
         const rmt3d_scene_desc &d = b->descs[i];
-        auto it = b->tuned.find((int)((long long)d.sys_size[0] * d.sys_size[1] * d.sys_size[2]));
+        auto it = b->tuned.find(tune_key(d));
         const int vd = it != b->tuned.end() ? it->second[0] : 2, vu = it != b->tuned.end() ? it->second[1] : 2;
         std::vector<double> key = {(double)d.sys_size[0], (double)d.sys_size[1], (double)d.sys_size[2],
                                    (double)d.periodic[0], (double)d.periodic[1], (double)d.periodic[2],
@@ -238,19 +246,22 @@ extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
     return RMT3D_OK;
 }
 
-// Autotune the multigrid smoothing counts per grid size: for each distinct
-// size in the batch, a probe copy of the first scene of that size is set up
-// and stepped `probe_steps` times per candidate; the fastest candidate is
-// applied to every scene of that size.  tuned_out (optional, 3 ints per
-// distinct size: cells, v_down, v_up) receives the choices.
+// Autotune the multigrid schedule per kind of scene (grid shape,
+// periodicity, precision and density form, the keys build_groups groups by):
+// a probe copy of the first scene of each kind is set up and stepped
+// `probe_steps` times per candidate -- smoothing counts (v_down, v_up) and
+// the cluster or per-phase launch of the solves -- and the fastest candidate
+// that ran without error is applied to every scene of that kind.  tuned_out
+// (optional, 4 ints per kind: cells, v_down, v_up, cluster launch) receives
+// the choices.
 extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
     drop_groups(b);
     static const int smooth[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
-    std::map<long long, int> first;
+    std::map<std::array<int, 8>, int> first;
     for (size_t i = 0; i < b->descs.size(); i++)
-        if (!first.count(cells(b->descs[i]))) first[cells(b->descs[i])] = (int)i;
+        if (!first.count(tune_key(b->descs[i]))) first[tune_key(b->descs[i])] = (int)i;
     int written = 0;
     for (auto &kv : first) {
         rmt3d_scene *probe = nullptr;
@@ -270,13 +281,13 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
                     return e;
                 }
                 int st = 0;
-                rmt3d_run(probe, 1, &st);  // settle the cycle predictor, build the graph
-                rmt3d_sync(probe);
+                // settle the cycle predictor, build the graph
+                if (rmt3d_run(probe, 1, &st) || rmt3d_sync(probe) || st) continue;
                 auto t0 = std::chrono::steady_clock::now();
-                rmt3d_run(probe, probe_steps, &st);
-                rmt3d_sync(probe);
+                const int er = rmt3d_run(probe, probe_steps, &st);
+                const int es = rmt3d_sync(probe);
                 double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-                if (st == 0 && dt < best) {
+                if (er == 0 && es == 0 && st == 0 && dt < best) {
                     best = dt;
                     bd = c[0];
                     bu = c[1];
@@ -284,14 +295,14 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
                 }
             }
         rmt3d_scene_destroy(probe);
-        b->tuned[(int)kv.first] = {bd, bu, bc};
+        b->tuned[kv.first] = {bd, bu, bc};
         for (size_t i = 0; i < b->descs.size(); i++)
-            if (cells(b->descs[i]) == kv.first) {
+            if (tune_key(b->descs[i]) == kv.first) {
                 if ((e = rmt3d_scene_set_schedule(b->scenes[i], bd, bu, 0))) return e;
                 if ((e = rmt3d_scene_set_mg_launch(b->scenes[i], bc))) return e;
             }
         if (tuned_out && written < max_out) {
-            tuned_out[4 * written] = (int)kv.first;
+            tuned_out[4 * written] = (int)cells(b->descs[kv.second]);
             tuned_out[4 * written + 1] = bd;
             tuned_out[4 * written + 2] = bu;
             tuned_out[4 * written + 3] = bc;

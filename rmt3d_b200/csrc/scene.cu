@@ -2750,26 +2750,17 @@ static_assert(kNoallocRed + (1 + kMeanBlocks) * sizeof(double) <= kNoallocHeader
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
 
 namespace {
-std::mutex g_noalloc_mu;
-std::vector<unsigned char *> g_noalloc_addr;  // per device, set up on first use
-
 // Device address of the scratch array for the current device.  The symbol's
 // name in host code is only a host-side stand-in, so the address is looked up
-// once per device with that device current.
+// with the device current, on every call: the lookup is cheap next to the
+// call's own synchronisation, and a cached address would go stale if the
+// host reset the device and the module were loaded again.
 int noalloc_scratch(unsigned char **out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail(RMT3D_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if ((int)g_noalloc_addr.size() <= dev) g_noalloc_addr.resize(dev + 1, nullptr);
-    if (!g_noalloc_addr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(RMT3D_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_noalloc_addr[dev] = (unsigned char *)p;
-    }
-    *out = g_noalloc_addr[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(RMT3D_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    *out = (unsigned char *)p;
     return RMT3D_OK;
 }
 }  // namespace

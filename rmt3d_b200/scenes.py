@@ -73,6 +73,27 @@ def multi_sphere(n=24, steps=100, spheres=(), mu=0.01, lid=1.0, wt_n=1.5, nlayer
     return s
 
 
+def ftest(n=16, steps=4, mu=0.01, frames=100000, T=None):
+    """The reference's manufactured-solution fluid test (sim_ftest,
+    Sim/sim_manager.cc:139-178) on a periodic unit box: a Taylor-Green-like
+    velocity decaying as cos(2 pi t) under the matching body force, with the
+    exact solution known at every time (has_exact 1)."""
+    if T is None:
+        T = frames
+    s = _HEAD.format(frames=frames, steps=steps, n=n, T=T, mu=mu).replace("sim_type objects", "sim_type ftest")
+    return s + "has_exact 1\n"
+
+
+def wall_sphere(n=24, steps=4, centre=(0.5, 0.5, 0.17), radius=0.12, wall_dist=0.1, gravity=-5.0, G=1.0,
+                rho=1.0, frames=100000, T=None):
+    """Lid-driven cavity with a sphere close to the bottom wall under gravity:
+    the wall repulsion (sim_objects::solid_acceleration, Sim/sim_manager.cc:
+    212-295, active within wall_dist of a wall) and the gravity of the solid
+    and of the fluid act from the first step."""
+    s = cavity_sphere(n, steps, G=G, rho=rho, radius=radius, centre=centre, frames=frames, T=T)
+    return s + "wall_dist %r\ngravity %r\n" % (wall_dist, gravity)
+
+
 def random_scene(seed, sizes=(32, 48, 64, 96), nobj=(1, 8), steps=100, mu=0.01):
     """One seeded multi-sphere cavity scene: radii U(0.08,0.15), centres
     rejection-sampled without overlap and at least 2 dx apart, G log-uniform in

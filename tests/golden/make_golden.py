@@ -9,7 +9,8 @@ extrapolated maps.  The oracle's Poisson solves run with RMT3D_SHIM_EXACT=1
 residual-tolerance noise.  Usage (in the build container, where the reference
 is present):
 
-    make -C oracle all nofma && make -C oracle VARDEN=1 all nofma
+    make -C oracle REF_DIR=<reference checkout> all nofma
+    make -C oracle REF_DIR=<reference checkout> VARDEN=1 all nofma
     python tests/golden/make_golden.py [case ...]
 
 The output case out16 holds the files the reference's stepper writes for the
@@ -46,6 +47,7 @@ from oracle import refdump  # noqa: E402
 from rmt3d_b200 import scenes  # noqa: E402
 
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+RUN_SIM = os.path.join(ROOT, "oracle", "_ref", "run_sim")
 # the reference rebuilt without FMA contraction (make -C oracle nofma)
 DRIVER_NOFMA = os.path.join(ROOT, "oracle", "_ref", "nofma", "ref_driver")
 
@@ -67,6 +69,11 @@ CASES = {
     # stress between the two solids is active from the first step
     "collide24": (scenes.multi_sphere(24, 4, spheres=[((0.29, 0.5, 0.5), 0.2, 1.0, 1.0),
                                                     ((0.71, 0.5, 0.5), 0.2, 2.0, 1.0)]), [0, 1, 4]),
+    # a sphere 0.05 above the bottom wall under gravity: wall repulsion and
+    # the gravity of solid and fluid (sim_manager.cc:212-295, sim_manager.hh:400-404)
+    "wall24": (scenes.wall_sphere(24, 4), [0, 1, 4]),
+    # the manufactured solution (sim_ftest) on a periodic box, with its body force
+    "ftest16": (scenes.ftest(16, 4), [0, 1, 4]),
 }
 # longer runs stored as interior (u, v, w, p) only
 LONG = {
@@ -256,6 +263,31 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
 
 
+def envelope_parts(cfg_text, steps, base, workdir, varden=False):
+    """The two parts of the rounding envelope, each as the rel-L2 change of
+    (velocity vector, pressure, reference map) against the fixture state:
+    (build without FMA contraction, exact solves), (the reference's own
+    residual-tolerance multigrid control, FMA build); plus the first one's
+    state (the no-FMA exact-mode reference)."""
+    shp = base["shape"]
+    sl = (slice(2, -2),) * 3
+    vb = base["fields"]["vel"].reshape(shp + (3,))[sl]
+    pb = base["fields"]["p"].reshape(shp)[sl]
+    x_b = base["refmaps"]["x"][base["refmaps"]["c"] != 0]
+    parts, nofma = [], None
+    drivers = ((DRIVER_VD_NOFMA, "1"), (DRIVER_VD, "0")) if varden else ((DRIVER_NOFMA, "1"), (DRIVER, "0"))
+    for drv, ex in drivers:
+        d = run(cfg_text, steps, workdir, drv, ex)
+        if nofma is None:
+            nofma = d
+        v = d["fields"]["vel"].reshape(shp + (3,))[sl]
+        p = d["fields"]["p"].reshape(shp)[sl]
+        x_d = d["refmaps"]["x"][d["refmaps"]["c"] != 0]
+        xe = _rel(x_d, x_b) if x_b.shape == x_d.shape and x_b.size else 0.0
+        parts.append(np.array([_rel(v, vb), _rel(p, pb), xe]))
+    return parts[0], parts[1], nofma
+
+
 def envelope(cfg_text, steps, base, workdir, varden=False):
     """Rounding envelope of the reference at this state: the largest rel-L2
     change of (velocity vector, pressure, reference map) between the fixture
@@ -279,9 +311,23 @@ def envelope(cfg_text, steps, base, workdir, varden=False):
     return env
 
 
+def runsim_error(cfg_text, workdir):
+    """The reference run_sim's own exact-solution report (Execs/run_sim.cc:
+    144-158: fluid_3d::error after the run): T, dh, dt and the mean squared
+    errors of u, v, w, p, as printed (%13.10f)."""
+    cfg = os.path.join(workdir, "err.cfg")
+    with open(cfg, "w") as fh:
+        fh.write(cfg_text)
+    env = dict(os.environ, RMT3D_SHIM_EXACT="1")
+    out = subprocess.run([RUN_SIM, cfg], check=True, capture_output=True, text=True, cwd=workdir, env=env).stdout
+    lines = out.splitlines()
+    i = [j for j, ln in enumerate(lines) if ln.startswith("#T dh dt erru_sq")][0]
+    return np.array([float(v) for v in lines[i + 1].split()])
+
+
 def main():
     if not (os.path.exists(DRIVER) and os.path.exists(DRIVER_NOFMA)):
-        sys.exit("build the reference first: make -C oracle all nofma")
+        sys.exit("build the reference first: make -C oracle REF_DIR=<reference checkout> all nofma")
     with tempfile.TemporaryDirectory() as wd:
         only = sys.argv[1:]
         for name, case in CASES.items():
@@ -294,8 +340,19 @@ def main():
                 d = run(txt, k, wd, DRIVER_VD if varden else DRIVER)
                 for key, val in compact(d).items():
                     arrays["s%d_%s" % (k, key)] = val
-                arrays["s%d_env" % k] = envelope(txt, k, d, wd, varden)
-                print(name, k, "envelope", arrays["s%d_env" % k])
+                envf, envt, dn = envelope_parts(txt, k, d, wd, varden)
+                arrays["s%d_env" % k] = np.maximum(envf, envt)
+                arrays["s%d_envf" % k] = envf
+                arrays["s%d_envt" % k] = envt
+                # the same state from the build without FMA contraction, exact
+                # solves: the rounding the CUDA path (built without contraction)
+                # follows
+                for key, val in compact(dn).items():
+                    arrays["n%d_%s" % (k, key)] = val
+                print(name, k, "envelope (nofma, tolerance)", envf, envt)
+            if "has_exact 1" in txt:
+                arrays["runsim_err"] = runsim_error(txt, wd)
+                print(name, "run_sim exact-solution errors", arrays["runsim_err"])
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
             print("wrote", name)
         if not only or "out16" in only:
@@ -322,9 +379,16 @@ def main():
                 "v": vel[:, 1].reshape(shp)[sl].copy(),
                 "w": vel[:, 2].reshape(shp)[sl].copy(),
                 "p": d["fields"]["p"].reshape(shp)[sl].copy(),
-                "env": envelope(txt, k, d, wd),
             }
-            print(name, "envelope", arrays["env"])
+            envf, envt, dn = envelope_parts(txt, k, d, wd)
+            arrays["env"] = np.maximum(envf, envt)
+            arrays["envf"] = envf
+            arrays["envt"] = envt
+            vn = dn["fields"]["vel"]
+            for c, nm in enumerate("uvw"):
+                arrays["n" + nm] = vn[:, c].reshape(shp)[sl].copy()
+            arrays["np"] = dn["fields"]["p"].reshape(shp)[sl].copy()
+            print(name, "envelope (nofma, tolerance)", envf, envt)
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
             print("wrote", name)
 

@@ -10,7 +10,7 @@ GOLDEN = os.path.join(HERE, "golden")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-from oracle.refdump import FIELD_DT, REFMAP_DT  # noqa: E402
+from rmt3d_b200.layout import FIELD_DT, REFMAP_DT  # noqa: E402
 
 
 def load_fixture(name):
@@ -23,9 +23,12 @@ def fixture_cfg(fx, path):
     return path
 
 
-def state(fx, k):
-    """State k of a fixture as a dict (shape, dt, time, fields...)."""
-    g = lambda key: fx["s%d_%s" % (k, key)]  # noqa: E731
+def state(fx, k, prefix="s"):
+    """State k of a fixture as a dict (shape, dt, time, fields...).  prefix
+    "s": the reference as built by its own flags (FMA contraction on), exact
+    solves; "n": the reference built without FMA contraction, exact solves --
+    the rounding the CUDA path, built without contraction, follows."""
+    g = lambda key: fx["%s%d_%s" % (prefix, k, key)]  # noqa: E731
     meta = g("meta")
     shp = tuple(int(v) for v in meta[4:7])
     return {
@@ -101,3 +104,38 @@ def compare_state(scene, st, nobj):
         xs = x.reshape(3, -1)
         out["xi"] = max(rel_l2(xs[c][both], xr[c][both]) for c in range(3))
     return out
+
+
+# ---- the manufactured solution of sim_ftest (Sim/sim_manager.cc:139-167) ----
+def ftest_velocity(x, y, z):
+    tp = 2 * np.pi
+    u = -np.sin(tp * x) * np.cos(tp * y) * np.cos(tp * z)
+    v = 0.5 * np.cos(tp * x) * np.sin(tp * y) * np.cos(tp * z)
+    w = 0.5 * np.cos(tp * x) * np.cos(tp * y) * np.sin(tp * z)
+    return u, v, w
+
+
+def ftest_exact(x, y, z, t, h, mu):
+    """sim_ftest::exact: velocity at the cell centre (x, y, z), pressure at the
+    cell's lower corner, at time t."""
+    tp = 2 * np.pi
+    u, v, w = ftest_velocity(x, y, z)
+    c = np.cos(tp * t)
+    xc, yc, zc = x - 0.5 * h, y - 0.5 * h, z - 0.5 * h
+    p = 3 * np.pi * mu * np.cos(tp * xc) * np.cos(tp * yc) * np.cos(tp * zc)
+    return u * c, v * c, w * c, p * (c - np.sin(tp * t) / (6 * np.pi * mu))
+
+
+def ftest_error(u, v, w, p, t, dx, mu, x0=0.0):
+    """fluid_3d::error (F3D_Source/fluid_3d.cc:2810-2858) on a periodic box
+    (node grid = cell grid): the mean squared error of u, v, w over the cells
+    and of p over the nodes.  u, v, w, p: interior arrays indexed [k, j, i]."""
+    o, n, m = u.shape
+    xs = x0 + (np.arange(m) + 0.5) * dx
+    ys = x0 + (np.arange(n) + 0.5) * dx
+    zs = x0 + (np.arange(o) + 0.5) * dx
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    eu, ev, ew, ep = ftest_exact(X, Y, Z, t, dx, mu)
+    cnt = m * n * o
+    return np.array([((eu - u) ** 2).sum() / cnt, ((ev - v) ** 2).sum() / cnt, ((ew - w) ** 2).sum() / cnt,
+                     ((ep - p) ** 2).sum() / cnt])

@@ -217,7 +217,7 @@ def test_group_failure_is_isolated(tmp_path):
         dims = (ctypes.c_int * 6)()
         L.rmt3d_get_dims(h, dims)
         sm4, sn4, so4 = dims[0], dims[1], dims[2]
-        from oracle.refdump import FIELD_DT, REFMAP_DT
+        from rmt3d_b200.layout import FIELD_DT, REFMAP_DT
         fa = np.zeros(sm4 * sn4 * so4, dtype=FIELD_DT)
         ra = np.zeros(sm4 * sn4 * so4, dtype=REFMAP_DT)
         cnt = ctypes.c_int()

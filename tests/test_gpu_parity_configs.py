@@ -1,0 +1,174 @@
+"""Parity at the benchmarked workloads' own sizes, against the reference run
+on the same .cfg at test time.
+
+The oracle (the reference's sources compiled by oracle/Makefile into
+oracle/_ref/) runs beside the GPU: every reference run of this module is
+started at once, as parallel host processes, when the first test asks for
+one.  Its compact dumps (``ref_driver ... fields k1,k2,...``) hold velocity
+and pressure after the listed steps.
+
+* The 64^3 lid-driven cavity with a neo-Hookean sphere (the bench workload):
+  the plain FP64 form, solving exactly, against the reference built without
+  FMA contraction after 1, 5 and 20 steps; the bound is the reference's own
+  rounding envelope (with against without contraction) at the same step.
+* The mixed form (FP32 V-cycles inside FP64 refinement, the reference's
+  residual-tolerance control) after 100 steps of that workload, against the
+  reference's own build run as run_sim runs it: within 1e-5 rel-L2 for the
+  velocity and the pressure.
+* The pre-stretched sphere relaxing in a periodic box at 64^3 (5 steps) and
+  128^3 (2 steps), FP64, against the no-FMA reference, bounded by the same
+  envelope.
+
+Every test prints its measured per-field errors.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import helpers as H
+import rmt3d_b200 as R
+from rmt3d_b200 import scenes
+
+sys.path.insert(0, H.ROOT)
+from oracle import refdump  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+REF = os.path.join(H.ROOT, "oracle", "_ref")
+DRIVER = os.path.join(REF, "ref_driver")
+DRIVER_NOFMA = os.path.join(REF, "nofma", "ref_driver")
+needs_ref = pytest.mark.skipif(not (os.path.exists(DRIVER) and os.path.exists(DRIVER_NOFMA)),
+                               reason="oracle/_ref not built")
+
+TOL = 1e-10
+ENV_FACTOR = 4
+MIXED_TOL = 1e-5
+
+# name -> (cfg text, steps to dump, build, exact solves)
+RUNS = {
+    "c64_nofma": (scenes.cavity_sphere(64, 100000, radius=0.2), [1, 5, 20], "nofma", True),
+    "c64_fma": (scenes.cavity_sphere(64, 100000, radius=0.2), [1, 5, 20], "fma", True),
+    "c64_tol100": (scenes.cavity_sphere(64, 100000, radius=0.2), [100], "fma", False),
+    "s64_nofma": (scenes.stretched_sphere(64, 100000, radius=0.3), [1, 5], "nofma", True),
+    "s64_fma": (scenes.stretched_sphere(64, 100000, radius=0.3), [1, 5], "fma", True),
+    "s128_nofma": (scenes.stretched_sphere(128, 100000, radius=0.3), [1, 2], "nofma", True),
+    "s128_fma": (scenes.stretched_sphere(128, 100000, radius=0.3), [1, 2], "fma", True),
+}
+
+
+class OracleRuns:
+    def __init__(self, wd):
+        self.wd = wd
+        self.procs = {}
+        for name, (txt, steps, build, exact) in RUNS.items():
+            d = os.path.join(wd, name)
+            os.makedirs(d)
+            with open(os.path.join(d, "case.cfg"), "w") as fh:
+                fh.write(txt)
+            env = dict(os.environ, RMT3D_SHIM_EXACT="1" if exact else "0")
+            drv = DRIVER_NOFMA if build == "nofma" else DRIVER
+            self.procs[name] = subprocess.Popen(
+                [drv, "case.cfg", str(max(steps)), "out", "fields", ",".join(str(k) for k in steps)],
+                cwd=d, env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+
+    def get(self, name, k):
+        p = self.procs[name]
+        if p.returncode is None:
+            out, _ = p.communicate()
+            assert p.returncode == 0, out[-2000:]
+        return refdump.read_fields(os.path.join(self.wd, name, "out_s%d.f64" % k))
+
+    def close(self):
+        for p in self.procs.values():
+            if p.returncode is None:
+                p.kill()
+                p.wait()
+
+
+@pytest.fixture(scope="module")
+def oracle_runs(tmp_path_factory):
+    runs = OracleRuns(str(tmp_path_factory.mktemp("oracle")))
+    yield runs
+    runs.close()
+
+
+def errors(sc, ref):
+    """rel-L2 per field: velocity components against the whole velocity's
+    norm, pressure against its own."""
+    sl = H.INTERIOR
+    rv = np.stack([ref[c][sl] for c in "uvw"])
+    scale = np.linalg.norm(rv)
+    out = {c: float(np.linalg.norm(sc.field(c)[sl] - ref[c][sl]) / scale) for c in "uvw"}
+    out["p"] = H.rel_l2(sc.field("p")[sl], ref["p"][sl])
+    return out
+
+
+def envelope(a, b):
+    """The reference's rounding envelope: rel-L2 of (velocity, pressure)
+    between its builds with and without FMA contraction."""
+    sl = H.INTERIOR
+    va, vb = np.stack([a[c][sl] for c in "uvw"]), np.stack([b[c][sl] for c in "uvw"])
+    return max(float(np.linalg.norm(va - vb) / np.linalg.norm(vb)), H.rel_l2(a["p"][sl], b["p"][sl]))
+
+
+def fp64_against_reference(tmp_path, oracle_runs, cfg_text, tag, steps):
+    cfg = scenes.write(str(tmp_path / (tag + ".cfg")), cfg_text)
+    sc = R.Scene.from_cfg(cfg, mg_exact=1)
+    try:
+        sc.prepare()
+        done = 0
+        for k in steps:
+            assert sc.run(k - done) == R.NORMAL_EXIT
+            done = k
+            ref = oracle_runs.get(tag + "_nofma", k)
+            alt = oracle_runs.get(tag + "_fma", k)
+            assert sc.time == pytest.approx(ref["time"], rel=1e-13)
+            e = errors(sc, ref)
+            env = envelope(alt, ref)
+            b = max(TOL, ENV_FACTOR * env)
+            print("\n%s step %d: %s (envelope %.3g, bound %.3g)" % (tag, k, e, env, b))
+            assert max(e.values()) < b, (k, e, env)
+    finally:
+        sc.close()
+
+
+@needs_ref
+def test_cavity_sphere64_fp64(tmp_path, oracle_runs):
+    """The bench workload, plain FP64, 20 steps."""
+    fp64_against_reference(tmp_path, oracle_runs, RUNS["c64_nofma"][0], "c64", [1, 5, 20])
+
+
+@needs_ref
+def test_cavity_sphere64_mixed_100_steps(tmp_path, oracle_runs):
+    """The mixed form after 100 steps of the bench workload, against the
+    reference's own run (its build, its residual-tolerance control)."""
+    cfg = scenes.write(str(tmp_path / "m.cfg"), RUNS["c64_tol100"][0])
+    sc = R.Scene.from_cfg(cfg, precision=R.MIXED)
+    try:
+        sc.prepare()
+        assert sc.run(100) == R.NORMAL_EXIT
+        ref = oracle_runs.get("c64_tol100", 100)
+        e = errors(sc, ref)
+        sl = H.INTERIOR
+        rv = np.stack([ref[c][sl] for c in "uvw"])
+        gv = np.stack([sc.field(c)[sl] for c in "uvw"])
+        e["velocity"] = float(np.linalg.norm(gv - rv) / np.linalg.norm(rv))
+        print("\nc64 mixed form after 100 steps against the reference: %s" % e)
+        assert e["velocity"] < MIXED_TOL and e["p"] < MIXED_TOL, e
+    finally:
+        sc.close()
+
+
+@needs_ref
+def test_stretched_sphere64_fp64(tmp_path, oracle_runs):
+    """The pre-stretched sphere, periodic 64^3, 5 steps."""
+    fp64_against_reference(tmp_path, oracle_runs, RUNS["s64_nofma"][0], "s64", [1, 5])
+
+
+@needs_ref
+def test_stretched_sphere128_fp64(tmp_path, oracle_runs):
+    """The pre-stretched sphere at the workload's 128^3, 2 steps."""
+    fp64_against_reference(tmp_path, oracle_runs, RUNS["s128_nofma"][0], "s128", [1, 2])

@@ -18,7 +18,7 @@ needs_ref = pytest.mark.skipif(not (os.path.exists(DRIVER) and os.path.exists(DR
 
 @needs_ref
 @pytest.mark.parametrize("name,k", [("cavity16", 1), ("sphere24", 1), ("stretch24", 0), ("varden24", 1),
-                                    ("multi24", 1), ("collide24", 1)])
+                                    ("multi24", 1), ("collide24", 1), ("wall24", 1), ("ftest16", 1)])
 def test_fixture_reproduces_from_reference(tmp_path, name, k):
     fx = H.load_fixture(name)
     cfg = H.fixture_cfg(fx, str(tmp_path / "case.cfg"))
@@ -35,8 +35,23 @@ def test_fixture_reproduces_from_reference(tmp_path, name, k):
     assert np.array_equal(d["ext_index"], st["ext_index"])
 
 
+def test_nofma_states_reproduce_from_reference(tmp_path):
+    """The no-FMA states (n<k>_*) are that build's exact-mode output."""
+    drv = os.path.join(H.ROOT, "oracle", "_ref", "nofma", "ref_driver")
+    if not os.path.exists(drv):
+        pytest.skip("oracle/_ref/nofma not built here")
+    fx = H.load_fixture("sphere24")
+    cfg = H.fixture_cfg(fx, str(tmp_path / "case.cfg"))
+    out = str(tmp_path / "o.bin")
+    env = dict(os.environ, RMT3D_SHIM_EXACT="1")
+    subprocess.run([drv, cfg, "1", out], check=True, capture_output=True, cwd=str(tmp_path), env=env)
+    d = refdump.read(out)
+    st = H.state(fx, 1, "n")
+    assert np.array_equal(d["fields"]["vel"].T, st["vel"]) and np.array_equal(d["fields"]["p"], st["p"])
+
+
 def test_fixture_invariants():
-    for name in ("cavity16", "sphere24", "stretch24", "varden24", "multi24", "collide24"):
+    for name in ("cavity16", "sphere24", "stretch24", "varden24", "multi24", "collide24", "wall24", "ftest16"):
         fx = H.load_fixture(name)
         for k in (0, 1):
             st = H.state(fx, k)
@@ -64,3 +79,16 @@ def test_long_cavity_fixture_shape():
     fx = H.load_fixture("cavity32_64")
     assert fx["u"].shape == (32, 32, 32)
     assert np.abs(fx["u"]).max() < 1.0 + 1e-9
+
+
+def test_ftest_error_restatement_matches_reference_report():
+    """The numpy restatement of fluid_3d::error (tests/helpers.py) gives the
+    reference run_sim's own printed exact-solution errors for its state."""
+    fx = H.load_fixture("ftest16")
+    st = H.state(fx, 4)
+    shp = st["shape"]
+    e = H.ftest_error(*[st["vel"][c].reshape(shp)[H.INTERIOR] for c in range(3)],
+                      st["p"].reshape(shp)[H.INTERIOR], st["time"], 1.0 / 16, 0.01)
+    printed = fx["runsim_err"]
+    assert st["time"] == pytest.approx(printed[0], rel=1e-12)
+    assert np.allclose(e, printed[3:], rtol=0, atol=6e-11), (e, printed)

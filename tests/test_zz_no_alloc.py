@@ -34,26 +34,30 @@ def _call(lib, desc, dt_basis, dvel, faces):
     return code, out.value
 
 
-def test_noalloc_div_u_matches_allocating_path(tmp_path):
+@pytest.mark.parametrize("name", ["cavity16", "stretch24"])
+def test_noalloc_div_u_matches_allocating_path(tmp_path, name):
+    """cavity16 has walls on every face; stretch24 is periodic on every axis,
+    where the right-hand side reads the periodic images in the ghost layers."""
     import torch
 
     lib = R.lib()
-    fx = H.load_fixture("cavity16")
-    sc = R.Scene.from_cfg(H.fixture_cfg(fx, str(tmp_path / "c16.cfg")))
+    fx = H.load_fixture(name)
+    sc = R.Scene.from_cfg(H.fixture_cfg(fx, str(tmp_path / (name + ".cfg"))))
     try:
         sc.prepare()
         assert sc.run(2) == R.NORMAL_EXIT
         expected = sc.diag(0)
         assert expected > 0
         dvel = [torch.from_numpy(sc.field(n).copy()).cuda() for n in ("du", "dv", "dw")]
-        faces = [torch.from_numpy(sc.field("fvel%d%d" % (f, f // 2)).copy()).cuda() for f in range(6)]
+        faces = [None if sc.desc.periodic[f // 2] else
+                 torch.from_numpy(sc.field("fvel%d%d" % (f, f // 2)).copy()).cuda() for f in range(6)]
         torch.cuda.synchronize()
         for _ in range(2):  # two calls in a row share the same scratch array
             code, got = _call(lib, sc.desc, sc.dt_reg, dvel, faces)
             assert code == _lib.OK, lib.rmt3d_last_error()
             assert abs(got - expected) <= TOL * abs(expected), (got, expected)
         # grids beyond the fixed scratch are refused, not truncated
-        big = R.desc_from_cfg(H.fixture_cfg(fx, str(tmp_path / "c16b.cfg")))
+        big = R.desc_from_cfg(H.fixture_cfg(fx, str(tmp_path / (name + "b.cfg"))))
         big.sys_size[0] = big.sys_size[1] = big.sys_size[2] = 96
         code, _ = _call(lib, big, sc.dt_reg, dvel, faces)
         assert code == _lib.ERR_TOO_LARGE
