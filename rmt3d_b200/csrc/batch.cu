@@ -28,14 +28,16 @@
 // knobs shared with scene.cu (defined there)
 extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts);
 extern "C" int rmt3d_scene_set_mg_launch(rmt3d_scene *s, int cluster);
+extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode, int tile_waves);
 
 struct rmt3d_batch {
     std::vector<rmt3d_scene *> scenes;
     std::vector<rmt3d_scene_desc> descs;
     std::vector<std::vector<int>> groups;  // scene indices per host thread
     std::vector<int> status;
-    // grid shape, periodicity, precision and density form -> (v_down, v_up, cluster launch)
-    std::map<std::array<int, 8>, std::array<int, 3>> tuned;
+    // grid shape, periodicity, precision and density form -> (v_down, v_up,
+    // cluster launch, smoother mode)
+    std::map<std::array<int, 8>, std::array<int, 4>> tuned;
     int nthreads = 1;
     // equally sized scenes stepped together: one graph per group, each
     // multigrid solve batched over the group's scenes
@@ -67,12 +69,12 @@ int build_groups(rmt3d_batch *b) {
     std::map<std::vector<double>, std::vector<int>> part;
     for (size_t i = 0; i < b->scenes.size(); i++) {
         const rmt3d_scene_desc &d = b->descs[i];
-        auto it = b->tuned.find(tune_key(d));
-        const int vd = it != b->tuned.end() ? it->second[0] : 2, vu = it != b->tuned.end() ? it->second[1] : 2;
+        int sch[4];
+        rmt3d::scene_schedule(b->scenes[i], sch);
         std::vector<double> key = {(double)d.sys_size[0], (double)d.sys_size[1], (double)d.sys_size[2],
                                    (double)d.periodic[0], (double)d.periodic[1], (double)d.periodic[2],
                                    (double)d.precision, (double)d.var_den, (double)d.mg_exact, d.mixed_rtol,
-                                   (double)vd, (double)vu};
+                                   (double)sch[0], (double)sch[1], (double)sch[2], (double)sch[3]};
         part[key].push_back((int)i);
     }
     for (auto &kv : part) {
@@ -249,16 +251,21 @@ extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
 // Autotune the multigrid schedule per kind of scene (grid shape,
 // periodicity, precision and density form, the keys build_groups groups by):
 // a probe copy of the first scene of each kind is set up and stepped
-// `probe_steps` times per candidate -- smoothing counts (v_down, v_up) and
-// the cluster or per-phase launch of the solves -- and the fastest candidate
-// that ran without error is applied to every scene of that kind.  tuned_out
-// (optional, 4 ints per kind: cells, v_down, v_up, cluster launch) receives
-// the choices.
+// `probe_steps` times per candidate and the fastest candidate that ran
+// without error is applied to every scene of that kind.  The candidates are
+// the smoothing counts (v_down, v_up), each solve as one thread-block-cluster
+// launch or as per-phase launches, and for the latter the smoother: one
+// launch per colour pass, or one per whole sweep on shared-memory tiles with
+// the z depth of the tiles set for about 4 or 8 blocks per SM.  tuned_out
+// (optional, 5 ints per kind: cells, v_down, v_up, cluster launch, smoother
+// (0 colour passes, otherwise the tiles' blocks per SM)) receives the choices.
 extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
     drop_groups(b);
     static const int smooth[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
+    // (cluster launch, smoother waves: 0 colour passes)
+    static const int launch[][2] = {{1, 0}, {0, 0}, {0, 4}, {0, 8}};
     std::map<std::array<int, 8>, int> first;
     for (size_t i = 0; i < b->descs.size(); i++)
         if (!first.count(tune_key(b->descs[i]))) first[tune_key(b->descs[i])] = (int)i;
@@ -272,11 +279,12 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
             return e;
         }
         double best = 1e300;
-        int bd = 2, bu = 2, bc = 0;
-        for (int cl : {1, 0})
+        int bd = 2, bu = 2, bc = 0, bs = 0;
+        for (auto &ln : launch)
             for (auto &c : smooth) {
-                if (rmt3d_scene_set_mg_launch(probe, cl)) continue;  // clusters unavailable
-                if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], 0))) {
+                if (rmt3d_scene_set_mg_launch(probe, ln[0])) continue;  // clusters unavailable
+                if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], 0)) ||
+                    (e = rmt3d_scene_set_smoother(probe, ln[1] ? 1 : 0, ln[1] ? ln[1] : 4))) {
                     rmt3d_scene_destroy(probe);
                     return e;
                 }
@@ -291,25 +299,40 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
                     best = dt;
                     bd = c[0];
                     bu = c[1];
-                    bc = cl;
+                    bc = ln[0];
+                    bs = ln[1];
                 }
             }
         rmt3d_scene_destroy(probe);
-        b->tuned[kv.first] = {bd, bu, bc};
+        b->tuned[kv.first] = {bd, bu, bc, bs};
         for (size_t i = 0; i < b->descs.size(); i++)
             if (tune_key(b->descs[i]) == kv.first) {
                 if ((e = rmt3d_scene_set_schedule(b->scenes[i], bd, bu, 0))) return e;
                 if ((e = rmt3d_scene_set_mg_launch(b->scenes[i], bc))) return e;
+                if ((e = rmt3d_scene_set_smoother(b->scenes[i], bs ? 1 : 0, bs ? bs : 4))) return e;
             }
         if (tuned_out && written < max_out) {
-            tuned_out[4 * written] = (int)cells(b->descs[kv.second]);
-            tuned_out[4 * written + 1] = bd;
-            tuned_out[4 * written + 2] = bu;
-            tuned_out[4 * written + 3] = bc;
+            tuned_out[5 * written] = (int)cells(b->descs[kv.second]);
+            tuned_out[5 * written + 1] = bd;
+            tuned_out[5 * written + 2] = bu;
+            tuned_out[5 * written + 3] = bc;
+            tuned_out[5 * written + 4] = bs;
         }
         written++;
     }
     if (n_out) *n_out = written;
+    return RMT3D_OK;
+}
+
+// The smoother of every scene of the batch (rmt3d_scene_set_smoother); the
+// groups are rebuilt at the next step.
+extern "C" int rmt3d_batch_set_smoother(rmt3d_batch *b, int mode, int tile_waves) {
+    if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
+    drop_groups(b);
+    for (auto *s : b->scenes) {
+        const int e = rmt3d_scene_set_smoother(s, mode, tile_waves);
+        if (e) return e;
+    }
     return RMT3D_OK;
 }
 

@@ -25,6 +25,9 @@ int steps_finish(rmt3d_scene *s, int *status);
 // status per scene.
 struct scene_group;
 int group_create(rmt3d_scene *const *scenes, int n, scene_group **out);
+// a scene's multigrid schedule, as groups must share it: v_down, v_up,
+// smoother mode, tile waves
+void scene_schedule(rmt3d_scene *s, int out[4]);
 int group_launch(scene_group *g, int nsteps);
 int group_finish(scene_group *g, int *status);
 void group_destroy(scene_group *g);

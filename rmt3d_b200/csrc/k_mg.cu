@@ -32,6 +32,7 @@
 #include "graph_build.h"
 #include "mg_ops.cuh"
 #include "mg_body.cuh"
+#include "mg_tile.cuh"
 #include "rmt3d_gpu.h"
 
 namespace rmt3d {
@@ -80,6 +81,24 @@ __global__ void k_fem_prolong(lvl_dev F, lvl_dev C, T *__restrict__ x, const T *
 template <typename T>
 __global__ void k_coarse_dense(int np, const double *__restrict__ B, T *__restrict__ x, const T *__restrict__ r) {
     body_coarse_dense<T>(np, B, x, r, blockIdx.x, gridDim.x);
+}
+
+// one whole sweep of a level on shared-memory tiles (mg_tile.cuh); blockIdx.z
+// is the z chunk of tz planes
+template <typename T, int KIND, bool VD>
+__global__ void __launch_bounds__(256) k_tile_sweep(lvl_dev L, const T *__restrict__ xin, T *__restrict__ xout,
+                                                    const T *__restrict__ r, const T *__restrict__ ri, int tz) {
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    using S = tile_shape<KIND>;
+    const int z0 = blockIdx.z * tz;
+    body_tile_sweep<T, KIND, VD>(L, xin, xout, r, ri, blockIdx.x * S::TX, blockIdx.y * S::TY, z0,
+                                 min(z0 + tz, L.n2), tile_smem);
+}
+
+template <typename T>
+__global__ void k_copy(const T *__restrict__ a, T *__restrict__ b, size_t n) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
 }
 
 // coarsest grid fallback: many Gauss-Seidel sweeps inside one thread block
@@ -148,6 +167,59 @@ __global__ void k_zero(T *a, size_t n) {
 static lvl_dev dev_of(const mg_level &l) { return lvl_dev{l.n[0], l.n[1], l.n[2], l.prd[0], l.prd[1], l.prd[2]}; }
 
 static dim3 blk3() { return dim3(32, 4, 2); }
+
+dim3 tile_grid(int kind, const int n[3], int B, int waves, int &tz, int &zb) {
+    const int TX = kind == MG_MAC ? tile_shape<0>::TX : tile_shape<1>::TX;
+    const int TY = kind == MG_MAC ? tile_shape<0>::TY : tile_shape<1>::TY;
+    const int tx = (n[0] + TX - 1) / TX, ty = (n[1] + TY - 1) / TY;
+    // enough z chunks for about `waves` blocks per SM, none thinner than 8 planes
+    int nz = (waves * 148 + tx * ty * B - 1) / (tx * ty * B);
+    nz = std::max(1, std::min(nz, (n[2] + 7) / 8));
+    tz = (n[2] + nz - 1) / nz;
+    zb = (n[2] + tz - 1) / tz;
+    return dim3(tx, ty, zb * B);
+}
+
+template <typename T, int KIND, bool VD>
+static int tile_attr(const void *fn) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem_bytes<T, KIND, VD>()) !=
+           cudaSuccess;
+}
+
+int tile_setup_batched();  // k_mgb.cu
+
+int tile_setup() {
+    static std::once_flag once;
+    static int err = 0;
+    std::call_once(once, []() {
+        err |= tile_attr<double, 0, false>((const void *)k_tile_sweep<double, 0, false>);
+        err |= tile_attr<double, 0, true>((const void *)k_tile_sweep<double, 0, true>);
+        err |= tile_attr<double, 1, false>((const void *)k_tile_sweep<double, 1, false>);
+        err |= tile_attr<double, 1, true>((const void *)k_tile_sweep<double, 1, true>);
+        err |= tile_attr<float, 0, false>((const void *)k_tile_sweep<float, 0, false>);
+        err |= tile_attr<float, 0, true>((const void *)k_tile_sweep<float, 0, true>);
+        err |= tile_attr<float, 1, false>((const void *)k_tile_sweep<float, 1, false>);
+        err |= tile_attr<float, 1, true>((const void *)k_tile_sweep<float, 1, true>);
+        err |= tile_setup_batched();
+    });
+    return err;
+}
+
+// one tiled sweep xin -> xout of level L
+template <typename T>
+static void tile_sweep(mg_kind kind, const mg_level &L, const T *xin, T *xout, const T *r, const T *ri, int waves,
+                       cudaStream_t st) {
+    int tz, zb;
+    const dim3 g = tile_grid(kind, L.n, 1, waves, tz, zb);
+    const lvl_dev d{L.n[0], L.n[1], L.n[2], L.prd[0], L.prd[1], L.prd[2]};
+    if (kind == MG_MAC) {
+        if (ri) k_tile_sweep<T, 0, true><<<g, 256, tile_smem_bytes<T, 0, true>(), st>>>(d, xin, xout, r, ri, tz);
+        else k_tile_sweep<T, 0, false><<<g, 256, tile_smem_bytes<T, 0, false>(), st>>>(d, xin, xout, r, ri, tz);
+    } else {
+        if (ri) k_tile_sweep<T, 1, true><<<g, 256, tile_smem_bytes<T, 1, true>(), st>>>(d, xin, xout, r, ri, tz);
+        else k_tile_sweep<T, 1, false><<<g, 256, tile_smem_bytes<T, 1, false>(), st>>>(d, xin, xout, r, ri, tz);
+    }
+}
 static dim3 grid3(int a, int b, int c) { return dim3((a + 31) / 32, (b + 3) / 4, (c + 1) / 2); }
 
 // Host copy of the level operator, for the coarsest-grid inverse.
@@ -401,6 +473,7 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
     }
     if (build_dense(st)) return fail(RMT3D_ERR_OOM, "coarse inverse allocation failed");
     if (set_coarse(coarse_pts)) return fail(RMT3D_ERR_CUDA, "coarse multigrid kernel configuration failed");
+    if (tile_setup()) return fail(RMT3D_ERR_CUDA, "tiled sweep kernel configuration failed");
     setup_cluster();
     {
         const char *e = getenv("RMT3D_MG_CLUSTER");
@@ -419,54 +492,69 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
         if (launches) (*launches)++;          \
     } while (0)
 
-void mg_solver::smooth(int l, int sweeps, cudaStream_t st) {
+int mg_solver::smooth(int l, int sweeps, int cur, cudaStream_t st) {
     mg_level &L = lv[l];
     lvl_dev d = dev_of(L);
     // algorithmic bytes of one colour pass: read x of the whole level, read r
-    // and write x of the updated colour
+    // and write x of the updated colour; of one tiled sweep: read x and r and
+    // write x of the whole level (and read 1/rho with variable density)
     const double npts = (double)L.npts();
     const bool timed = prof && l == 0 && prof->target == (kind == MG_FEM ? 0 : 1);
+    double *xb[2] = {L.x, L.res};
     for (int s = 0; s < sweeps; s++) {
-        if (kind == MG_MAC) {
+        if (smoother == 1) {
+            if (timed) prof->begin(st);
+            LAUNCH(tile_sweep<double>(kind, L, xb[cur], xb[cur ^ 1], L.r, L.ri, tile_waves, st));
+            if (timed) prof->end(st, npts, 8.0 * npts * (L.ri ? 4 : 3));
+            cur ^= 1;
+        } else if (kind == MG_MAC) {
             dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 2; c++) {
                 if (timed) prof->begin(st);
-                LAUNCH(k_mac_rb<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c, L.ri));
+                LAUNCH(k_mac_rb<double><<<g, blk3(), 0, st>>>(d, xb[cur], L.r, c, L.ri));
                 if (timed) prof->end(st, npts / 2, 8.0 * (npts + npts / 2 + npts / 2));
             }
         } else {
             dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 4; c++) {
                 if (timed) prof->begin(st);
-                LAUNCH(k_fem_gs<double><<<g, blk3(), 0, st>>>(d, L.x, L.r, c, L.ri));
+                LAUNCH(k_fem_gs<double><<<g, blk3(), 0, st>>>(d, xb[cur], L.r, c, L.ri));
                 if (timed) prof->end(st, npts / 4, 8.0 * (npts + npts / 4 + npts / 4));
             }
         }
     }
+    return cur;
 }
 
-void mg_solver::smooth_f32(int l, int sweeps, cudaStream_t st) {
+int mg_solver::smooth_f32(int l, int sweeps, int cur, cudaStream_t st) {
     mg_level &L = lv[l];
     lvl_dev d = dev_of(L);
     const double npts = (double)L.npts();
     const bool timed = prof && l == 0 && prof->target == (kind == MG_FEM ? 0 : 1);
+    float *xb[2] = {L.xs, L.ress};
     for (int s = 0; s < sweeps; s++) {
-        if (kind == MG_MAC) {
+        if (smoother == 1) {
+            if (timed) prof->begin(st);
+            LAUNCH(tile_sweep<float>(kind, L, xb[cur], xb[cur ^ 1], L.rs, L.ris, tile_waves, st));
+            if (timed) prof->end(st, npts, 4.0 * npts * (L.ris ? 4 : 3));
+            cur ^= 1;
+        } else if (kind == MG_MAC) {
             dim3 g((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 2; c++) {
                 if (timed) prof->begin(st);
-                LAUNCH(k_mac_rb<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c, L.ris));
+                LAUNCH(k_mac_rb<float><<<g, blk3(), 0, st>>>(d, xb[cur], L.rs, c, L.ris));
                 if (timed) prof->end(st, npts / 2, 4.0 * (npts + npts / 2 + npts / 2));
             }
         } else {
             dim3 g(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, (L.n[2] + 1) / 2);
             for (int c = 0; c < 4; c++) {
                 if (timed) prof->begin(st);
-                LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, L.xs, L.rs, c, L.ris));
+                LAUNCH(k_fem_gs<float><<<g, blk3(), 0, st>>>(d, xb[cur], L.rs, c, L.ris));
                 if (timed) prof->end(st, npts / 4, 4.0 * (npts + npts / 4 + npts / 4));
             }
         }
     }
+    return cur;
 }
 
 // level table of the coarse sub-cycle kernel
@@ -496,64 +584,70 @@ static pmg_args coarse_args(const mg_solver &m) {
     return A;
 }
 
-void mg_solver::cycle(int l, cudaStream_t st) {
+int mg_solver::cycle(int l, cudaStream_t st) {
     mg_level &F = lv[l];
     lvl_dev fd = dev_of(F);
     if (l == cf && l < (int)lv.size() - 1) {
         LAUNCH(k_mg_coarse<double><<<1, kCoarseThreads, coarse_smem_bytes(lv, l, 8), st>>>(coarse_args(*this), l));
-        return;
+        return 0;
     }
     if (l == (int)lv.size() - 1) {
         if (dense) LAUNCH(k_coarse_dense<double><<<((int)F.npts() + 7) / 8, 256, 0, st>>>((int)F.npts(), dense, F.x, F.r));
         else if (kind == MG_MAC) LAUNCH(k_coarse_solve<double, 0><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
         else LAUNCH(k_coarse_solve<double, 1><<<1, 512, 0, st>>>(fd, F.x, F.r, 80));
-        return;
+        return 0;
     }
-    smooth(l, v_down, st);
+    // the level's solution moves between its x and residual arrays with the
+    // tiled sweeps; the residual goes to whichever of the two is free
+    int cur = smooth(l, v_down, 0, st);
+    double *xb[2] = {F.x, F.res};
     mg_level &C = lv[l + 1];
     lvl_dev cd = dev_of(C);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
     if (kind == MG_MAC) {
-        LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
-        LAUNCH(k_mac_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r, C.x));
+        LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.r, xb[cur ^ 1], nullptr, F.ri)));
+        LAUNCH(k_mac_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.r, C.x));
     } else {
-        LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
-        LAUNCH(k_fem_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, F.res, C.r, C.x));
+        LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.r, xb[cur ^ 1], nullptr, F.ri)));
+        LAUNCH(k_fem_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.r, C.x));
     }
-    cycle(l + 1, st);
-    if (kind == MG_MAC) LAUNCH(k_mac_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, F.x, C.x));
-    else LAUNCH(k_fem_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, F.x, C.x));
-    smooth(l, v_up, st);
+    const int cc = cycle(l + 1, st);
+    const double *xc = cc ? C.res : C.x;
+    if (kind == MG_MAC) LAUNCH(k_mac_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, xb[cur], xc));
+    else LAUNCH(k_fem_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, xb[cur], xc));
+    return smooth(l, v_up, cur, st);
 }
 
-void mg_solver::cycle_f32(int l, cudaStream_t st) {
+int mg_solver::cycle_f32(int l, cudaStream_t st) {
     mg_level &F = lv[l];
     lvl_dev fd = dev_of(F);
     if (l == cf && l < (int)lv.size() - 1) {
         LAUNCH(k_mg_coarse<float><<<1, kCoarseThreads, coarse_smem_bytes(lv, l, 4), st>>>(coarse_args(*this), l));
-        return;
+        return 0;
     }
     if (l == (int)lv.size() - 1) {
         if (dense) LAUNCH(k_coarse_dense<float><<<((int)F.npts() + 7) / 8, 256, 0, st>>>((int)F.npts(), dense, F.xs, F.rs));
         else if (kind == MG_MAC) LAUNCH(k_coarse_solve<float, 0><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
         else LAUNCH(k_coarse_solve<float, 1><<<1, 512, 0, st>>>(fd, F.xs, F.rs, 80));
-        return;
+        return 0;
     }
-    smooth_f32(l, v_down, st);
+    int cur = smooth_f32(l, v_down, 0, st);
+    float *xb[2] = {F.xs, F.ress};
     mg_level &C = lv[l + 1];
     lvl_dev cd = dev_of(C);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
     if (kind == MG_MAC) {
-        LAUNCH((k_resid<float, 0><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr, F.ris)));
-        LAUNCH(k_mac_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs, C.xs));
+        LAUNCH((k_resid<float, 0><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.rs, xb[cur ^ 1], nullptr, F.ris)));
+        LAUNCH(k_mac_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.rs, C.xs));
     } else {
-        LAUNCH((k_resid<float, 1><<<gf, blk3(), 0, st>>>(fd, F.xs, F.rs, F.ress, nullptr, F.ris)));
-        LAUNCH(k_fem_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, F.ress, C.rs, C.xs));
+        LAUNCH((k_resid<float, 1><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.rs, xb[cur ^ 1], nullptr, F.ris)));
+        LAUNCH(k_fem_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.rs, C.xs));
     }
-    cycle_f32(l + 1, st);
-    if (kind == MG_MAC) LAUNCH(k_mac_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, F.xs, C.xs));
-    else LAUNCH(k_fem_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, F.xs, C.xs));
-    smooth_f32(l, v_up, st);
+    const int cc = cycle_f32(l + 1, st);
+    const float *xc = cc ? C.ress : C.xs;
+    if (kind == MG_MAC) LAUNCH(k_mac_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, xb[cur], xc));
+    else LAUNCH(k_fem_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, xb[cur], xc));
+    return smooth_f32(l, v_up, cur, st);
 }
 
 // One refinement step of the mixed form: FP64 residual, FP32 V-cycle on the
@@ -568,13 +662,18 @@ void mg_solver::refine_step(cudaStream_t st) {
     else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
     LAUNCH(k_to_f32<<<nb, 256, 0, st>>>(F.res, F.rs, n));
     LAUNCH(k_zero<float><<<nb, 256, 0, st>>>(F.xs, n));
-    cycle_f32(0, st);
-    LAUNCH(k_add_f32<<<nb, 256, 0, st>>>(F.x, F.xs, n));
+    const int cur = cycle_f32(0, st);
+    LAUNCH(k_add_f32<<<nb, 256, 0, st>>>(F.x, cur ? F.ress : F.xs, n));
 }
 
 void mg_solver::iterate(cudaStream_t st) {
-    if (mixed) refine_step(st);
-    else cycle(0, st);
+    if (mixed) {
+        refine_step(st);
+    } else if (cycle(0, st)) {
+        // the fine level's solution ended in its residual array
+        const size_t n = lv[0].npts();
+        LAUNCH(k_copy<double><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(lv[0].res, lv[0].x, n));
+    }
 }
 
 // ---- device-side control of one solve ---------------------------------------

@@ -18,6 +18,7 @@
 #include "mg.h"
 #include "mg_body.cuh"
 #include "mg_ops.cuh"
+#include "mg_tile.cuh"
 #include "rmt3d_gpu.h"
 
 namespace rmt3d {
@@ -82,6 +83,38 @@ __global__ void k_fem_prolong_b(lvl_dev F, lvl_dev C, T *const *x, T *const *xc,
     MGB_SCENE(zb)
     body_fem_prolong<T>(F, C, x[b_], xc[b_], blockIdx.x, blockIdx.y, bz_);
 }
+// one tiled sweep (mg_tile.cuh) of every running scene: blockIdx.z = scene x
+// z chunk
+template <typename T, int KIND, bool VD>
+__global__ void __launch_bounds__(256) k_tile_sweep_b(lvl_dev L, T *const *xin, T *const *xout, T *const *r,
+                                                      const T *const *ri, const int *run, int zb, int tz) {
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    MGB_SCENE(zb)
+    using S = tile_shape<KIND>;
+    const int z0 = bz_ * tz;
+    body_tile_sweep<T, KIND, VD>(L, xin[b_], xout[b_], r[b_], VD ? ri[b_] : nullptr, blockIdx.x * S::TX,
+                                 blockIdx.y * S::TY, z0, min(z0 + tz, L.n2), tile_smem);
+}
+
+template <typename T, int KIND, bool VD>
+static int tile_attr_b() {
+    return cudaFuncSetAttribute((const void *)k_tile_sweep_b<T, KIND, VD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tile_smem_bytes<T, KIND, VD>()) != cudaSuccess;
+}
+
+int tile_setup_batched() {
+    return tile_attr_b<double, 0, false>() | tile_attr_b<double, 0, true>() | tile_attr_b<double, 1, false>() |
+           tile_attr_b<double, 1, true>() | tile_attr_b<float, 0, false>() | tile_attr_b<float, 0, true>() |
+           tile_attr_b<float, 1, false>() | tile_attr_b<float, 1, true>();
+}
+
+template <typename T>
+__global__ void k_copy_b(T *const *a, T *const *b, size_t n, const int *run) {
+    if (!run[blockIdx.y]) return;
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) b[blockIdx.y][i] = a[blockIdx.y][i];
+}
+
 // one-dimensional phases: blockIdx.y is the scene
 template <typename T>
 __global__ void k_coarse_dense_b(int np, const double *__restrict__ B, T *const *x, T *const *r, const int *run) {
@@ -177,10 +210,13 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
     rtol = s0.rtol;
     v_down = s0.v_down;
     v_up = s0.v_up;
+    smoother = s0.smoother;
+    tile_waves = s0.tile_waves;
     dense = s0.dense;
     for (const mg_solver *m : solvers) {
         bool same = m->kind == kind && m->lv.size() == lv.size() && m->mixed == mixed && m->exact == exact &&
-                    m->vd == vd && m->rtol == rtol && m->dense == dense && m->v_down == v_down && m->v_up == v_up;
+                    m->vd == vd && m->rtol == rtol && m->dense == dense && m->v_down == v_down && m->v_up == v_up &&
+                    m->smoother == smoother && m->tile_waves == tile_waves;
         for (size_t l = 0; same && l < lv.size(); l++)
             for (int d = 0; d < 3; d++) same = same && m->lv[l].n[d] == lv[l].n[d] && m->lv[l].prd[d] == lv[l].prd[d];
         if (!same) return fail(RMT3D_ERR_INVALID, "scenes of a multigrid group must match in size, form and schedule");
@@ -232,30 +268,54 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
 }
 
 template <typename T>
-static void smooth_b(mg_group &g, int l, int sweeps, cudaStream_t st, T *const *x, T *const *r, const T *const *ri) {
+static void tile_sweep_b(mg_group &g, int l, T *const *xin, T *const *xout, T *const *r, const T *const *ri,
+                         cudaStream_t st) {
+    const mg_level &L = g.lv[l];
+    const lvl_dev d = ldv(L);
+    int tz, zb;
+    const dim3 gr = tile_grid(g.kind, L.n, g.B, g.tile_waves, tz, zb);
+    if (g.kind == MG_MAC) {
+        if (ri) k_tile_sweep_b<T, 0, true><<<gr, 256, tile_smem_bytes<T, 0, true>(), st>>>(d, xin, xout, r, ri, g.run, zb, tz);
+        else k_tile_sweep_b<T, 0, false><<<gr, 256, tile_smem_bytes<T, 0, false>(), st>>>(d, xin, xout, r, ri, g.run, zb, tz);
+    } else {
+        if (ri) k_tile_sweep_b<T, 1, true><<<gr, 256, tile_smem_bytes<T, 1, true>(), st>>>(d, xin, xout, r, ri, g.run, zb, tz);
+        else k_tile_sweep_b<T, 1, false><<<gr, 256, tile_smem_bytes<T, 1, false>(), st>>>(d, xin, xout, r, ri, g.run, zb, tz);
+    }
+    g.body_kernels++;
+}
+
+// ν sweeps of level l starting in array `cur` (0 x, 1 residual array);
+// returns the array holding the result
+template <typename T>
+static int smooth_b(mg_group &g, int l, int sweeps, int cur, cudaStream_t st, T *const *const xb[2], T *const *r,
+                    const T *const *ri) {
     const mg_level &L = g.lv[l];
     const lvl_dev d = ldv(L);
     for (int s = 0; s < sweeps; s++) {
-        if (g.kind == MG_MAC) {
+        if (g.smoother == 1) {
+            tile_sweep_b<T>(g, l, xb[cur], xb[cur ^ 1], r, ri, st);
+            cur ^= 1;
+        } else if (g.kind == MG_MAC) {
             int zb = (L.n[2] + 1) / 2;
             dim3 gr((L.n[0] / 2 + 1 + 31) / 32, (L.n[1] + 3) / 4, zb * g.B);
             for (int c = 0; c < 2; c++) {
-                k_mac_rb_b<T><<<gr, gblk(), 0, st>>>(d, x, r, ri, c, g.run, zb);
+                k_mac_rb_b<T><<<gr, gblk(), 0, st>>>(d, xb[cur], r, ri, c, g.run, zb);
                 g.body_kernels++;
             }
         } else {
             int zb = (L.n[2] + 1) / 2;
             dim3 gr(((L.n[0] + 1) / 2 + 31) / 32, ((L.n[1] + 1) / 2 + 3) / 4, zb * g.B);
             for (int c = 0; c < 4; c++) {
-                k_fem_gs_b<T><<<gr, gblk(), 0, st>>>(d, x, r, ri, c, g.run, zb);
+                k_fem_gs_b<T><<<gr, gblk(), 0, st>>>(d, xb[cur], r, ri, c, g.run, zb);
                 g.body_kernels++;
             }
         }
     }
+    return cur;
 }
 
 template <typename T>
-static void cycle_b(mg_group &g, int l, cudaStream_t st) {
+static int cycle_b(mg_group &g, int l, cudaStream_t st) {
     const bool f32 = sizeof(T) == 4;
     auto X = [&](int q) { return f32 ? (T *const *)g.tab[q].xs : (T *const *)g.tab[q].x; };
     auto Rr = [&](int q) { return f32 ? (T *const *)g.tab[q].rs : (T *const *)g.tab[q].r; };
@@ -276,32 +336,39 @@ static void cycle_b(mg_group &g, int l, cudaStream_t st) {
                 k_coarse_solve_b<T, 1><<<g.B, 512, 0, st>>>(ldv(F), X(l), Rr(l), 80, g.run);
             g.body_kernels++;
         }
-        return;
+        return 0;
     }
-    smooth_b<T>(g, l, g.v_down, st, X(l), Rr(l), RI(l));
+    T *const *const xb[2] = {X(l), S(l)};
+    int cur = smooth_b<T>(g, l, g.v_down, 0, st, xb, Rr(l), RI(l));
     const mg_level &C = g.lv[l + 1];
     int zbf, zbc;
     const dim3 gf = ggrid(F.n[0], F.n[1], F.n[2], g.B, zbf), gc = ggrid(C.n[0], C.n[1], C.n[2], g.B, zbc);
     if (g.kind == MG_MAC) {
-        k_resid_b<T, 0><<<gf, gblk(), 0, st>>>(ldv(F), X(l), Rr(l), S(l), RI(l), nullptr, g.run, zbf);
-        k_mac_restrict_b<T><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), S(l), Rr(l + 1), X(l + 1), g.run, zbc);
+        k_resid_b<T, 0><<<gf, gblk(), 0, st>>>(ldv(F), xb[cur], Rr(l), xb[cur ^ 1], RI(l), nullptr, g.run, zbf);
+        k_mac_restrict_b<T><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur ^ 1], Rr(l + 1), X(l + 1), g.run, zbc);
     } else {
-        k_resid_b<T, 1><<<gf, gblk(), 0, st>>>(ldv(F), X(l), Rr(l), S(l), RI(l), nullptr, g.run, zbf);
-        k_fem_restrict_b<T><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), S(l), Rr(l + 1), X(l + 1), g.run, zbc);
+        k_resid_b<T, 1><<<gf, gblk(), 0, st>>>(ldv(F), xb[cur], Rr(l), xb[cur ^ 1], RI(l), nullptr, g.run, zbf);
+        k_fem_restrict_b<T><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur ^ 1], Rr(l + 1), X(l + 1), g.run, zbc);
     }
     g.body_kernels += 2;
-    cycle_b<T>(g, l + 1, st);
-    if (g.kind == MG_MAC) k_mac_prolong_b<T><<<gf, gblk(), 0, st>>>(ldv(F), ldv(C), X(l), X(l + 1), g.run, zbf);
-    else k_fem_prolong_b<T><<<gf, gblk(), 0, st>>>(ldv(F), ldv(C), X(l), X(l + 1), g.run, zbf);
+    const int cc = cycle_b<T>(g, l + 1, st);
+    T *const *xc = cc ? S(l + 1) : X(l + 1);
+    if (g.kind == MG_MAC) k_mac_prolong_b<T><<<gf, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur], xc, g.run, zbf);
+    else k_fem_prolong_b<T><<<gf, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur], xc, g.run, zbf);
     g.body_kernels++;
-    smooth_b<T>(g, l, g.v_up, st, X(l), Rr(l), RI(l));
+    return smooth_b<T>(g, l, g.v_up, cur, st, xb, Rr(l), RI(l));
 }
 
 // one iteration for every running scene: a V-cycle, or the mixed form's
 // refinement step (FP64 residual, FP32 V-cycle on the correction, update)
 void mg_group::iterate(cudaStream_t st) {
     if (!mixed) {
-        cycle_b<double>(*this, 0, st);
+        if (cycle_b<double>(*this, 0, st)) {
+            // the fine level's solution ended in its residual array
+            const size_t n = lv[0].npts();
+            k_copy_b<double><<<dim3((unsigned)((n + 255) / 256), B), 256, 0, st>>>(tab[0].res, tab[0].x, n, run);
+            body_kernels++;
+        }
         return;
     }
     const mg_level &F = lv[0];
@@ -316,8 +383,8 @@ void mg_group::iterate(cudaStream_t st) {
     k_to_f32_b<<<g1, 256, 0, st>>>(tab[0].res, tab[0].rs, n, run);
     k_zero_b<float><<<g1, 256, 0, st>>>(tab[0].xs, n, run);
     body_kernels += 3;
-    cycle_b<float>(*this, 0, st);
-    k_add_f32_b<<<g1, 256, 0, st>>>(tab[0].x, tab[0].xs, n, run);
+    const int cur = cycle_b<float>(*this, 0, st);
+    k_add_f32_b<<<g1, 256, 0, st>>>(tab[0].x, cur ? tab[0].ress : tab[0].xs, n, run);
     body_kernels++;
 }
 

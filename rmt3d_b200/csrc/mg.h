@@ -115,6 +115,11 @@ class mg_solver {
     double *rhs() { return lv[0].r; }
     double *sol() { return lv[0].x; }
     double *dense = nullptr;  // inverse of the coarsest operator (row-major), or null
+    // smoothing: 0 one launch per colour pass (in place); 1 one launch per
+    // whole sweep on shared-memory tiles (mg_tile.cuh), alternating between
+    // a level's x and its residual array
+    int smoother = 0;
+    int tile_waves = 4;  // z chunks of the tiled sweep: about this many blocks per SM
     int cf = 0;  // first level whose whole sub-cycle runs in one CTA
     int coarse_pts = 0;  // largest level handed to the one-CTA sub-cycle (0: none)
     int set_coarse(int pts);
@@ -144,12 +149,20 @@ class mg_solver {
     int build_solve_graph();
     void launch_body(cudaStream_t st, bool armed, unsigned long long h);
     void iterate(cudaStream_t st);
-    void cycle(int l, cudaStream_t st);
-    void cycle_f32(int l, cudaStream_t st);
-    void smooth(int l, int sweeps, cudaStream_t st);
-    void smooth_f32(int l, int sweeps, cudaStream_t st);
+    // a V-cycle from level l down; returns the array holding the level's
+    // solution afterwards (0 its x, 1 its residual array)
+    int cycle(int l, cudaStream_t st);
+    int cycle_f32(int l, cudaStream_t st);
+    int smooth(int l, int sweeps, int cur, cudaStream_t st);
+    int smooth_f32(int l, int sweeps, int cur, cudaStream_t st);
     void refine_step(cudaStream_t st);
 };
+
+// grid of the tiled sweep over a level of n points per axis for B scenes:
+// (x tiles, y tiles, z chunks per scene); tz = planes per chunk
+dim3 tile_grid(int kind, const int n[3], int B, int waves, int &tz, int &zb);
+// the tiled sweep kernels' shared-memory limits (once per process)
+int tile_setup();
 
 // One multigrid solve for every scene of a group of equally sized scenes
 // with the same form and schedule, each phase one launch over all of them
@@ -170,6 +183,7 @@ class mg_group {
     bool mixed = false, exact = false, vd = false;
     double tol = 0, rtol = 0;
     int v_down = 2, v_up = 2;
+    int smoother = 0, tile_waves = 4;
     const double *dense = nullptr;
     std::vector<mgb_level_tab> tab;  // device tables per level
     mg_ctl **ctls = nullptr;         // device table of the scenes' control blocks

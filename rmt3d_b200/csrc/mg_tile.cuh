@@ -1,0 +1,463 @@
+// One whole Gauss-Seidel sweep (every colour) of a multigrid level in one
+// launch, on shared-memory tiles.
+//
+// The colour passes of a sweep depend on each other: pass c reads the values
+// pass c-1 wrote at distance one.  A block owns an output tile of TX x TY
+// points in x, y and a chunk of planes in z.  It stages the tile with a halo
+// of H = C points (C colours) in x and y, and streams the planes in z through
+// a ring of C + 2 planes in shared memory as a wavefront: in iteration t it
+// loads plane t, then runs pass 0 on plane t-1, pass 1 on plane t-2, ...,
+// pass C-1 on plane t-C, and writes plane t-C back.  Pass c on plane q needs
+// planes q-1..q+1 after pass c-1, which the wavefront provides: plane q+1
+// received pass c-1 earlier in the same iteration, plane q-1 one iteration
+// before (and pass c there touched only colour-c points, which pass c on
+// plane q does not read: no two coupled points share a colour).  In x and y
+// the region a pass can compute exactly shrinks by one point per pass, so
+// after C passes the halo is used up; the halo's points are computed by the
+// neighbouring blocks as well (overlapped tiling), and a z chunk recomputes H
+// planes above and below it.  Walls end the halo: a point on a wall reads
+// nothing beyond it.  Periodic axes load the wrapped points.
+//
+// Every point's update is the single-colour kernels' expression (mg_ops.cuh)
+// with the same operands in the same order, read from the tile instead of
+// global memory, so a tiled sweep gives exactly the bits of C colour passes.
+// Blocks read the level's values from `xin` and write the swept values to
+// `xout` (another array): a block's halo must see the values before the
+// sweep, which an in-place update by neighbouring blocks would overwrite.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "mg_ops.cuh"
+
+namespace rmt3d {
+
+template <int KIND>
+struct tile_shape {
+    static constexpr int C = KIND == 0 ? 2 : 4;  // colours of a sweep
+    static constexpr int H = C;                  // halo in x and y
+    static constexpr int TX = 32;
+    static constexpr int TY = KIND == 0 ? 16 : 8;
+    static constexpr int WX = TX + 2 * H, WY = TY + 2 * H;
+    static constexpr int R = C + 2;  // planes in the ring
+    static constexpr int NT = 256;   // threads per block
+    // variable density: 1/rho per cell.  MAC cells are the points; the FEM
+    // tile of cells is one wider (node i uses cells i-1 and i)
+    static constexpr int CX = KIND == 0 ? WX : WX + 1, CY = KIND == 0 ? WY : WY + 1;
+};
+
+template <typename T, int KIND, bool VD>
+constexpr size_t tile_smem_bytes() {
+    using S = tile_shape<KIND>;
+    return (size_t)S::R * S::WX * S::WY * sizeof(T) + (VD ? (size_t)S::R * S::CX * S::CY * sizeof(T) : 0);
+}
+
+// ---- stencils on the tile ---------------------------------------------------
+// A point's neighbours are read through three plane pointers (z-1, z, z+1)
+// and the offset o = lx + WX * ly of the point in its plane.
+
+template <typename T, int WX>
+struct tile_acc {
+    const T *pm, *pc, *pp;
+    int o;
+    __device__ __forceinline__ T operator()(int a, int b, int c) const {
+        const T *pl = c < 0 ? pm : (c > 0 ? pp : pc);
+        return pl[o + a + WX * b];
+    }
+};
+
+// mac_offdiag on the tile
+template <typename T, int WX>
+__device__ __forceinline__ T mac_offdiag_t(const lvl_dev L, const tile_acc<T, WX> &A, int i, int j, int k, T &diag) {
+    if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
+        diag = (T)-6;
+        return ((A(-1, 0, 0) + A(1, 0, 0)) + (A(0, -1, 0) + A(0, 1, 0))) + (A(0, 0, -1) + A(0, 0, 1));
+    }
+    T s = 0;
+    int missing = 0;
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int c[3] = {i, j, k};
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+#pragma unroll
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+            if (wrapi(c[d] + sgn, n[d], p[d]) < 0) {
+                missing++;
+                continue;
+            }
+            s += A(d == 0 ? sgn : 0, d == 1 ? sgn : 0, d == 2 ? sgn : 0);
+        }
+    }
+    diag = (T)(-6 + missing);
+    return s;
+}
+
+// mac_offdiag_vd on the tile (Rv: 1/rho of the points)
+template <typename T, int WX>
+__device__ __forceinline__ T mac_offdiag_vd_t(const lvl_dev L, const tile_acc<T, WX> &A, const tile_acc<T, WX> &Rv,
+                                              int i, int j, int k, T &diag) {
+    const T rc = Rv(0, 0, 0);
+    if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
+        const T ax1 = (T)0.5 * (Rv(-1, 0, 0) + rc), ax2 = (T)0.5 * (rc + Rv(1, 0, 0));
+        const T ay1 = (T)0.5 * (Rv(0, -1, 0) + rc), ay2 = (T)0.5 * (rc + Rv(0, 1, 0));
+        const T az1 = (T)0.5 * (Rv(0, 0, -1) + rc), az2 = (T)0.5 * (rc + Rv(0, 0, 1));
+        T s = 0, csum = 0;
+        s += ax1 * A(-1, 0, 0) + ax2 * A(1, 0, 0);
+        csum += ax1 + ax2;
+        s += ay1 * A(0, -1, 0) + ay2 * A(0, 1, 0);
+        csum += ay1 + ay2;
+        s += az1 * A(0, 0, -1) + az2 * A(0, 0, 1);
+        csum += az1 + az2;
+        diag = (T)(-6) * (csum / (T)6);
+        return s;
+    }
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int c[3] = {i, j, k};
+    T s = 0, csum = 0;
+    int cnt = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const bool lo = wrapi(c[d] - 1, n[d], p[d]) >= 0, hi = wrapi(c[d] + 1, n[d], p[d]) >= 0;
+        const int da = d == 0, db = d == 1, dc = d == 2;
+        if (lo && hi) {
+            const T a1 = (T)0.5 * (Rv(-da, -db, -dc) + rc), a2 = (T)0.5 * (rc + Rv(da, db, dc));
+            s += a1 * A(-da, -db, -dc) + a2 * A(da, db, dc);
+            csum += a1 + a2;
+            cnt += 2;
+        } else if (lo) {
+            const T a1 = (T)0.5 * (Rv(-da, -db, -dc) + rc);
+            s += a1 * A(-da, -db, -dc);
+            csum += a1;
+            cnt += 1;
+        } else if (hi) {
+            const T a2 = (T)0.5 * (rc + Rv(da, db, dc));
+            s += a2 * A(da, db, dc);
+            csum += a2;
+            cnt += 1;
+        }
+    }
+    diag = (T)(-cnt) * (csum / (T)cnt);
+    return s;
+}
+
+// fem_offdiag on the tile
+template <typename T, int WX>
+__device__ __forceinline__ T fem_offdiag_t(const lvl_dev L, const tile_acc<T, WX> &A, int i, int j, int k, T &diag) {
+    if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
+        T e = (A(-1, -1, 0) + A(1, -1, 0)) + (A(-1, 1, 0) + A(1, 1, 0));
+        e += (A(-1, 0, -1) + A(1, 0, -1)) + (A(0, -1, -1) + A(0, 1, -1));
+        e += (A(-1, 0, 1) + A(1, 0, 1)) + (A(0, -1, 1) + A(0, 1, 1));
+        T q = (A(-1, -1, -1) + A(1, -1, -1)) + (A(-1, 1, -1) + A(1, 1, -1));
+        q += (A(-1, -1, 1) + A(1, -1, 1)) + (A(-1, 1, 1) + A(1, 1, 1));
+        diag = (T)32;
+        return (T)-2 * e - q;
+    }
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int c[3] = {i, j, k};
+    bool bd[3], ok[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        bd[d] = !p[d] && (c[d] == 0 || c[d] == n[d] - 1);
+#pragma unroll
+        for (int o = -1; o <= 1; o++) ok[d][o + 1] = wrapi(c[d] + o, n[d], p[d]) >= 0;
+    }
+    T s = 0;
+#pragma unroll
+    for (int oc = 0; oc < 3; oc++) {
+        if (!ok[2][oc]) continue;
+#pragma unroll
+        for (int ob = 0; ob < 3; ob++) {
+            if (!ok[1][ob]) continue;
+#pragma unroll
+            for (int oa = 0; oa < 3; oa++) {
+                if (!ok[0][oa]) continue;
+                const int nz = (oa != 1) + (ob != 1) + (oc != 1);
+                if (nz == 0 || nz == 1) continue;  // centre handled below, faces are 0
+                T co = (nz == 2) ? (T)-2 : (T)-1;
+                const int halve = (bd[0] && oa == 1) + (bd[1] && ob == 1) + (bd[2] && oc == 1);
+                if (halve == 1) co *= (T)0.5;
+                else if (halve == 2) co *= (T)0.25;
+                s += co * A(oa - 1, ob - 1, oc - 1);
+            }
+        }
+    }
+    const int hc = bd[0] + bd[1] + bd[2];
+    diag = (T)32 / (T)(1 << hc);
+    return s;
+}
+
+// fem_offdiag_vd on the tile.  Rv reads the cells of the tile of cells: the
+// cell below-left-front of the node is Rv(0, 0, 0) (its plane pointer pc is
+// the cell plane k-1), the one above-right-back Rv(1, 1, 1).
+template <typename T, int WX, int CX>
+__device__ __forceinline__ T fem_offdiag_vd_t(const lvl_dev L, const tile_acc<T, WX> &A, const tile_acc<T, CX> &Rv,
+                                              int i, int j, int k, T &diag) {
+    if (i > 0 && i < L.n0 - 1 && j > 0 && j < L.n1 - 1 && k > 0 && k < L.n2 - 1) {
+        T v[2][2][2];
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) v[a][b][e] = Rv(e, b, a);
+        T s = 0;
+#pragma unroll
+        for (int oc = 0; oc < 3; oc++)
+#pragma unroll
+            for (int ob = 0; ob < 3; ob++)
+#pragma unroll
+                for (int oa = 0; oa < 3; oa++) {
+                    const int nz = (oa != 1) + (ob != 1) + (oc != 1);
+                    if (nz <= 1) continue;
+                    const T xv = A(oa - 1, ob - 1, oc - 1);
+                    T cf;
+                    if (nz == 3) {
+                        cf = -v[oc >> 1][ob >> 1][oa >> 1];
+                    } else if (oc == 1) {
+                        cf = (T)-2 * ((v[0][ob >> 1][oa >> 1] + v[1][ob >> 1][oa >> 1]) * (T)0.5);
+                    } else if (ob == 1) {
+                        cf = (T)-2 * ((v[oc >> 1][0][oa >> 1] + v[oc >> 1][1][oa >> 1]) * (T)0.5);
+                    } else {
+                        cf = (T)-2 * ((v[oc >> 1][ob >> 1][0] + v[oc >> 1][ob >> 1][1]) * (T)0.5);
+                    }
+                    s += cf * xv;
+                }
+        T c8 = 0;
+#pragma unroll
+        for (int a = 0; a < 2; a++)
+#pragma unroll
+            for (int b = 0; b < 2; b++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) c8 += v[a][b][e];
+        diag = (T)32 * (c8 * (T)0.125);
+        return s;
+    }
+    const int n[3] = {L.n0, L.n1, L.n2}, p[3] = {L.p0, L.p1, L.p2};
+    const int nc[3] = {p[0] ? n[0] : n[0] - 1, p[1] ? n[1] : n[1] - 1, p[2] ? n[2] : n[2] - 1};
+    const int c[3] = {i, j, k};
+    bool cell[3][2];  // the cells below / above the node on each axis exist
+    bool bd[3], ok[3][3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        bd[d] = !p[d] && (c[d] == 0 || c[d] == n[d] - 1);
+        cell[d][0] = (c[d] - 1 >= 0) || p[d];
+        cell[d][1] = (c[d] < nc[d]) || p[d];
+#pragma unroll
+        for (int o = -1; o <= 1; o++) ok[d][o + 1] = wrapi(c[d] + o, n[d], p[d]) >= 0;
+    }
+    T v[2][2][2];
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) v[a][b][e] = (cell[0][e] && cell[1][b] && cell[2][a]) ? Rv(e, b, a) : (T)0;
+    T s = 0;
+#pragma unroll
+    for (int oc = 0; oc < 3; oc++) {
+#pragma unroll
+        for (int ob = 0; ob < 3; ob++) {
+#pragma unroll
+            for (int oa = 0; oa < 3; oa++) {
+                const int nz = (oa != 1) + (ob != 1) + (oc != 1);
+                if (nz <= 1) continue;
+                if (!ok[2][oc] || !ok[1][ob] || !ok[0][oa]) continue;
+                T co = (nz == 2) ? (T)-2 : (T)-1;
+                const int halve = (bd[0] && oa == 1) + (bd[1] && ob == 1) + (bd[2] && oc == 1);
+                if (halve == 1) co *= (T)0.5;
+                else if (halve == 2) co *= (T)0.25;
+                T sum = 0;
+                int num = 0;
+#pragma unroll
+                for (int a = (oc == 2 ? 1 : 0); a <= (oc == 0 ? 0 : 1); a++)
+#pragma unroll
+                    for (int b = (ob == 2 ? 1 : 0); b <= (ob == 0 ? 0 : 1); b++)
+#pragma unroll
+                        for (int e = (oa == 2 ? 1 : 0); e <= (oa == 0 ? 0 : 1); e++)
+                            if (cell[2][a] && cell[1][b] && cell[0][e]) {
+                                sum += v[a][b][e];
+                                num++;
+                            }
+                s += co * div_pow2(sum, num) * A(oa - 1, ob - 1, oc - 1);
+            }
+        }
+    }
+    T sum = 0;
+    int num = 0;
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++)
+#pragma unroll
+            for (int e = 0; e < 2; e++)
+                if (cell[2][a] && cell[1][b] && cell[0][e]) {
+                    sum += v[a][b][e];
+                    num++;
+                }
+    const int hc = bd[0] + bd[1] + bd[2];
+    diag = ((T)32 / (T)(1 << hc)) * div_pow2(sum, num);
+    return s;
+}
+
+// ---- the sweep ----------------------------------------------------------------
+// Global coordinate of local index l on an axis whose tile starts at u0:
+// wrapped on a periodic axis, -1 outside a walled one.
+__device__ __forceinline__ int tile_coord(int u, int n, int prd) {
+    if (u < 0) return prd ? ((u % n) + n) % n : -1;
+    if (u >= n) return prd ? u % n : -1;
+    return u;
+}
+
+// One sweep of the level over the output tile starting at (X0, Y0) and the
+// planes [z0, z1): reads xin, writes xout (both the level's layout).
+template <typename T, int KIND, bool VD>
+__device__ __forceinline__ void body_tile_sweep(const lvl_dev L, const T *__restrict__ xin, T *__restrict__ xout,
+                                                const T *__restrict__ r, const T *__restrict__ ri, int X0, int Y0,
+                                                int z0, int z1, unsigned char *smem) {
+    using S = tile_shape<KIND>;
+    constexpr int C = S::C, H = S::H, WX = S::WX, WY = S::WY, R = S::R, CX = S::CX, CY = S::CY;
+    T *xs = reinterpret_cast<T *>(smem);
+    T *rs = xs + R * WX * WY;  // 1/rho planes (VD)
+    const int tid = threadIdx.x;
+    const int n0 = L.n0, n1 = L.n1, n2 = L.n2;
+    const size_t sy = (size_t)n0, sz = (size_t)n0 * n1;
+    // planes this block loads: its chunk and H more on each side, ended by walls
+    int zs = z0 - H, ze = z1 + H - 1;
+    const bool wall_lo = !L.p2 && zs < 0, wall_hi = !L.p2 && ze > n2 - 1;
+    if (wall_lo) zs = 0;
+    if (wall_hi) ze = n2 - 1;
+    // 1/rho cells of the FEM nodes: cell planes from zs-1 (cell k-1 of node k)
+    const int nc0 = L.p0 ? n0 : n0 - 1, nc1 = L.p1 ? n1 : n1 - 1, nc2 = L.p2 ? n2 : n2 - 1;
+
+    auto load_plane = [&](int t) {
+        const int gz = tile_coord(t, n2, L.p2);
+        T *pl = xs + (((t % R) + R) % R) * WX * WY;
+        for (int e = tid; e < WX * WY; e += S::NT) {
+            const int lx = e % WX, ly = e / WX;
+            const int gx = tile_coord(X0 - H + lx, n0, L.p0), gy = tile_coord(Y0 - H + ly, n1, L.p1);
+            pl[e] = (gx >= 0 && gy >= 0 && gz >= 0) ? xin[gx + sy * gy + sz * gz] : (T)0;
+        }
+        if constexpr (VD) {
+            if constexpr (KIND == 0) {
+                T *cp = rs + (((t % R) + R) % R) * CX * CY;
+                for (int e = tid; e < CX * CY; e += S::NT) {
+                    const int lx = e % CX, ly = e / CX;
+                    const int gx = tile_coord(X0 - H + lx, n0, L.p0), gy = tile_coord(Y0 - H + ly, n1, L.p1);
+                    cp[e] = (gx >= 0 && gy >= 0 && gz >= 0) ? ri[gx + sy * gy + sz * gz] : (T)0;
+                }
+            }
+        }
+    };
+    // FEM 1/rho: cell plane t (cells between node planes t and t+1)
+    auto load_cells = [&](int t) {
+        if constexpr (VD && KIND == 1) {
+            const int cz = tile_coord(t, nc2, L.p2);
+            T *cp = rs + (((t % R) + R) % R) * CX * CY;
+            for (int e = tid; e < CX * CY; e += S::NT) {
+                const int lx = e % CX, ly = e / CX;
+                const int cx = tile_coord(X0 - H - 1 + lx, nc0, L.p0), cy = tile_coord(Y0 - H - 1 + ly, nc1, L.p1);
+                cp[e] = (cx >= 0 && cy >= 0 && cz >= 0) ? ri[cx + (size_t)nc0 * (cy + (size_t)nc1 * cz)] : (T)0;
+            }
+        }
+    };
+
+    if (VD && KIND == 1) load_cells(zs - 1);
+    for (int t = zs; t <= ze + C; t++) {
+        if (t <= ze) {
+            load_plane(t);
+            load_cells(t);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const int q = t - 1 - c;
+            // planes where pass c is exact: all of them next to a wall, one
+            // fewer per pass at an open end of the chunk
+            const int qlo = wall_lo ? zs : zs + c + 1, qhi = wall_hi ? ze : ze - c - 1;
+            if (q >= qlo && q <= qhi) {
+                // x and y range of pass c, in global (unwrapped) coordinates
+                int xlo = X0 - H + c + 1, xhi = X0 + S::TX + H - 2 - c;
+                int ylo = Y0 - H + c + 1, yhi = Y0 + S::TY + H - 2 - c;
+                if (!L.p0) {
+                    xlo = max(xlo, 0);
+                    xhi = min(xhi, n0 - 1);
+                }
+                if (!L.p1) {
+                    ylo = max(ylo, 0);
+                    yhi = min(yhi, n1 - 1);
+                }
+                const T *pm = xs + ((((q - 1) % R) + R) % R) * WX * WY;
+                T *pc = xs + (((q % R) + R) % R) * WX * WY;
+                const T *pp = xs + ((((q + 1) % R) + R) % R) * WX * WY;
+                const int gz = tile_coord(q, n2, L.p2);
+                // points of colour c in the range
+                int px, py, nx, ny;
+                if constexpr (KIND == 1) {
+                    px = (xlo & 1) == (c & 1) ? xlo : xlo + 1;
+                    py = (ylo & 1) == ((c >> 1) & 1) ? ylo : ylo + 1;
+                    nx = xhi >= px ? (xhi - px) / 2 + 1 : 0;
+                    ny = yhi >= py ? (yhi - py) / 2 + 1 : 0;
+                } else {
+                    nx = (xhi - xlo + 2) / 2;  // points of one parity per row, at most
+                    ny = yhi - ylo + 1;
+                    px = xlo;
+                    py = ylo;
+                }
+                for (int e = tid; e < nx * ny; e += S::NT) {
+                    int ux, uy;
+                    if constexpr (KIND == 1) {
+                        ux = px + 2 * (e % nx);
+                        uy = py + 2 * (e / nx);
+                    } else {
+                        uy = py + e / nx;
+                        const int x0 = xlo + (((xlo + uy + q + c) & 1) ? 1 : 0);  // first of colour c in the row
+                        ux = x0 + 2 * (e % nx);
+                        if (ux > xhi) continue;
+                    }
+                    const int lx = ux - (X0 - H), ly = uy - (Y0 - H);
+                    const int gx = tile_coord(ux, n0, L.p0), gy = tile_coord(uy, n1, L.p1);
+                    const int o = lx + WX * ly;
+                    tile_acc<T, WX> A{pm, pc, pp, o};
+                    const T rv = r[gx + sy * gy + sz * gz];
+                    T diag, s;
+                    if constexpr (KIND == 0) {
+                        if constexpr (VD) {
+                            const T *rm = rs + ((((q - 1) % R) + R) % R) * CX * CY;
+                            const T *rc = rs + (((q % R) + R) % R) * CX * CY;
+                            const T *rp = rs + ((((q + 1) % R) + R) % R) * CX * CY;
+                            tile_acc<T, CX> Rv{rm, rc, rp, lx + CX * ly};
+                            s = mac_offdiag_vd_t<T, WX>(L, A, Rv, gx, gy, gz, diag);
+                        } else {
+                            s = mac_offdiag_t<T, WX>(L, A, gx, gy, gz, diag);
+                        }
+                        pc[o] = (rv - s) / diag;
+                    } else {
+                        if constexpr (VD) {
+                            // cells (node - 1) and node: the cell tile is one
+                            // wider, its local index lx is the cell left of node lx
+                            const T *cm = rs + ((((q - 1) % R) + R) % R) * CX * CY;
+                            const T *cc = rs + (((q % R) + R) % R) * CX * CY;
+                            tile_acc<T, CX> Rv{nullptr, cm, cc, lx + CX * ly};
+                            s = fem_offdiag_vd_t<T, WX, CX>(L, A, Rv, gx, gy, gz, diag);
+                            pc[o] = (rv - s) / diag;
+                        } else {
+                            s = fem_offdiag_t<T, WX>(L, A, gx, gy, gz, diag);
+                            pc[o] = (rv - s) * fem_inv_diag<T>(L, gx, gy, gz);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // plane t-C has had every pass: write the block's output part
+        const int q = t - C;
+        if (q >= z0 && q < z1 && q >= 0 && q < n2) {
+            const T *pl = xs + (((q % R) + R) % R) * WX * WY;
+            for (int e = tid; e < S::TX * S::TY; e += S::NT) {
+                const int ux = X0 + e % S::TX, uy = Y0 + e / S::TX;
+                if (ux < n0 && uy < n1) xout[ux + sy * uy + sz * q] = pl[(ux - X0 + H) + WX * (uy - Y0 + H)];
+            }
+        }
+    }
+}
+
+}  // namespace rmt3d

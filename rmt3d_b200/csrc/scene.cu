@@ -2630,6 +2630,27 @@ extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, in
     return RMT3D_OK;
 }
 
+namespace rmt3d {
+void scene_schedule(rmt3d_scene *s, int out[4]) {
+    out[0] = s->mac.v_down;
+    out[1] = s->mac.v_up;
+    out[2] = s->mac.smoother;
+    out[3] = s->mac.tile_waves;
+}
+}  // namespace rmt3d
+
+extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode, int tile_waves) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (mode < 0 || mode > 1) return fail(RMT3D_ERR_INVALID, "smoother mode must be 0 (colour passes) or 1 (tiled sweeps)");
+    if (tile_waves < 1 || tile_waves > 64) return fail(RMT3D_ERR_INVALID, "tile_waves outside 1..64");
+    s->mac.smoother = s->fem.smoother = mode;
+    s->mac.tile_waves = s->fem.tile_waves = tile_waves;
+    s->mac.invalidate();
+    s->fem.invalidate();
+    mark_dirty(s);
+    return RMT3D_OK;
+}
+
 extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     // mirrors the allocations of rmt3d_scene_create and mg_solver::setup
     if (!d || d->sys_size[0] < 1 || d->sys_size[1] < 1 || d->sys_size[2] < 1) return 0;
