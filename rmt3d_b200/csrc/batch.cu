@@ -345,12 +345,18 @@ extern "C" int rmt3d_batch_destroy(rmt3d_batch *b) {
 }
 
 // ---------------------------------------------------------------------------
-// Serving loop: requests arrive over time; each is admitted when a slot (a
-// host worker with its own stream) is free and its device footprint fits the
-// remaining HBM budget.  Admitted requests run concurrently on the device
-// (continuous batching: a request that arrives while others run starts as
-// soon as a slot and memory free up, without waiting for a batch boundary).
-// Per-step and per-request latencies are recorded.
+// Serving loop with continuous batching.  Requests arrive over time.  A pool
+// of set-up threads admits each arrived request, in arrival order, when its
+// device footprint fits the remaining HBM budget and fewer than max_slots
+// requests are in the system, and sets its scene up (initialize, dt fit,
+// pressure pre-iterations) on the scene's own stream while the running
+// scenes keep stepping.  The stepping thread runs in rounds: scenes of the
+// same kind (grid shape, periodicity, form, schedule) step together as one
+// group graph -- each multigrid solve batched over the group -- for up to
+// kServeRound steps, the groups of all kinds in flight at once; at the end of
+// a round finished requests leave, their memory returns to the budget, and
+// newly set-up requests join their kind's group.  A group is rebuilt only
+// when its membership changes.
 // ---------------------------------------------------------------------------
 extern "C" int rmt3d_scene_checksum(rmt3d_scene *s, double out[4]);
 extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d);
@@ -362,6 +368,24 @@ double pct(std::vector<double> v, double q) {
     double pos = q * (v.size() - 1);
     size_t lo = (size_t)pos, hi = std::min(lo + 1, v.size() - 1);
     return v[lo] + (pos - lo) * (v[hi] - v[lo]);
+}
+
+constexpr int kServeRound = 10;  // steps per round of the stepping thread
+
+struct served {
+    int id;
+    rmt3d_scene *s;
+    int left;   // steps still to run
+    size_t fp;  // footprint held against the budget
+};
+
+// the kind of a scene: what a group's members must share
+std::array<double, 14> serve_key(rmt3d_scene *s, const rmt3d_scene_desc &d) {
+    int sch[4];
+    rmt3d::scene_schedule(s, sch);
+    return {(double)d.sys_size[0], (double)d.sys_size[1], (double)d.sys_size[2], (double)d.periodic[0],
+            (double)d.periodic[1], (double)d.periodic[2], (double)d.precision, (double)d.var_den,
+            (double)d.mg_exact, d.mixed_rtol, (double)sch[0], (double)sch[1], (double)sch[2], (double)sch[3]};
 }
 }  // namespace
 
@@ -376,97 +400,179 @@ extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budge
     std::mutex mu;
     std::vector<char> taken(nreq, 0);
     size_t used = 0;
-    int done = 0;
+    int in_system = 0;  // admitted and not yet finished
+    int finished = 0;
+    std::vector<served> ready;  // set up, waiting for the next round
     std::atomic<int> first_err{0};
     std::string err_msg;
     std::vector<std::vector<double>> step_ms(nreq);
+    for (int i = 0; i < nreq; i++) memset(&results[i], 0, sizeof(results[i]));
     const auto t0 = std::chrono::steady_clock::now();
     auto now_s = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
-    std::vector<long long> cellsteps(max_slots, 0);
-    auto worker = [&](int slot) {
+    auto note_err = [&](int e) {
+        if (e && !first_err.exchange(e)) {
+            std::lock_guard<std::mutex> lk(mu);
+            err_msg = rmt3d_last_error();
+        }
+    };
+    // ---- set-up threads: admission by budget and slots, then set-up ----
+    auto setup_worker = [&]() {
         cudaSetDevice(dev);
-        while (true) {
+        while (!first_err) {
             int pick = -1;
             size_t fp = 0;
             {
                 std::lock_guard<std::mutex> lk(mu);
-                if (done >= nreq || first_err) return;
-                double t = now_s();
-                // earliest arrived request that fits the free budget
+                bool any_left = false;
+                const double t = now_s();
                 for (int i = 0; i < nreq; i++) {
-                    if (taken[i] || reqs[i].arrival_s > t) continue;
-                    size_t f = rmt3d_scene_footprint(&reqs[i].desc);
-                    if (used + f <= hbm_budget) {
+                    if (taken[i]) continue;
+                    any_left = true;
+                    if (reqs[i].arrival_s > t) break;  // arrival order
+                    const size_t f = rmt3d_scene_footprint(&reqs[i].desc);
+                    if (in_system < max_slots && used + f <= hbm_budget) {
                         pick = i;
                         fp = f;
-                        break;
                     }
+                    break;  // the earliest waiting request goes first
                 }
+                if (!any_left) return;
                 if (pick >= 0) {
                     taken[pick] = 1;
                     used += fp;
-                } else {
-                    bool any_left = false;
-                    for (int i = 0; i < nreq; i++)
-                        if (!taken[i]) any_left = true;
-                    if (!any_left) return;
+                    in_system++;
                 }
             }
             if (pick < 0) {
                 std::this_thread::sleep_for(std::chrono::microseconds(200));
                 continue;
             }
-            rmt3d_request_result &R = results[pick];
-            memset(&R, 0, sizeof(R));
-            R.admit_s = now_s();
+            results[pick].admit_s = now_s();
             rmt3d_scene *s = nullptr;
             int e = rmt3d_scene_create(&reqs[pick].desc, nullptr, &s);
             if (!e) e = rmt3d_prepare(s);
-            int st = 0;
-            for (int k = 0; !e && k < reqs[pick].steps && st == 0; k++) {
-                auto a = std::chrono::steady_clock::now();
-                e = rmt3d_step(s, 0, &st);
-                if (!e) e = rmt3d_sync(s);
-                step_ms[pick].push_back(
-                    1e3 * std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count());
+            if (e) {
+                note_err(e);
+                if (s) rmt3d_scene_destroy(s);
+                return;
             }
-            if (!e) e = rmt3d_scene_checksum(s, R.checksum);
-            R.finish_s = now_s();
-            R.latency_s = R.finish_s - reqs[pick].arrival_s;
-            R.status = e ? e : st;
-            R.steps_done = (int)step_ms[pick].size();
-            R.step_p50_ms = pct(step_ms[pick], 0.5);
-            R.step_p99_ms = pct(step_ms[pick], 0.99);
-            cellsteps[slot] += (long long)R.steps_done * reqs[pick].desc.sys_size[0] * reqs[pick].desc.sys_size[1] *
-                               reqs[pick].desc.sys_size[2];
-            if (e && !first_err.exchange(e)) {
-                std::lock_guard<std::mutex> lk(mu);
-                err_msg = rmt3d_last_error();
-            }
-            rmt3d_scene_destroy(s);
             std::lock_guard<std::mutex> lk(mu);
-            used -= fp;
-            done++;
+            ready.push_back(served{pick, s, reqs[pick].steps, fp});
         }
     };
     std::vector<std::thread> th;
-    for (int k = 0; k < max_slots; k++) th.emplace_back(worker, k);
+    const int nsetup = std::max(1, std::min(4, max_slots));
+    for (int k = 0; k < nsetup; k++) th.emplace_back(setup_worker);
+
+    // ---- the stepping thread (this one): rounds over the kinds' groups ----
+    struct kind_group {
+        std::vector<served> m;
+        rmt3d::scene_group *g = nullptr;
+        bool dirty = true;
+    };
+    std::map<std::array<double, 14>, kind_group> kinds;
+    long long cellsteps = 0;
+    while (!first_err) {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (finished >= nreq) break;
+            for (auto &r : ready) {
+                kind_group &kg = kinds[serve_key(r.s, reqs[r.id].desc)];
+                kg.m.push_back(r);
+                kg.dirty = true;
+            }
+            ready.clear();
+        }
+        bool any = false;
+        std::vector<std::pair<kind_group *, int>> launched;
+        for (auto &kv : kinds) {
+            kind_group &kg = kv.second;
+            if (kg.m.empty()) continue;
+            if (kg.dirty) {
+                if (kg.g) rmt3d::group_destroy(kg.g);
+                kg.g = nullptr;
+                std::vector<rmt3d_scene *> sc;
+                for (auto &r : kg.m) sc.push_back(r.s);
+                int e = rmt3d::group_create(sc.data(), (int)sc.size(), &kg.g);
+                if (e) {
+                    note_err(e);
+                    break;
+                }
+                kg.dirty = false;
+            }
+            int k = kServeRound;
+            for (auto &r : kg.m) k = std::min(k, r.left);
+            int e = rmt3d::group_launch(kg.g, k);
+            if (e) {
+                note_err(e);
+                break;
+            }
+            launched.emplace_back(&kg, k);
+            any = true;
+        }
+        if (!any) {
+            std::this_thread::sleep_for(std::chrono::microseconds(200));
+            continue;
+        }
+        const auto ta = std::chrono::steady_clock::now();
+        for (auto &lk_ : launched) {
+            kind_group &kg = *lk_.first;
+            const int k = lk_.second;
+            std::vector<int> st(kg.m.size(), 0);
+            int e = rmt3d::group_finish(kg.g, st.data());
+            const double ms = 1e3 * std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count() / k;
+            std::vector<served> keep;
+            for (size_t j = 0; j < kg.m.size(); j++) {
+                served &r = kg.m[j];
+                rmt3d_request_result &R = results[r.id];
+                for (int q = 0; q < k; q++) step_ms[r.id].push_back(ms);
+                r.left -= k;
+                if (r.left > 0 && st[j] == 0 && !e) {
+                    keep.push_back(r);
+                    continue;
+                }
+                // finished (or failed): the result, then the memory back
+                R.steps_done = reqs[r.id].steps - std::max(r.left, 0);
+                R.status = e ? e : st[j];
+                if (rmt3d_scene_checksum(r.s, R.checksum) && !R.status) R.status = RMT3D_ERR_CUDA;
+                R.finish_s = now_s();
+                R.latency_s = R.finish_s - reqs[r.id].arrival_s;
+                R.step_p50_ms = pct(step_ms[r.id], 0.5);
+                R.step_p99_ms = pct(step_ms[r.id], 0.99);
+                cellsteps += (long long)R.steps_done * reqs[r.id].desc.sys_size[0] * reqs[r.id].desc.sys_size[1] *
+                             reqs[r.id].desc.sys_size[2];
+                kg.dirty = true;
+                if (kg.g) rmt3d::group_destroy(kg.g);  // before its member goes
+                kg.g = nullptr;
+                rmt3d_scene_destroy(r.s);
+                std::lock_guard<std::mutex> lk(mu);
+                used -= r.fp;
+                in_system--;
+                finished++;
+            }
+            kg.m.swap(keep);
+            note_err(e);
+        }
+    }
     for (auto &x : th) x.join();
+    for (auto &kv : kinds) {
+        if (kv.second.g) rmt3d::group_destroy(kv.second.g);
+        for (auto &r : kv.second.m) rmt3d_scene_destroy(r.s);
+    }
+    for (auto &r : ready) rmt3d_scene_destroy(r.s);
     const double wall = now_s();
     if (summary) {
         std::vector<double> lat, steps;
-        long long cs = 0;
         for (int i = 0; i < nreq; i++) {
             lat.push_back(results[i].latency_s);
             steps.insert(steps.end(), step_ms[i].begin(), step_ms[i].end());
         }
-        for (long long c : cellsteps) cs += c;
         summary->wall_s = wall;
         summary->request_p50_s = pct(lat, 0.5);
         summary->request_p99_s = pct(lat, 0.99);
         summary->step_p50_ms = pct(steps, 0.5);
         summary->step_p99_ms = pct(steps, 0.99);
-        summary->cellsteps_per_s = cs / wall;
+        summary->cellsteps_per_s = cellsteps / wall;
         summary->requests = nreq;
     }
     if (first_err) return rmt3d::fail(first_err, err_msg);

@@ -5,9 +5,10 @@
 // pass c-1 wrote at distance one.  A block owns an output tile of TX x TY
 // points in x, y and a chunk of planes in z.  It stages the tile with a halo
 // of H = C points (C colours) in x and y, and streams the planes in z through
-// a ring of C + 2 planes in shared memory as a wavefront: in iteration t it
-// loads plane t, then runs pass 0 on plane t-1, pass 1 on plane t-2, ...,
-// pass C-1 on plane t-C, and writes plane t-C back.  Pass c on plane q needs
+// a ring of C + 3 planes in shared memory as a wavefront: in iteration t it
+// starts the asynchronous copy (cp.async) of plane t+1, waits for plane t (x
+// and the right-hand side), runs pass 0 on plane t-1, pass 1 on plane t-2,
+// ..., pass C-1 on plane t-C, and writes plane t-C back.  Pass c on plane q needs
 // planes q-1..q+1 after pass c-1, which the wavefront provides: plane q+1
 // received pass c-1 earlier in the same iteration, plane q-1 one iteration
 // before (and pass c there touched only colour-c points, which pass c on
@@ -38,18 +39,34 @@ struct tile_shape {
     static constexpr int TX = 32;
     static constexpr int TY = KIND == 0 ? 16 : 8;
     static constexpr int WX = TX + 2 * H, WY = TY + 2 * H;
-    static constexpr int R = C + 2;  // planes in the ring
+    // planes in the ring: C + 2 in use at once, one more being fetched
+    static constexpr int R = C + 3;
     static constexpr int NT = 256;   // threads per block
     // variable density: 1/rho per cell.  MAC cells are the points; the FEM
     // tile of cells is one wider (node i uses cells i-1 and i)
     static constexpr int CX = KIND == 0 ? WX : WX + 1, CY = KIND == 0 ? WY : WY + 1;
 };
 
+// x and right-hand-side rings, and the 1/rho ring with variable density
 template <typename T, int KIND, bool VD>
 constexpr size_t tile_smem_bytes() {
     using S = tile_shape<KIND>;
-    return (size_t)S::R * S::WX * S::WY * sizeof(T) + (VD ? (size_t)S::R * S::CX * S::CY * sizeof(T) : 0);
+    return 2 * (size_t)S::R * S::WX * S::WY * sizeof(T) + (VD ? (size_t)S::R * S::CX * S::CY * sizeof(T) : 0);
 }
+
+// asynchronous global -> shared copy of one element (LDGSTS), committed per plane
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N committed groups of this thread are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // ---- stencils on the tile ---------------------------------------------------
 // A point's neighbours are read through three plane pointers (z-1, z, z+1)
@@ -316,7 +333,8 @@ __device__ __forceinline__ void body_tile_sweep(const lvl_dev L, const T *__rest
     using S = tile_shape<KIND>;
     constexpr int C = S::C, H = S::H, WX = S::WX, WY = S::WY, R = S::R, CX = S::CX, CY = S::CY;
     T *xs = reinterpret_cast<T *>(smem);
-    T *rs = xs + R * WX * WY;  // 1/rho planes (VD)
+    T *rr = xs + R * WX * WY;  // right-hand-side planes
+    T *rs = rr + R * WX * WY;  // 1/rho planes (VD)
     const int tid = threadIdx.x;
     const int n0 = L.n0, n1 = L.n1, n2 = L.n2;
     const size_t sy = (size_t)n0, sz = (size_t)n0 * n1;
@@ -327,45 +345,56 @@ __device__ __forceinline__ void body_tile_sweep(const lvl_dev L, const T *__rest
     if (wall_hi) ze = n2 - 1;
     // 1/rho cells of the FEM nodes: cell planes from zs-1 (cell k-1 of node k)
     const int nc0 = L.p0 ? n0 : n0 - 1, nc1 = L.p1 ? n1 : n1 - 1, nc2 = L.p2 ? n2 : n2 - 1;
+    auto slot = [&](int t) { return ((t % R) + R) % R; };
 
-    auto load_plane = [&](int t) {
+    // plane t of x and r (and of 1/rho for MAC), fetched asynchronously;
+    // points outside a walled domain are zero
+    auto fetch_plane = [&](int t) {
         const int gz = tile_coord(t, n2, L.p2);
-        T *pl = xs + (((t % R) + R) % R) * WX * WY;
+        T *pl = xs + slot(t) * WX * WY;
+        T *pr = rr + slot(t) * WX * WY;
         for (int e = tid; e < WX * WY; e += S::NT) {
             const int lx = e % WX, ly = e / WX;
             const int gx = tile_coord(X0 - H + lx, n0, L.p0), gy = tile_coord(Y0 - H + ly, n1, L.p1);
-            pl[e] = (gx >= 0 && gy >= 0 && gz >= 0) ? xin[gx + sy * gy + sz * gz] : (T)0;
-        }
-        if constexpr (VD) {
-            if constexpr (KIND == 0) {
-                T *cp = rs + (((t % R) + R) % R) * CX * CY;
-                for (int e = tid; e < CX * CY; e += S::NT) {
-                    const int lx = e % CX, ly = e / CX;
-                    const int gx = tile_coord(X0 - H + lx, n0, L.p0), gy = tile_coord(Y0 - H + ly, n1, L.p1);
-                    cp[e] = (gx >= 0 && gy >= 0 && gz >= 0) ? ri[gx + sy * gy + sz * gz] : (T)0;
-                }
+            if (gx >= 0 && gy >= 0 && gz >= 0) {
+                const size_t gi = gx + sy * gy + sz * gz;
+                cp_async_elem(pl + e, xin + gi);
+                cp_async_elem(pr + e, r + gi);
+                if constexpr (VD && KIND == 0) cp_async_elem(rs + slot(t) * CX * CY + e, ri + gi);
+            } else {
+                pl[e] = (T)0;
+                pr[e] = (T)0;
+                if constexpr (VD && KIND == 0) rs[slot(t) * CX * CY + e] = (T)0;
             }
         }
     };
     // FEM 1/rho: cell plane t (cells between node planes t and t+1)
-    auto load_cells = [&](int t) {
+    auto fetch_cells = [&](int t) {
         if constexpr (VD && KIND == 1) {
             const int cz = tile_coord(t, nc2, L.p2);
-            T *cp = rs + (((t % R) + R) % R) * CX * CY;
+            T *cp = rs + slot(t) * CX * CY;
             for (int e = tid; e < CX * CY; e += S::NT) {
                 const int lx = e % CX, ly = e / CX;
                 const int cx = tile_coord(X0 - H - 1 + lx, nc0, L.p0), cy = tile_coord(Y0 - H - 1 + ly, nc1, L.p1);
-                cp[e] = (cx >= 0 && cy >= 0 && cz >= 0) ? ri[cx + (size_t)nc0 * (cy + (size_t)nc1 * cz)] : (T)0;
+                if (cx >= 0 && cy >= 0 && cz >= 0) cp_async_elem(cp + e, ri + cx + (size_t)nc0 * (cy + (size_t)nc1 * cz));
+                else cp[e] = (T)0;
             }
         }
     };
 
-    if (VD && KIND == 1) load_cells(zs - 1);
+    // prologue: the first plane (and the cell plane below it)
+    if (VD && KIND == 1) fetch_cells(zs - 1);
+    fetch_plane(zs);
+    fetch_cells(zs);
+    cp_async_commit();
     for (int t = zs; t <= ze + C; t++) {
-        if (t <= ze) {
-            load_plane(t);
-            load_cells(t);
+        // fetch plane t+1 while the passes of this iteration run
+        if (t + 1 <= ze) {
+            fetch_plane(t + 1);
+            fetch_cells(t + 1);
         }
+        cp_async_commit();
+        cp_async_wait<1>();  // plane t has landed
         __syncthreads();
 #pragma unroll
         for (int c = 0; c < C; c++) {
@@ -385,9 +414,10 @@ __device__ __forceinline__ void body_tile_sweep(const lvl_dev L, const T *__rest
                     ylo = max(ylo, 0);
                     yhi = min(yhi, n1 - 1);
                 }
-                const T *pm = xs + ((((q - 1) % R) + R) % R) * WX * WY;
-                T *pc = xs + (((q % R) + R) % R) * WX * WY;
-                const T *pp = xs + ((((q + 1) % R) + R) % R) * WX * WY;
+                const T *pm = xs + slot(q - 1) * WX * WY;
+                T *pc = xs + slot(q) * WX * WY;
+                const T *pp = xs + slot(q + 1) * WX * WY;
+                const T *prq = rr + slot(q) * WX * WY;
                 const int gz = tile_coord(q, n2, L.p2);
                 // points of colour c in the range
                 int px, py, nx, ny;
@@ -417,14 +447,12 @@ __device__ __forceinline__ void body_tile_sweep(const lvl_dev L, const T *__rest
                     const int gx = tile_coord(ux, n0, L.p0), gy = tile_coord(uy, n1, L.p1);
                     const int o = lx + WX * ly;
                     tile_acc<T, WX> A{pm, pc, pp, o};
-                    const T rv = r[gx + sy * gy + sz * gz];
+                    const T rv = prq[o];
                     T diag, s;
                     if constexpr (KIND == 0) {
                         if constexpr (VD) {
-                            const T *rm = rs + ((((q - 1) % R) + R) % R) * CX * CY;
-                            const T *rc = rs + (((q % R) + R) % R) * CX * CY;
-                            const T *rp = rs + ((((q + 1) % R) + R) % R) * CX * CY;
-                            tile_acc<T, CX> Rv{rm, rc, rp, lx + CX * ly};
+                            tile_acc<T, CX> Rv{rs + slot(q - 1) * CX * CY, rs + slot(q) * CX * CY,
+                                               rs + slot(q + 1) * CX * CY, lx + CX * ly};
                             s = mac_offdiag_vd_t<T, WX>(L, A, Rv, gx, gy, gz, diag);
                         } else {
                             s = mac_offdiag_t<T, WX>(L, A, gx, gy, gz, diag);
@@ -434,9 +462,8 @@ __device__ __forceinline__ void body_tile_sweep(const lvl_dev L, const T *__rest
                         if constexpr (VD) {
                             // cells (node - 1) and node: the cell tile is one
                             // wider, its local index lx is the cell left of node lx
-                            const T *cm = rs + ((((q - 1) % R) + R) % R) * CX * CY;
-                            const T *cc = rs + (((q % R) + R) % R) * CX * CY;
-                            tile_acc<T, CX> Rv{nullptr, cm, cc, lx + CX * ly};
+                            tile_acc<T, CX> Rv{nullptr, rs + slot(q - 1) * CX * CY, rs + slot(q) * CX * CY,
+                                               lx + CX * ly};
                             s = fem_offdiag_vd_t<T, WX, CX>(L, A, Rv, gx, gy, gz, diag);
                             pc[o] = (rv - s) / diag;
                         } else {
@@ -451,7 +478,7 @@ __device__ __forceinline__ void body_tile_sweep(const lvl_dev L, const T *__rest
         // plane t-C has had every pass: write the block's output part
         const int q = t - C;
         if (q >= z0 && q < z1 && q >= 0 && q < n2) {
-            const T *pl = xs + (((q % R) + R) % R) * WX * WY;
+            const T *pl = xs + slot(q) * WX * WY;
             for (int e = tid; e < S::TX * S::TY; e += S::NT) {
                 const int ux = X0 + e % S::TX, uy = Y0 + e / S::TX;
                 if (ux < n0 && uy < n1) xout[ux + sy * uy + sz * q] = pl[(ux - X0 + H) + WX * (uy - Y0 + H)];

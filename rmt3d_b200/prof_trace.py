@@ -1,11 +1,12 @@
 """Kernel trace of the batched form: every kernel executed inside the group
 step graphs, timed by CUPTI (through torch.profiler), summed per kernel.
 
-    python -m rmt3d_b200.prof_trace <n> [steps=5]
+    python -m rmt3d_b200.prof_trace <n> [steps=5] [smoother=-1]
 
 Builds the scenes of the batched workload (rmt3d_b200.scenes.random_scene,
 seeds 0-31) whose grid is n^3, variable density, mixed form; prepares them as
-one batch, runs 3 warm-up steps, times `steps` batch steps, then traces
+one batch (smoother -1: the autotuner's choice per scene kind; 0 colour
+passes; 1 tiled sweeps), runs 3 warm-up steps, times `steps` batch steps, then traces
 `steps` more.  Prints the wall time per batch step, the summed kernel time
 per batch step and the largest kernels.  Kernels of concurrent scenes
 overlap, so a kernel's duration includes the time it shares the device.
@@ -27,6 +28,7 @@ from rmt3d_b200 import scenes  # noqa: E402
 def main():
     size = int(sys.argv[1]) if len(sys.argv) > 1 else 96
     steps = int(sys.argv[2]) if len(sys.argv) > 2 else 5
+    smoother = int(sys.argv[3]) if len(sys.argv) > 3 else -1
     wd = tempfile.mkdtemp()
     descs = []
     for seed in range(32):
@@ -39,6 +41,10 @@ def main():
         descs.append(d)
     b = R.Batch(descs)
     b.prepare()
+    if smoother < 0:
+        print("autotuned", b.autotune(probe_steps=2))
+    else:
+        b.set_smoother(smoother, 4)
     b.step(3)
     torch.cuda.synchronize()
     t = time.perf_counter()

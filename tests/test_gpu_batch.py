@@ -4,11 +4,11 @@ A batch steps independent scenes of uneven grid sizes together (each on its
 own stream, kernels overlapping on the device); the serving loop admits
 requests over time under an HBM budget.  Each scene's result must be the same
 as when the scene runs alone.  Every reduction (the step's and the
-checksum's) sums in a fixed order, and a served scene runs the same kernels
-as a scene alone, so serving matches bit for bit.  A scene stepped inside a
-group of several scenes runs its least-squares extrapolation with 4 lanes per
-frontier cell instead of a warp (more cells in flight when the GPU is shared),
-which regroups those sums: grouped scenes match to round-off (SAME_TOL).
+checksum's) sums in a fixed order.  A scene stepped inside a group of
+several scenes -- in a batch, or served next to requests of its kind --
+runs its least-squares extrapolation with 4 lanes per frontier cell instead
+of a warp (more cells in flight when the GPU is shared), which regroups
+those sums: grouped scenes match to round-off (SAME_TOL).
 """
 import numpy as np
 import pytest
@@ -141,7 +141,8 @@ def test_serve_same_alone_and_in_mix(tmp_path):
         assert r["status"] == R.NORMAL_EXIT and r["steps_done"] == n
         assert r["admit_s"] >= arr - 1e-6
         _, alone = _alone(d, n)
-        assert list(r["checksum"]) == list(alone), (r["checksum"], alone)
+        # requests of one kind step as a group: round-off against alone
+        assert max(_same_checksum(r["checksum"], alone)) < SAME_TOL, (r["checksum"], alone)
 
 
 def test_serve_admission_by_budget(tmp_path):

