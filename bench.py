@@ -424,7 +424,7 @@ def run_ours(args):
         sc = R.Scene(d, stream=stream.cuda_stream)
         sc.set_schedule(tuned[0], tuned[1], 0)
         sc.set_mg_launch(tuned[2])
-        sc.set_smoother(1 if tuned[3] else 0, tuned[3] if tuned[3] else 4)
+        sc.set_smoother(tuned[3])
         sc.prepare()
         sc.schedule = tuned
         return sc

@@ -342,10 +342,9 @@ int rmt3d_div_u_noalloc(const int sys_size[3], const int periodic[3], const doub
 /* Multigrid smoother of the scene's solves (no counterpart in the reference,
  * whose PGMG smoothing is a library internal): mode 0 issues one launch per
  * colour pass of the Gauss-Seidel sweeps; mode 1 one launch per whole sweep,
- * staging shared-memory tiles with overlapped halos and streaming the planes
- * in z (tile_waves: z chunks for about that many blocks per SM).  Both give
- * the same bits. */
-int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode, int tile_waves);
+ * each block staging a box with an overlapped halo in shared memory and
+ * running every colour pass there.  Both give the same bits. */
+int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode);
 
 /* Launch timing of one kernel class for roofline measurement (no counterpart
  * in the reference, which has no device code): kernel 0 = FEM Gauss-Seidel
@@ -376,13 +375,12 @@ int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out);
  * precision, density form) by timing candidates on a probe scene: the
  * smoothing counts (v_down, v_up), as the reference's mg_opt searches them
  * (Utilities/mg_probs.hh:80-208), the cluster or per-phase launch of the
- * solves, and the smoother (colour passes, or tiled sweeps with tiles deep
- * enough in z for 4 or 8 blocks per SM); tuned_out gets (cells, v_down,
- * v_up, cluster, smoother: 0 colour passes, else blocks per SM) per kind */
+ * solves, and the smoother (colour passes or tiled sweeps); tuned_out gets
+ * (cells, v_down, v_up, cluster, smoother) per kind */
 int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out);
 
 /* rmt3d_scene_set_smoother on every scene of the batch. */
-int rmt3d_batch_set_smoother(rmt3d_batch *b, int mode, int tile_waves);
+int rmt3d_batch_set_smoother(rmt3d_batch *b, int mode);
 int rmt3d_batch_destroy(rmt3d_batch *b);
 
 /* Multigrid schedule of one scene: V(v_down, v_up) smoothing counts, and the

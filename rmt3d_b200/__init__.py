@@ -264,10 +264,10 @@ class Scene:
         launch per phase in a graph loop."""
         _lib.check(lib().rmt3d_scene_set_mg_launch(self._h, int(cluster)))
 
-    def set_smoother(self, mode, tile_waves=4):
+    def set_smoother(self, mode):
         """Multigrid smoothing: 0 one launch per colour pass, 1 one launch per
         whole sweep on shared-memory tiles (the same bits)."""
-        _lib.check(lib().rmt3d_scene_set_smoother(self._h, int(mode), int(tile_waves)))
+        _lib.check(lib().rmt3d_scene_set_smoother(self._h, int(mode)))
 
     def checksum(self):
         """Sums of u^2, v^2, w^2, p^2 over the interior cells."""
@@ -465,16 +465,15 @@ class Batch:
 
     def autotune(self, probe_steps=3):
         """Per kind of scene: {cells: (v_down, v_up, cluster, smoother)} chosen
-        by timing candidates (smoother 0: colour passes, else the tiled
-        sweep's blocks per SM)."""
+        by timing candidates (smoother 0: colour passes, 1: tiled sweeps)."""
         buf = (ctypes.c_int * (5 * self.n))()
         n = ctypes.c_int()
         _lib.check(lib().rmt3d_batch_autotune(self._h, probe_steps, buf, self.n, ctypes.byref(n)))
         return {buf[5 * i]: tuple(buf[5 * i + 1:5 * i + 5]) for i in range(min(n.value, self.n))}
 
-    def set_smoother(self, mode, tile_waves=4):
+    def set_smoother(self, mode):
         """The multigrid smoother of every scene (Scene.set_smoother)."""
-        _lib.check(lib().rmt3d_batch_set_smoother(self._h, int(mode), int(tile_waves)))
+        _lib.check(lib().rmt3d_batch_set_smoother(self._h, int(mode)))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -176,11 +176,11 @@ SIGNATURES = {
     "rmt3d_batch_size": (_I, [_P, _IP]),
     "rmt3d_batch_scene": (_I, [_P, _I, ctypes.POINTER(_P)]),
     "rmt3d_batch_autotune": (_I, [_P, _I, _IP, _I, _IP]),
-    "rmt3d_batch_set_smoother": (_I, [_P, _I, _I]),
+    "rmt3d_batch_set_smoother": (_I, [_P, _I]),
     "rmt3d_batch_destroy": (_I, [_P]),
     "rmt3d_scene_set_schedule": (_I, [_P, _I, _I, _I]),
     "rmt3d_scene_set_mg_launch": (_I, [_P, _I]),
-    "rmt3d_scene_set_smoother": (_I, [_P, _I, _I]),
+    "rmt3d_scene_set_smoother": (_I, [_P, _I]),
     "rmt3d_scene_footprint": (ctypes.c_size_t, [ctypes.POINTER(SceneDesc)]),
     "rmt3d_scene_checksum": (_I, [_P, _DP]),
     "rmt3d_serve": (_I, [ctypes.POINTER(Request), _I, ctypes.c_size_t, _I,

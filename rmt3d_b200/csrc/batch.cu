@@ -28,7 +28,7 @@
 // knobs shared with scene.cu (defined there)
 extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts);
 extern "C" int rmt3d_scene_set_mg_launch(rmt3d_scene *s, int cluster);
-extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode, int tile_waves);
+extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode);
 
 struct rmt3d_batch {
     std::vector<rmt3d_scene *> scenes;
@@ -255,17 +255,16 @@ extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
 // without error is applied to every scene of that kind.  The candidates are
 // the smoothing counts (v_down, v_up), each solve as one thread-block-cluster
 // launch or as per-phase launches, and for the latter the smoother: one
-// launch per colour pass, or one per whole sweep on shared-memory tiles with
-// the z depth of the tiles set for about 4 or 8 blocks per SM.  tuned_out
-// (optional, 5 ints per kind: cells, v_down, v_up, cluster launch, smoother
-// (0 colour passes, otherwise the tiles' blocks per SM)) receives the choices.
+// launch per colour pass, or one per whole sweep on shared-memory tiles.
+// tuned_out (optional, 5 ints per kind: cells, v_down, v_up, cluster launch,
+// smoother) receives the choices.
 extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
     drop_groups(b);
     static const int smooth[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
-    // (cluster launch, smoother waves: 0 colour passes)
-    static const int launch[][2] = {{1, 0}, {0, 0}, {0, 4}, {0, 8}};
+    // (cluster launch, smoother: 0 colour passes, 1 tiled sweeps)
+    static const int launch[][2] = {{1, 0}, {0, 0}, {0, 1}};
     std::map<std::array<int, 8>, int> first;
     for (size_t i = 0; i < b->descs.size(); i++)
         if (!first.count(tune_key(b->descs[i]))) first[tune_key(b->descs[i])] = (int)i;
@@ -284,7 +283,7 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
             for (auto &c : smooth) {
                 if (rmt3d_scene_set_mg_launch(probe, ln[0])) continue;  // clusters unavailable
                 if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], 0)) ||
-                    (e = rmt3d_scene_set_smoother(probe, ln[1] ? 1 : 0, ln[1] ? ln[1] : 4))) {
+                    (e = rmt3d_scene_set_smoother(probe, ln[1]))) {
                     rmt3d_scene_destroy(probe);
                     return e;
                 }
@@ -309,7 +308,7 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
             if (tune_key(b->descs[i]) == kv.first) {
                 if ((e = rmt3d_scene_set_schedule(b->scenes[i], bd, bu, 0))) return e;
                 if ((e = rmt3d_scene_set_mg_launch(b->scenes[i], bc))) return e;
-                if ((e = rmt3d_scene_set_smoother(b->scenes[i], bs ? 1 : 0, bs ? bs : 4))) return e;
+                if ((e = rmt3d_scene_set_smoother(b->scenes[i], bs))) return e;
             }
         if (tuned_out && written < max_out) {
             tuned_out[5 * written] = (int)cells(b->descs[kv.second]);
@@ -326,11 +325,11 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
 
 // The smoother of every scene of the batch (rmt3d_scene_set_smoother); the
 // groups are rebuilt at the next step.
-extern "C" int rmt3d_batch_set_smoother(rmt3d_batch *b, int mode, int tile_waves) {
+extern "C" int rmt3d_batch_set_smoother(rmt3d_batch *b, int mode) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     drop_groups(b);
     for (auto *s : b->scenes) {
-        const int e = rmt3d_scene_set_smoother(s, mode, tile_waves);
+        const int e = rmt3d_scene_set_smoother(s, mode);
         if (e) return e;
     }
     return RMT3D_OK;

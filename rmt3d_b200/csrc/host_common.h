@@ -26,7 +26,7 @@ int steps_finish(rmt3d_scene *s, int *status);
 struct scene_group;
 int group_create(rmt3d_scene *const *scenes, int n, scene_group **out);
 // a scene's multigrid schedule, as groups must share it: v_down, v_up,
-// smoother mode, tile waves
+// smoother mode, cluster launch
 void scene_schedule(rmt3d_scene *s, int out[4]);
 int group_launch(scene_group *g, int nsteps);
 int group_finish(scene_group *g, int *status);

@@ -4,6 +4,8 @@
 // replaces; floating-point expressions keep the reference's association order
 // so that, built without FMA contraction, results track the reference's CPU
 // run to rounding.
+#include <cuda.h>
+
 #include "dev_common.cuh"
 #include "kernels.h"
 
@@ -585,6 +587,182 @@ __global__ void __launch_bounds__(256, 3) k_edge_vel(grid_dev g, const fields_de
         double d = dh2[dim] * (2 * (f % 2) - 1);
         for (int c = 0; c < 3; c++) F->fvel[3 * f + c][ind] = vel[c] + d * nv[dim][c] + adv[c] + dt2 * acc[c];
     }
+}
+
+// -------------------------------------------------------------------------
+// The same computation with the velocity staged through TMA.  A block owns
+// 32 x 8 cells in x, y and a chunk of planes in z; the planes of u, v, w with
+// a halo of two cells in x and y stream through a ring of shared-memory
+// planes, each plane brought in by three tiled bulk-tensor copies
+// (cp.async.bulk.tensor, one per component) that complete on the plane's
+// mbarrier.  Three planes ahead of the one being computed are in flight.
+// Each cell's slopes read the five-point lines of the velocity from the ring
+// -- the operands k_edge_vel reads from global memory, in the same order --
+// so the face states are bit-identical.  The rest (stress divergence,
+// pressure gradient, body and solid forces) reads global memory as before.
+// The tensor maps cover the scene's own velocity arrays (no multicast).
+// -------------------------------------------------------------------------
+constexpr int kEvX = 32, kEvY = 8, kEvW = kEvX + 4, kEvH = kEvY + 4, kEvRing = 6;
+constexpr unsigned kEvPlaneBytes = kEvW * kEvH * sizeof(double);  // one component of one plane
+
+__device__ __forceinline__ void ev_mbar_init(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"((unsigned)__cvta_generic_to_shared(bar)) : "memory");
+}
+// thread 0: expect the three copies of a plane and start them
+__device__ __forceinline__ void ev_fetch(uint64_t *bar, double *dst, const CUtensorMap *tm0, const CUtensorMap *tm1,
+                                         const CUtensorMap *tm2, int x, int y, int z) {
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(b), "r"(3 * kEvPlaneBytes) : "memory");
+    const CUtensorMap *tms[3] = {tm0, tm1, tm2};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst + c * kEvW * kEvH);
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n"
+            ::"r"(d), "l"((unsigned long long)tms[c]), "r"(x), "r"(y), "r"(z), "r"(b)
+            : "memory");
+    }
+}
+// bounded wait for a phase of a plane's mbarrier: false if it did not
+// complete within the limit (the copies are of valid global memory, so this
+// does not happen; the bound keeps a fault from turning into a hang)
+__device__ __forceinline__ bool ev_wait(uint64_t *bar, unsigned parity) {
+    const unsigned b = (unsigned)__cvta_generic_to_shared(bar);
+    for (int it = 0; it < (1 << 22); it++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(b), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(256, 2) k_edge_vel_tma(grid_dev g, const fields_dev *__restrict__ F,
+                                                         const __grid_constant__ CUtensorMap tmu,
+                                                         const __grid_constant__ CUtensorMap tmv,
+                                                         const __grid_constant__ CUtensorMap tmw, const double *lx,
+                                                         const double *ly, const double *lz, double cdt,
+                                                         const double *time_p, int var_den, int tz, int *err) {
+    extern __shared__ __align__(128) unsigned char ev_smem[];
+    double *ring = reinterpret_cast<double *>(ev_smem);  // [kEvRing][3][kEvH][kEvW]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ev_smem + (size_t)kEvRing * 3 * kEvPlaneBytes);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const bool lead = tx == 0 && ty == 0;
+    const int i0 = 2 + kEvX * blockIdx.x, j0 = 2 + kEvY * blockIdx.y;
+    const int k0 = 2 + tz * blockIdx.z, k1 = min(k0 + tz, g.so + 2);  // interior planes [k0, k1)
+    const int p0 = k0 - 2, p1 = k1 + 1;                             // planes staged [p0, p1]
+    if (lead) {
+        for (int q = 0; q < kEvRing; q++) ev_mbar_init(bar + q);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    auto slot = [&](int p) { return (p - p0) % kEvRing; };
+    auto fetch = [&](int p) {
+        ev_fetch(bar + slot(p), ring + (size_t)slot(p) * 3 * kEvW * kEvH, &tmu, &tmv, &tmw, i0 - 2, j0 - 2, p);
+    };
+    // prologue: the five planes of the first cell plane and one more
+    if (lead)
+        for (int p = p0; p <= min(p0 + 5, p1); p++) fetch(p);
+    const int i = i0 + tx, j = j0 + ty;
+    const bool mine = i < g.sm + 2 && j < g.sn + 2;
+    const double time = *time_p;  // device-resident simulation time
+    const double dhsp[3] = {g.dxsp, g.dysp, g.dzsp};
+    const double dh2[3] = {g.dx * 0.5, g.dy * 0.5, g.dz * 0.5};
+    const double dt2 = cdt * 0.5;
+    bool ok = true;
+    for (int k = k0; k < k1; k++) {
+        // planes k-2 .. k+2 have landed (k+2 is the newest one needed)
+        for (int p = (k == k0 ? p0 : k + 2); p <= k + 2 && ok; p++) ok = ev_wait(bar + slot(p), ((p - p0) / kEvRing) & 1);
+        if (!ok) break;
+        if (mine) {
+            const int ind = gidx(g, i, j, k);
+            const int o = (ty + 2) * kEvW + (tx + 2);
+            const double *pl[5];
+#pragma unroll
+            for (int d = 0; d < 5; d++) pl[d] = ring + (size_t)slot(k - 2 + d) * 3 * kEvW * kEvH;
+            double nv[3][3];
+            double vel[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const double *u2 = pl[2] + c * kEvW * kEvH;
+                vel[c] = u2[o];
+                nv[0][c] = dhsp[0] * mono_diff(u2[o - 2], u2[o - 1], u2[o], u2[o + 1], u2[o + 2]);
+                nv[1][c] = dhsp[1] * mono_diff(u2[o - 2 * kEvW], u2[o - kEvW], u2[o], u2[o + kEvW], u2[o + 2 * kEvW]);
+                nv[2][c] = dhsp[2] * mono_diff(pl[0][c * kEvW * kEvH + o], pl[1][c * kEvW * kEvH + o], u2[o],
+                                               pl[3][c * kEvW * kEvH + o], pl[4][c * kEvW * kEvH + o]);
+            }
+            double acc[3] = {0, 0, 0};
+            acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
+            double adv[3] = {0, 0, 0};
+            for (int a = 0; a < 3; a++) {
+                for (int b = 0; b < 3; b++) adv[a] -= vel[b] * nv[b][a];
+                adv[a] *= dt2;
+            }
+            for (int f = 0; f < 6; f++) {
+                int dim = f / 2;
+                double d = dh2[dim] * (2 * (f % 2) - 1);
+                for (int c = 0; c < 3; c++) F->fvel[3 * f + c][ind] = vel[c] + d * nv[dim][c] + adv[c] + dt2 * acc[c];
+            }
+        }
+        // every thread is done with plane k-2: its slot takes plane k+4
+        __syncthreads();
+        if (lead && k + 4 <= p1) fetch(k + 4);
+    }
+    if (!ok && tx == 0 && ty == 0) atomicAdd(err, 1);
+    // no copy is left in flight: every fetched plane was waited for, or the
+    // block gave up on a wait (recorded above); let outstanding copies land
+    // before the shared memory goes away
+    if (!ok)
+        for (int p = p0; p <= p1; p++) ev_wait(bar + slot(p), ((p - p0) / kEvRing) & 1);
+}
+
+size_t edge_vel_tma_smem() { return (size_t)kEvRing * 3 * kEvPlaneBytes + kEvRing * sizeof(uint64_t); }
+
+// Tiled tensor map of one velocity array (the ghosted box, FP64) for
+// k_edge_vel_tma: box of kEvW x kEvH x 1 elements.  Needs 16-byte row
+// strides (sm + 4 even).  Returns false if the map cannot be made.
+bool edge_vel_tensor_map(const grid_dev &g, const double *base, CUtensorMap *out) {
+    if ((g.sm4 * sizeof(double)) % 16 != 0 || ((uintptr_t)base) % 16 != 0) return false;
+    typedef CUresult (*encode_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static encode_fn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !p)
+            return false;
+        fn = (encode_fn)p;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)g.sm4, (cuuint64_t)g.sn4, (cuuint64_t)g.so4};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.sm4 * sizeof(double), (cuuint64_t)g.smn4 * sizeof(double)};
+    const cuuint32_t box[3] = {kEvW, kEvH, 1}, estr[3] = {1, 1, 1};
+    return fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// launch of k_edge_vel_tma over the interior: z chunks of tz planes
+void launch_edge_vel_tma(const grid_dev &g, const fields_dev *F, const CUtensorMap tm[3], const double *lx,
+                         const double *ly, const double *lz, double cdt, const double *time_p, int var_den, int *err,
+                         cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_edge_vel_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)edge_vel_tma_smem());
+        attr = true;
+    }
+    const int tx = (g.sm + kEvX - 1) / kEvX, ty = (g.sn + kEvY - 1) / kEvY;
+    // z chunks for about 4 blocks per SM, at least 8 planes each
+    int nz = (4 * 148 + tx * ty - 1) / (tx * ty);
+    nz = nz < 1 ? 1 : (nz > (g.so + 7) / 8 ? (g.so + 7) / 8 : nz);
+    const int tz = (g.so + nz - 1) / nz;
+    const dim3 grid(tx, ty, (g.so + tz - 1) / tz);
+    k_edge_vel_tma<<<grid, dim3(kEvX, kEvY), edge_vel_tma_smem(), st>>>(g, F, tm[0], tm[1], tm[2], lx, ly, lz, cdt,
+                                                                       time_p, var_den, tz, err);
 }
 
 // -------------------------------------------------------------------------

@@ -83,16 +83,15 @@ __global__ void k_coarse_dense(int np, const double *__restrict__ B, T *__restri
     body_coarse_dense<T>(np, B, x, r, blockIdx.x, gridDim.x);
 }
 
-// one whole sweep of a level on shared-memory tiles (mg_tile.cuh); blockIdx.z
-// is the z chunk of tz planes
+// one whole sweep of a level on shared-memory tiles (mg_tile.cuh), one block
+// per output box
 template <typename T, int KIND, bool VD>
-__global__ void __launch_bounds__(256) k_tile_sweep(lvl_dev L, const T *__restrict__ xin, T *__restrict__ xout,
-                                                    const T *__restrict__ r, const T *__restrict__ ri, int tz) {
+__global__ void __launch_bounds__(512) k_tile_sweep(lvl_dev L, const T *__restrict__ xin, T *__restrict__ xout,
+                                                    const T *__restrict__ r, const T *__restrict__ ri) {
     extern __shared__ __align__(16) unsigned char tile_smem[];
-    using S = tile_shape<KIND>;
-    const int z0 = blockIdx.z * tz;
-    body_tile_sweep<T, KIND, VD>(L, xin, xout, r, ri, blockIdx.x * S::TX, blockIdx.y * S::TY, z0,
-                                 min(z0 + tz, L.n2), tile_smem);
+    using S = tile_shape<T, KIND, VD>;
+    body_tile_sweep<T, KIND, VD>(L, xin, xout, r, ri, blockIdx.x * S::TX, blockIdx.y * S::TY, blockIdx.z * S::TZ,
+                                 tile_smem);
 }
 
 template <typename T>
@@ -167,18 +166,7 @@ __global__ void k_zero(T *a, size_t n) {
 static lvl_dev dev_of(const mg_level &l) { return lvl_dev{l.n[0], l.n[1], l.n[2], l.prd[0], l.prd[1], l.prd[2]}; }
 
 static dim3 blk3() { return dim3(32, 4, 2); }
-
-dim3 tile_grid(int kind, const int n[3], int B, int waves, int &tz, int &zb) {
-    const int TX = kind == MG_MAC ? tile_shape<0>::TX : tile_shape<1>::TX;
-    const int TY = kind == MG_MAC ? tile_shape<0>::TY : tile_shape<1>::TY;
-    const int tx = (n[0] + TX - 1) / TX, ty = (n[1] + TY - 1) / TY;
-    // enough z chunks for about `waves` blocks per SM, none thinner than 8 planes
-    int nz = (waves * 148 + tx * ty * B - 1) / (tx * ty * B);
-    nz = std::max(1, std::min(nz, (n[2] + 7) / 8));
-    tz = (n[2] + nz - 1) / nz;
-    zb = (n[2] + tz - 1) / tz;
-    return dim3(tx, ty, zb * B);
-}
+static dim3 grid3(int a, int b, int c) { return dim3((a + 31) / 32, (b + 3) / 4, (c + 1) / 2); }
 
 template <typename T, int KIND, bool VD>
 static int tile_attr(const void *fn) {
@@ -206,21 +194,25 @@ int tile_setup() {
 }
 
 // one tiled sweep xin -> xout of level L
-template <typename T>
-static void tile_sweep(mg_kind kind, const mg_level &L, const T *xin, T *xout, const T *r, const T *ri, int waves,
-                       cudaStream_t st) {
-    int tz, zb;
-    const dim3 g = tile_grid(kind, L.n, 1, waves, tz, zb);
+template <typename T, int KIND, bool VD>
+static void tile_sweep_k(const mg_level &L, const T *xin, T *xout, const T *r, const T *ri, cudaStream_t st) {
+    using S = tile_shape<T, KIND, VD>;
+    const dim3 g((L.n[0] + S::TX - 1) / S::TX, (L.n[1] + S::TY - 1) / S::TY, (L.n[2] + S::TZ - 1) / S::TZ);
     const lvl_dev d{L.n[0], L.n[1], L.n[2], L.prd[0], L.prd[1], L.prd[2]};
+    k_tile_sweep<T, KIND, VD><<<g, S::NT, tile_smem_bytes<T, KIND, VD>(), st>>>(d, xin, xout, r, ri);
+}
+
+template <typename T>
+static void tile_sweep(mg_kind kind, const mg_level &L, const T *xin, T *xout, const T *r, const T *ri,
+                       cudaStream_t st) {
     if (kind == MG_MAC) {
-        if (ri) k_tile_sweep<T, 0, true><<<g, 256, tile_smem_bytes<T, 0, true>(), st>>>(d, xin, xout, r, ri, tz);
-        else k_tile_sweep<T, 0, false><<<g, 256, tile_smem_bytes<T, 0, false>(), st>>>(d, xin, xout, r, ri, tz);
+        if (ri) tile_sweep_k<T, 0, true>(L, xin, xout, r, ri, st);
+        else tile_sweep_k<T, 0, false>(L, xin, xout, r, ri, st);
     } else {
-        if (ri) k_tile_sweep<T, 1, true><<<g, 256, tile_smem_bytes<T, 1, true>(), st>>>(d, xin, xout, r, ri, tz);
-        else k_tile_sweep<T, 1, false><<<g, 256, tile_smem_bytes<T, 1, false>(), st>>>(d, xin, xout, r, ri, tz);
+        if (ri) tile_sweep_k<T, 1, true>(L, xin, xout, r, ri, st);
+        else tile_sweep_k<T, 1, false>(L, xin, xout, r, ri, st);
     }
 }
-static dim3 grid3(int a, int b, int c) { return dim3((a + 31) / 32, (b + 3) / 4, (c + 1) / 2); }
 
 // Host copy of the level operator, for the coarsest-grid inverse.
 static void host_stencil_row(mg_kind kind, const mg_level &L, int i, int j, int k, std::vector<double> &row) {
@@ -504,7 +496,7 @@ int mg_solver::smooth(int l, int sweeps, int cur, cudaStream_t st) {
     for (int s = 0; s < sweeps; s++) {
         if (smoother == 1) {
             if (timed) prof->begin(st);
-            LAUNCH(tile_sweep<double>(kind, L, xb[cur], xb[cur ^ 1], L.r, L.ri, tile_waves, st));
+            LAUNCH(tile_sweep<double>(kind, L, xb[cur], xb[cur ^ 1], L.r, L.ri, st));
             if (timed) prof->end(st, npts, 8.0 * npts * (L.ri ? 4 : 3));
             cur ^= 1;
         } else if (kind == MG_MAC) {
@@ -535,7 +527,7 @@ int mg_solver::smooth_f32(int l, int sweeps, int cur, cudaStream_t st) {
     for (int s = 0; s < sweeps; s++) {
         if (smoother == 1) {
             if (timed) prof->begin(st);
-            LAUNCH(tile_sweep<float>(kind, L, xb[cur], xb[cur ^ 1], L.rs, L.ris, tile_waves, st));
+            LAUNCH(tile_sweep<float>(kind, L, xb[cur], xb[cur ^ 1], L.rs, L.ris, st));
             if (timed) prof->end(st, npts, 4.0 * npts * (L.ris ? 4 : 3));
             cur ^= 1;
         } else if (kind == MG_MAC) {

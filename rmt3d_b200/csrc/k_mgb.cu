@@ -84,16 +84,15 @@ __global__ void k_fem_prolong_b(lvl_dev F, lvl_dev C, T *const *x, T *const *xc,
     body_fem_prolong<T>(F, C, x[b_], xc[b_], blockIdx.x, blockIdx.y, bz_);
 }
 // one tiled sweep (mg_tile.cuh) of every running scene: blockIdx.z = scene x
-// z chunk
+// z box
 template <typename T, int KIND, bool VD>
-__global__ void __launch_bounds__(256) k_tile_sweep_b(lvl_dev L, T *const *xin, T *const *xout, T *const *r,
-                                                      const T *const *ri, const int *run, int zb, int tz) {
+__global__ void __launch_bounds__(512) k_tile_sweep_b(lvl_dev L, T *const *xin, T *const *xout, T *const *r,
+                                                      const T *const *ri, const int *run, int zb) {
     extern __shared__ __align__(16) unsigned char tile_smem[];
     MGB_SCENE(zb)
-    using S = tile_shape<KIND>;
-    const int z0 = bz_ * tz;
+    using S = tile_shape<T, KIND, VD>;
     body_tile_sweep<T, KIND, VD>(L, xin[b_], xout[b_], r[b_], VD ? ri[b_] : nullptr, blockIdx.x * S::TX,
-                                 blockIdx.y * S::TY, z0, min(z0 + tz, L.n2), tile_smem);
+                                 blockIdx.y * S::TY, bz_ * S::TZ, tile_smem);
 }
 
 template <typename T, int KIND, bool VD>
@@ -211,12 +210,11 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
     v_down = s0.v_down;
     v_up = s0.v_up;
     smoother = s0.smoother;
-    tile_waves = s0.tile_waves;
     dense = s0.dense;
     for (const mg_solver *m : solvers) {
         bool same = m->kind == kind && m->lv.size() == lv.size() && m->mixed == mixed && m->exact == exact &&
                     m->vd == vd && m->rtol == rtol && m->dense == dense && m->v_down == v_down && m->v_up == v_up &&
-                    m->smoother == smoother && m->tile_waves == tile_waves;
+                    m->smoother == smoother;
         for (size_t l = 0; same && l < lv.size(); l++)
             for (int d = 0; d < 3; d++) same = same && m->lv[l].n[d] == lv[l].n[d] && m->lv[l].prd[d] == lv[l].prd[d];
         if (!same) return fail(RMT3D_ERR_INVALID, "scenes of a multigrid group must match in size, form and schedule");
@@ -267,19 +265,26 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
     return cudaGetLastError() == cudaSuccess ? 0 : fail(RMT3D_ERR_CUDA, "group table upload failed");
 }
 
+template <typename T, int KIND, bool VD>
+static void tile_sweep_bk(mg_group &g, const mg_level &L, T *const *xin, T *const *xout, T *const *r,
+                          const T *const *ri, cudaStream_t st) {
+    using S = tile_shape<T, KIND, VD>;
+    const int zb = (L.n[2] + S::TZ - 1) / S::TZ;
+    const dim3 gr((L.n[0] + S::TX - 1) / S::TX, (L.n[1] + S::TY - 1) / S::TY, zb * g.B);
+    k_tile_sweep_b<T, KIND, VD><<<gr, S::NT, tile_smem_bytes<T, KIND, VD>(), st>>>(ldv(L), xin, xout, r, ri, g.run,
+                                                                                     zb);
+}
+
 template <typename T>
 static void tile_sweep_b(mg_group &g, int l, T *const *xin, T *const *xout, T *const *r, const T *const *ri,
                          cudaStream_t st) {
     const mg_level &L = g.lv[l];
-    const lvl_dev d = ldv(L);
-    int tz, zb;
-    const dim3 gr = tile_grid(g.kind, L.n, g.B, g.tile_waves, tz, zb);
     if (g.kind == MG_MAC) {
-        if (ri) k_tile_sweep_b<T, 0, true><<<gr, 256, tile_smem_bytes<T, 0, true>(), st>>>(d, xin, xout, r, ri, g.run, zb, tz);
-        else k_tile_sweep_b<T, 0, false><<<gr, 256, tile_smem_bytes<T, 0, false>(), st>>>(d, xin, xout, r, ri, g.run, zb, tz);
+        if (ri) tile_sweep_bk<T, 0, true>(g, L, xin, xout, r, ri, st);
+        else tile_sweep_bk<T, 0, false>(g, L, xin, xout, r, ri, st);
     } else {
-        if (ri) k_tile_sweep_b<T, 1, true><<<gr, 256, tile_smem_bytes<T, 1, true>(), st>>>(d, xin, xout, r, ri, g.run, zb, tz);
-        else k_tile_sweep_b<T, 1, false><<<gr, 256, tile_smem_bytes<T, 1, false>(), st>>>(d, xin, xout, r, ri, g.run, zb, tz);
+        if (ri) tile_sweep_bk<T, 1, true>(g, L, xin, xout, r, ri, st);
+        else tile_sweep_bk<T, 1, false>(g, L, xin, xout, r, ri, st);
     }
     g.body_kernels++;
 }

@@ -1,6 +1,7 @@
 // Kernel declarations and small by-value argument structs shared between the
 // kernel translation units and the host orchestration (scene.cu).
 #pragma once
+#include <cuda.h>
 #include <stdint.h>
 
 #include "dev_common.cuh"
@@ -48,6 +49,11 @@ __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F, const int
 __global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt);
 __global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
                            const double *lz, double cdt, const double *time_p, int var_den);
+// the velocity edge states with TMA-staged velocity tiles (k_fluid.cu)
+bool edge_vel_tensor_map(const grid_dev &g, const double *base, CUtensorMap *out);
+void launch_edge_vel_tma(const grid_dev &g, const fields_dev *F, const CUtensorMap tm[3], const double *lx,
+                         const double *ly, const double *lz, double cdt, const double *time_p, int var_den, int *err,
+                         cudaStream_t st);
 __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F);
 __global__ void k_mac_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, double cdt);
 __global__ void k_mac_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x);

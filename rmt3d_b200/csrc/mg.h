@@ -119,7 +119,6 @@ class mg_solver {
     // whole sweep on shared-memory tiles (mg_tile.cuh), alternating between
     // a level's x and its residual array
     int smoother = 0;
-    int tile_waves = 4;  // z chunks of the tiled sweep: about this many blocks per SM
     int cf = 0;  // first level whose whole sub-cycle runs in one CTA
     int coarse_pts = 0;  // largest level handed to the one-CTA sub-cycle (0: none)
     int set_coarse(int pts);
@@ -158,9 +157,6 @@ class mg_solver {
     void refine_step(cudaStream_t st);
 };
 
-// grid of the tiled sweep over a level of n points per axis for B scenes:
-// (x tiles, y tiles, z chunks per scene); tz = planes per chunk
-dim3 tile_grid(int kind, const int n[3], int B, int waves, int &tz, int &zb);
 // the tiled sweep kernels' shared-memory limits (once per process)
 int tile_setup();
 
@@ -183,7 +179,7 @@ class mg_group {
     bool mixed = false, exact = false, vd = false;
     double tol = 0, rtol = 0;
     int v_down = 2, v_up = 2;
-    int smoother = 0, tile_waves = 4;
+    int smoother = 0;
     const double *dense = nullptr;
     std::vector<mgb_level_tab> tab;  // device tables per level
     mg_ctl **ctls = nullptr;         // device table of the scenes' control blocks

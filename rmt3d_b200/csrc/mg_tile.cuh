@@ -2,22 +2,16 @@
 // launch, on shared-memory tiles.
 //
 // The colour passes of a sweep depend on each other: pass c reads the values
-// pass c-1 wrote at distance one.  A block owns an output tile of TX x TY
-// points in x, y and a chunk of planes in z.  It stages the tile with a halo
-// of H = C points (C colours) in x and y, and streams the planes in z through
-// a ring of C + 3 planes in shared memory as a wavefront: in iteration t it
-// starts the asynchronous copy (cp.async) of plane t+1, waits for plane t (x
-// and the right-hand side), runs pass 0 on plane t-1, pass 1 on plane t-2,
-// ..., pass C-1 on plane t-C, and writes plane t-C back.  Pass c on plane q needs
-// planes q-1..q+1 after pass c-1, which the wavefront provides: plane q+1
-// received pass c-1 earlier in the same iteration, plane q-1 one iteration
-// before (and pass c there touched only colour-c points, which pass c on
-// plane q does not read: no two coupled points share a colour).  In x and y
-// the region a pass can compute exactly shrinks by one point per pass, so
-// after C passes the halo is used up; the halo's points are computed by the
-// neighbouring blocks as well (overlapped tiling), and a z chunk recomputes H
-// planes above and below it.  Walls end the halo: a point on a wall reads
-// nothing beyond it.  Periodic axes load the wrapped points.
+// pass c-1 wrote at distance one.  A block owns an output box of TX x TY x TZ
+// points and copies the box with a halo of H = C points (C colours) on every
+// side -- x, the right-hand side and, with variable density, 1/rho -- into
+// shared memory with asynchronous copies (cp.async).  It then runs the C
+// passes there, separated by barriers: pass c updates the colour-c points of
+// the box shrunk by c + 1 points on every side, the region whose neighbours
+// are exact after pass c - 1, so after C passes the output box is exact.  The
+// halo's points are computed by the neighbouring blocks as well (overlapped
+// tiling).  Walls end the halo: a point on a wall reads nothing beyond it, so
+// the region does not shrink there.  Periodic axes load the wrapped points.
 //
 // Every point's update is the single-colour kernels' expression (mg_ops.cuh)
 // with the same operands in the same order, read from the tile instead of
@@ -32,26 +26,27 @@
 
 namespace rmt3d {
 
-template <int KIND>
+template <typename T, int KIND, bool VD>
 struct tile_shape {
     static constexpr int C = KIND == 0 ? 2 : 4;  // colours of a sweep
-    static constexpr int H = C;                  // halo in x and y
+    static constexpr int H = C;                  // halo on every side
     static constexpr int TX = 32;
     static constexpr int TY = KIND == 0 ? 16 : 8;
-    static constexpr int WX = TX + 2 * H, WY = TY + 2 * H;
-    // planes in the ring: C + 2 in use at once, one more being fetched
-    static constexpr int R = C + 3;
-    static constexpr int NT = 256;   // threads per block
+    // z depth: the box, its right-hand side and 1/rho fit the shared memory
+    static constexpr int TZ = (KIND == 1 && VD && sizeof(T) == 8) ? 4 : 8;
+    static constexpr int WX = TX + 2 * H, WY = TY + 2 * H, WZ = TZ + 2 * H;
+    static constexpr int NT = 512;  // threads per block
     // variable density: 1/rho per cell.  MAC cells are the points; the FEM
-    // tile of cells is one wider (node i uses cells i-1 and i)
-    static constexpr int CX = KIND == 0 ? WX : WX + 1, CY = KIND == 0 ? WY : WY + 1;
+    // box of cells is one wider per axis (node i uses cells i-1 and i)
+    static constexpr int CX = KIND == 0 ? WX : WX + 1, CY = KIND == 0 ? WY : WY + 1,
+                         CZ = KIND == 0 ? WZ : WZ + 1;
 };
 
-// x and right-hand-side rings, and the 1/rho ring with variable density
+// x and right-hand-side boxes, and the 1/rho box with variable density
 template <typename T, int KIND, bool VD>
 constexpr size_t tile_smem_bytes() {
-    using S = tile_shape<KIND>;
-    return 2 * (size_t)S::R * S::WX * S::WY * sizeof(T) + (VD ? (size_t)S::R * S::CX * S::CY * sizeof(T) : 0);
+    using S = tile_shape<T, KIND, VD>;
+    return 2 * (size_t)S::WX * S::WY * S::WZ * sizeof(T) + (VD ? (size_t)S::CX * S::CY * S::CZ * sizeof(T) : 0);
 }
 
 // asynchronous global -> shared copy of one element (LDGSTS), committed per plane
@@ -324,166 +319,128 @@ __device__ __forceinline__ int tile_coord(int u, int n, int prd) {
     return u;
 }
 
-// One sweep of the level over the output tile starting at (X0, Y0) and the
-// planes [z0, z1): reads xin, writes xout (both the level's layout).
+// One sweep of the level over the output box starting at (X0, Y0, Z0): reads
+// xin, writes xout (both the level's layout).
 template <typename T, int KIND, bool VD>
 __device__ __forceinline__ void body_tile_sweep(const lvl_dev L, const T *__restrict__ xin, T *__restrict__ xout,
                                                 const T *__restrict__ r, const T *__restrict__ ri, int X0, int Y0,
-                                                int z0, int z1, unsigned char *smem) {
-    using S = tile_shape<KIND>;
-    constexpr int C = S::C, H = S::H, WX = S::WX, WY = S::WY, R = S::R, CX = S::CX, CY = S::CY;
+                                                int Z0, unsigned char *smem) {
+    using S = tile_shape<T, KIND, VD>;
+    constexpr int C = S::C, H = S::H, WX = S::WX, WY = S::WY, WZ = S::WZ, CX = S::CX, CY = S::CY, CZ = S::CZ;
+    constexpr int WXY = WX * WY, WN = WXY * WZ;
     T *xs = reinterpret_cast<T *>(smem);
-    T *rr = xs + R * WX * WY;  // right-hand-side planes
-    T *rs = rr + R * WX * WY;  // 1/rho planes (VD)
+    T *rr = xs + WN;  // right-hand side
+    T *rs = rr + WN;  // 1/rho (VD)
     const int tid = threadIdx.x;
     const int n0 = L.n0, n1 = L.n1, n2 = L.n2;
     const size_t sy = (size_t)n0, sz = (size_t)n0 * n1;
-    // planes this block loads: its chunk and H more on each side, ended by walls
-    int zs = z0 - H, ze = z1 + H - 1;
-    const bool wall_lo = !L.p2 && zs < 0, wall_hi = !L.p2 && ze > n2 - 1;
-    if (wall_lo) zs = 0;
-    if (wall_hi) ze = n2 - 1;
-    // 1/rho cells of the FEM nodes: cell planes from zs-1 (cell k-1 of node k)
-    const int nc0 = L.p0 ? n0 : n0 - 1, nc1 = L.p1 ? n1 : n1 - 1, nc2 = L.p2 ? n2 : n2 - 1;
-    auto slot = [&](int t) { return ((t % R) + R) % R; };
-
-    // plane t of x and r (and of 1/rho for MAC), fetched asynchronously;
-    // points outside a walled domain are zero
-    auto fetch_plane = [&](int t) {
-        const int gz = tile_coord(t, n2, L.p2);
-        T *pl = xs + slot(t) * WX * WY;
-        T *pr = rr + slot(t) * WX * WY;
-        for (int e = tid; e < WX * WY; e += S::NT) {
-            const int lx = e % WX, ly = e / WX;
-            const int gx = tile_coord(X0 - H + lx, n0, L.p0), gy = tile_coord(Y0 - H + ly, n1, L.p1);
-            if (gx >= 0 && gy >= 0 && gz >= 0) {
-                const size_t gi = gx + sy * gy + sz * gz;
-                cp_async_elem(pl + e, xin + gi);
-                cp_async_elem(pr + e, r + gi);
-                if constexpr (VD && KIND == 0) cp_async_elem(rs + slot(t) * CX * CY + e, ri + gi);
-            } else {
-                pl[e] = (T)0;
-                pr[e] = (T)0;
-                if constexpr (VD && KIND == 0) rs[slot(t) * CX * CY + e] = (T)0;
-            }
+    // the box with its halo, copied asynchronously; points outside a walled
+    // domain are zero (no point of the passes reads them)
+    for (int e = tid; e < WN; e += S::NT) {
+        const int lx = e % WX, ly = (e / WX) % WY, lz = e / WXY;
+        const int gx = tile_coord(X0 - H + lx, n0, L.p0), gy = tile_coord(Y0 - H + ly, n1, L.p1),
+                  gz = tile_coord(Z0 - H + lz, n2, L.p2);
+        if (gx >= 0 && gy >= 0 && gz >= 0) {
+            const size_t gi = gx + sy * gy + sz * gz;
+            cp_async_elem(xs + e, xin + gi);
+            cp_async_elem(rr + e, r + gi);
+            if constexpr (VD && KIND == 0) cp_async_elem(rs + e, ri + gi);
+        } else {
+            xs[e] = (T)0;
+            rr[e] = (T)0;
+            if constexpr (VD && KIND == 0) rs[e] = (T)0;
         }
-    };
-    // FEM 1/rho: cell plane t (cells between node planes t and t+1)
-    auto fetch_cells = [&](int t) {
-        if constexpr (VD && KIND == 1) {
-            const int cz = tile_coord(t, nc2, L.p2);
-            T *cp = rs + slot(t) * CX * CY;
-            for (int e = tid; e < CX * CY; e += S::NT) {
-                const int lx = e % CX, ly = e / CX;
-                const int cx = tile_coord(X0 - H - 1 + lx, nc0, L.p0), cy = tile_coord(Y0 - H - 1 + ly, nc1, L.p1);
-                if (cx >= 0 && cy >= 0 && cz >= 0) cp_async_elem(cp + e, ri + cx + (size_t)nc0 * (cy + (size_t)nc1 * cz));
-                else cp[e] = (T)0;
-            }
+    }
+    if constexpr (VD && KIND == 1) {
+        // the cells around the box's nodes: cell c lies between nodes c and c+1
+        const int nc0 = L.p0 ? n0 : n0 - 1, nc1 = L.p1 ? n1 : n1 - 1, nc2 = L.p2 ? n2 : n2 - 1;
+        for (int e = tid; e < CX * CY * CZ; e += S::NT) {
+            const int lx = e % CX, ly = (e / CX) % CY, lz = e / (CX * CY);
+            const int cx = tile_coord(X0 - H - 1 + lx, nc0, L.p0), cy = tile_coord(Y0 - H - 1 + ly, nc1, L.p1),
+                      cz = tile_coord(Z0 - H - 1 + lz, nc2, L.p2);
+            if (cx >= 0 && cy >= 0 && cz >= 0) cp_async_elem(rs + e, ri + cx + (size_t)nc0 * (cy + (size_t)nc1 * cz));
+            else rs[e] = (T)0;
         }
-    };
-
-    // prologue: the first plane (and the cell plane below it)
-    if (VD && KIND == 1) fetch_cells(zs - 1);
-    fetch_plane(zs);
-    fetch_cells(zs);
+    }
     cp_async_commit();
-    for (int t = zs; t <= ze + C; t++) {
-        // fetch plane t+1 while the passes of this iteration run
-        if (t + 1 <= ze) {
-            fetch_plane(t + 1);
-            fetch_cells(t + 1);
-        }
-        cp_async_commit();
-        cp_async_wait<1>();  // plane t has landed
-        __syncthreads();
+    cp_async_wait<0>();
+    __syncthreads();
+    const int T0[3] = {X0, Y0, Z0}, TT[3] = {S::TX, S::TY, S::TZ}, NN[3] = {n0, n1, n2}, PP[3] = {L.p0, L.p1, L.p2};
 #pragma unroll
-        for (int c = 0; c < C; c++) {
-            const int q = t - 1 - c;
-            // planes where pass c is exact: all of them next to a wall, one
-            // fewer per pass at an open end of the chunk
-            const int qlo = wall_lo ? zs : zs + c + 1, qhi = wall_hi ? ze : ze - c - 1;
-            if (q >= qlo && q <= qhi) {
-                // x and y range of pass c, in global (unwrapped) coordinates
-                int xlo = X0 - H + c + 1, xhi = X0 + S::TX + H - 2 - c;
-                int ylo = Y0 - H + c + 1, yhi = Y0 + S::TY + H - 2 - c;
-                if (!L.p0) {
-                    xlo = max(xlo, 0);
-                    xhi = min(xhi, n0 - 1);
-                }
-                if (!L.p1) {
-                    ylo = max(ylo, 0);
-                    yhi = min(yhi, n1 - 1);
-                }
-                const T *pm = xs + slot(q - 1) * WX * WY;
-                T *pc = xs + slot(q) * WX * WY;
-                const T *pp = xs + slot(q + 1) * WX * WY;
-                const T *prq = rr + slot(q) * WX * WY;
-                const int gz = tile_coord(q, n2, L.p2);
-                // points of colour c in the range
-                int px, py, nx, ny;
-                if constexpr (KIND == 1) {
-                    px = (xlo & 1) == (c & 1) ? xlo : xlo + 1;
-                    py = (ylo & 1) == ((c >> 1) & 1) ? ylo : ylo + 1;
-                    nx = xhi >= px ? (xhi - px) / 2 + 1 : 0;
-                    ny = yhi >= py ? (yhi - py) / 2 + 1 : 0;
+    for (int c = 0; c < C; c++) {
+        // the range of pass c on each axis, in global (unwrapped) coordinates:
+        // the box shrunk by c + 1, but not past a wall
+        int lo[3], hi[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            lo[d] = T0[d] - H + c + 1;
+            hi[d] = T0[d] + TT[d] + H - 2 - c;
+            if (!PP[d]) {
+                lo[d] = max(lo[d], 0);
+                hi[d] = min(hi[d], NN[d] - 1);
+            }
+        }
+        int px, py, nx, ny;
+        const int nz = hi[2] - lo[2] + 1;
+        if constexpr (KIND == 1) {  // colour c: (x, y) parities (c & 1, c >> 1), every z
+            px = (lo[0] & 1) == (c & 1) ? lo[0] : lo[0] + 1;
+            py = (lo[1] & 1) == ((c >> 1) & 1) ? lo[1] : lo[1] + 1;
+            nx = hi[0] >= px ? (hi[0] - px) / 2 + 1 : 0;
+            ny = hi[1] >= py ? (hi[1] - py) / 2 + 1 : 0;
+        } else {  // colour c: parity of x + y + z; at most half a row each
+            px = lo[0];
+            py = lo[1];
+            nx = (hi[0] - lo[0] + 2) / 2;
+            ny = hi[1] - lo[1] + 1;
+        }
+        const int total = nx * ny * (nz > 0 ? nz : 0);
+        for (int e = tid; e < total; e += S::NT) {
+            int ux, uy;
+            const int uz = lo[2] + e / (nx * ny);
+            const int exy = e % (nx * ny);
+            if constexpr (KIND == 1) {
+                ux = px + 2 * (exy % nx);
+                uy = py + 2 * (exy / nx);
+            } else {
+                uy = py + exy / nx;
+                ux = lo[0] + (((lo[0] + uy + uz + c) & 1) ? 1 : 0) + 2 * (exy % nx);
+                if (ux > hi[0]) continue;
+            }
+            const int lx = ux - (X0 - H), ly = uy - (Y0 - H), lz = uz - (Z0 - H);
+            const int gx = tile_coord(ux, n0, L.p0), gy = tile_coord(uy, n1, L.p1), gz = tile_coord(uz, n2, L.p2);
+            const int o = lx + WX * ly + WXY * lz;
+            tile_acc<T, WX> A{xs - WXY, xs, xs + WXY, o};
+            const T rv = rr[o];
+            T diag, s;
+            if constexpr (KIND == 0) {
+                if constexpr (VD) {
+                    tile_acc<T, WX> Rv{rs - WXY, rs, rs + WXY, o};
+                    s = mac_offdiag_vd_t<T, WX>(L, A, Rv, gx, gy, gz, diag);
                 } else {
-                    nx = (xhi - xlo + 2) / 2;  // points of one parity per row, at most
-                    ny = yhi - ylo + 1;
-                    px = xlo;
-                    py = ylo;
+                    s = mac_offdiag_t<T, WX>(L, A, gx, gy, gz, diag);
                 }
-                for (int e = tid; e < nx * ny; e += S::NT) {
-                    int ux, uy;
-                    if constexpr (KIND == 1) {
-                        ux = px + 2 * (e % nx);
-                        uy = py + 2 * (e / nx);
-                    } else {
-                        uy = py + e / nx;
-                        const int x0 = xlo + (((xlo + uy + q + c) & 1) ? 1 : 0);  // first of colour c in the row
-                        ux = x0 + 2 * (e % nx);
-                        if (ux > xhi) continue;
-                    }
-                    const int lx = ux - (X0 - H), ly = uy - (Y0 - H);
-                    const int gx = tile_coord(ux, n0, L.p0), gy = tile_coord(uy, n1, L.p1);
-                    const int o = lx + WX * ly;
-                    tile_acc<T, WX> A{pm, pc, pp, o};
-                    const T rv = prq[o];
-                    T diag, s;
-                    if constexpr (KIND == 0) {
-                        if constexpr (VD) {
-                            tile_acc<T, CX> Rv{rs + slot(q - 1) * CX * CY, rs + slot(q) * CX * CY,
-                                               rs + slot(q + 1) * CX * CY, lx + CX * ly};
-                            s = mac_offdiag_vd_t<T, WX>(L, A, Rv, gx, gy, gz, diag);
-                        } else {
-                            s = mac_offdiag_t<T, WX>(L, A, gx, gy, gz, diag);
-                        }
-                        pc[o] = (rv - s) / diag;
-                    } else {
-                        if constexpr (VD) {
-                            // cells (node - 1) and node: the cell tile is one
-                            // wider, its local index lx is the cell left of node lx
-                            tile_acc<T, CX> Rv{nullptr, rs + slot(q - 1) * CX * CY, rs + slot(q) * CX * CY,
-                                               lx + CX * ly};
-                            s = fem_offdiag_vd_t<T, WX, CX>(L, A, Rv, gx, gy, gz, diag);
-                            pc[o] = (rv - s) / diag;
-                        } else {
-                            s = fem_offdiag_t<T, WX>(L, A, gx, gy, gz, diag);
-                            pc[o] = (rv - s) * fem_inv_diag<T>(L, gx, gy, gz);
-                        }
-                    }
+                xs[o] = (rv - s) / diag;
+            } else {
+                if constexpr (VD) {
+                    // the cell box is one wider: local cell (lx, ly, lz) is the
+                    // cell below-left-front of local node (lx, ly, lz)
+                    const T *cp = rs + CX * CY * lz;
+                    tile_acc<T, CX> Rv{nullptr, cp, cp + CX * CY, lx + CX * ly};
+                    s = fem_offdiag_vd_t<T, WX, CX>(L, A, Rv, gx, gy, gz, diag);
+                    xs[o] = (rv - s) / diag;
+                } else {
+                    s = fem_offdiag_t<T, WX>(L, A, gx, gy, gz, diag);
+                    xs[o] = (rv - s) * fem_inv_diag<T>(L, gx, gy, gz);
                 }
             }
-            __syncthreads();
         }
-        // plane t-C has had every pass: write the block's output part
-        const int q = t - C;
-        if (q >= z0 && q < z1 && q >= 0 && q < n2) {
-            const T *pl = xs + slot(q) * WX * WY;
-            for (int e = tid; e < S::TX * S::TY; e += S::NT) {
-                const int ux = X0 + e % S::TX, uy = Y0 + e / S::TX;
-                if (ux < n0 && uy < n1) xout[ux + sy * uy + sz * q] = pl[(ux - X0 + H) + WX * (uy - Y0 + H)];
-            }
-        }
+        __syncthreads();
+    }
+    // the output box
+    for (int e = tid; e < S::TX * S::TY * S::TZ; e += S::NT) {
+        const int ux = X0 + e % S::TX, uy = Y0 + (e / S::TX) % S::TY, uz = Z0 + e / (S::TX * S::TY);
+        if (ux < n0 && uy < n1 && uz < n2)
+            xout[ux + sy * uy + sz * uz] = xs[(ux - X0 + H) + WX * (uy - Y0 + H) + WXY * (uz - Z0 + H)];
     }
 }
 

@@ -11,6 +11,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+
 #include "graph_build.h"
 #include "host_common.h"
 #include "kernels.h"
@@ -93,7 +95,7 @@ struct scene_ctl {
     int status;  // status of the failing step
     int run_flag;  // the current step of a group graph runs for this scene
     int counters[8];  // [0..1] frontier sizes, [2] extrapolation errors, [3] corrector problems,
-                      // [4] redraw fatal, [5] refmap-derivative errors
+                      // [4] redraw fatal, [5] refmap-derivative errors, [7] TMA waits that gave up
     mg_ctl mac, fem;
 };
 
@@ -129,6 +131,10 @@ struct rmt3d_scene {
     // lanes per frontier cell of the least-squares extrapolation: a warp when
     // the scene steps on its own, 4 when it steps inside a group with others
     int extrap_lanes = 32;
+    // velocity edge states through TMA-staged tiles (k_edge_vel_tma): the
+    // tensor maps of vel[0..2], made when the rows are 16-byte aligned
+    bool edge_tma = false;
+    CUtensorMap tm_vel[3];
     int *mlist = nullptr, *mcnt = nullptr;  // cells holding a map, for the stress kernel
     // passive tracers (dump_code bit 1 and ntracers > 0, fluid_3d.cc:217-219)
     int ntr = 0;
@@ -743,8 +749,12 @@ static void advance_half(rmt3d_scene *s) {
 // compute_half_time_edge_velocities/refmap with their limited derivatives
 static void ph_edges(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    k_edge_vel<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, &s->ctl->time,
-                                                            s->d.var_den);
+    if (s->edge_tma)
+        launch_edge_vel_tma(g, s->dF, s->tm_vel, s->lx, s->ly, s->lz, s->dt, &s->ctl->time, s->d.var_den,
+                            s->counters + 7, s->st);
+    else
+        k_edge_vel<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, &s->ctl->time,
+                                                                s->d.var_den);
     s->count();
     if (g.n_obj > 0) {
         k_edge_refmap<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->counters + 5);
@@ -1005,6 +1015,11 @@ static int step_forward(rmt3d_scene *s, int debug, int stop = 99) {
     compute_stress(s);
     if (stop <= 1) return RMT3D_OK;
     ph_edges(s);
+    if (s->edge_tma) {
+        int e = read_ctl(s);
+        if (e) return e;
+        if (s->h_counters[7] > 0) return fail(RMT3D_ERR_CUDA, "k_edge_vel_tma: a staged velocity plane never arrived");
+    }
     if (stop <= 2) return RMT3D_OK;
     ph_upwind(s);
     if (stop <= 3) return RMT3D_OK;
@@ -1069,7 +1084,8 @@ __global__ void k_step_branch(scene_ctl *c, cudaGraphConditionalHandle h_rest, c
 // The step's status, in the order the eager step reports them.
 __global__ void k_step_end(scene_ctl *c, int with_objects) {
     int st = 0;
-    if (c->mac.nan) st = RMT3D_ERR_NAN;
+    if (c->counters[7] > 0) st = RMT3D_ERR_CUDA;  // a TMA-staged tile never arrived
+    else if (c->mac.nan) st = RMT3D_ERR_NAN;
     else if (with_objects && (c->counters[2] > 0 || c->counters[5] > 0)) st = RMT3D_ERR_EXTRAP;
     else if (with_objects && c->counters[3] != 0) st = RMT3D_REFMAP_UPDATE_ERR;
     else if (c->fem.nan) st = RMT3D_PROJECTION_ERR;
@@ -1217,7 +1233,8 @@ __global__ void k_gstep_seg3(const int *fem_part, cudaGraphConditionalHandle h) 
 __global__ void k_gstep_end(scene_ctl *c, int with_objects) {
     if (!c->run_flag) return;
     int st = 0;
-    if (c->mac.nan) st = RMT3D_ERR_NAN;
+    if (c->counters[7] > 0) st = RMT3D_ERR_CUDA;  // a TMA-staged tile never arrived
+    else if (c->mac.nan) st = RMT3D_ERR_NAN;
     else if (with_objects && (c->counters[2] > 0 || c->counters[5] > 0)) st = RMT3D_ERR_EXTRAP;
     else if (with_objects && c->counters[3] != 0) st = RMT3D_REFMAP_UPDATE_ERR;
     else if (c->fem.nan) st = RMT3D_PROJECTION_ERR;
@@ -1818,6 +1835,15 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     s->mac.h_ctl = &s->h_ctl->mac;
     s->fem.ctl = &s->ctl->fem;
     s->fem.h_ctl = &s->h_ctl->fem;
+    {
+        // RMT3D_EDGE_TMA=0 keeps the plain-load edge kernel (same bits)
+        const char *et = getenv("RMT3D_EDGE_TMA");
+        if (!(et && et[0] == '0')) {
+            bool ok = true;
+            for (int c = 0; c < 3 && ok; c++) ok = edge_vel_tensor_map(s->g, s->hF.vel[c], &s->tm_vel[c]);
+            s->edge_tma = ok;
+        }
+    }
     {
         const char *ge = getenv("RMT3D_GRAPH");
         s->use_graph = !(ge && ge[0] == '0');
@@ -2635,16 +2661,14 @@ void scene_schedule(rmt3d_scene *s, int out[4]) {
     out[0] = s->mac.v_down;
     out[1] = s->mac.v_up;
     out[2] = s->mac.smoother;
-    out[3] = s->mac.tile_waves;
+    out[3] = s->mac.use_cluster ? 1 : 0;
 }
 }  // namespace rmt3d
 
-extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode, int tile_waves) {
+extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     if (mode < 0 || mode > 1) return fail(RMT3D_ERR_INVALID, "smoother mode must be 0 (colour passes) or 1 (tiled sweeps)");
-    if (tile_waves < 1 || tile_waves > 64) return fail(RMT3D_ERR_INVALID, "tile_waves outside 1..64");
     s->mac.smoother = s->fem.smoother = mode;
-    s->mac.tile_waves = s->fem.tile_waves = tile_waves;
     s->mac.invalidate();
     s->fem.invalidate();
     mark_dirty(s);

@@ -26,7 +26,7 @@ cfg = scenes.write(os.path.join(wd, 'w.cfg'), text)
 d = R.desc_from_cfg(cfg); d.precision = prec; d.var_den = vd
 sc = R.Scene(d)
 sc.set_schedule(vdn, vup, 0)
-sc.set_smoother(smoother, 4)
+sc.set_smoother(smoother)
 sc.prepare()
 sc.step_forward(0)
 sc.sync()

@@ -44,7 +44,7 @@ def main():
     if smoother < 0:
         print("autotuned", b.autotune(probe_steps=2))
     else:
-        b.set_smoother(smoother, 4)
+        b.set_smoother(smoother)
     b.step(3)
     torch.cuda.synchronize()
     t = time.perf_counter()
