@@ -114,12 +114,14 @@ typedef struct {
     double mixed_rtol; /* mixed form only: a solve also ends once its max-norm
                           residual is below mixed_rtol times the max-norm of
                           its right-hand side, and skips the two insurance
-                          cycles (the form's accuracy target is 1e-5 rel-L2);
-                          0 keeps the reference's control.  Default 1e-5
-                          (64^3 cavity + sphere, 100 steps: velocity 3e-8
-                          and pressure 6e-8 rel-L2 from the FP64 form, the
-                          same as at 1e-7 with 2.8 + 2.3 V-cycles per step
-                          instead of 4.9 + 3.3). */
+                          cycles (the form's accuracy target is 1e-5 rel-L2
+                          after 100 steps); 0 keeps the reference's control.
+                          Default 2e-6: over the 64 seeded scenes of the
+                          batched workload (32^3-96^3, 1-8 spheres, variable
+                          density), 100 steps, the largest rel-L2 from the
+                          FP64 form is 3.4e-7 (velocity and pressure); at
+                          5e-6 it is 9.3e-6, at 1e-5 three scenes exceed
+                          1e-5 (largest 4e-5); below 2e-6 nothing changes. */
     rmt3d_run_desc run;
 } rmt3d_scene_desc;
 

@@ -64,7 +64,7 @@ extern "C" int rmt3d_desc_defaults(rmt3d_scene_desc *d) {
     d->sys_size[0] = d->sys_size[1] = d->sys_size[2] = 96;
     d->sim_type = RMT3D_SIM_FTEST;
     d->precision = RMT3D_FP64;
-    d->mixed_rtol = 1e-5;
+    d->mixed_rtol = 2e-6;
     // run controls, sim_params.cc:12-22
     rmt3d_run_desc &r = d->run;
     r.chkpt_freq = 1;
