@@ -425,6 +425,7 @@ def run_ours(args):
         sc.set_schedule(tuned[0], tuned[1], 0)
         sc.set_mg_launch(tuned[2])
         sc.set_smoother(tuned[3])
+        sc.set_coarse_cluster(tuned[4])
         sc.prepare()
         sc.schedule = tuned
         return sc

@@ -348,6 +348,13 @@ int rmt3d_div_u_noalloc(const int sys_size[3], const int periodic[3], const doub
  * running every colour pass there.  Both give the same bits. */
 int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode);
 
+/* The coarse part of every V-cycle -- the levels of at most `pts` points
+ * below the finest, down to the coarsest, with their smoothing, residuals,
+ * transfers and the dense coarsest solve -- as one launch of a thread-block
+ * cluster (16 CTAs, or 8) instead of one full-GPU launch per phase; 0 keeps
+ * per-phase launches.  No counterpart in the reference. */
+int rmt3d_scene_set_coarse_cluster(rmt3d_scene *s, int pts);
+
 /* Launch timing of one kernel class for roofline measurement (no counterpart
  * in the reference, which has no device code): kernel 0 = FEM Gauss-Seidel
  * colour pass on the finest level, 1 = MAC red-black pass on the finest level,
@@ -377,8 +384,10 @@ int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out);
  * precision, density form) by timing candidates on a probe scene: the
  * smoothing counts (v_down, v_up), as the reference's mg_opt searches them
  * (Utilities/mg_probs.hh:80-208), the cluster or per-phase launch of the
- * solves, and the smoother (colour passes or tiled sweeps); tuned_out gets
- * (cells, v_down, v_up, cluster, smoother) per kind */
+ * solves, the smoother (colour passes or tiled sweeps) and the coarse
+ * levels run as one cluster launch per V-cycle (rmt3d_scene_set_coarse_cluster);
+ * tuned_out gets (cells, v_down, v_up, cluster, smoother, coarse cluster
+ * points) per kind */
 int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out);
 
 /* rmt3d_scene_set_smoother on every scene of the batch. */

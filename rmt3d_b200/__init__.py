@@ -269,6 +269,11 @@ class Scene:
         whole sweep on shared-memory tiles (the same bits)."""
         _lib.check(lib().rmt3d_scene_set_smoother(self._h, int(mode)))
 
+    def set_coarse_cluster(self, pts):
+        """Run the V-cycles' levels of at most `pts` points (below the finest)
+        as one thread-block-cluster launch per cycle; 0: per-phase launches."""
+        _lib.check(lib().rmt3d_scene_set_coarse_cluster(self._h, int(pts)))
+
     def checksum(self):
         """Sums of u^2, v^2, w^2, p^2 over the interior cells."""
         out = (ctypes.c_double * 4)()
@@ -464,12 +469,13 @@ class Batch:
         return out.reshape(dims[2], dims[1], dims[0])
 
     def autotune(self, probe_steps=3):
-        """Per kind of scene: {cells: (v_down, v_up, cluster, smoother)} chosen
-        by timing candidates (smoother 0: colour passes, 1: tiled sweeps)."""
-        buf = (ctypes.c_int * (5 * self.n))()
+        """Per kind of scene: {cells: (v_down, v_up, cluster, smoother,
+        coarse cluster points)} chosen by timing candidates (smoother 0:
+        colour passes, 1: tiled sweeps)."""
+        buf = (ctypes.c_int * (6 * self.n))()
         n = ctypes.c_int()
         _lib.check(lib().rmt3d_batch_autotune(self._h, probe_steps, buf, self.n, ctypes.byref(n)))
-        return {buf[5 * i]: tuple(buf[5 * i + 1:5 * i + 5]) for i in range(min(n.value, self.n))}
+        return {buf[6 * i]: tuple(buf[6 * i + 1:6 * i + 6]) for i in range(min(n.value, self.n))}
 
     def set_smoother(self, mode):
         """The multigrid smoother of every scene (Scene.set_smoother)."""

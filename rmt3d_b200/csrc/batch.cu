@@ -29,6 +29,7 @@
 extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, int coarse_pts);
 extern "C" int rmt3d_scene_set_mg_launch(rmt3d_scene *s, int cluster);
 extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode);
+extern "C" int rmt3d_scene_set_coarse_cluster(rmt3d_scene *s, int pts);
 
 struct rmt3d_batch {
     std::vector<rmt3d_scene *> scenes;
@@ -37,7 +38,7 @@ struct rmt3d_batch {
     std::vector<int> status;
     // grid shape, periodicity, precision and density form -> (v_down, v_up,
     // cluster launch, smoother mode)
-    std::map<std::array<int, 8>, std::array<int, 4>> tuned;
+    std::map<std::array<int, 8>, std::array<int, 5>> tuned;
     int nthreads = 1;
     // equally sized scenes stepped together: one graph per group, each
     // multigrid solve batched over the group's scenes
@@ -69,12 +70,12 @@ int build_groups(rmt3d_batch *b) {
     std::map<std::vector<double>, std::vector<int>> part;
     for (size_t i = 0; i < b->scenes.size(); i++) {
         const rmt3d_scene_desc &d = b->descs[i];
-        int sch[4];
+        int sch[5];
         rmt3d::scene_schedule(b->scenes[i], sch);
         std::vector<double> key = {(double)d.sys_size[0], (double)d.sys_size[1], (double)d.sys_size[2],
                                    (double)d.periodic[0], (double)d.periodic[1], (double)d.periodic[2],
                                    (double)d.precision, (double)d.var_den, (double)d.mg_exact, d.mixed_rtol,
-                                   (double)sch[0], (double)sch[1], (double)sch[2], (double)sch[3]};
+                                   (double)sch[0], (double)sch[1], (double)sch[2], (double)sch[3], (double)sch[4]};
         part[key].push_back((int)i);
     }
     for (auto &kv : part) {
@@ -254,17 +255,20 @@ extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
 // `probe_steps` times per candidate and the fastest candidate that ran
 // without error is applied to every scene of that kind.  The candidates are
 // the smoothing counts (v_down, v_up), each solve as one thread-block-cluster
-// launch or as per-phase launches, and for the latter the smoother: one
-// launch per colour pass, or one per whole sweep on shared-memory tiles.
-// tuned_out (optional, 5 ints per kind: cells, v_down, v_up, cluster launch,
-// smoother) receives the choices.
+// launch or as per-phase launches, and for the latter the smoother (one
+// launch per colour pass, or one per whole sweep on shared-memory tiles) and
+// the levels (none, up to 5000 or up to 40000 points) whose part of each
+// V-cycle runs as one cluster launch.  tuned_out (optional, 6 ints per kind:
+// cells, v_down, v_up, cluster launch, smoother, coarse cluster points)
+// receives the choices.
 extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
     drop_groups(b);
     static const int smooth[][2] = {{2, 2}, {1, 1}, {1, 2}, {2, 1}, {3, 3}};
-    // (cluster launch, smoother: 0 colour passes, 1 tiled sweeps)
-    static const int launch[][2] = {{1, 0}, {0, 0}, {0, 1}};
+    // (whole solve as one cluster launch, smoother: 0 colour passes, 1 tiled
+    // sweeps, largest level of the coarse part run as one cluster launch)
+    static const int launch[][3] = {{1, 0, 0}, {0, 0, 0}, {0, 1, 0}, {0, 0, 5000}, {0, 0, 40000}, {0, 1, 5000}};
     std::map<std::array<int, 8>, int> first;
     for (size_t i = 0; i < b->descs.size(); i++)
         if (!first.count(tune_key(b->descs[i]))) first[tune_key(b->descs[i])] = (int)i;
@@ -278,10 +282,11 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
             return e;
         }
         double best = 1e300;
-        int bd = 2, bu = 2, bc = 0, bs = 0;
+        int bd = 2, bu = 2, bc = 0, bs = 0, bcc = 0;
         for (auto &ln : launch)
             for (auto &c : smooth) {
                 if (rmt3d_scene_set_mg_launch(probe, ln[0])) continue;  // clusters unavailable
+                if (rmt3d_scene_set_coarse_cluster(probe, ln[2])) continue;  // clusters unavailable
                 if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], 0)) ||
                     (e = rmt3d_scene_set_smoother(probe, ln[1]))) {
                     rmt3d_scene_destroy(probe);
@@ -300,22 +305,25 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
                     bu = c[1];
                     bc = ln[0];
                     bs = ln[1];
+                    bcc = ln[2];
                 }
             }
         rmt3d_scene_destroy(probe);
-        b->tuned[kv.first] = {bd, bu, bc, bs};
+        b->tuned[kv.first] = {bd, bu, bc, bs, bcc};
         for (size_t i = 0; i < b->descs.size(); i++)
             if (tune_key(b->descs[i]) == kv.first) {
                 if ((e = rmt3d_scene_set_schedule(b->scenes[i], bd, bu, 0))) return e;
                 if ((e = rmt3d_scene_set_mg_launch(b->scenes[i], bc))) return e;
                 if ((e = rmt3d_scene_set_smoother(b->scenes[i], bs))) return e;
+                if ((e = rmt3d_scene_set_coarse_cluster(b->scenes[i], bcc))) return e;
             }
         if (tuned_out && written < max_out) {
-            tuned_out[5 * written] = (int)cells(b->descs[kv.second]);
-            tuned_out[5 * written + 1] = bd;
-            tuned_out[5 * written + 2] = bu;
-            tuned_out[5 * written + 3] = bc;
-            tuned_out[5 * written + 4] = bs;
+            tuned_out[6 * written] = (int)cells(b->descs[kv.second]);
+            tuned_out[6 * written + 1] = bd;
+            tuned_out[6 * written + 2] = bu;
+            tuned_out[6 * written + 3] = bc;
+            tuned_out[6 * written + 4] = bs;
+            tuned_out[6 * written + 5] = bcc;
         }
         written++;
     }
@@ -379,12 +387,13 @@ struct served {
 };
 
 // the kind of a scene: what a group's members must share
-std::array<double, 14> serve_key(rmt3d_scene *s, const rmt3d_scene_desc &d) {
-    int sch[4];
+std::array<double, 15> serve_key(rmt3d_scene *s, const rmt3d_scene_desc &d) {
+    int sch[5];
     rmt3d::scene_schedule(s, sch);
     return {(double)d.sys_size[0], (double)d.sys_size[1], (double)d.sys_size[2], (double)d.periodic[0],
             (double)d.periodic[1], (double)d.periodic[2], (double)d.precision, (double)d.var_den,
-            (double)d.mg_exact, d.mixed_rtol, (double)sch[0], (double)sch[1], (double)sch[2], (double)sch[3]};
+            (double)d.mg_exact, d.mixed_rtol, (double)sch[0], (double)sch[1], (double)sch[2], (double)sch[3],
+            (double)sch[4]};
 }
 }  // namespace
 
@@ -469,7 +478,7 @@ extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budge
         rmt3d::scene_group *g = nullptr;
         bool dirty = true;
     };
-    std::map<std::array<double, 14>, kind_group> kinds;
+    std::map<std::array<double, 15>, kind_group> kinds;
     long long cellsteps = 0;
     while (!first_err) {
         {

@@ -26,8 +26,8 @@ int steps_finish(rmt3d_scene *s, int *status);
 struct scene_group;
 int group_create(rmt3d_scene *const *scenes, int n, scene_group **out);
 // a scene's multigrid schedule, as groups must share it: v_down, v_up,
-// smoother mode, cluster launch
-void scene_schedule(rmt3d_scene *s, int out[4]);
+// smoother mode, cluster launch, cluster coarse sub-cycle's largest level
+void scene_schedule(rmt3d_scene *s, int out[5]);
 int group_launch(scene_group *g, int nsteps);
 int group_finish(scene_group *g, int *status);
 void group_destroy(scene_group *g);

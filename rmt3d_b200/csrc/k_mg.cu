@@ -576,9 +576,26 @@ static pmg_args coarse_args(const mg_solver &m) {
     return A;
 }
 
+int mg_solver::set_cluster_coarse(int pts) {
+    cluster_coarse_pts = pts;
+    ccl = -1;
+    if (pts > 0 && cluster_size > 0)
+        for (int l = 1; l + 1 < (int)lv.size(); l++)
+            if (lv[l].npts() <= (size_t)pts) {
+                ccl = l;
+                break;
+            }
+    invalidate();
+    return 0;
+}
+
 int mg_solver::cycle(int l, cudaStream_t st) {
     mg_level &F = lv[l];
     lvl_dev fd = dev_of(F);
+    if (l == ccl) {
+        LAUNCH(coarse_cluster(*this, l, false, st));
+        return 0;
+    }
     if (l == cf && l < (int)lv.size() - 1) {
         LAUNCH(k_mg_coarse<double><<<1, kCoarseThreads, coarse_smem_bytes(lv, l, 8), st>>>(coarse_args(*this), l));
         return 0;
@@ -613,6 +630,10 @@ int mg_solver::cycle(int l, cudaStream_t st) {
 int mg_solver::cycle_f32(int l, cudaStream_t st) {
     mg_level &F = lv[l];
     lvl_dev fd = dev_of(F);
+    if (l == ccl) {
+        LAUNCH(coarse_cluster(*this, l, true, st));
+        return 0;
+    }
     if (l == cf && l < (int)lv.size() - 1) {
         LAUNCH(k_mg_coarse<float><<<1, kCoarseThreads, coarse_smem_bytes(lv, l, 4), st>>>(coarse_args(*this), l));
         return 0;

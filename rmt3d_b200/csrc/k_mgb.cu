@@ -194,6 +194,7 @@ static dim3 ggrid(int a, int b, int c, int B, int &zb) {
 
 mg_group::~mg_group() {
     if (dev_tables) cudaFree(dev_tables);
+    if (dargs) cudaFree(dargs);
 }
 
 int mg_group::setup(const std::vector<mg_solver *> &solvers) {
@@ -210,11 +211,13 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
     v_down = s0.v_down;
     v_up = s0.v_up;
     smoother = s0.smoother;
+    ccl = s0.ccl;
+    csize = s0.cluster_size;
     dense = s0.dense;
     for (const mg_solver *m : solvers) {
         bool same = m->kind == kind && m->lv.size() == lv.size() && m->mixed == mixed && m->exact == exact &&
                     m->vd == vd && m->rtol == rtol && m->dense == dense && m->v_down == v_down && m->v_up == v_up &&
-                    m->smoother == smoother;
+                    m->smoother == smoother && m->ccl == ccl && m->cluster_size == csize;
         for (size_t l = 0; same && l < lv.size(); l++)
             for (int d = 0; d < 3; d++) same = same && m->lv[l].n[d] == lv[l].n[d] && m->lv[l].prd[d] == lv[l].prd[d];
         if (!same) return fail(RMT3D_ERR_INVALID, "scenes of a multigrid group must match in size, form and schedule");
@@ -262,6 +265,13 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
     mx = (unsigned long long **)(d + L * 8 * B + B);
     part = (int *)(d + nptr);
     run = part + B;
+    if (ccl >= 0) {
+        std::vector<pmg_args> ha;
+        for (const mg_solver *m : solvers) ha.push_back(level_args(*m));
+        if (cudaMalloc(&dargs, B * sizeof(pmg_args)) != cudaSuccess)
+            return fail(RMT3D_ERR_OOM, "group table allocation failed");
+        cudaMemcpy(dargs, ha.data(), B * sizeof(pmg_args), cudaMemcpyHostToDevice);
+    }
     return cudaGetLastError() == cudaSuccess ? 0 : fail(RMT3D_ERR_CUDA, "group table upload failed");
 }
 
@@ -328,6 +338,11 @@ static int cycle_b(mg_group &g, int l, cudaStream_t st) {
     auto RI = [&](int q) { return f32 ? (const T *const *)g.tab[q].ris : (const T *const *)g.tab[q].ri; };
     const mg_level &F = g.lv[l];
     const int nl = (int)g.lv.size();
+    if (l == g.ccl) {
+        coarse_cluster_b(g.dargs, g.run, g.B, l, g.csize, sizeof(T) == 4, st);
+        g.body_kernels++;
+        return 0;
+    }
     if (l == nl - 1) {
         if (g.dense) {
             const int np = (int)F.npts();

@@ -66,10 +66,12 @@ __device__ double cl_max(cg::cluster_group &cl, double m) {
     return all;
 }
 
+// a V-cycle from level l0 down (l0 > 0: the coarse part of a cycle whose
+// finer levels run elsewhere; level l0's x starts at zero)
 template <typename T>
-__device__ void cl_vcycle(const pmg_args &A, cg::cluster_group &cl, int t0, int ts) {
+__device__ void cl_vcycle(const pmg_args &A, cg::cluster_group &cl, int t0, int ts, int l0 = 0) {
     const int nc = A.kind == 0 ? 2 : 4;
-    for (int l = 0; l < A.nlev - 1; l++) {
+    for (int l = l0; l < A.nlev - 1; l++) {
         const pmg_level &F = A.lv[l];
         for (int s = 0; s < A.v_down; s++)
             for (int c = 0; c < nc; c++) {
@@ -108,7 +110,7 @@ __device__ void cl_vcycle(const pmg_args &A, cg::cluster_group &cl, int t0, int 
                 }
         }
     }
-    for (int l = A.nlev - 2; l >= 0; l--) {
+    for (int l = A.nlev - 2; l >= l0; l--) {
         const pmg_level &F = A.lv[l];
         const pmg_level &C = A.lv[l + 1];
         ph_prolong<T>(A.kind, ldev(F), ldev(C), LX<T>(F), LX<T>(C), t0, ts);
@@ -231,6 +233,44 @@ __global__ void __launch_bounds__(kClThreads, 1) k_mg_cluster(cmg_args P) {
     }
 }
 
+// The coarse part of a V-cycle -- levels l0 .. coarsest, smoothing,
+// residuals, transfers and the dense coarsest solve -- in one cluster launch
+// instead of one full-GPU launch per phase: these levels are small, and each
+// of their phases is a launch latency long when issued on its own.
+template <typename T>
+__global__ void __launch_bounds__(kClThreads, 1) k_mg_coarse_cluster(pmg_args A, int l0) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int t0 = (int)cl.block_rank() * blockDim.x + threadIdx.x;
+    const int ts = (int)cl.num_blocks() * blockDim.x;
+    cl_vcycle<T>(A, cl, t0, ts, l0);
+}
+
+// the same for every running scene of a group: cluster b works on scene b
+template <typename T>
+__global__ void __launch_bounds__(kClThreads, 1) k_mg_coarse_cluster_b(const pmg_args *A, const int *run, int l0) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int b = blockIdx.x / (int)cl.num_blocks();
+    if (!run[b]) return;  // the whole cluster leaves together
+    const int t0 = (int)cl.block_rank() * blockDim.x + threadIdx.x;
+    const int ts = (int)cl.num_blocks() * blockDim.x;
+    cl_vcycle<T>(A[b], cl, t0, ts, l0);
+}
+
+static cudaError_t coarse_cluster_launch(const void *fn, void **args, int clusters, int csize, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(clusters * csize);
+    cfg.blockDim = dim3(kClThreads);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = csize;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 // ---- host side -------------------------------------------------------------
 int mg_solver::setup_cluster() {
     cluster_size = 0;
@@ -252,6 +292,13 @@ int mg_solver::setup_cluster() {
         int n = 0;
         if (cudaOccupancyMaxActiveClusters(&n, k_mg_cluster, &cfg) == cudaSuccess && n >= 1) {
             cluster_size = c;
+            for (const void *fn : {(const void *)k_mg_coarse_cluster<double>, (const void *)k_mg_coarse_cluster<float>,
+                                   (const void *)k_mg_coarse_cluster_b<double>,
+                                   (const void *)k_mg_coarse_cluster_b<float>})
+                if (cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+                    cudaGetLastError();
+                    cluster_size = 0;
+                }
             return 0;
         }
         cudaGetLastError();
@@ -259,7 +306,7 @@ int mg_solver::setup_cluster() {
     return 0;
 }
 
-static pmg_args level_args(const mg_solver &m) {
+pmg_args level_args(const mg_solver &m) {
     pmg_args A;
     memset(&A, 0, sizeof(A));
     A.kind = (m.kind == MG_MAC) ? 0 : 1;
@@ -308,4 +355,20 @@ cudaError_t mg_solver::launch_cluster(cudaStream_t st) {
     return cudaLaunchKernelEx(&cfg, k_mg_cluster, P);
 }
 
+}  // namespace rmt3d
+
+namespace rmt3d {
+cudaError_t coarse_cluster(const mg_solver &m, int l0, bool f32, cudaStream_t st) {
+    pmg_args A = level_args(m);
+    void *args[2] = {&A, &l0};
+    return coarse_cluster_launch(f32 ? (const void *)k_mg_coarse_cluster<float> : (const void *)k_mg_coarse_cluster<double>,
+                                 args, 1, m.cluster_size, st);
+}
+
+cudaError_t coarse_cluster_b(const pmg_args *A, const int *run, int B, int l0, int csize, bool f32, cudaStream_t st) {
+    void *args[3] = {(void *)&A, (void *)&run, &l0};
+    return coarse_cluster_launch(f32 ? (const void *)k_mg_coarse_cluster_b<float>
+                                     : (const void *)k_mg_coarse_cluster_b<double>,
+                                 args, B, csize, st);
+}
 }  // namespace rmt3d

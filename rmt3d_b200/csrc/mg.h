@@ -73,6 +73,7 @@ constexpr int kMgIP = 16;
 constexpr int kMgMaxCycles = 4096;  // bound on the cycles of one solve
 
 struct graph_builder;
+struct pmg_args;
 
 class mg_solver {
   public:
@@ -119,6 +120,11 @@ class mg_solver {
     // whole sweep on shared-memory tiles (mg_tile.cuh), alternating between
     // a level's x and its residual array
     int smoother = 0;
+    // first level (>= 1) of the coarse part of a V-cycle run as one
+    // thread-block-cluster launch (k_mg_coarse_cluster), -1 none
+    int ccl = -1;
+    int cluster_coarse_pts = 0;  // largest level handed to that launch (0: none)
+    int set_cluster_coarse(int pts);
     int cf = 0;  // first level whose whole sub-cycle runs in one CTA
     int coarse_pts = 0;  // largest level handed to the one-CTA sub-cycle (0: none)
     int set_coarse(int pts);
@@ -157,6 +163,13 @@ class mg_solver {
     void refine_step(cudaStream_t st);
 };
 
+// the coarse part of a V-cycle from level l0 in one cluster launch: one
+// scene, or every running scene of a group (one cluster each; A: device
+// array of the scenes' level tables)
+class mg_solver;
+cudaError_t coarse_cluster(const mg_solver &m, int l0, bool f32, cudaStream_t st);
+cudaError_t coarse_cluster_b(const pmg_args *A, const int *run, int B, int l0, int csize, bool f32, cudaStream_t st);
+pmg_args level_args(const mg_solver &m);
 // the tiled sweep kernels' shared-memory limits (once per process)
 int tile_setup();
 
@@ -180,6 +193,8 @@ class mg_group {
     double tol = 0, rtol = 0;
     int v_down = 2, v_up = 2;
     int smoother = 0;
+    int ccl = -1, csize = 0;     // the cluster coarse sub-cycle (see mg_solver)
+    pmg_args *dargs = nullptr;   // device copies of the scenes' level tables for it
     const double *dense = nullptr;
     std::vector<mgb_level_tab> tab;  // device tables per level
     mg_ctl **ctls = nullptr;         // device table of the scenes' control blocks

@@ -2666,13 +2666,25 @@ extern "C" int rmt3d_scene_set_schedule(rmt3d_scene *s, int v_down, int v_up, in
 }
 
 namespace rmt3d {
-void scene_schedule(rmt3d_scene *s, int out[4]) {
+void scene_schedule(rmt3d_scene *s, int out[5]) {
     out[0] = s->mac.v_down;
     out[1] = s->mac.v_up;
     out[2] = s->mac.smoother;
     out[3] = s->mac.use_cluster ? 1 : 0;
+    out[4] = s->mac.cluster_coarse_pts;
 }
 }  // namespace rmt3d
+
+extern "C" int rmt3d_scene_set_coarse_cluster(rmt3d_scene *s, int pts) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (pts < 0) return fail(RMT3D_ERR_INVALID, "negative level size");
+    if (pts > 0 && (!s->mac.cluster_size || !s->fem.cluster_size))
+        return fail(RMT3D_ERR_UNSUPPORTED, "thread-block clusters of 8 or more CTAs are not available");
+    s->mac.set_cluster_coarse(pts);
+    s->fem.set_cluster_coarse(pts);
+    mark_dirty(s);
+    return RMT3D_OK;
+}
 
 extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
