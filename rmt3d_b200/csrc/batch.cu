@@ -357,13 +357,14 @@ extern "C" int rmt3d_batch_destroy(rmt3d_batch *b) {
 // device footprint fits the remaining HBM budget and fewer than max_slots
 // requests are in the system, and sets its scene up (initialize, dt fit,
 // pressure pre-iterations) on the scene's own stream while the running
-// scenes keep stepping.  The stepping thread runs in rounds: scenes of the
-// same kind (grid shape, periodicity, form, schedule) step together as one
-// group graph -- each multigrid solve batched over the group -- for up to
-// kServeRound steps, the groups of all kinds in flight at once; at the end of
-// a round finished requests leave, their memory returns to the budget, and
-// newly set-up requests join their kind's group.  A group is rebuilt only
-// when its membership changes.
+// scenes keep stepping.  Scenes of the same kind (grid shape, periodicity,
+// form, schedule) step together as one group graph -- each multigrid solve
+// batched over the group -- in rounds of up to kServeRound steps.  Every
+// kind's group runs its rounds on its own: the stepping thread polls the
+// groups and, as soon as a round ends, lets finished requests leave (their
+// memory returns to the budget), lets newly set-up requests of that kind
+// join, and starts the next round.  A group is rebuilt only when its
+// membership changes.
 // ---------------------------------------------------------------------------
 extern "C" int rmt3d_scene_checksum(rmt3d_scene *s, double out[4]);
 extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d);
@@ -472,11 +473,16 @@ extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budge
     const int nsetup = std::max(1, std::min(4, max_slots));
     for (int k = 0; k < nsetup; k++) th.emplace_back(setup_worker);
 
-    // ---- the stepping thread (this one): rounds over the kinds' groups ----
+    // ---- the stepping thread (this one): each kind's group runs its rounds
+    // on its own; the thread polls the groups and relaunches each one as soon
+    // as its round ends, so small and large kinds do not wait for each other
     struct kind_group {
-        std::vector<served> m;
+        std::vector<served> m;        // members of the running or next round
+        std::vector<served> joining;  // set up, joining at the next round
         rmt3d::scene_group *g = nullptr;
-        bool dirty = true;
+        bool dirty = true, busy = false;
+        int k = 0;  // steps of the round in flight
+        std::chrono::steady_clock::time_point t_launch;
     };
     std::map<std::array<double, 15>, kind_group> kinds;
     long long cellsteps = 0;
@@ -484,17 +490,59 @@ extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budge
         {
             std::lock_guard<std::mutex> lk(mu);
             if (finished >= nreq) break;
-            for (auto &r : ready) {
-                kind_group &kg = kinds[serve_key(r.s, reqs[r.id].desc)];
-                kg.m.push_back(r);
-                kg.dirty = true;
-            }
+            for (auto &r : ready) kinds[serve_key(r.s, reqs[r.id].desc)].joining.push_back(r);
             ready.clear();
         }
-        bool any = false;
-        std::vector<std::pair<kind_group *, int>> launched;
+        bool progress = false;
         for (auto &kv : kinds) {
             kind_group &kg = kv.second;
+            if (kg.busy) {
+                if (!rmt3d::group_done(kg.g)) continue;
+                // the round ended: results of the members that are done
+                progress = true;
+                kg.busy = false;
+                std::vector<int> st(kg.m.size(), 0);
+                int e = rmt3d::group_finish(kg.g, st.data());
+                const double ms =
+                    1e3 * std::chrono::duration<double>(std::chrono::steady_clock::now() - kg.t_launch).count() / kg.k;
+                std::vector<served> keep;
+                for (size_t j = 0; j < kg.m.size(); j++) {
+                    served &r = kg.m[j];
+                    rmt3d_request_result &R = results[r.id];
+                    for (int q = 0; q < kg.k; q++) step_ms[r.id].push_back(ms);
+                    r.left -= kg.k;
+                    if (r.left > 0 && st[j] == 0 && !e) {
+                        keep.push_back(r);
+                        continue;
+                    }
+                    R.steps_done = reqs[r.id].steps - std::max(r.left, 0);
+                    R.status = e ? e : st[j];
+                    if (rmt3d_scene_checksum(r.s, R.checksum) && !R.status) R.status = RMT3D_ERR_CUDA;
+                    R.finish_s = now_s();
+                    R.latency_s = R.finish_s - reqs[r.id].arrival_s;
+                    R.step_p50_ms = pct(step_ms[r.id], 0.5);
+                    R.step_p99_ms = pct(step_ms[r.id], 0.99);
+                    cellsteps += (long long)R.steps_done * reqs[r.id].desc.sys_size[0] *
+                                 reqs[r.id].desc.sys_size[1] * reqs[r.id].desc.sys_size[2];
+                    kg.dirty = true;
+                    if (kg.g) rmt3d::group_destroy(kg.g);  // before its member goes
+                    kg.g = nullptr;
+                    rmt3d_scene_destroy(r.s);
+                    std::lock_guard<std::mutex> lk(mu);
+                    used -= r.fp;
+                    in_system--;
+                    finished++;
+                }
+                kg.m.swap(keep);
+                note_err(e);
+                if (e) break;
+            }
+            // not busy: start the next round with the members and the joiners
+            if (!kg.joining.empty()) {
+                kg.m.insert(kg.m.end(), kg.joining.begin(), kg.joining.end());
+                kg.joining.clear();
+                kg.dirty = true;
+            }
             if (kg.m.empty()) continue;
             if (kg.dirty) {
                 if (kg.g) rmt3d::group_destroy(kg.g);
@@ -510,62 +558,29 @@ extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budge
             }
             int k = kServeRound;
             for (auto &r : kg.m) k = std::min(k, r.left);
+            kg.t_launch = std::chrono::steady_clock::now();
             int e = rmt3d::group_launch(kg.g, k);
             if (e) {
                 note_err(e);
                 break;
             }
-            launched.emplace_back(&kg, k);
-            any = true;
+            kg.k = k;
+            kg.busy = true;
+            progress = true;
         }
-        if (!any) {
-            std::this_thread::sleep_for(std::chrono::microseconds(200));
-            continue;
-        }
-        const auto ta = std::chrono::steady_clock::now();
-        for (auto &lk_ : launched) {
-            kind_group &kg = *lk_.first;
-            const int k = lk_.second;
-            std::vector<int> st(kg.m.size(), 0);
-            int e = rmt3d::group_finish(kg.g, st.data());
-            const double ms = 1e3 * std::chrono::duration<double>(std::chrono::steady_clock::now() - ta).count() / k;
-            std::vector<served> keep;
-            for (size_t j = 0; j < kg.m.size(); j++) {
-                served &r = kg.m[j];
-                rmt3d_request_result &R = results[r.id];
-                for (int q = 0; q < k; q++) step_ms[r.id].push_back(ms);
-                r.left -= k;
-                if (r.left > 0 && st[j] == 0 && !e) {
-                    keep.push_back(r);
-                    continue;
-                }
-                // finished (or failed): the result, then the memory back
-                R.steps_done = reqs[r.id].steps - std::max(r.left, 0);
-                R.status = e ? e : st[j];
-                if (rmt3d_scene_checksum(r.s, R.checksum) && !R.status) R.status = RMT3D_ERR_CUDA;
-                R.finish_s = now_s();
-                R.latency_s = R.finish_s - reqs[r.id].arrival_s;
-                R.step_p50_ms = pct(step_ms[r.id], 0.5);
-                R.step_p99_ms = pct(step_ms[r.id], 0.99);
-                cellsteps += (long long)R.steps_done * reqs[r.id].desc.sys_size[0] * reqs[r.id].desc.sys_size[1] *
-                             reqs[r.id].desc.sys_size[2];
-                kg.dirty = true;
-                if (kg.g) rmt3d::group_destroy(kg.g);  // before its member goes
-                kg.g = nullptr;
-                rmt3d_scene_destroy(r.s);
-                std::lock_guard<std::mutex> lk(mu);
-                used -= r.fp;
-                in_system--;
-                finished++;
-            }
-            kg.m.swap(keep);
-            note_err(e);
-        }
+        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(100));
     }
+    // a failure can leave rounds in flight: wait for them before the scenes go
+    for (auto &kv : kinds)
+        if (kv.second.busy && kv.second.g) {
+            std::vector<int> st(kv.second.m.size(), 0);
+            rmt3d::group_finish(kv.second.g, st.data());
+        }
     for (auto &x : th) x.join();
     for (auto &kv : kinds) {
         if (kv.second.g) rmt3d::group_destroy(kv.second.g);
         for (auto &r : kv.second.m) rmt3d_scene_destroy(r.s);
+        for (auto &r : kv.second.joining) rmt3d_scene_destroy(r.s);
     }
     for (auto &r : ready) rmt3d_scene_destroy(r.s);
     const double wall = now_s();

@@ -30,6 +30,9 @@ int group_create(rmt3d_scene *const *scenes, int n, scene_group **out);
 void scene_schedule(rmt3d_scene *s, int out[5]);
 int group_launch(scene_group *g, int nsteps);
 int group_finish(scene_group *g, int *status);
+// true once the group's launched steps have all run (group_finish then
+// returns without waiting)
+bool group_done(scene_group *g);
 void group_destroy(scene_group *g);
 long long group_mg_launches(const scene_group *g);
 

@@ -756,9 +756,11 @@ void launch_edge_vel_tma(const grid_dev &g, const fields_dev *F, const CUtensorM
         attr = true;
     }
     const int tx = (g.sm + kEvX - 1) / kEvX, ty = (g.sn + kEvY - 1) / kEvY;
-    // z chunks for about 4 blocks per SM, at least 8 planes each
-    int nz = (4 * 148 + tx * ty - 1) / (tx * ty);
-    nz = nz < 1 ? 1 : (nz > (g.so + 7) / 8 ? (g.so + 7) / 8 : nz);
+    // z chunks for about 8 blocks per SM (two resident, four waves): a
+    // block's planes are a serial pipeline, so many short chunks keep more
+    // planes in flight than a few long ones; at least 2 planes each
+    int nz = (8 * 148 + tx * ty - 1) / (tx * ty);
+    nz = nz < 1 ? 1 : (nz > (g.so + 1) / 2 ? (g.so + 1) / 2 : nz);
     const int tz = (g.so + nz - 1) / nz;
     const dim3 grid(tx, ty, (g.so + tz - 1) / tz);
     k_edge_vel_tma<<<grid, dim3(kEvX, kEvY), edge_vel_tma_smem(), st>>>(g, F, tm[0], tm[1], tm[2], lx, ly, lz, cdt,

@@ -398,119 +398,10 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
     return true;
 }
 
-// The same fit from one gather over the candidates instead of two.  The
-// weighted moments are taken about the frontier cell's own centre c (small
-// offsets e' = d - c, so no digits cancel): S0 = sum w, S1 = sum w e',
-// S2 = sum w e' e'^T, R1 = sum w xi, X = sum w e' xi^T.  With the weighted
-// means d_avg = c + S1/S0 and xi_avg = R1/S0 the mean-centred normal matrix
-// and right-hand side of the two-gather form are S2 - S1 S1^T / S0 and
-// X - S1 R1^T / S0, the same quantities up to rounding, and the candidates'
-// eligibility and weights are decided exactly as there.
-template <int W, int LANES>
-__device__ bool ls_radius_1p(const grid_dev &g, const objmap_dev &m, int R, int L, int lane, int ii, int jj, int kk,
-                             int ind, bool directional, const double (&gph)[3], double cx, double cy, double cz,
-                             const double *lx, const double *ly, const double *lz, const double *wpow, double wt,
-                             double (&val)[3]) {
-    const int w = W ? W : 2 * R + 1, nc = w * w * w;
-    auto wpw = [&](int e) { return e < kPowTab ? wpow[e] : pow(wt, (double)e); };
-    double s0 = 0, s1[3] = {0, 0, 0}, s2[6] = {0, 0, 0, 0, 0, 0}, r1[3] = {0, 0, 0}, xm[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    int cnt = 0;
-    for (int s = lane; s < nc; s += LANES) {
-        int p = s % w - R, q = (s / w) % w - R, r = s / (w * w) - R;
-        if (ii + p > g.sm4 - 1 || ii + p < 0) continue;
-        if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
-        if (kk + r > g.so4 - 1 || kk + r < 0) continue;
-        int qi = ind + p + g.sm4 * q + g.smn4 * r;
-        int cd = m.code[qi];
-        if (cd < 0 || cd >= L) continue;
-        double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
-        double wgt = wpw(abs(p) + abs(q) + abs(r));
-        if (directional) {
-            double ev[3] = {cx - d[0], cy - d[1], cz - d[2]};
-            double dw = 0, en = 0;
-            for (int pp = 0; pp < 3; pp++) {
-                dw += ev[pp] * gph[pp];
-                en += ev[pp] * ev[pp];
-            }
-            en = sqrt(en);
-            dw /= en;
-            dw *= wgt;
-            if (!(dw > 0)) continue;
-            wgt = dw;
-        }
-        cnt++;
-        const double e0 = d[0] - cx, e1 = d[1] - cy, e2 = d[2] - cz;
-        const double v0 = m.xp[0][qi], v1 = m.xp[1][qi], v2 = m.xp[2][qi];
-        s0 += wgt;
-        const double we0 = wgt * e0, we1 = wgt * e1, we2 = wgt * e2;
-        s1[0] += we0;
-        s1[1] += we1;
-        s1[2] += we2;
-        s2[0] += we0 * e0;
-        s2[1] += we1 * e1;
-        s2[2] += we2 * e2;
-        s2[3] += we0 * e1;
-        s2[4] += we0 * e2;
-        s2[5] += we1 * e2;
-        r1[0] += wgt * v0;
-        r1[1] += wgt * v1;
-        r1[2] += wgt * v2;
-        xm[0] += we0 * v0;
-        xm[1] += we1 * v0;
-        xm[2] += we2 * v0;
-        xm[3] += we0 * v1;
-        xm[4] += we1 * v1;
-        xm[5] += we2 * v1;
-        xm[6] += we0 * v2;
-        xm[7] += we1 * v2;
-        xm[8] += we2 * v2;
-    }
-    const unsigned gm = group_mask<LANES>();
-    for (int off = LANES / 2; off > 0; off >>= 1) cnt += __shfl_xor_sync(gm, cnt, off);
-    if (cnt == 0) return false;
-    s0 = group_sum<LANES>(s0, gm);
-    for (int c = 0; c < 3; c++) {
-        s1[c] = group_sum<LANES>(s1[c], gm);
-        r1[c] = group_sum<LANES>(r1[c], gm);
-    }
-    for (int c = 0; c < 6; c++) s2[c] = group_sum<LANES>(s2[c], gm);
-    for (int c = 0; c < 9; c++) xm[c] = group_sum<LANES>(xm[c], gm);
-    const double m1[3] = {s1[0] / s0, s1[1] / s0, s1[2] / s0};  // d_avg - c
-    double ravg[3];
-    for (int c = 0; c < 3; c++) ravg[c] = r1[c] / s0;
-    double a[6] = {s2[0] - s1[0] * m1[0], s2[1] - s1[1] * m1[1], s2[2] - s1[2] * m1[2],
-                   s2[3] - s1[0] * m1[1], s2[4] - s1[0] * m1[2], s2[5] - s1[1] * m1[2]};
-    double rhs[9];
-    for (int c = 0; c < 3; c++)
-        for (int i = 0; i < 3; i++) rhs[3 * c + i] = xm[3 * c + i] - m1[i] * r1[c];
-    // mat3 A(XX, XY, XZ, XY, YY, YZ, XZ, YZ, ZZ) and its inverse
-    const double a11 = a[0], a12 = a[3], a13 = a[4], a21 = a[3], a22 = a[1], a23 = a[5], a31 = a[4],
-                 a32 = a[5], a33 = a[2];
-    double det = a11 * (a22 * a33 - a23 * a32) + a21 * (a13 * a32 - a12 * a33) + a31 * (a12 * a23 - a13 * a22);
-    if (fabs(det) < 1e-17) return false;
-    double id = 1 / det;
-    double inv[9] = {(a22 * a33 - a23 * a32) * id, (a13 * a32 - a12 * a33) * id, (a12 * a23 - a13 * a22) * id,
-                     (a23 * a31 - a21 * a33) * id, (a11 * a33 - a13 * a31) * id, (a13 * a21 - a11 * a23) * id,
-                     (a21 * a32 - a22 * a31) * id, (a12 * a31 - a11 * a32) * id, (a11 * a22 - a12 * a21) * id};
-    // the frontier cell relative to the weighted mean position: -(d_avg - c)
-    double ps[3] = {-m1[0], -m1[1], -m1[2]};
-    for (int c = 0; c < 3; c++) {
-        double co0 = inv[0] * rhs[3 * c] + inv[1] * rhs[3 * c + 1] + inv[2] * rhs[3 * c + 2];
-        double co1 = inv[3] * rhs[3 * c] + inv[4] * rhs[3 * c + 1] + inv[5] * rhs[3 * c + 2];
-        double co2 = inv[6] * rhs[3 * c] + inv[7] * rhs[3 * c + 1] + inv[8] * rhs[3 * c + 2];
-        double v = ravg[c];
-        v += co0 * ps[0];
-        v += co1 * ps[1];
-        v += co2 * ps[2];
-        val[c] = v;
-    }
-    return true;
-}
-
 // Every object's frontier in one launch: lane group w (LANES lanes)
 // takes entry w of the concatenated frontiers.  The weights wt^n (n = |p|+|q|+|r|) come from a
 // per-block table of the same pow() values.
-template <int LANES, bool ONEPASS>
+template <int LANES>
 __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, const int *front, const int *cnt, int L,
                                int max_rs, double wt, const double *lx, const double *ly, const double *lz,
                                int *err) {
@@ -576,22 +467,12 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
         double val[3] = {0, 0, 0};
         for (int R = 2; R <= max_rs && !success; R++) {
 #define LS_ARGS g, m, R, L, lane, ii, jj, kk, ind, directional, gph, cx, cy, cz, lx, ly, lz, wpow, wt, val
-            if (ONEPASS) {
-                switch (R) {
-                    case 2: success = ls_radius_1p<5, LANES>(LS_ARGS); break;
-                    case 3: success = ls_radius_1p<7, LANES>(LS_ARGS); break;
-                    case 4: success = ls_radius_1p<9, LANES>(LS_ARGS); break;
-                    case 5: success = ls_radius_1p<11, LANES>(LS_ARGS); break;
-                    default: success = ls_radius_1p<0, LANES>(LS_ARGS); break;
-                }
-            } else {
-                switch (R) {
-                    case 2: success = ls_radius<5, LANES>(LS_ARGS); break;
-                    case 3: success = ls_radius<7, LANES>(LS_ARGS); break;
-                    case 4: success = ls_radius<9, LANES>(LS_ARGS); break;
-                    case 5: success = ls_radius<11, LANES>(LS_ARGS); break;
-                    default: success = ls_radius<0, LANES>(LS_ARGS); break;
-                }
+            switch (R) {
+                case 2: success = ls_radius<5, LANES>(LS_ARGS); break;
+                case 3: success = ls_radius<7, LANES>(LS_ARGS); break;
+                case 4: success = ls_radius<9, LANES>(LS_ARGS); break;
+                case 5: success = ls_radius<11, LANES>(LS_ARGS); break;
+                default: success = ls_radius<0, LANES>(LS_ARGS); break;
             }
 #undef LS_ARGS
         }
@@ -609,15 +490,10 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
     }
 }
 
-#define EXTRAP_INST(LN, OP)                                                                                     \
-    template __global__ void k_extrap_layer<LN, OP>(grid_dev, const fields_dev *__restrict__, const int *, const int *, \
-                                                    int, int, double, const double *, const double *, const double *, \
-                                                    int *);
-EXTRAP_INST(4, false)
-EXTRAP_INST(32, false)
-EXTRAP_INST(4, true)
-EXTRAP_INST(32, true)
-#undef EXTRAP_INST
+template __global__ void k_extrap_layer<4>(grid_dev, const fields_dev *__restrict__, const int *, const int *, int,
+                                            int, double, const double *, const double *, const double *, int *);
+template __global__ void k_extrap_layer<32>(grid_dev, const fields_dev *__restrict__, const int *, const int *, int,
+                                             int, double, const double *, const double *, const double *, int *);
 
 // communicate_a_layer on one rank (fluid_3d_comm.cc:203-280): image-backed
 // ghosts receive the maps of the layer just made at their image (periodic

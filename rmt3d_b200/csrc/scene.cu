@@ -131,9 +131,6 @@ struct rmt3d_scene {
     // lanes per frontier cell of the least-squares extrapolation: a warp when
     // the scene steps on its own, 4 when it steps inside a group with others
     int extrap_lanes = 32;
-    // least-squares fits from one gather over the candidates (shifted
-    // moments); RMT3D_EXTRAP_TWOPASS=1 keeps the two-gather form
-    bool extrap_onepass = true;
     // velocity edge states through TMA-staged tiles (k_edge_vel_tma): the
     // tensor maps of vel[0..2], made when the rows are 16-byte aligned
     bool edge_tma = false;
@@ -326,8 +323,7 @@ static void extrapolate(rmt3d_scene *s, bool lay_ready = false) {
     }
     int cur = 0;
     for (int L = 1; L <= s->d.nlayers; L++) {
-        auto kern = s->extrap_onepass ? (s->extrap_lanes == 4 ? k_extrap_layer<4, true> : k_extrap_layer<32, true>)
-                                      : (s->extrap_lanes == 4 ? k_extrap_layer<4, false> : k_extrap_layer<32, false>);
+        auto kern = s->extrap_lanes == 4 ? k_extrap_layer<4> : k_extrap_layer<32>;
         kern<<<per_warp_blocks, 128, 0, s->st>>>(g, s->dF, s->front[cur], cnt[cur], L, s->d.max_extrap_rs,
                                                  s->d.weight_fac, s->lx, s->ly, s->lz, s->counters + 2);
         s->count();
@@ -1484,6 +1480,8 @@ int group_launch(scene_group *G, int nsteps) {
     return 0;
 }
 
+bool group_done(scene_group *G) { return cudaStreamQuery(G->st) != cudaErrorNotReady; }
+
 int group_finish(scene_group *G, int *status) {
     CK(cudaStreamSynchronize(G->st));
     CK(cudaGetLastError());
@@ -1840,10 +1838,6 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     s->mac.h_ctl = &s->h_ctl->mac;
     s->fem.ctl = &s->ctl->fem;
     s->fem.h_ctl = &s->h_ctl->fem;
-    {
-        const char *tp = getenv("RMT3D_EXTRAP_TWOPASS");
-        s->extrap_onepass = !(tp && tp[0] == '1');
-    }
     {
         // RMT3D_EDGE_TMA=0 keeps the plain-load edge kernel (same bits)
         const char *et = getenv("RMT3D_EDGE_TMA");

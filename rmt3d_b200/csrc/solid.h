@@ -13,9 +13,8 @@ __global__ void k_lay_init(grid_dev g, const fields_dev *__restrict__ F, uint8_t
 __global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int from_primary, uint8_t *lay, int *inl,
                            int next, int *nfront, int *ncnt);
 __global__ void k_lay_ghost(grid_dev g, uint8_t *lay, int *inl, int next, int *nfront, int *ncnt);
-// LANES lanes per frontier cell (4 or 32); ONEPASS: the fit from one gather
-// over the candidates (shifted moments) instead of two
-template <int LANES, bool ONEPASS>
+// LANES lanes per frontier cell; instantiated for 4 and 32
+template <int LANES>
 __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, const int *front, const int *cnt, int L,
                                int max_rs, double wt, const double *lx, const double *ly, const double *lz,
                                int *err);
