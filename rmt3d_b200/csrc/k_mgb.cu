@@ -192,12 +192,17 @@ static dim3 ggrid(int a, int b, int c, int B, int &zb) {
     return dim3((a + 31) / 32, (b + 3) / 4, zb * B);
 }
 
-mg_group::~mg_group() {
-    if (dev_tables) cudaFree(dev_tables);
-    if (dargs) cudaFree(dargs);
+void mg_group::release() {
+    if (dev_tables) cudaFreeAsync(dev_tables, tstream);
+    if (dargs) cudaFreeAsync(dargs, tstream);
+    dev_tables = nullptr;
+    dargs = nullptr;
 }
 
-int mg_group::setup(const std::vector<mg_solver *> &solvers) {
+mg_group::~mg_group() { release(); }
+
+int mg_group::setup(const std::vector<mg_solver *> &solvers, cudaStream_t st) {
+    tstream = st;
     if (solvers.empty() || solvers.size() > 1024) return fail(RMT3D_ERR_INVALID, "group of 1..1024 scenes");
     const mg_solver &s0 = *solvers[0];
     B = (int)solvers.size();
@@ -227,7 +232,8 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
     const size_t L = lv.size();
     const size_t nptr = L * 8 * B + 2 * B;
     const size_t bytes = nptr * sizeof(void *) + 2 * B * sizeof(int);
-    if (cudaMalloc(&dev_tables, bytes) != cudaSuccess) return fail(RMT3D_ERR_OOM, "group table allocation failed");
+    if (cudaMallocAsync(&dev_tables, bytes, st) != cudaSuccess)
+        return fail(RMT3D_ERR_OOM, "group table allocation failed");
     std::vector<void *> h(nptr, nullptr);
     for (size_t l = 0; l < L; l++)
         for (int b = 0; b < B; b++) {
@@ -246,8 +252,8 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
         h[L * 8 * B + b] = solvers[b]->ctl;
         h[L * 8 * B + B + b] = solvers[b]->max_slots();
     }
-    cudaMemcpy(dev_tables, h.data(), nptr * sizeof(void *), cudaMemcpyHostToDevice);
-    cudaMemset((char *)dev_tables + nptr * sizeof(void *), 0, 2 * B * sizeof(int));
+    cudaMemcpyAsync(dev_tables, h.data(), nptr * sizeof(void *), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync((char *)dev_tables + nptr * sizeof(void *), 0, 2 * B * sizeof(int), st);
     void **d = (void **)dev_tables;
     tab.resize(L);
     for (size_t l = 0; l < L; l++) {
@@ -268,10 +274,12 @@ int mg_group::setup(const std::vector<mg_solver *> &solvers) {
     if (ccl >= 0) {
         std::vector<pmg_args> ha;
         for (const mg_solver *m : solvers) ha.push_back(level_args(*m));
-        if (cudaMalloc(&dargs, B * sizeof(pmg_args)) != cudaSuccess)
+        if (cudaMallocAsync(&dargs, B * sizeof(pmg_args), st) != cudaSuccess)
             return fail(RMT3D_ERR_OOM, "group table allocation failed");
-        cudaMemcpy(dargs, ha.data(), B * sizeof(pmg_args), cudaMemcpyHostToDevice);
+        cudaMemcpyAsync(dargs, ha.data(), B * sizeof(pmg_args), cudaMemcpyHostToDevice, st);
+        cudaStreamSynchronize(st);  // the host copy of the tables goes out of scope
     }
+    cudaStreamSynchronize(st);
     return cudaGetLastError() == cudaSuccess ? 0 : fail(RMT3D_ERR_CUDA, "group table upload failed");
 }
 

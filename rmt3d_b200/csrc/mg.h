@@ -207,12 +207,16 @@ class mg_group {
     mg_group(const mg_group &) = delete;
     mg_group &operator=(const mg_group &) = delete;
     ~mg_group();
-    int setup(const std::vector<mg_solver *> &solvers);
+    // tables allocated stream-ordered on st (no device-wide synchronisation
+    // when groups come and go next to running ones)
+    int setup(const std::vector<mg_solver *> &solvers, cudaStream_t st);
+    void release();  // frees the tables on the set-up stream (still alive)
     // append the group's solve (arming kernel + WHILE loop) to the capture
     int capture(cudaStream_t cur, graph_builder &gb);
 
   private:
     void *dev_tables = nullptr;
+    cudaStream_t tstream = nullptr;
     void iterate(cudaStream_t st);
 };
 

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1245,6 +1246,34 @@ __global__ void k_gstep_end(scene_ctl *c, int with_objects) {
     c->steps++;
 }
 
+// Small pinned host blocks (the control mirrors) are recycled within the
+// process instead of being freed: cudaFreeHost would synchronise the whole
+// device, which scenes that come and go next to running ones (serving) must
+// not do.
+namespace {
+std::mutex g_pin_mu;
+std::map<size_t, std::vector<void *>> g_pin_free;
+}  // namespace
+
+static void *pinned_get(size_t n) {
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        auto &v = g_pin_free[n];
+        if (!v.empty()) {
+            void *p = v.back();
+            v.pop_back();
+            return p;
+        }
+    }
+    void *p = nullptr;
+    return cudaMallocHost(&p, n) == cudaSuccess ? p : nullptr;
+}
+
+static void pinned_put(void *p, size_t n) {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free[n].push_back(p);
+}
+
 namespace rmt3d {
 struct scene_group {
     std::vector<rmt3d_scene *> sc;
@@ -1260,6 +1289,9 @@ struct scene_group {
     long long mg_launches = 0;        // batched multigrid kernels issued so far
     std::vector<pending_steps_g> pend;
     ~scene_group() {
+        if (st) cudaStreamSynchronize(st);
+        mac.release();  // stream-ordered frees on st, before st goes
+        fem.release();
         if (exec) cudaGraphExecDestroy(exec);
         gb.release();
         for (cudaStream_t b : br) cudaStreamDestroy(b);
@@ -1422,9 +1454,9 @@ int group_create(rmt3d_scene *const *scenes, int n, scene_group **out) {
             return fail(RMT3D_ERR_INVALID, "scenes of a group must have the same grid");
         }
     }
-    int e = G->mac.setup(ms);
-    if (!e) e = G->fem.setup(fs);
-    if (!e && cudaStreamCreateWithFlags(&G->st, cudaStreamNonBlocking) != cudaSuccess) e = RMT3D_ERR_CUDA;
+    int e = cudaStreamCreateWithFlags(&G->st, cudaStreamNonBlocking) != cudaSuccess ? RMT3D_ERR_CUDA : 0;
+    if (!e) e = G->mac.setup(ms, G->st);
+    if (!e) e = G->fem.setup(fs, G->st);
     if (!e && cudaEventCreateWithFlags(&G->ev_fork, cudaEventDisableTiming) != cudaSuccess) e = RMT3D_ERR_CUDA;
     for (int b = 0; b < n && !e; b++) {
         cudaStream_t bs;
@@ -1814,8 +1846,9 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     e |= s->alloc(&s->ctl, 1) | s->alloc(&s->d_mean, 1 + kMeanBlocks) | s->alloc(&s->d_red, 4) |
          s->alloc(&s->mean_ticket, 1) | s->alloc(&s->d_diag, kDiagVals * (1 + kMeanBlocks)) |
          s->alloc(&s->diag_ticket, 1);
-    if (e || cudaMallocHost(&s->h_ctl, sizeof(scene_ctl)) != cudaSuccess ||
-        cudaMallocHost(&s->h_scalar, sizeof(double)) != cudaSuccess) {
+    s->h_ctl = (scene_ctl *)pinned_get(sizeof(scene_ctl));
+    s->h_scalar = (double *)pinned_get(sizeof(double));
+    if (e || !s->h_ctl || !s->h_scalar) {
         rmt3d_scene_destroy(s);
         return fail(RMT3D_ERR_OOM, "allocation failed");
     }
@@ -1839,9 +1872,13 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     s->fem.ctl = &s->ctl->fem;
     s->fem.h_ctl = &s->h_ctl->fem;
     {
-        // RMT3D_EDGE_TMA=0 keeps the plain-load edge kernel (same bits)
+        // The TMA-staged edge kernel where it was measured faster (x extent
+        // of 128 cells and more: 4.5% per FP64 step at 128^3; equal at 96^3,
+        // 7% slower at 64^3, where its 32 x 8 tiles leave too few blocks);
+        // RMT3D_EDGE_TMA=0 or 1 forces either form (the same bits)
         const char *et = getenv("RMT3D_EDGE_TMA");
-        if (!(et && et[0] == '0')) {
+        const bool want = et ? et[0] == '1' : s->g.sm >= 128;
+        if (want) {
             bool ok = true;
             for (int c = 0; c < 3 && ok; c++) ok = edge_vel_tensor_map(s->g, s->hF.vel[c], &s->tm_vel[c]);
             s->edge_tma = ok;
@@ -2773,8 +2810,8 @@ extern "C" int rmt3d_scene_destroy(rmt3d_scene *s) {
     s->mac.release();
     s->fem.release();
     cudaStreamSynchronize(s->st);
-    if (s->h_ctl) cudaFreeHost(s->h_ctl);
-    if (s->h_scalar) cudaFreeHost(s->h_scalar);
+    if (s->h_ctl) pinned_put(s->h_ctl, sizeof(scene_ctl));
+    if (s->h_scalar) pinned_put(s->h_scalar, sizeof(double));
     if (s->own_stream) cudaStreamDestroy(s->st);
     delete s;
     return RMT3D_OK;
