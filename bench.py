@@ -365,6 +365,11 @@ def form_served(R, args):
     bad = [r["status"] for r in res if r["status"] != 0]
     if bad:
         raise RuntimeError("served requests failed: %s" % bad)
+    # the same stream with requests of one kind stepped as one group graph
+    reqs_g = serve_stream(R, wd, args.serve_seconds, 20.0, args.serve_steps, 7, R.MIXED)
+    res_g, summ_g = R.serve(reqs_g, budget, args.serve_slots, grouped=True)
+    if any(r["status"] != 0 for r in res_g):
+        raise RuntimeError("grouped served requests failed")
     cells = sum(d.sys_size[0] * d.sys_size[1] * d.sys_size[2] * n for _, n, d in reqs)
     # the same stream, plain FP64, one request after another
     serial = serve_stream(R, wd, args.serve_seconds, 20.0, args.serve_steps, 7, R.FP64)
@@ -375,6 +380,10 @@ def form_served(R, args):
             "request_latency_s": {"p50": summ["request_p50_s"], "p99": summ["request_p99_s"]},
             "step_latency_ms": {"p50": summ["step_p50_ms"], "p99": summ["step_p99_ms"]},
             "wall_s": summ["wall_s"], "hbm_budget_gb": budget / 1e9, "slots": args.serve_slots,
+            "grouped": {"value": summ_g["cellsteps_per_s"] / 1e6, "wall_s": summ_g["wall_s"],
+                        "request_latency_s": {"p50": summ_g["request_p50_s"], "p99": summ_g["request_p99_s"]},
+                        "step_latency_ms": {"p50": summ_g["step_p50_ms"], "p99": summ_g["step_p99_ms"]},
+                        "form": "requests of one kind stepped as one group graph (rmt3d_serve_grouped)"},
             "serial_fp64": {"value": summ_s["cellsteps_per_s"] / 1e6, "wall_s": summ_s["wall_s"],
                             "step_latency_ms": {"p50": summ_s["step_p50_ms"], "p99": summ_s["step_p99_ms"]}},
             "cellsteps": cells,

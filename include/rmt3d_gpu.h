@@ -436,15 +436,22 @@ typedef struct {
     int requests;
 } rmt3d_serve_summary;
 
-/* Run a request stream with continuous batching: a request is admitted in
- * arrival order when fewer than max_slots requests are in the system and its
- * footprint fits hbm_budget bytes, and is set up while the others step;
- * admitted scenes of the same kind (grid shape, periodicity, form, schedule)
- * step together as one group graph in rounds of up to 10 steps, the kinds'
- * groups in flight at once, and join or leave their group between rounds;
- * results[i] for request i. */
+/* Run a request stream with continuous batching: admission when a slot
+ * (max_slots concurrent scenes) is free and the request's footprint fits
+ * hbm_budget bytes; admitted scenes run concurrently, each on its own stream,
+ * and later arrivals join as slots and memory free up; results[i] for
+ * request i. */
 int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budget, int max_slots,
                 rmt3d_request_result *results, rmt3d_serve_summary *summary);
+
+/* The same stream with requests of one kind (grid shape, periodicity, form,
+ * schedule) stepped together as one group graph (batched multigrid over the
+ * group), each kind's group in rounds of up to 10 steps, polled and restarted
+ * as they end, with requests joining and leaving between rounds; admission in
+ * arrival order by footprint and max_slots requests in the system, set-up
+ * overlapped with stepping. */
+int rmt3d_serve_grouped(const rmt3d_request *reqs, int nreq, size_t hbm_budget, int max_slots,
+                        rmt3d_request_result *results, rmt3d_serve_summary *summary);
 
 /* Synchronise the scene's stream. */
 int rmt3d_sync(rmt3d_scene *s);

@@ -493,9 +493,10 @@ class Batch:
             pass
 
 
-def serve(requests, hbm_budget, max_slots):
+def serve(requests, hbm_budget, max_slots, grouped=False):
     """Run a request stream [(arrival_s, steps, desc), ...] through the serving
-    loop; returns (per-request result dicts, summary dict)."""
+    loop (grouped: requests of one kind stepped as one group graph); returns
+    (per-request result dicts, summary dict)."""
     L = lib()
     n = len(requests)
     reqs = (_lib.Request * n)()
@@ -505,7 +506,8 @@ def serve(requests, hbm_budget, max_slots):
         reqs[i].desc = desc
     res = (_lib.RequestResult * n)()
     summ = _lib.ServeSummary()
-    _lib.check(L.rmt3d_serve(reqs, n, hbm_budget, max_slots, res, ctypes.byref(summ)))
+    fn = L.rmt3d_serve_grouped if grouped else L.rmt3d_serve
+    _lib.check(fn(reqs, n, hbm_budget, max_slots, res, ctypes.byref(summ)))
 
     def as_dict(st):
         out = {}

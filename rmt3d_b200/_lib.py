@@ -186,6 +186,8 @@ SIGNATURES = {
     "rmt3d_scene_checksum": (_I, [_P, _DP]),
     "rmt3d_serve": (_I, [ctypes.POINTER(Request), _I, ctypes.c_size_t, _I,
                          ctypes.POINTER(RequestResult), ctypes.POINTER(ServeSummary)]),
+    "rmt3d_serve_grouped": (_I, [ctypes.POINTER(Request), _I, ctypes.c_size_t, _I,
+                                 ctypes.POINTER(RequestResult), ctypes.POINTER(ServeSummary)]),
     "rmt3d_div_u_noalloc": (_I, [_IP, _IP, _DP, _D, ctypes.POINTER(_P), ctypes.POINTER(_P), _P, _DP]),
 }
 

@@ -352,19 +352,32 @@ extern "C" int rmt3d_batch_destroy(rmt3d_batch *b) {
 }
 
 // ---------------------------------------------------------------------------
-// Serving loop with continuous batching.  Requests arrive over time.  A pool
-// of set-up threads admits each arrived request, in arrival order, when its
-// device footprint fits the remaining HBM budget and fewer than max_slots
-// requests are in the system, and sets its scene up (initialize, dt fit,
-// pressure pre-iterations) on the scene's own stream while the running
-// scenes keep stepping.  Scenes of the same kind (grid shape, periodicity,
-// form, schedule) step together as one group graph -- each multigrid solve
-// batched over the group -- in rounds of up to kServeRound steps.  Every
-// kind's group runs its rounds on its own: the stepping thread polls the
-// groups and, as soon as a round ends, lets finished requests leave (their
-// memory returns to the budget), lets newly set-up requests of that kind
-// join, and starts the next round.  A group is rebuilt only when its
+// Serving loops with continuous batching: requests arrive over time and are
+// admitted while others run, as slots and memory free up; their work
+// overlaps on the device.
+//
+// rmt3d_serve (streams): each admitted request is a scene on its own stream,
+// stepped by one of max_slots host workers; the workers' kernels overlap on
+// the device.  A request is admitted when a worker is free and its device
+// footprint fits the remaining HBM budget (the earliest arrived request that
+// fits goes first).
+//
+// rmt3d_serve_grouped: a pool of set-up threads admits each arrived request,
+// in arrival order, when its footprint fits the budget and fewer than
+// max_slots requests are in the system, and sets its scene up while the
+// running scenes keep stepping.  Scenes of the same kind (grid shape,
+// periodicity, form, schedule) step together as one group graph -- each
+// multigrid solve batched over the group -- in rounds of up to kServeRound
+// steps.  Every kind's group runs its rounds on its own: the stepping thread
+// polls the groups and, as soon as a round ends, lets finished requests leave
+// (their memory returns to the budget), lets newly set-up requests of that
+// kind join, and starts the next round.  A group is rebuilt only when its
 // membership changes.
+//
+// Measured on the served workload's stream (mixed form, 100 steps per
+// request) the stream form delivers more: the large grids fill the GPU on
+// their own, and a group pays its rebuilds, its rounds and, in each batched
+// solve, the cycles of its slowest member.
 // ---------------------------------------------------------------------------
 extern "C" int rmt3d_scene_checksum(rmt3d_scene *s, double out[4]);
 extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d);
@@ -398,8 +411,8 @@ std::array<double, 15> serve_key(rmt3d_scene *s, const rmt3d_scene_desc &d) {
 }
 }  // namespace
 
-extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budget, int max_slots,
-                           rmt3d_request_result *results, rmt3d_serve_summary *summary) {
+extern "C" int rmt3d_serve_grouped(const rmt3d_request *reqs, int nreq, size_t hbm_budget, int max_slots,
+                                   rmt3d_request_result *results, rmt3d_serve_summary *summary) {
     if (!reqs || nreq < 1 || !results || max_slots < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "bad serve arguments");
     for (int i = 0; i < nreq; i++)
         if (rmt3d_scene_footprint(&reqs[i].desc) > hbm_budget)
@@ -596,6 +609,114 @@ extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budge
         summary->step_p50_ms = pct(steps, 0.5);
         summary->step_p99_ms = pct(steps, 0.99);
         summary->cellsteps_per_s = cellsteps / wall;
+        summary->requests = nreq;
+    }
+    if (first_err) return rmt3d::fail(first_err, err_msg);
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_serve(const rmt3d_request *reqs, int nreq, size_t hbm_budget, int max_slots,
+                           rmt3d_request_result *results, rmt3d_serve_summary *summary) {
+    if (!reqs || nreq < 1 || !results || max_slots < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "bad serve arguments");
+    for (int i = 0; i < nreq; i++)
+        if (rmt3d_scene_footprint(&reqs[i].desc) > hbm_budget)
+            return rmt3d::fail(RMT3D_ERR_TOO_LARGE, "request " + std::to_string(i) + " exceeds the HBM budget");
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::mutex mu;
+    std::vector<char> taken(nreq, 0);
+    size_t used = 0;
+    int done = 0;
+    std::atomic<int> first_err{0};
+    std::string err_msg;
+    std::vector<std::vector<double>> step_ms(nreq);
+    const auto t0 = std::chrono::steady_clock::now();
+    auto now_s = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+    std::vector<long long> cellsteps(max_slots, 0);
+    auto worker = [&](int slot) {
+        cudaSetDevice(dev);
+        while (true) {
+            int pick = -1;
+            size_t fp = 0;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (done >= nreq || first_err) return;
+                double t = now_s();
+                // earliest arrived request that fits the free budget
+                for (int i = 0; i < nreq; i++) {
+                    if (taken[i] || reqs[i].arrival_s > t) continue;
+                    size_t f = rmt3d_scene_footprint(&reqs[i].desc);
+                    if (used + f <= hbm_budget) {
+                        pick = i;
+                        fp = f;
+                        break;
+                    }
+                }
+                if (pick >= 0) {
+                    taken[pick] = 1;
+                    used += fp;
+                } else {
+                    bool any_left = false;
+                    for (int i = 0; i < nreq; i++)
+                        if (!taken[i]) any_left = true;
+                    if (!any_left) return;
+                }
+            }
+            if (pick < 0) {
+                std::this_thread::sleep_for(std::chrono::microseconds(200));
+                continue;
+            }
+            rmt3d_request_result &R = results[pick];
+            memset(&R, 0, sizeof(R));
+            R.admit_s = now_s();
+            rmt3d_scene *s = nullptr;
+            int e = rmt3d_scene_create(&reqs[pick].desc, nullptr, &s);
+            if (!e) e = rmt3d_prepare(s);
+            int st = 0;
+            for (int k = 0; !e && k < reqs[pick].steps && st == 0; k++) {
+                auto a = std::chrono::steady_clock::now();
+                e = rmt3d_step(s, 0, &st);
+                if (!e) e = rmt3d_sync(s);
+                step_ms[pick].push_back(
+                    1e3 * std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count());
+            }
+            if (!e) e = rmt3d_scene_checksum(s, R.checksum);
+            R.finish_s = now_s();
+            R.latency_s = R.finish_s - reqs[pick].arrival_s;
+            R.status = e ? e : st;
+            R.steps_done = (int)step_ms[pick].size();
+            R.step_p50_ms = pct(step_ms[pick], 0.5);
+            R.step_p99_ms = pct(step_ms[pick], 0.99);
+            cellsteps[slot] += (long long)R.steps_done * reqs[pick].desc.sys_size[0] * reqs[pick].desc.sys_size[1] *
+                               reqs[pick].desc.sys_size[2];
+            if (e && !first_err.exchange(e)) {
+                std::lock_guard<std::mutex> lk(mu);
+                err_msg = rmt3d_last_error();
+            }
+            rmt3d_scene_destroy(s);
+            std::lock_guard<std::mutex> lk(mu);
+            used -= fp;
+            done++;
+        }
+    };
+    std::vector<std::thread> th;
+    for (int k = 0; k < max_slots; k++) th.emplace_back(worker, k);
+    for (auto &x : th) x.join();
+    const double wall = now_s();
+    if (summary) {
+        std::vector<double> lat, steps;
+        long long cs = 0;
+        for (int i = 0; i < nreq; i++) {
+            lat.push_back(results[i].latency_s);
+            steps.insert(steps.end(), step_ms[i].begin(), step_ms[i].end());
+        }
+        for (long long c : cellsteps) cs += c;
+        summary->wall_s = wall;
+        summary->request_p50_s = pct(lat, 0.5);
+        summary->request_p99_s = pct(lat, 0.99);
+        summary->step_p50_ms = pct(steps, 0.5);
+        summary->step_p99_ms = pct(steps, 0.99);
+        summary->cellsteps_per_s = cs / wall;
         summary->requests = nreq;
     }
     if (first_err) return rmt3d::fail(first_err, err_msg);
