@@ -65,6 +65,16 @@ __global__ void k_mac_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ res, 
                                T *__restrict__ xc0) {
     body_mac_restrict<T>(F, C, res, rc, xc0, blockIdx.x, blockIdx.y, blockIdx.z);
 }
+template <int KIND>
+__global__ void k_resid_to_f32(lvl_dev L, const double *__restrict__ x, const double *__restrict__ r,
+                               const double *__restrict__ ri, float *__restrict__ rs, float *__restrict__ xs) {
+    body_resid_to_f32<KIND>(L, x, r, ri, rs, xs, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+template <typename T, int KIND>
+__global__ void k_resid_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ x, const T *__restrict__ r,
+                                 const T *__restrict__ ri, T *__restrict__ rc, T *__restrict__ xc0) {
+    body_resid_restrict<T, KIND>(F, C, x, r, ri, rc, xc0, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 template <typename T>
 __global__ void k_mac_prolong(lvl_dev F, lvl_dev C, T *__restrict__ x, const T *__restrict__ xc) {
     body_mac_prolong<T>(F, C, x, xc, blockIdx.x, blockIdx.y, blockIdx.z);
@@ -613,13 +623,10 @@ int mg_solver::cycle(int l, cudaStream_t st) {
     mg_level &C = lv[l + 1];
     lvl_dev cd = dev_of(C);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
-    if (kind == MG_MAC) {
-        LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.r, xb[cur ^ 1], nullptr, F.ri)));
-        LAUNCH(k_mac_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.r, C.x));
-    } else {
-        LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.r, xb[cur ^ 1], nullptr, F.ri)));
-        LAUNCH(k_fem_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.r, C.x));
-    }
+    // the residual of the smoothed solution, restricted (one pass)
+    if (kind == MG_MAC) LAUNCH((k_resid_restrict<double, 0><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur], F.r, F.ri, C.r, C.x)));
+    else LAUNCH((k_resid_restrict<double, 1><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur], F.r, F.ri, C.r, C.x)));
+    (void)gf;
     const int cc = cycle(l + 1, st);
     const double *xc = cc ? C.res : C.x;
     if (kind == MG_MAC) LAUNCH(k_mac_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, xb[cur], xc));
@@ -649,13 +656,9 @@ int mg_solver::cycle_f32(int l, cudaStream_t st) {
     mg_level &C = lv[l + 1];
     lvl_dev cd = dev_of(C);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
-    if (kind == MG_MAC) {
-        LAUNCH((k_resid<float, 0><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.rs, xb[cur ^ 1], nullptr, F.ris)));
-        LAUNCH(k_mac_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.rs, C.xs));
-    } else {
-        LAUNCH((k_resid<float, 1><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.rs, xb[cur ^ 1], nullptr, F.ris)));
-        LAUNCH(k_fem_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.rs, C.xs));
-    }
+    if (kind == MG_MAC) LAUNCH((k_resid_restrict<float, 0><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur], F.rs, F.ris, C.rs, C.xs)));
+    else LAUNCH((k_resid_restrict<float, 1><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur], F.rs, F.ris, C.rs, C.xs)));
+    (void)gf;
     const int cc = cycle_f32(l + 1, st);
     const float *xc = cc ? C.ress : C.xs;
     if (kind == MG_MAC) LAUNCH(k_mac_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, xb[cur], xc));
@@ -671,10 +674,9 @@ void mg_solver::refine_step(cudaStream_t st) {
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]);
     size_t n = F.npts();
     unsigned nb = (unsigned)((n + 255) / 256);
-    if (kind == MG_MAC) LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
-    else LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.res, nullptr, F.ri)));
-    LAUNCH(k_to_f32<<<nb, 256, 0, st>>>(F.res, F.rs, n));
-    LAUNCH(k_zero<float><<<nb, 256, 0, st>>>(F.xs, n));
+    // FP64 residual -> FP32 right-hand side, FP32 start value zero (one pass)
+    if (kind == MG_MAC) LAUNCH((k_resid_to_f32<0><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.ri, F.rs, F.xs)));
+    else LAUNCH((k_resid_to_f32<1><<<gf, blk3(), 0, st>>>(fd, F.x, F.r, F.ri, F.rs, F.xs)));
     const int cur = cycle_f32(0, st);
     LAUNCH(k_add_f32<<<nb, 256, 0, st>>>(F.x, cur ? F.ress : F.xs, n));
 }

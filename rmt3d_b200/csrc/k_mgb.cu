@@ -73,6 +73,19 @@ __global__ void k_fem_restrict_b(lvl_dev F, lvl_dev C, T *const *res, T *const *
     MGB_SCENE(zb)
     body_fem_restrict<T>(F, C, res[b_], rc[b_], xc[b_], blockIdx.x, blockIdx.y, bz_);
 }
+template <int KIND>
+__global__ void k_resid_to_f32_b(lvl_dev L, double *const *x, double *const *r, const double *const *ri,
+                                 float *const *rs, float *const *xs, const int *run, int zb) {
+    MGB_SCENE(zb)
+    body_resid_to_f32<KIND>(L, x[b_], r[b_], ri ? ri[b_] : nullptr, rs[b_], xs[b_], blockIdx.x, blockIdx.y, bz_);
+}
+template <typename T, int KIND>
+__global__ void k_resid_restrict_b(lvl_dev F, lvl_dev C, T *const *x, T *const *r, const T *const *ri, T *const *rc,
+                                   T *const *xc, const int *run, int zb) {
+    MGB_SCENE(zb)
+    body_resid_restrict<T, KIND>(F, C, x[b_], r[b_], ri ? ri[b_] : nullptr, rc[b_], xc[b_], blockIdx.x, blockIdx.y,
+                                 bz_);
+}
 template <typename T>
 __global__ void k_mac_prolong_b(lvl_dev F, lvl_dev C, T *const *x, T *const *xc, const int *run, int zb) {
     MGB_SCENE(zb)
@@ -371,14 +384,14 @@ static int cycle_b(mg_group &g, int l, cudaStream_t st) {
     const mg_level &C = g.lv[l + 1];
     int zbf, zbc;
     const dim3 gf = ggrid(F.n[0], F.n[1], F.n[2], g.B, zbf), gc = ggrid(C.n[0], C.n[1], C.n[2], g.B, zbc);
-    if (g.kind == MG_MAC) {
-        k_resid_b<T, 0><<<gf, gblk(), 0, st>>>(ldv(F), xb[cur], Rr(l), xb[cur ^ 1], RI(l), nullptr, g.run, zbf);
-        k_mac_restrict_b<T><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur ^ 1], Rr(l + 1), X(l + 1), g.run, zbc);
-    } else {
-        k_resid_b<T, 1><<<gf, gblk(), 0, st>>>(ldv(F), xb[cur], Rr(l), xb[cur ^ 1], RI(l), nullptr, g.run, zbf);
-        k_fem_restrict_b<T><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur ^ 1], Rr(l + 1), X(l + 1), g.run, zbc);
-    }
-    g.body_kernels += 2;
+    // the residual of the smoothed solution, restricted (one pass)
+    if (g.kind == MG_MAC)
+        k_resid_restrict_b<T, 0><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur], Rr(l), RI(l), Rr(l + 1), X(l + 1),
+                                                         g.run, zbc);
+    else
+        k_resid_restrict_b<T, 1><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur], Rr(l), RI(l), Rr(l + 1), X(l + 1),
+                                                         g.run, zbc);
+    g.body_kernels++;
     const int cc = cycle_b<T>(g, l + 1, st);
     T *const *xc = cc ? S(l + 1) : X(l + 1);
     if (g.kind == MG_MAC) k_mac_prolong_b<T><<<gf, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur], xc, g.run, zbf);
@@ -404,13 +417,12 @@ void mg_group::iterate(cudaStream_t st) {
     const dim3 gf = ggrid(F.n[0], F.n[1], F.n[2], B, zbf);
     const size_t n = F.npts();
     const dim3 g1((unsigned)((n + 255) / 256), B);
+    // FP64 residual -> FP32 right-hand side, FP32 start value zero (one pass)
     if (kind == MG_MAC)
-        k_resid_b<double, 0><<<gf, gblk(), 0, st>>>(ldv(F), tab[0].x, tab[0].r, tab[0].res, tab[0].ri, nullptr, run, zbf);
+        k_resid_to_f32_b<0><<<gf, gblk(), 0, st>>>(ldv(F), tab[0].x, tab[0].r, tab[0].ri, tab[0].rs, tab[0].xs, run, zbf);
     else
-        k_resid_b<double, 1><<<gf, gblk(), 0, st>>>(ldv(F), tab[0].x, tab[0].r, tab[0].res, tab[0].ri, nullptr, run, zbf);
-    k_to_f32_b<<<g1, 256, 0, st>>>(tab[0].res, tab[0].rs, n, run);
-    k_zero_b<float><<<g1, 256, 0, st>>>(tab[0].xs, n, run);
-    body_kernels += 3;
+        k_resid_to_f32_b<1><<<gf, gblk(), 0, st>>>(ldv(F), tab[0].x, tab[0].r, tab[0].ri, tab[0].rs, tab[0].xs, run, zbf);
+    body_kernels++;
     const int cur = cycle_b<float>(*this, 0, st);
     k_add_f32_b<<<g1, 256, 0, st>>>(tab[0].x, cur ? tab[0].ress : tab[0].xs, n, run);
     body_kernels++;
