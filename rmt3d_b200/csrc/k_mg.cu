@@ -70,11 +70,6 @@ __global__ void k_resid_to_f32(lvl_dev L, const double *__restrict__ x, const do
                                const double *__restrict__ ri, float *__restrict__ rs, float *__restrict__ xs) {
     body_resid_to_f32<KIND>(L, x, r, ri, rs, xs, blockIdx.x, blockIdx.y, blockIdx.z);
 }
-template <typename T, int KIND>
-__global__ void k_resid_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ x, const T *__restrict__ r,
-                                 const T *__restrict__ ri, T *__restrict__ rc, T *__restrict__ xc0) {
-    body_resid_restrict<T, KIND>(F, C, x, r, ri, rc, xc0, blockIdx.x, blockIdx.y, blockIdx.z);
-}
 template <typename T>
 __global__ void k_mac_prolong(lvl_dev F, lvl_dev C, T *__restrict__ x, const T *__restrict__ xc) {
     body_mac_prolong<T>(F, C, x, xc, blockIdx.x, blockIdx.y, blockIdx.z);
@@ -476,6 +471,7 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
     if (build_dense(st)) return fail(RMT3D_ERR_OOM, "coarse inverse allocation failed");
     if (set_coarse(coarse_pts)) return fail(RMT3D_ERR_CUDA, "coarse multigrid kernel configuration failed");
     if (tile_setup()) return fail(RMT3D_ERR_CUDA, "tiled sweep kernel configuration failed");
+
     setup_cluster();
     {
         const char *e = getenv("RMT3D_MG_CLUSTER");
@@ -623,10 +619,13 @@ int mg_solver::cycle(int l, cudaStream_t st) {
     mg_level &C = lv[l + 1];
     lvl_dev cd = dev_of(C);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
-    // the residual of the smoothed solution, restricted (one pass)
-    if (kind == MG_MAC) LAUNCH((k_resid_restrict<double, 0><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur], F.r, F.ri, C.r, C.x)));
-    else LAUNCH((k_resid_restrict<double, 1><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur], F.r, F.ri, C.r, C.x)));
-    (void)gf;
+    if (kind == MG_MAC) {
+        LAUNCH((k_resid<double, 0><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.r, xb[cur ^ 1], nullptr, F.ri)));
+        LAUNCH(k_mac_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.r, C.x));
+    } else {
+        LAUNCH((k_resid<double, 1><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.r, xb[cur ^ 1], nullptr, F.ri)));
+        LAUNCH(k_fem_restrict<double><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.r, C.x));
+    }
     const int cc = cycle(l + 1, st);
     const double *xc = cc ? C.res : C.x;
     if (kind == MG_MAC) LAUNCH(k_mac_prolong<double><<<gf, blk3(), 0, st>>>(fd, cd, xb[cur], xc));
@@ -656,9 +655,13 @@ int mg_solver::cycle_f32(int l, cudaStream_t st) {
     mg_level &C = lv[l + 1];
     lvl_dev cd = dev_of(C);
     dim3 gf = grid3(F.n[0], F.n[1], F.n[2]), gc = grid3(C.n[0], C.n[1], C.n[2]);
-    if (kind == MG_MAC) LAUNCH((k_resid_restrict<float, 0><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur], F.rs, F.ris, C.rs, C.xs)));
-    else LAUNCH((k_resid_restrict<float, 1><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur], F.rs, F.ris, C.rs, C.xs)));
-    (void)gf;
+    if (kind == MG_MAC) {
+        LAUNCH((k_resid<float, 0><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.rs, xb[cur ^ 1], nullptr, F.ris)));
+        LAUNCH(k_mac_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.rs, C.xs));
+    } else {
+        LAUNCH((k_resid<float, 1><<<gf, blk3(), 0, st>>>(fd, xb[cur], F.rs, xb[cur ^ 1], nullptr, F.ris)));
+        LAUNCH(k_fem_restrict<float><<<gc, blk3(), 0, st>>>(fd, cd, xb[cur ^ 1], C.rs, C.xs));
+    }
     const int cc = cycle_f32(l + 1, st);
     const float *xc = cc ? C.ress : C.xs;
     if (kind == MG_MAC) LAUNCH(k_mac_prolong<float><<<gf, blk3(), 0, st>>>(fd, cd, xb[cur], xc));

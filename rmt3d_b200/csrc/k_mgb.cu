@@ -79,13 +79,6 @@ __global__ void k_resid_to_f32_b(lvl_dev L, double *const *x, double *const *r, 
     MGB_SCENE(zb)
     body_resid_to_f32<KIND>(L, x[b_], r[b_], ri ? ri[b_] : nullptr, rs[b_], xs[b_], blockIdx.x, blockIdx.y, bz_);
 }
-template <typename T, int KIND>
-__global__ void k_resid_restrict_b(lvl_dev F, lvl_dev C, T *const *x, T *const *r, const T *const *ri, T *const *rc,
-                                   T *const *xc, const int *run, int zb) {
-    MGB_SCENE(zb)
-    body_resid_restrict<T, KIND>(F, C, x[b_], r[b_], ri ? ri[b_] : nullptr, rc[b_], xc[b_], blockIdx.x, blockIdx.y,
-                                 bz_);
-}
 template <typename T>
 __global__ void k_mac_prolong_b(lvl_dev F, lvl_dev C, T *const *x, T *const *xc, const int *run, int zb) {
     MGB_SCENE(zb)
@@ -384,14 +377,14 @@ static int cycle_b(mg_group &g, int l, cudaStream_t st) {
     const mg_level &C = g.lv[l + 1];
     int zbf, zbc;
     const dim3 gf = ggrid(F.n[0], F.n[1], F.n[2], g.B, zbf), gc = ggrid(C.n[0], C.n[1], C.n[2], g.B, zbc);
-    // the residual of the smoothed solution, restricted (one pass)
-    if (g.kind == MG_MAC)
-        k_resid_restrict_b<T, 0><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur], Rr(l), RI(l), Rr(l + 1), X(l + 1),
-                                                         g.run, zbc);
-    else
-        k_resid_restrict_b<T, 1><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur], Rr(l), RI(l), Rr(l + 1), X(l + 1),
-                                                         g.run, zbc);
-    g.body_kernels++;
+    if (g.kind == MG_MAC) {
+        k_resid_b<T, 0><<<gf, gblk(), 0, st>>>(ldv(F), xb[cur], Rr(l), xb[cur ^ 1], RI(l), nullptr, g.run, zbf);
+        k_mac_restrict_b<T><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur ^ 1], Rr(l + 1), X(l + 1), g.run, zbc);
+    } else {
+        k_resid_b<T, 1><<<gf, gblk(), 0, st>>>(ldv(F), xb[cur], Rr(l), xb[cur ^ 1], RI(l), nullptr, g.run, zbf);
+        k_fem_restrict_b<T><<<gc, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur ^ 1], Rr(l + 1), X(l + 1), g.run, zbc);
+    }
+    g.body_kernels += 2;
     const int cc = cycle_b<T>(g, l + 1, st);
     T *const *xc = cc ? S(l + 1) : X(l + 1);
     if (g.kind == MG_MAC) k_mac_prolong_b<T><<<gf, gblk(), 0, st>>>(ldv(F), ldv(C), xb[cur], xc, g.run, zbf);

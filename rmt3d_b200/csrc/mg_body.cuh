@@ -114,62 +114,6 @@ __device__ __forceinline__ void body_mac_restrict(lvl_dev F, lvl_dev C, const T 
     xc0[I + C.n0 * (J + C.n1 * K)] = 0;
 }
 
-// The residual and its restriction in one pass: each coarse point computes
-// the residuals of the fine points it restricts (the expression of
-// body_resid) and sums them as the restriction does, in the same order --
-// the same bits as body_resid followed by body_*_restrict, without the
-// residual array and without a launch.  A fine residual that several coarse
-// points need is computed by each of them.
-template <typename T, int KIND>
-__device__ __forceinline__ T fine_resid(lvl_dev F, const T *__restrict__ x, const T *__restrict__ r,
-                                        const T *__restrict__ ri, int i, int j, int k) {
-    T diag;
-    const T s = op_offdiag<T>(KIND, F, x, ri, i, j, k, diag);
-    const int id = i + F.n0 * (j + F.n1 * k);
-    return r[id] - s - diag * x[id];
-}
-
-template <typename T, int KIND>
-__device__ __forceinline__ void body_resid_restrict(lvl_dev F, lvl_dev C, const T *__restrict__ x,
-                                                    const T *__restrict__ r, const T *__restrict__ ri,
-                                                    T *__restrict__ rc, T *__restrict__ xc0, int bx_, int by_,
-                                                    int bz_) {
-    int I = bx_ * blockDim.x + threadIdx.x;
-    int J = by_ * blockDim.y + threadIdx.y;
-    int K = bz_ * blockDim.z + threadIdx.z;
-    if (I >= C.n0 || J >= C.n1 || K >= C.n2) return;
-    T s = 0;
-    if (KIND == 0) {
-        for (int c = 0; c < 2; c++)
-            for (int b = 0; b < 2; b++)
-                for (int a = 0; a < 2; a++) s += fine_resid<T, 0>(F, x, r, ri, 2 * I + a, 2 * J + b, 2 * K + c);
-    } else {
-        const int nf[3] = {F.n0, F.n1, F.n2}, p[3] = {F.p0, F.p1, F.p2};
-        const int cc[3] = {I, J, K};
-        int idx[3][3];
-        T w[3][3];
-        for (int d = 0; d < 3; d++)
-            for (int o = -1; o <= 1; o++) {
-                int v = wrapi(2 * cc[d] + o, nf[d], p[d]);
-                idx[d][o + 1] = v;
-                w[d][o + 1] = (v < 0) ? (T)0 : (o == 0 ? (T)1 : (T)0.5);
-            }
-        for (int oc = 0; oc < 3; oc++) {
-            if (idx[2][oc] < 0) continue;
-            for (int ob = 0; ob < 3; ob++) {
-                if (idx[1][ob] < 0) continue;
-                for (int oa = 0; oa < 3; oa++) {
-                    if (idx[0][oa] < 0) continue;
-                    s += w[0][oa] * w[1][ob] * w[2][oc] *
-                         fine_resid<T, 1>(F, x, r, ri, idx[0][oa], idx[1][ob], idx[2][oc]);
-                }
-            }
-        }
-    }
-    rc[I + C.n0 * (J + C.n1 * K)] = (T)0.5 * s;
-    xc0[I + C.n0 * (J + C.n1 * K)] = 0;
-}
-
 template <typename T>
 __device__ __forceinline__ void body_mac_prolong(lvl_dev F, lvl_dev C, T *__restrict__ x, const T *__restrict__ xc, int bx_, int by_, int bz_) {
     int i = bx_ * blockDim.x + threadIdx.x;
