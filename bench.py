@@ -473,22 +473,28 @@ def run_ours(args):
         return percentiles(out)
 
     def e2e(sc, k, bufs):
-        """through the public API with host buffers: dt in, u/v/w/p out to
-        pinned host memory every step"""
+        """through the public API with host buffers: dt in, and u/v/w/p out to
+        pinned host memory every step (rmt3d_snapshot_fields: each step's
+        fields reach the host while the next step runs; the last one is
+        waited for inside the timed region)"""
         start = torch.cuda.Event(enable_timing=True)
         stop = torch.cuda.Event(enable_timing=True)
         barrier()
+        t0 = time.perf_counter()
         start.record(stream)
         for _ in range(k):
             sc.set_dt(sc.dt)
             if sc.step_forward(0) != R.NORMAL_EXIT:
                 raise RuntimeError("step failed")
-            for j, nm in enumerate(("u", "v", "w", "p")):
-                R.lib().rmt3d_get_field(sc._h, R.FIELD_INDEX[nm], bufs[j].data_ptr())
+            sc.snapshot(("u", "v", "w", "p"), bufs)
+        sc.snapshot_wait()
         stop.record(stream)
         stop.synchronize()
+        wall = time.perf_counter() - t0
         barrier()
-        return max_over_ranks(start.elapsed_time(stop))
+        # the last host copy ends on the snapshot's copy stream: take the
+        # larger of the event span and the host clock around the loop
+        return max_over_ranks(max(start.elapsed_time(stop), 1e3 * wall))
 
     cells = n ** 3
     clk = ClockSampler(local)

@@ -231,6 +231,17 @@ int rmt3d_get_dims(rmt3d_scene *s, int dims[6]);
  *        27..35 sigma[F][c]. */
 int rmt3d_get_field(rmt3d_scene *s, int which, double *host_dst);
 
+/* The fields `which[0..n-1]` (numbering of rmt3d_get_field) copied to the
+ * host buffers host_dst[0..n-1] (ncell doubles each; pinned memory lets the
+ * copies overlap compute) without waiting: the fields are copied to device
+ * staging buffers in the scene's stream order, then to the host on a copy
+ * stream of the scene's own, so the next step can start at once.  A later
+ * snapshot waits (on the device) for the previous one to reach the host.
+ * rmt3d_snapshot_wait returns once the last snapshot is in host memory.  No
+ * counterpart in the reference (its fields are in host memory already). */
+int rmt3d_snapshot_fields(rmt3d_scene *s, const int *which, int n, double *const *host_dst);
+int rmt3d_snapshot_wait(rmt3d_scene *s);
+
 /* Reference-map export for object slot obj (0-based): per cell the map code
  * (-1 none, 0 primary, L>0 extrapolation layer L) and x[3], xpred[3]. */
 int rmt3d_get_refmap(rmt3d_scene *s, int obj, int *code, double *x, double *xpred);

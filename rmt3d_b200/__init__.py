@@ -274,6 +274,17 @@ class Scene:
         as one thread-block-cluster launch per cycle; 0: per-phase launches."""
         _lib.check(lib().rmt3d_scene_set_coarse_cluster(self._h, int(pts)))
 
+    def snapshot(self, names, host_bufs):
+        """Start copying the named fields to host buffers (objects with
+        data_ptr(), e.g. pinned torch tensors of ncell doubles) without
+        waiting; snapshot_wait() returns once they are in host memory."""
+        which = (ctypes.c_int * len(names))(*[FIELD_INDEX[n] for n in names])
+        dst = (ctypes.c_void_p * len(names))(*[b.data_ptr() for b in host_bufs])
+        _lib.check(lib().rmt3d_snapshot_fields(self._h, which, len(names), dst))
+
+    def snapshot_wait(self):
+        _lib.check(lib().rmt3d_snapshot_wait(self._h))
+
     def checksum(self):
         """Sums of u^2, v^2, w^2, p^2 over the interior cells."""
         out = (ctypes.c_double * 4)()

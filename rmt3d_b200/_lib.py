@@ -182,6 +182,8 @@ SIGNATURES = {
     "rmt3d_scene_set_mg_launch": (_I, [_P, _I]),
     "rmt3d_scene_set_smoother": (_I, [_P, _I]),
     "rmt3d_scene_set_coarse_cluster": (_I, [_P, _I]),
+    "rmt3d_snapshot_fields": (_I, [_P, _IP, _I, ctypes.POINTER(_P)]),
+    "rmt3d_snapshot_wait": (_I, [_P]),
     "rmt3d_scene_footprint": (ctypes.c_size_t, [ctypes.POINTER(SceneDesc)]),
     "rmt3d_scene_checksum": (_I, [_P, _DP]),
     "rmt3d_serve": (_I, [ctypes.POINTER(Request), _I, ctypes.c_size_t, _I,

@@ -132,6 +132,12 @@ struct rmt3d_scene {
     // lanes per frontier cell of the least-squares extrapolation: a warp when
     // the scene steps on its own, 4 when it steps inside a group with others
     int extrap_lanes = 32;
+    // rmt3d_snapshot_fields: device staging copies and their own copy stream
+    double *snap = nullptr;
+    size_t snap_cap = 0;  // doubles
+    cudaStream_t cst = nullptr;
+    cudaEvent_t ev_snap = nullptr, ev_d2h = nullptr;
+    bool d2h_pending = false;
     // velocity edge states through TMA-staged tiles (k_edge_vel_tma): the
     // tensor maps of vel[0..2], made when the rows are 16-byte aligned
     bool edge_tma = false;
@@ -2268,6 +2274,42 @@ extern "C" int rmt3d_get_field(rmt3d_scene *s, int which, double *dst) {
     return RMT3D_OK;
 }
 
+extern "C" int rmt3d_snapshot_fields(rmt3d_scene *s, const int *which, int n, double *const *host_dst) {
+    if (!s || !which || !host_dst || n < 1 || n > 36) return fail(RMT3D_ERR_INVALID, "bad snapshot arguments");
+    const size_t nc = s->g.ncell;
+    for (int i = 0; i < n; i++)
+        if (!field_ptr(s, which[i]) || !host_dst[i]) return fail(RMT3D_ERR_INVALID, "unknown field or null buffer");
+    if (!s->cst) {
+        CK(cudaStreamCreateWithFlags(&s->cst, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&s->ev_snap, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s->ev_d2h, cudaEventDisableTiming));
+    }
+    // the staging copies of the previous snapshot must have reached the host
+    if (s->d2h_pending) CK(cudaStreamWaitEvent(s->st, s->ev_d2h, 0));
+    if (s->snap_cap < n * nc) {
+        if (s->snap) CK(cudaFreeAsync(s->snap, s->st));
+        s->snap = nullptr;
+        CK(cudaMallocAsync((void **)&s->snap, n * nc * sizeof(double), s->st));
+        s->snap_cap = n * nc;
+    }
+    for (int i = 0; i < n; i++)
+        CK(cudaMemcpyAsync(s->snap + i * nc, field_ptr(s, which[i]), nc * sizeof(double), cudaMemcpyDeviceToDevice,
+                           s->st));
+    CK(cudaEventRecord(s->ev_snap, s->st));
+    CK(cudaStreamWaitEvent(s->cst, s->ev_snap, 0));
+    for (int i = 0; i < n; i++)
+        CK(cudaMemcpyAsync(host_dst[i], s->snap + i * nc, nc * sizeof(double), cudaMemcpyDeviceToHost, s->cst));
+    CK(cudaEventRecord(s->ev_d2h, s->cst));
+    s->d2h_pending = true;
+    return RMT3D_OK;
+}
+
+extern "C" int rmt3d_snapshot_wait(rmt3d_scene *s) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (s->cst) CK(cudaStreamSynchronize(s->cst));
+    return RMT3D_OK;
+}
+
 extern "C" int rmt3d_get_refmap(rmt3d_scene *s, int obj, int *code, double *x, double *xpred) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     if (obj < 0 || obj >= s->g.n_obj) return fail(RMT3D_ERR_INVALID, "object index out of range");
@@ -2803,6 +2845,13 @@ extern "C" int rmt3d_profile_read(rmt3d_scene *s, double *ms_total, long long *l
 extern "C" int rmt3d_scene_destroy(rmt3d_scene *s) {
     if (!s) return RMT3D_OK;
     cudaStreamSynchronize(s->st);
+    if (s->cst) {
+        cudaStreamSynchronize(s->cst);
+        cudaStreamDestroy(s->cst);
+        cudaEventDestroy(s->ev_snap);
+        cudaEventDestroy(s->ev_d2h);
+    }
+    if (s->snap) cudaFreeAsync(s->snap, s->st);
     for (cudaEvent_t e : s->prof.ev) cudaEventDestroy(e);
     if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
     s->gb.release();
