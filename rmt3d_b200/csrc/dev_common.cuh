@@ -43,6 +43,7 @@ struct grid_dev {
     int n_obj;
     int sim_type;
     int has_exact;
+    int f32face;          // face states stored in FP32 (the mixed form), else FP64
     double gravity;
     double K_stiff, wall_dist, winv, min_wall_acc, wall_acc_mult;
     int walls[6];
@@ -73,6 +74,25 @@ __device__ inline double mono_diff(double u0, double u1, double u2, double u3, d
     double cen = 0.5 * (u3 - u1);
     double neigh_delf = (del_f(u0, u1, u2) + del_f(u2, u3, u4)) / 6.0;
     return rsign(cen) * rmin(dlim, fabs(4.0 / 3.0 * cen - neigh_delf));
+}
+
+// The same slope in FP32 (the mixed form's advection stencil), written on the
+// successive differences d0 = u1 - u0, ..., d3 = u4 - u3, of which every term
+// of mono_diff is a sum.
+__device__ __forceinline__ float del_lim_f(float a, float b) {
+    const float t1 = 2 * a, t2 = 2 * b;
+    return t1 * t2 > 0 ? fminf(fabsf(t1), fabsf(t2)) : 0.f;
+}
+__device__ __forceinline__ float del_f_f(float a, float b) {
+    const float cen = 0.5f * (a + b);
+    return (cen >= 0.f ? 1.f : -1.f) * fminf(fabsf(cen), del_lim_f(a, b));
+}
+__device__ __forceinline__ float mono_diff_f(float u0, float u1, float u2, float u3, float u4) {
+    const float d0 = u1 - u0, d1 = u2 - u1, d2 = u3 - u2, d3 = u4 - u3;
+    const float dlim = del_lim_f(d1, d2);
+    const float cen = 0.5f * (d1 + d2);
+    const float neigh = (del_f_f(d0, d1) + del_f_f(d2, d3)) * (1.f / 6.f);
+    return (cen >= 0.f ? 1.f : -1.f) * fminf(dlim, fabsf(4.f / 3.f * cen - neigh));
 }
 
 // ---- transition-zone functions (sim_manager.hh:259-280) ------------------
@@ -127,12 +147,39 @@ struct fields_dev {
     double *vel[3];
     double *p, *dp, *q;
     double *dvel[3];
-    double *fvel[18];
+    double *fvel[18];     // face states, FP64 form (null in the mixed form)
+    float *fvel32[18];    // face states, mixed form (null in the FP64 form)
     double *sigma[9];
     double *rho;  // VAR_DEN density per cell (fluid_3d.hh:160)
     objmap_dev om[kMaxObj];
     unsigned int *flags;  // scratch per-cell flags (extrapolation frontier)
 };
+
+// Velocity face states fvel[f][c] (fields.hh:296), written by the edge
+// extrapolation and read by the upwinding, both projections and the momentum
+// update.  The plain form keeps them in FP64; the mixed form keeps them in
+// FP32, as intermediate values of the advection stencils (the velocity, the
+// pressure and the reference maps stay FP64).  face_ptr picks the array of a
+// kernel instantiated for one form; face_ld / face_st serve kernels that run
+// in both forms and read g.f32face, which is uniform over the launch.
+template <typename FT>
+__device__ __forceinline__ FT *face_ptr(const fields_dev *__restrict__ F, int a);
+template <>
+__device__ __forceinline__ double *face_ptr<double>(const fields_dev *__restrict__ F, int a) {
+    return F->fvel[a];
+}
+template <>
+__device__ __forceinline__ float *face_ptr<float>(const fields_dev *__restrict__ F, int a) {
+    return F->fvel32[a];
+}
+__device__ __forceinline__ double face_ld(const grid_dev &g, const fields_dev *__restrict__ F, int a, int ind) {
+    return g.f32face ? (double)F->fvel32[a][ind] : F->fvel[a][ind];
+}
+__device__ __forceinline__ void face_st(const grid_dev &g, const fields_dev *__restrict__ F, int a, int ind,
+                                        double v) {
+    if (g.f32face) F->fvel32[a][ind] = (float)v;
+    else F->fvel[a][ind] = v;
+}
 
 // Bit o set when object o holds a map (code >= 0) at cell ind.  The codes are
 // loaded four objects at a time, so a cell costs one memory round trip per

@@ -85,7 +85,8 @@ __global__ void k_macro_cells(grid_dev g, const fields_dev *__restrict__ F, cons
             v[3] += 0.5 * u * u;
         }
         double div = 0;
-        for (int f = 0; f < 3; f++) div += dhsp[f] * (F->fvel[3 * (2 * f + 1) + f][ind] - F->fvel[3 * (2 * f) + f][ind]);
+        for (int f = 0; f < 3; f++)
+            div += dhsp[f] * (face_ld(g, F, 3 * (2 * f + 1) + f, ind) - face_ld(g, F, 3 * (2 * f) + f, ind));
         v[6] = fmax(v[6], div);
         v[7] = fmax(v[7], -div);
         for (int o = 0; o < g.n_obj; o++) {
@@ -176,8 +177,9 @@ __device__ double slice_value(const grid_dev &g, const fields_dev *__restrict__ 
         case 7: return F->p[eid];
         case 18: return r[i + g.fm * (j + g.fn * k)];
         case 19:
-            return g.dxsp * (F->fvel[3][eid] - F->fvel[0][eid]) + g.dysp * (F->fvel[10][eid] - F->fvel[7][eid]) +
-                   g.dzsp * (F->fvel[17][eid] - F->fvel[14][eid]);
+            return g.dxsp * (face_ld(g, F, 3, eid) - face_ld(g, F, 0, eid)) +
+                   g.dysp * (face_ld(g, F, 10, eid) - face_ld(g, F, 7, eid)) +
+                   g.dzsp * (face_ld(g, F, 17, eid) - face_ld(g, F, 14, eid));
         case 20: return var_den ? F->rho[eid] : 0.;
         case 21: return 100.;
         default: break;

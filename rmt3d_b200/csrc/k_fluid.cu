@@ -40,6 +40,7 @@ __global__ void k_periodic_copy(grid_dev g, ptr_list pl, int corner) {
     if (!ghost) return;
     int dst = gidx(g, i, j, k), from = gidx(g, src[0], src[1], src[2]);
     for (int a = 0; a < pl.n; a++) pl.p[a][dst] = pl.p[a][from];
+    for (int a = 0; a < pl.nf; a++) pl.fp[a][dst] = pl.fp[a][from];
     for (int a = 0; a < pl.ni; a++) pl.ip[a][dst] = pl.ip[a][from];
 }
 
@@ -112,8 +113,8 @@ __global__ void k_bc_cf(grid_dev g, int walls, bc_faces bcs, const fields_dev *F
     for (int c = 0; c < 3; c++) {
         double f = bc.bcv[c];
         if (bc.bct[c] == 2) f = (3 * bc.h * bc.bcv[c] * sgn + 9 * F->vel[c][i0] - F->vel[c][i1]) * 0.125;
-        F->fvel[3 * face + c][i0] = f;
-        F->fvel[3 * inner + c][gi] = f;
+        face_st(g, F, 3 * face + c, i0, f);
+        face_st(g, F, 3 * inner + c, gi, f);
     }
 }
 
@@ -546,35 +547,12 @@ __device__ void acceleration(const grid_dev &g, const fields_dev *__restrict__ F
     }
 }
 
-// -------------------------------------------------------------------------
-// Limited slopes + half-step edge extrapolation of the velocity:
-// normal_derivatives_velocity (fluid_3d.cc:582-617) fused with
-// compute_half_time_edge_velocities (:1038-1066) and field::godunov_extrap
-// (fields.hh:147-177, non-TANG branch).  Interior cells.
-// -------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 3) k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
-                           const double *lz, double cdt, const double *time_p, int var_den) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
-    int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-    int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
-    if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
-    const double time = *time_p;  // device-resident simulation time
-    const int ind = gidx(g, i, j, k);
-    const int strides[3] = {1, g.sm4, g.smn4};
-    const double dhsp[3] = {g.dxsp, g.dysp, g.dzsp};
-    double nv[3][3];
-    double vel[3];
-    for (int c = 0; c < 3; c++) vel[c] = F->vel[c][ind];
-    for (int d = 0; d < 3; d++) {
-        int s = strides[d];
-        for (int c = 0; c < 3; c++) {
-            const double *u = F->vel[c];
-            nv[d][c] = dhsp[d] * mono_diff(u[ind - 2 * s], u[ind - s], u[ind], u[ind + s], u[ind + 2 * s]);
-        }
-    }
-    double acc[3] = {0, 0, 0};
-    acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
-    // halves as products (the same bits as the divisions, far fewer instructions)
+// The six face states of a cell from its velocity, slopes and acceleration,
+// FP64 in the reference's order of operations (fields.hh:147-177; halves as
+// products, the same bits as the divisions).
+__device__ __forceinline__ void edge_store_f64(const grid_dev &g, const fields_dev *__restrict__ F, int ind,
+                                               const double (&vel)[3], const double (&nv)[3][3],
+                                               const double (&acc)[3], double cdt) {
     const double dh2[3] = {g.dx * 0.5, g.dy * 0.5, g.dz * 0.5};
     const double dt2 = cdt * 0.5;
     double adv[3] = {0, 0, 0};
@@ -588,6 +566,80 @@ __global__ void __launch_bounds__(256, 3) k_edge_vel(grid_dev g, const fields_de
         for (int c = 0; c < 3; c++) F->fvel[3 * f + c][ind] = vel[c] + d * nv[dim][c] + adv[c] + dt2 * acc[c];
     }
 }
+// The mixed form's FP32 face states: the same formula in FP32 with fused
+// multiply-adds (the acceleration is formed in FP64 and rounded once).
+__device__ __forceinline__ void edge_store_f32(const grid_dev &g, const fields_dev *__restrict__ F, int ind,
+                                               const float (&vel)[3], const float (&nv)[3][3],
+                                               const double (&acc)[3], double cdt) {
+    const float dh2[3] = {(float)(g.dx * 0.5), (float)(g.dy * 0.5), (float)(g.dz * 0.5)};
+    const float dt2 = (float)(cdt * 0.5);
+    float base[3];
+    for (int a = 0; a < 3; a++) {
+        float adv = 0.f;
+        for (int b = 0; b < 3; b++) adv = fmaf(-vel[b], nv[b][a], adv);
+        base[a] = vel[a] + fmaf(adv, dt2, (float)(cdt * 0.5 * acc[a]));
+    }
+    for (int f = 0; f < 6; f++) {
+        int dim = f / 2;
+        float d = (f % 2) ? dh2[dim] : -dh2[dim];
+        for (int c = 0; c < 3; c++) F->fvel32[3 * f + c][ind] = fmaf(d, nv[dim][c], base[c]);
+    }
+}
+
+// -------------------------------------------------------------------------
+// Limited slopes + half-step edge extrapolation of the velocity:
+// normal_derivatives_velocity (fluid_3d.cc:582-617) fused with
+// compute_half_time_edge_velocities (:1038-1066) and field::godunov_extrap
+// (fields.hh:147-177, non-TANG branch).  Interior cells.
+// -------------------------------------------------------------------------
+template <typename FT>
+__global__ void __launch_bounds__(256, 3) k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx,
+                                                     const double *ly, const double *lz, double cdt,
+                                                     const double *time_p, int var_den) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
+    if (i >= g.sm + 2 || j >= g.sn + 2 || k >= g.so + 2) return;
+    const double time = *time_p;  // device-resident simulation time
+    const int ind = gidx(g, i, j, k);
+    const int strides[3] = {1, g.sm4, g.smn4};
+    if constexpr (sizeof(FT) == 8) {
+        const double dhsp[3] = {g.dxsp, g.dysp, g.dzsp};
+        double nv[3][3];
+        double vel[3];
+        for (int c = 0; c < 3; c++) vel[c] = F->vel[c][ind];
+        for (int d = 0; d < 3; d++) {
+            int s = strides[d];
+            for (int c = 0; c < 3; c++) {
+                const double *u = F->vel[c];
+                nv[d][c] = dhsp[d] * mono_diff(u[ind - 2 * s], u[ind - s], u[ind], u[ind + s], u[ind + 2 * s]);
+            }
+        }
+        double acc[3] = {0, 0, 0};
+        acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
+        edge_store_f64(g, F, ind, vel, nv, acc, cdt);
+    } else {
+        const float dhsp[3] = {(float)g.dxsp, (float)g.dysp, (float)g.dzsp};
+        float nv[3][3];
+        float vel[3];
+        for (int c = 0; c < 3; c++) vel[c] = (float)F->vel[c][ind];
+        for (int d = 0; d < 3; d++) {
+            int s = strides[d];
+            for (int c = 0; c < 3; c++) {
+                const double *u = F->vel[c];
+                nv[d][c] = dhsp[d] * mono_diff_f((float)u[ind - 2 * s], (float)u[ind - s], vel[c], (float)u[ind + s],
+                                                 (float)u[ind + 2 * s]);
+            }
+        }
+        double acc[3] = {0, 0, 0};
+        acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
+        edge_store_f32(g, F, ind, vel, nv, acc, cdt);
+    }
+}
+template __global__ void k_edge_vel<double>(grid_dev, const fields_dev *__restrict__, const double *, const double *,
+                                            const double *, double, const double *, int);
+template __global__ void k_edge_vel<float>(grid_dev, const fields_dev *__restrict__, const double *, const double *,
+                                           const double *, double, const double *, int);
 
 // -------------------------------------------------------------------------
 // The same computation with the velocity staged through TMA.  A block owns
@@ -640,6 +692,7 @@ __device__ __forceinline__ bool ev_wait(uint64_t *bar, unsigned parity) {
     return false;
 }
 
+template <typename FT>
 __global__ void __launch_bounds__(256, 2) k_edge_vel_tma(grid_dev g, const fields_dev *__restrict__ F,
                                                          const __grid_constant__ CUtensorMap tmu,
                                                          const __grid_constant__ CUtensorMap tmv,
@@ -669,9 +722,6 @@ __global__ void __launch_bounds__(256, 2) k_edge_vel_tma(grid_dev g, const field
     const int i = i0 + tx, j = j0 + ty;
     const bool mine = i < g.sm + 2 && j < g.sn + 2;
     const double time = *time_p;  // device-resident simulation time
-    const double dhsp[3] = {g.dxsp, g.dysp, g.dzsp};
-    const double dh2[3] = {g.dx * 0.5, g.dy * 0.5, g.dz * 0.5};
-    const double dt2 = cdt * 0.5;
     bool ok = true;
     for (int k = k0; k < k1; k++) {
         // planes k-2 .. k+2 have landed (k+2 is the newest one needed)
@@ -683,28 +733,41 @@ __global__ void __launch_bounds__(256, 2) k_edge_vel_tma(grid_dev g, const field
             const double *pl[5];
 #pragma unroll
             for (int d = 0; d < 5; d++) pl[d] = ring + (size_t)slot(k - 2 + d) * 3 * kEvW * kEvH;
-            double nv[3][3];
-            double vel[3];
+            if constexpr (sizeof(FT) == 8) {
+                const double dhsp[3] = {g.dxsp, g.dysp, g.dzsp};
+                double nv[3][3];
+                double vel[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const double *u2 = pl[2] + c * kEvW * kEvH;
-                vel[c] = u2[o];
-                nv[0][c] = dhsp[0] * mono_diff(u2[o - 2], u2[o - 1], u2[o], u2[o + 1], u2[o + 2]);
-                nv[1][c] = dhsp[1] * mono_diff(u2[o - 2 * kEvW], u2[o - kEvW], u2[o], u2[o + kEvW], u2[o + 2 * kEvW]);
-                nv[2][c] = dhsp[2] * mono_diff(pl[0][c * kEvW * kEvH + o], pl[1][c * kEvW * kEvH + o], u2[o],
-                                               pl[3][c * kEvW * kEvH + o], pl[4][c * kEvW * kEvH + o]);
-            }
-            double acc[3] = {0, 0, 0};
-            acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
-            double adv[3] = {0, 0, 0};
-            for (int a = 0; a < 3; a++) {
-                for (int b = 0; b < 3; b++) adv[a] -= vel[b] * nv[b][a];
-                adv[a] *= dt2;
-            }
-            for (int f = 0; f < 6; f++) {
-                int dim = f / 2;
-                double d = dh2[dim] * (2 * (f % 2) - 1);
-                for (int c = 0; c < 3; c++) F->fvel[3 * f + c][ind] = vel[c] + d * nv[dim][c] + adv[c] + dt2 * acc[c];
+                for (int c = 0; c < 3; c++) {
+                    const double *u2 = pl[2] + c * kEvW * kEvH;
+                    vel[c] = u2[o];
+                    nv[0][c] = dhsp[0] * mono_diff(u2[o - 2], u2[o - 1], u2[o], u2[o + 1], u2[o + 2]);
+                    nv[1][c] = dhsp[1] * mono_diff(u2[o - 2 * kEvW], u2[o - kEvW], u2[o], u2[o + kEvW], u2[o + 2 * kEvW]);
+                    nv[2][c] = dhsp[2] * mono_diff(pl[0][c * kEvW * kEvH + o], pl[1][c * kEvW * kEvH + o], u2[o],
+                                                   pl[3][c * kEvW * kEvH + o], pl[4][c * kEvW * kEvH + o]);
+                }
+                double acc[3] = {0, 0, 0};
+                acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
+                edge_store_f64(g, F, ind, vel, nv, acc, cdt);
+            } else {
+                const float dhsp[3] = {(float)g.dxsp, (float)g.dysp, (float)g.dzsp};
+                float nv[3][3];
+                float vel[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const double *u2 = pl[2] + c * kEvW * kEvH;
+                    vel[c] = (float)u2[o];
+                    nv[0][c] = dhsp[0] * mono_diff_f((float)u2[o - 2], (float)u2[o - 1], vel[c], (float)u2[o + 1],
+                                                     (float)u2[o + 2]);
+                    nv[1][c] = dhsp[1] * mono_diff_f((float)u2[o - 2 * kEvW], (float)u2[o - kEvW], vel[c],
+                                                     (float)u2[o + kEvW], (float)u2[o + 2 * kEvW]);
+                    nv[2][c] = dhsp[2] * mono_diff_f((float)pl[0][c * kEvW * kEvH + o], (float)pl[1][c * kEvW * kEvH + o],
+                                                     vel[c], (float)pl[3][c * kEvW * kEvH + o],
+                                                     (float)pl[4][c * kEvW * kEvH + o]);
+                }
+                double acc[3] = {0, 0, 0};
+                acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
+                edge_store_f32(g, F, ind, vel, nv, acc, cdt);
             }
         }
         // every thread is done with plane k-2: its slot takes plane k+4
@@ -752,7 +815,10 @@ void launch_edge_vel_tma(const grid_dev &g, const fields_dev *F, const CUtensorM
                          cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_edge_vel_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)edge_vel_tma_smem());
+        cudaFuncSetAttribute(k_edge_vel_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)edge_vel_tma_smem());
+        cudaFuncSetAttribute(k_edge_vel_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)edge_vel_tma_smem());
         attr = true;
     }
     const int tx = (g.sm + kEvX - 1) / kEvX, ty = (g.sn + kEvY - 1) / kEvY;
@@ -763,8 +829,12 @@ void launch_edge_vel_tma(const grid_dev &g, const fields_dev *F, const CUtensorM
     nz = nz < 1 ? 1 : (nz > (g.so + 1) / 2 ? (g.so + 1) / 2 : nz);
     const int tz = (g.so + nz - 1) / nz;
     const dim3 grid(tx, ty, (g.so + tz - 1) / tz);
-    k_edge_vel_tma<<<grid, dim3(kEvX, kEvY), edge_vel_tma_smem(), st>>>(g, F, tm[0], tm[1], tm[2], lx, ly, lz, cdt,
-                                                                       time_p, var_den, tz, err);
+    if (g.f32face)
+        k_edge_vel_tma<float><<<grid, dim3(kEvX, kEvY), edge_vel_tma_smem(), st>>>(g, F, tm[0], tm[1], tm[2], lx, ly,
+                                                                                  lz, cdt, time_p, var_den, tz, err);
+    else
+        k_edge_vel_tma<double><<<grid, dim3(kEvX, kEvY), edge_vel_tma_smem(), st>>>(g, F, tm[0], tm[1], tm[2], lx, ly,
+                                                                                   lz, cdt, time_p, var_den, tz, err);
 }
 
 // -------------------------------------------------------------------------
@@ -794,6 +864,7 @@ __device__ inline void set_refmap(double norml, double normr, double &ml, double
     }
 }
 
+template <typename FT>
 __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -814,7 +885,7 @@ __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F) {
             const int nb = ind + strides[dir];
             const int ff = 2 * dir + 1, nf = ff ^ 1;
             const int a1 = (dir + 1) % 3, a2 = (dir + 2) % 3;
-            const double norml = F->fvel[3 * ff + dir][ind], normr = F->fvel[3 * nf + dir][nb];
+            const double norml = face_ptr<FT>(F, 3 * ff + dir)[ind], normr = face_ptr<FT>(F, 3 * nf + dir)[nb];
             double ml = m.fx[3 * ff + dir][ind], vl = m.fx[3 * ff + a1][ind], wl = m.fx[3 * ff + a2][ind];
             double mr = m.fx[3 * nf + dir][nb], vr = m.fx[3 * nf + a1][nb], wr = m.fx[3 * nf + a2][nb];
             set_refmap(norml, normr, ml, vl, wl, mr, vr, wr);
@@ -830,8 +901,10 @@ __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F) {
         const int nb = ind + strides[dir];
         const int ff = 2 * dir + 1, nf = ff ^ 1;
         const int a1 = (dir + 1) % 3, a2 = (dir + 2) % 3;
-        double nl = F->fvel[3 * ff + dir][ind], vl = F->fvel[3 * ff + a1][ind], wl = F->fvel[3 * ff + a2][ind];
-        double nr = F->fvel[3 * nf + dir][nb], vr = F->fvel[3 * nf + a1][nb], wr = F->fvel[3 * nf + a2][nb];
+        FT *const fl[3] = {face_ptr<FT>(F, 3 * ff + dir), face_ptr<FT>(F, 3 * ff + a1), face_ptr<FT>(F, 3 * ff + a2)};
+        FT *const fr[3] = {face_ptr<FT>(F, 3 * nf + dir), face_ptr<FT>(F, 3 * nf + a1), face_ptr<FT>(F, 3 * nf + a2)};
+        FT nl = fl[0][ind], vl = fl[1][ind], wl = fl[2][ind];
+        FT nr = fr[0][nb], vr = fr[1][nb], wr = fr[2][nb];
         if (nl + nr > 0 && nl > 0) {
             nr = nl;
             vr = vl;
@@ -842,19 +915,21 @@ __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F) {
             wl = wr;
         } else {
             nl = nr = 0;
-            double t = 0.5 * (vl + vr);
+            FT t = (FT)0.5 * (vl + vr);
             vl = vr = t;
-            t = 0.5 * (wl + wr);
+            t = (FT)0.5 * (wl + wr);
             wl = wr = t;
         }
-        F->fvel[3 * ff + dir][ind] = nl;
-        F->fvel[3 * ff + a1][ind] = vl;
-        F->fvel[3 * ff + a2][ind] = wl;
-        F->fvel[3 * nf + dir][nb] = nr;
-        F->fvel[3 * nf + a1][nb] = vr;
-        F->fvel[3 * nf + a2][nb] = wr;
+        fl[0][ind] = nl;
+        fl[1][ind] = vl;
+        fl[2][ind] = wl;
+        fr[0][nb] = nr;
+        fr[1][nb] = vr;
+        fr[2][nb] = wr;
     }
 }
+template __global__ void k_upwind<double>(grid_dev, const fields_dev *__restrict__);
+template __global__ void k_upwind<float>(grid_dev, const fields_dev *__restrict__);
 
 // -------------------------------------------------------------------------
 // MAC projection: rhs (fill_mac_rhs, fluid_3d.cc:2244-2265), solution
@@ -868,7 +943,7 @@ __global__ void k_mac_rhs(grid_dev g, const fields_dev *__restrict__ F, double *
     const int ind = gidx(g, i + 2, j + 2, k + 2);
     const double fac = g.dx / (2 * cdt);
     double s = 0;
-    for (int f = 0; f < 3; f++) s += fac * (F->fvel[3 * (2 * f + 1) + f][ind] - F->fvel[3 * (2 * f) + f][ind]);
+    for (int f = 0; f < 3; f++) s += fac * (face_ld(g, F, 3 * (2 * f + 1) + f, ind) - face_ld(g, F, 3 * (2 * f) + f, ind));
     r[i + g.sm * (j + g.sn * k)] = s;
 }
 
@@ -900,16 +975,18 @@ __global__ void k_sub_qgrad(grid_dev g, const fields_dev *__restrict__ F, double
             down = fac * (q[ind] - q[ind - s]);
             up = fac * (q[ind + s] - q[ind]);
         }
-        F->fvel[3 * (2 * f) + f][ind] -= down;
-        F->fvel[3 * (2 * f + 1) + f][ind] -= up;
+        face_st(g, F, 3 * (2 * f) + f, ind, face_ld(g, F, 3 * (2 * f) + f, ind) - down);
+        face_st(g, F, 3 * (2 * f + 1) + f, ind, face_ld(g, F, 3 * (2 * f + 1) + f, ind) - up);
     }
 }
 
 // -------------------------------------------------------------------------
 // Explicit momentum update, fluid_3d::compute_ustar (fluid_3d.cc:1309-1352).
 // -------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 3) k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
-                        const double *lz, double cdt, const double *time_p, int var_den) {
+template <typename FT>
+__global__ void __launch_bounds__(256, 3) k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx,
+                                                  const double *ly, const double *lz, double cdt,
+                                                  const double *time_p, int var_den) {
     int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
     int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
     int k = blockIdx.z * blockDim.z + threadIdx.z + 2;
@@ -918,18 +995,32 @@ __global__ void __launch_bounds__(256, 3) k_ustar(grid_dev g, const fields_dev *
     const int ind = gidx(g, i, j, k);
     double acc[3] = {0, 0, 0};
     acceleration(g, F, lx, ly, lz, i, j, k, time, var_den != 0, acc);
-    double fv[18];
-    for (int a = 0; a < 18; a++) fv[a] = F->fvel[a][ind];
-    double avgs[3];
-    avgs[0] = -0.5 * cdt * (fv[0] + fv[3]) * g.dxsp;
-    avgs[1] = -0.5 * cdt * (fv[3 * 2 + 1] + fv[3 * 3 + 1]) * g.dysp;
-    avgs[2] = -0.5 * cdt * (fv[3 * 4 + 2] + fv[3 * 5 + 2]) * g.dzsp;
+    FT fv[18];
+    for (int a = 0; a < 18; a++) fv[a] = face_ptr<FT>(F, a)[ind];
     double dv[3];
-    for (int d = 0; d < 3; d++) {
-        dv[d] = avgs[0] * (fv[3 + d] - fv[d]) + avgs[1] * (fv[9 + d] - fv[6 + d]) + avgs[2] * (fv[15 + d] - fv[12 + d]);
-        acc[d] *= cdt;
+    if constexpr (sizeof(FT) == 8) {
+        double avgs[3];
+        avgs[0] = -0.5 * cdt * (fv[0] + fv[3]) * g.dxsp;
+        avgs[1] = -0.5 * cdt * (fv[3 * 2 + 1] + fv[3 * 3 + 1]) * g.dysp;
+        avgs[2] = -0.5 * cdt * (fv[3 * 4 + 2] + fv[3 * 5 + 2]) * g.dzsp;
+        for (int d = 0; d < 3; d++) {
+            dv[d] = avgs[0] * (fv[3 + d] - fv[d]) + avgs[1] * (fv[9 + d] - fv[6 + d]) + avgs[2] * (fv[15 + d] - fv[12 + d]);
+            acc[d] *= cdt;
+        }
+        for (int d = 0; d < 3; d++) dv[d] += acc[d];
+    } else {
+        // the mixed form: the advective increment in FP32 from the FP32 face
+        // states, added to the FP64 velocity with the FP64 acceleration term
+        const float hdt = (float)(-0.5 * cdt);
+        const float avgs[3] = {hdt * (fv[0] + fv[3]) * (float)g.dxsp, hdt * (fv[3 * 2 + 1] + fv[3 * 3 + 1]) * (float)g.dysp,
+                               hdt * (fv[3 * 4 + 2] + fv[3 * 5 + 2]) * (float)g.dzsp};
+        for (int d = 0; d < 3; d++) {
+            float t = avgs[0] * (fv[3 + d] - fv[d]);
+            t = fmaf(avgs[1], fv[9 + d] - fv[6 + d], t);
+            t = fmaf(avgs[2], fv[15 + d] - fv[12 + d], t);
+            dv[d] = (double)t + acc[d] * cdt;
+        }
     }
-    for (int d = 0; d < 3; d++) dv[d] += acc[d];
     for (int d = 0; d < 3; d++) {
         double dd = 0.;
         dd += dv[d];
@@ -937,6 +1028,10 @@ __global__ void __launch_bounds__(256, 3) k_ustar(grid_dev g, const fields_dev *
         F->vel[d][ind] += dd;
     }
 }
+template __global__ void k_ustar<double>(grid_dev, const fields_dev *__restrict__, const double *, const double *,
+                                         const double *, double, const double *, int);
+template __global__ void k_ustar<float>(grid_dev, const fields_dev *__restrict__, const double *, const double *,
+                                        const double *, double, const double *, int);
 
 // -------------------------------------------------------------------------
 // FEM projection right-hand side, fluid_3d::fill_pp_rhs (fluid_3d.cc:
@@ -1003,7 +1098,7 @@ __global__ void k_fem_rhs(grid_dev g, const fields_dev *__restrict__ F, double *
                 if (!ok) continue;
                 const int lid = inds[0] + 2 * inds[1] + 4 * inds[2];
                 const int cell = gidx(g, e[0] + 2, e[1] + 2, e[2] + 2);
-                double val = -F->fvel[3 * face + nd][cell] * gp.v[lid][nd];
+                double val = -face_ld(g, F, 3 * face + nd, cell) * gp.v[lid][nd];
                 s += val;
             }
     }

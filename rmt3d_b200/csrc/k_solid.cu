@@ -79,9 +79,9 @@ __global__ void k_refmap_predict(grid_dev g, const fields_dev *__restrict__ F, d
         const objmap_dev &m = F->om[o];
         if (m.code[ind] != 0) continue;
         double avgs[3];
-        avgs[0] = -0.5 * cdt * (F->fvel[0][ind] + F->fvel[3][ind]) * g.dxsp;
-        avgs[1] = -0.5 * cdt * (F->fvel[7][ind] + F->fvel[10][ind]) * g.dysp;
-        avgs[2] = -0.5 * cdt * (F->fvel[14][ind] + F->fvel[17][ind]) * g.dzsp;
+        avgs[0] = -0.5 * cdt * (face_ld(g, F, 0, ind) + face_ld(g, F, 3, ind)) * g.dxsp;
+        avgs[1] = -0.5 * cdt * (face_ld(g, F, 7, ind) + face_ld(g, F, 10, ind)) * g.dysp;
+        avgs[2] = -0.5 * cdt * (face_ld(g, F, 14, ind) + face_ld(g, F, 17, ind)) * g.dzsp;
         for (int d = 0; d < 3; d++) {
             double dx = avgs[0] * (m.fx[3 + d][ind] - m.fx[d][ind]) + avgs[1] * (m.fx[9 + d][ind] - m.fx[6 + d][ind]) +
                         avgs[2] * (m.fx[15 + d][ind] - m.fx[12 + d][ind]);

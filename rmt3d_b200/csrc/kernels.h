@@ -12,7 +12,8 @@ namespace rmt3d {
 struct ptr_list {
     double *p[40];
     int *ip[4];
-    int n, ni;
+    float *fp[18];
+    int n, ni, nf;
 };
 
 // one physical boundary face (face_gm, fields.hh:661-850)
@@ -47,6 +48,8 @@ __global__ void k_bc_cc(grid_dev g, int n, bc_face lo, bc_face hi, double *u, do
 __global__ void k_bc_cf(grid_dev g, int walls, bc_faces bcs, const fields_dev *F);
 __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F, const int *list, const int *cnt);
 __global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt);
+// FT: the face states' type, double in the plain form, float in the mixed form
+template <typename FT>
 __global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
                            const double *lz, double cdt, const double *time_p, int var_den);
 // the velocity edge states with TMA-staged velocity tiles (k_fluid.cu)
@@ -54,10 +57,12 @@ bool edge_vel_tensor_map(const grid_dev &g, const double *base, CUtensorMap *out
 void launch_edge_vel_tma(const grid_dev &g, const fields_dev *F, const CUtensorMap tm[3], const double *lx,
                          const double *ly, const double *lz, double cdt, const double *time_p, int var_den, int *err,
                          cudaStream_t st);
+template <typename FT>
 __global__ void k_upwind(grid_dev g, const fields_dev *__restrict__ F);
 __global__ void k_mac_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, double cdt);
 __global__ void k_mac_extract(grid_dev g, const fields_dev *__restrict__ F, const double *x);
 __global__ void k_sub_qgrad(grid_dev g, const fields_dev *__restrict__ F, double cdt, int var_den);
+template <typename FT>
 __global__ void k_ustar(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
                         const double *lz, double cdt, const double *time_p, int var_den);
 __global__ void k_fem_rhs(grid_dev g, const fields_dev *__restrict__ F, double *r, gradphi_t gp);

@@ -212,6 +212,51 @@ static cudaError_t copy_sync(rmt3d_scene *s, void *dst, const void *src, size_t 
     return cudaStreamSynchronize(s->st);
 }
 
+// The velocity face states are FP32 in the mixed form (g.f32face): zeroed,
+// read and written from the host through these, widened to and narrowed from
+// FP64 on the host side.
+// The mixed form keeps the face states in FP32 unless the environment sets
+// RMT3D_FACE32=0 (a measurement switch; the plain form is always FP64).
+static bool face32(const rmt3d_scene_desc &d) {
+    if (d.precision != RMT3D_MIXED) return false;
+    const char *e = getenv("RMT3D_FACE32");
+    return !(e && e[0] == '0');
+}
+
+static cudaError_t zero_faces(rmt3d_scene *s) {
+    const size_t n = s->g.ncell;
+    for (int c = 0; c < 18; c++) {
+        cudaError_t e = s->g.f32face ? cudaMemsetAsync(s->hF.fvel32[c], 0, n * sizeof(float), s->st)
+                                     : cudaMemsetAsync(s->hF.fvel[c], 0, n * sizeof(double), s->st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+static int faces_to_host(rmt3d_scene *s, int c, double *dst) {
+    const size_t n = s->g.ncell;
+    if (!s->g.f32face) {
+        CK(copy_sync(s, dst, s->hF.fvel[c], n * sizeof(double), cudaMemcpyDeviceToHost));
+        return RMT3D_OK;
+    }
+    std::vector<float> t(n);
+    CK(copy_sync(s, t.data(), s->hF.fvel32[c], n * sizeof(float), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < n; i++) dst[i] = t[i];
+    return RMT3D_OK;
+}
+
+static int faces_from_host(rmt3d_scene *s, int c, const double *src) {
+    const size_t n = s->g.ncell;
+    if (!s->g.f32face) {
+        CK(copy_sync(s, s->hF.fvel[c], src, n * sizeof(double), cudaMemcpyHostToDevice));
+        return RMT3D_OK;
+    }
+    std::vector<float> t(n);
+    for (size_t i = 0; i < n; i++) t[i] = (float)src[i];
+    CK(copy_sync(s, s->hF.fvel32[c], t.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    return RMT3D_OK;
+}
+
 // ---------------------------------------------------------------------------
 // ghost-frame helpers
 // ---------------------------------------------------------------------------
@@ -221,6 +266,7 @@ static void periodic(rmt3d_scene *s, std::initializer_list<double *> arrs, std::
     ptr_list pl;
     pl.n = 0;
     pl.ni = 0;
+    pl.nf = 0;
     for (double *a : arrs) pl.p[pl.n++] = a;
     for (int *a : iarrs) pl.ip[pl.ni++] = a;
     k_periodic_copy<<<grd(s->g.sm4, s->g.sn4, s->g.so4), blk(), 0, s->st>>>(s->g, pl, corner);
@@ -259,9 +305,13 @@ static void fill_boundary_cf(rmt3d_scene *s) {
     }
     if (g.prd[0] || g.prd[1] || g.prd[2]) {
         ptr_list pl;
-        pl.n = 18;
+        pl.n = g.f32face ? 0 : 18;
         pl.ni = 0;
-        for (int a = 0; a < 18; a++) pl.p[a] = s->hF.fvel[a];
+        pl.nf = g.f32face ? 18 : 0;
+        for (int a = 0; a < 18; a++) {
+            pl.p[a] = s->hF.fvel[a];
+            pl.fp[a] = s->hF.fvel32[a];
+        }
         k_periodic_copy<<<grd(g.sm4, g.sn4, g.so4), blk(), 0, s->st>>>(g, pl, 0);
         s->count();
     }
@@ -280,6 +330,7 @@ static void comm_face_maps(rmt3d_scene *s) {
         ptr_list pl;
         pl.n = 18;
         pl.ni = 0;
+        pl.nf = 0;
         for (int a = 0; a < 18; a++) pl.p[a] = s->hF.om[o].fx[a];
         k_periodic_copy<<<grd(g.sm4, g.sn4, g.so4), blk(), 0, s->st>>>(g, pl, 0);
         s->count();
@@ -294,6 +345,7 @@ static void comm_primary(rmt3d_scene *s) {
         objmap_dev &m = s->hF.om[o];
         ptr_list pl;
         pl.n = 0;
+        pl.nf = 0;
         for (int a = 0; a < 3; a++) pl.p[pl.n++] = m.x[a];
         for (int a = 0; a < 3; a++) pl.p[pl.n++] = m.xp[a];
         pl.ni = 1;
@@ -552,7 +604,7 @@ static int init_fluid(rmt3d_scene *s) {
         CK(cudaMemsetAsync(s->hF.q, 0, n * 8, s->st));
         CK(cudaMemsetAsync(s->hF.dp, 0, n * 8, s->st));
         for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(s->hF.dvel[c], 0, n * 8, s->st));
-        for (int c = 0; c < 18; c++) CK(cudaMemsetAsync(s->hF.fvel[c], 0, n * 8, s->st));
+        CK(zero_faces(s));
         for (int c = 0; c < 9; c++) CK(cudaMemsetAsync(s->hF.sigma[c], 0, n * 8, s->st));
         CK(cudaMemcpyAsync(s->h_scalar, s->d_red, sizeof(double), cudaMemcpyDeviceToHost, s->st));
         CK(cudaStreamSynchronize(s->st));
@@ -580,7 +632,7 @@ static int init_fluid(rmt3d_scene *s) {
     CK(cudaMemsetAsync(s->hF.q, 0, n * 8, s->st));
     CK(cudaMemsetAsync(s->hF.dp, 0, n * 8, s->st));
     for (int c = 0; c < 3; c++) CK(cudaMemsetAsync(s->hF.dvel[c], 0, n * 8, s->st));
-    for (int c = 0; c < 18; c++) CK(cudaMemsetAsync(s->hF.fvel[c], 0, n * 8, s->st));
+    CK(zero_faces(s));
     for (int c = 0; c < 9; c++) CK(cudaMemsetAsync(s->hF.sigma[c], 0, n * 8, s->st));
     if (s->d.var_den) {
         std::vector<double> r(n, s->d.frho);
@@ -760,9 +812,12 @@ static void ph_edges(rmt3d_scene *s) {
     if (s->edge_tma)
         launch_edge_vel_tma(g, s->dF, s->tm_vel, s->lx, s->ly, s->lz, s->dt, &s->ctl->time, s->d.var_den,
                             s->counters + 7, s->st);
+    else if (g.f32face)
+        k_edge_vel<float><<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
+                                                                       &s->ctl->time, s->d.var_den);
     else
-        k_edge_vel<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, &s->ctl->time,
-                                                                s->d.var_den);
+        k_edge_vel<double><<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
+                                                                        &s->ctl->time, s->d.var_den);
     s->count();
     if (g.n_obj > 0) {
         k_edge_refmap<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->counters + 5);
@@ -776,7 +831,8 @@ static void ph_upwind(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     fill_boundary_cf(s);
     comm_face_maps(s);
-    k_upwind<<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
+    if (g.f32face) k_upwind<float><<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
+    else k_upwind<double><<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
     s->count();
     fill_boundary_cf(s);
 }
@@ -827,8 +883,12 @@ static void ph_revert(rmt3d_scene *s) {
 // compute_ustar (fluid_3d.cc:1309-1352) and its boundary fills
 static void ph_ustar(rmt3d_scene *s) {
     const grid_dev &g = s->g;
-    k_ustar<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt, &s->ctl->time,
-                                                         s->d.var_den);
+    if (g.f32face)
+        k_ustar<float><<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
+                                                                    &s->ctl->time, s->d.var_den);
+    else
+        k_ustar<double><<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
+                                                                     &s->ctl->time, s->d.var_den);
     s->count();
     fill_boundary_cc(s);
     comm_dvel(s);
@@ -1699,6 +1759,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     g.n_obj = d.n_obj;
     g.sim_type = d.sim_type;
     g.has_exact = d.has_exact;
+    g.f32face = face32(d);
     g.gravity = d.gravity;
     for (int f = 0; f < 6; f++) {
         g.walls[f] = d.walls[f];
@@ -1824,7 +1885,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     memset(&F, 0, sizeof(F));
     for (int c = 0; c < 3 && !e; c++) e |= s->alloc(&F.vel[c], n) | s->alloc(&F.dvel[c], n);
     e |= s->alloc(&F.p, n) | s->alloc(&F.dp, n) | s->alloc(&F.q, n);
-    for (int c = 0; c < 18 && !e; c++) e |= s->alloc(&F.fvel[c], n);
+    for (int c = 0; c < 18 && !e; c++) e |= g.f32face ? s->alloc(&F.fvel32[c], n) : s->alloc(&F.fvel[c], n);
     for (int c = 0; c < 9 && !e; c++) e |= s->alloc(&F.sigma[c], n);
     if (d.var_den) e |= s->alloc(&F.rho, n);
     for (int o = 0; o < d.n_obj && !e; o++) {
@@ -1981,7 +2042,7 @@ static int read_chk_pt(rmt3d_scene *s, const char *dir, int *status) {
     if (ce == cudaSuccess) ce = cudaMemsetAsync(F.dp, 0, n * 8, s->st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(F.q, 0, n * 8, s->st);
     for (int c = 0; c < 3 && ce == cudaSuccess; c++) ce = cudaMemsetAsync(F.dvel[c], 0, n * 8, s->st);
-    for (int c = 0; c < 18 && ce == cudaSuccess; c++) ce = cudaMemsetAsync(F.fvel[c], 0, n * 8, s->st);
+    if (ce == cudaSuccess) ce = zero_faces(s);
     for (int c = 0; c < 9 && ce == cudaSuccess; c++) ce = cudaMemsetAsync(F.sigma[c], 0, n * 8, s->st);
     int hbad = 0;
     if (ce == cudaSuccess) {
@@ -2260,13 +2321,17 @@ static double *field_ptr(rmt3d_scene *s, int which) {
     if (which == 4) return F.dp;
     if (which == 5) return F.q;
     if (which >= 6 && which < 9) return F.dvel[which - 6];
-    if (which >= 9 && which < 27) return F.fvel[which - 9];
+    if (which >= 9 && which < 27) return F.fvel[which - 9];  // null for the mixed form's FP32 faces
     if (which >= 27 && which < 36) return F.sigma[which - 27];
     return nullptr;
 }
 
 extern "C" int rmt3d_get_field(rmt3d_scene *s, int which, double *dst) {
     if (!s || !dst) return fail(RMT3D_ERR_INVALID, "null argument");
+    if (which >= 9 && which < 27 && s->g.f32face) {
+        CK(cudaStreamSynchronize(s->st));
+        return faces_to_host(s, which - 9, dst);
+    }
     double *p = field_ptr(s, which);
     if (!p) return fail(RMT3D_ERR_INVALID, "unknown field");
     CK(cudaStreamSynchronize(s->st));
@@ -2278,7 +2343,8 @@ extern "C" int rmt3d_snapshot_fields(rmt3d_scene *s, const int *which, int n, do
     if (!s || !which || !host_dst || n < 1 || n > 36) return fail(RMT3D_ERR_INVALID, "bad snapshot arguments");
     const size_t nc = s->g.ncell;
     for (int i = 0; i < n; i++)
-        if (!field_ptr(s, which[i]) || !host_dst[i]) return fail(RMT3D_ERR_INVALID, "unknown field or null buffer");
+        if (!field_ptr(s, which[i]) || !host_dst[i])
+            return fail(RMT3D_ERR_INVALID, "unknown field, FP32 face state (read it with rmt3d_get_field), or null buffer");
     if (!s->cst) {
         CK(cudaStreamCreateWithFlags(&s->cst, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&s->ev_snap, cudaEventDisableTiming));
@@ -2348,7 +2414,14 @@ extern "C" int rmt3d_import_reference(rmt3d_scene *s, const void *field_aos, con
     int e = 0;
     for (int c = 0; c < 3; c++) e |= put(s->hF.vel[c], fa, F_N, F_VEL + c) | put(s->hF.dvel[c], fa, F_N, F_DVEL + c);
     e |= put(s->hF.p, fa, F_N, F_P) | put(s->hF.dp, fa, F_N, F_DP) | put(s->hF.q, fa, F_N, F_Q);
-    for (int c = 0; c < 18; c++) e |= put(s->hF.fvel[c], fa, F_N, F_FVEL + c);
+    for (int c = 0; c < 18; c++) {
+        if (!s->g.f32face) {
+            e |= put(s->hF.fvel[c], fa, F_N, F_FVEL + c);
+            continue;
+        }
+        for (size_t i = 0; i < n; i++) buf[i] = fa[i * F_N + F_FVEL + c];
+        e |= faces_from_host(s, c, buf.data());
+    }
     for (int c = 0; c < 9; c++) e |= put(s->hF.sigma[c], fa, F_N, F_SIGMA + c);
     if (e) return e;
     const int no = s->g.n_obj;
@@ -2419,7 +2492,14 @@ extern "C" int rmt3d_export_reference(rmt3d_scene *s, void *field_aos, void *ref
         int e = 0;
         for (int c = 0; c < 3; c++) e |= get(s->hF.vel[c], F_VEL + c) | get(s->hF.dvel[c], F_DVEL + c);
         e |= get(s->hF.p, F_P) | get(s->hF.dp, F_DP) | get(s->hF.q, F_Q);
-        for (int c = 0; c < 18; c++) e |= get(s->hF.fvel[c], F_FVEL + c);
+        for (int c = 0; c < 18; c++) {
+            if (!s->g.f32face) {
+                e |= get(s->hF.fvel[c], F_FVEL + c);
+                continue;
+            }
+            e |= faces_to_host(s, c, buf.data());
+            for (size_t i = 0; i < n; i++) fa[i * F_N + F_FVEL + c] = buf[i];
+        }
         for (int c = 0; c < 9; c++) e |= get(s->hF.sigma[c], F_SIGMA + c);
         if (e) return e;
     }
@@ -2773,7 +2853,7 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     // mirrors the allocations of rmt3d_scene_create and mg_solver::setup
     if (!d || d->sys_size[0] < 1 || d->sys_size[1] < 1 || d->sys_size[2] < 1) return 0;
     const size_t n = (size_t)(d->sys_size[0] + 4) * (d->sys_size[1] + 4) * (d->sys_size[2] + 4);
-    size_t b = n * sizeof(double) * (36 + (d->var_den ? 1 : 0));
+    size_t b = n * sizeof(double) * (18 + (d->var_den ? 1 : 0)) + n * 18 * (face32(*d) ? sizeof(float) : sizeof(double));
     b += (size_t)d->n_obj * n * (2 * sizeof(int) + 51 * sizeof(double));
     if (d->n_obj > 0)
         b += (size_t)d->n_obj * n * (sizeof(uint8_t) + 3 * sizeof(int)) + 2 * kMaxObj * sizeof(int) +
