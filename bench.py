@@ -435,6 +435,7 @@ def run_ours(args):
         sc.set_mg_launch(tuned[2])
         sc.set_smoother(tuned[3])
         sc.set_coarse_cluster(tuned[4])
+        sc.set_block_shape(tuned[5])
         sc.prepare()
         sc.schedule = tuned
         return sc

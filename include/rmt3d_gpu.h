@@ -366,6 +366,15 @@ int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode);
  * per-phase launches.  No counterpart in the reference. */
 int rmt3d_scene_set_coarse_cluster(rmt3d_scene *s, int pts);
 
+/* Block shape of the bulk stencil kernels of the step (stress, edge states,
+ * upwinding, projections' right-hand sides and corrections, momentum
+ * update): the tile of cells one 256-thread block covers, by index --
+ * 0: 32x4x2 (default), 1: 32x8x1, 2: 64x4x1, 3: 32x2x4, 4: 128x2x1.  Every
+ * cell's result is independent of the shape (the same bits).  No counterpart
+ * in the reference. */
+#define RMT3D_BLOCK_SHAPES 5
+int rmt3d_scene_set_block_shape(rmt3d_scene *s, int shape);
+
 /* Launch timing of one kernel class for roofline measurement (no counterpart
  * in the reference, which has no device code): kernel 0 = FEM Gauss-Seidel
  * colour pass on the finest level, 1 = MAC red-black pass on the finest level,
@@ -397,8 +406,10 @@ int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out);
  * (Utilities/mg_probs.hh:80-208), the cluster or per-phase launch of the
  * solves, the smoother (colour passes or tiled sweeps) and the coarse
  * levels run as one cluster launch per V-cycle (rmt3d_scene_set_coarse_cluster);
- * tuned_out gets (cells, v_down, v_up, cluster, smoother, coarse cluster
- * points) per kind */
+ * then, under the chosen schedule, the block shape of the bulk stencil
+ * kernels (rmt3d_scene_set_block_shape).  tuned_out gets 7 ints per kind:
+ * (cells, v_down, v_up, cluster, smoother, coarse cluster points, block
+ * shape) */
 int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out);
 
 /* rmt3d_scene_set_smoother on every scene of the batch. */

@@ -274,6 +274,11 @@ class Scene:
         as one thread-block-cluster launch per cycle; 0: per-phase launches."""
         _lib.check(lib().rmt3d_scene_set_coarse_cluster(self._h, int(pts)))
 
+    def set_block_shape(self, shape):
+        """Block shape of the bulk stencil kernels by index (0: 32x4x2,
+        1: 32x8x1, 2: 64x4x1, 3: 32x2x4, 4: 128x2x1; the same bits)."""
+        _lib.check(lib().rmt3d_scene_set_block_shape(self._h, int(shape)))
+
     def snapshot(self, names, host_bufs):
         """Start copying the named fields to host buffers (objects with
         data_ptr(), e.g. pinned torch tensors of ncell doubles) without
@@ -481,12 +486,13 @@ class Batch:
 
     def autotune(self, probe_steps=3):
         """Per kind of scene: {cells: (v_down, v_up, cluster, smoother,
-        coarse cluster points)} chosen by timing candidates (smoother 0:
-        colour passes, 1: tiled sweeps)."""
-        buf = (ctypes.c_int * (6 * self.n))()
+        coarse cluster points, block shape)} chosen by timing candidates
+        (smoother 0: colour passes, 1: tiled sweeps; block shape as in
+        Scene.set_block_shape)."""
+        buf = (ctypes.c_int * (7 * self.n))()
         n = ctypes.c_int()
         _lib.check(lib().rmt3d_batch_autotune(self._h, probe_steps, buf, self.n, ctypes.byref(n)))
-        return {buf[6 * i]: tuple(buf[6 * i + 1:6 * i + 6]) for i in range(min(n.value, self.n))}
+        return {buf[7 * i]: tuple(buf[7 * i + 1:7 * i + 7]) for i in range(min(n.value, self.n))}
 
     def set_smoother(self, mode):
         """The multigrid smoother of every scene (Scene.set_smoother)."""

@@ -10,6 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librmt3d_gpu.so")
 
 MAX_OBJ = 16
+BLOCK_SHAPES = 5  # RMT3D_BLOCK_SHAPES
 MAX_VEL_PROF = 8
 
 OK = 0
@@ -182,6 +183,7 @@ SIGNATURES = {
     "rmt3d_scene_set_mg_launch": (_I, [_P, _I]),
     "rmt3d_scene_set_smoother": (_I, [_P, _I]),
     "rmt3d_scene_set_coarse_cluster": (_I, [_P, _I]),
+    "rmt3d_scene_set_block_shape": (_I, [_P, _I]),
     "rmt3d_snapshot_fields": (_I, [_P, _IP, _I, ctypes.POINTER(_P)]),
     "rmt3d_snapshot_wait": (_I, [_P]),
     "rmt3d_scene_footprint": (ctypes.c_size_t, [ctypes.POINTER(SceneDesc)]),

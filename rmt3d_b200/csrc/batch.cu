@@ -38,7 +38,7 @@ struct rmt3d_batch {
     std::vector<int> status;
     // grid shape, periodicity, precision and density form -> (v_down, v_up,
     // cluster launch, smoother mode)
-    std::map<std::array<int, 8>, std::array<int, 5>> tuned;
+    std::map<std::array<int, 8>, std::array<int, 6>> tuned;
     int nthreads = 1;
     // equally sized scenes stepped together: one graph per group, each
     // multigrid solve batched over the group's scenes
@@ -258,9 +258,11 @@ extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
 // launch or as per-phase launches, and for the latter the smoother (one
 // launch per colour pass, or one per whole sweep on shared-memory tiles) and
 // the levels (none, up to 5000 or up to 40000 points) whose part of each
-// V-cycle runs as one cluster launch.  tuned_out (optional, 6 ints per kind:
-// cells, v_down, v_up, cluster launch, smoother, coarse cluster points)
-// receives the choices.
+// V-cycle runs as one cluster launch.  With the fastest of those, the block
+// shapes of the bulk stencil kernels are timed in turn
+// (rmt3d_scene_set_block_shape).  tuned_out (optional, 7 ints per kind:
+// cells, v_down, v_up, cluster launch, smoother, coarse cluster points,
+// block shape) receives the choices.
 extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_out, int max_out, int *n_out) {
     if (!b) return rmt3d::fail(RMT3D_ERR_INVALID, "null batch");
     if (probe_steps < 1) return rmt3d::fail(RMT3D_ERR_INVALID, "probe_steps < 1");
@@ -308,22 +310,42 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
                     bcc = ln[2];
                 }
             }
+        // block shapes of the bulk kernels under the chosen schedule (shape 0
+        // keeps the time measured above)
+        int bb = 0;
+        if (!rmt3d_scene_set_mg_launch(probe, bc) && !rmt3d_scene_set_coarse_cluster(probe, bcc) &&
+            !rmt3d_scene_set_schedule(probe, bd, bu, 0) && !rmt3d_scene_set_smoother(probe, bs))
+            for (int shape = 1; shape < RMT3D_BLOCK_SHAPES; shape++) {
+                if (rmt3d_scene_set_block_shape(probe, shape)) break;
+                int st = 0;
+                if (rmt3d_run(probe, 1, &st) || rmt3d_sync(probe) || st) continue;
+                auto t0 = std::chrono::steady_clock::now();
+                const int er = rmt3d_run(probe, probe_steps, &st);
+                const int es = rmt3d_sync(probe);
+                double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                if (er == 0 && es == 0 && st == 0 && dt < best) {
+                    best = dt;
+                    bb = shape;
+                }
+            }
         rmt3d_scene_destroy(probe);
-        b->tuned[kv.first] = {bd, bu, bc, bs, bcc};
+        b->tuned[kv.first] = {bd, bu, bc, bs, bcc, bb};
         for (size_t i = 0; i < b->descs.size(); i++)
             if (tune_key(b->descs[i]) == kv.first) {
                 if ((e = rmt3d_scene_set_schedule(b->scenes[i], bd, bu, 0))) return e;
                 if ((e = rmt3d_scene_set_mg_launch(b->scenes[i], bc))) return e;
                 if ((e = rmt3d_scene_set_smoother(b->scenes[i], bs))) return e;
                 if ((e = rmt3d_scene_set_coarse_cluster(b->scenes[i], bcc))) return e;
+                if ((e = rmt3d_scene_set_block_shape(b->scenes[i], bb))) return e;
             }
         if (tuned_out && written < max_out) {
-            tuned_out[6 * written] = (int)cells(b->descs[kv.second]);
-            tuned_out[6 * written + 1] = bd;
-            tuned_out[6 * written + 2] = bu;
-            tuned_out[6 * written + 3] = bc;
-            tuned_out[6 * written + 4] = bs;
-            tuned_out[6 * written + 5] = bcc;
+            tuned_out[7 * written] = (int)cells(b->descs[kv.second]);
+            tuned_out[7 * written + 1] = bd;
+            tuned_out[7 * written + 2] = bu;
+            tuned_out[7 * written + 3] = bc;
+            tuned_out[7 * written + 4] = bs;
+            tuned_out[7 * written + 5] = bcc;
+            tuned_out[7 * written + 6] = bb;
         }
         written++;
     }

@@ -373,9 +373,9 @@ int mg_solver::set_coarse(int pts) {
 // device, so scenes that come and go do not stall the others.
 void mg_solver::release() {
     if (!alloc_stream) return;
+    if (slab) cudaFreeAsync(slab, alloc_stream);
+    slab = nullptr;
     for (auto &l : lv) {
-        for (void *p : {(void *)l.x, (void *)l.r, (void *)l.res, (void *)l.xs, (void *)l.rs, (void *)l.ress})
-            if (p) cudaFreeAsync(p, alloc_stream);
         l.x = l.r = l.res = nullptr;
         l.xs = l.rs = l.ress = nullptr;
     }
@@ -433,7 +433,8 @@ size_t mg_solver::footprint(mg_kind k, const int n[3], const int prd[3], bool mi
     std::vector<mg_level> v;
     if (plan(k, n, prd, v)) return 0;
     size_t b = 0;
-    for (auto &l : v) b += l.npts() * (3 * sizeof(double) + (mixed_form ? 3 * sizeof(float) : 0));
+    for (auto &l : v)
+        b += 3 * slab_pad(l.npts() * sizeof(double)) + (mixed_form ? 3 * slab_pad(l.npts() * sizeof(float)) : 0);
     // the coarsest-level inverse is shared by all solvers with that level
     // (one copy per distinct level shape in the process) and not counted here
     return b + 2 * sizeof(double);
@@ -448,24 +449,31 @@ int mg_solver::setup(mg_kind k, const int n[3], const int prd[3], bool mixed_for
     int pe = plan(k, n, prd, lv);
     if (pe) return pe;
     alloc_stream = st;
+    // all levels in one allocation, level by level, each array on a 256-byte
+    // boundary: the arrays' relative placement is the same for every solver
+    // whatever the state of the memory pool
+    size_t total = 0;
+    for (auto &l : lv)
+        total += 3 * slab_pad(l.npts() * sizeof(double)) + (mixed ? 3 * slab_pad(l.npts() * sizeof(float)) : 0);
+    if (cudaMallocAsync((void **)&slab, total, st) != cudaSuccess) return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
+    bytes_alloc += total;
+    cudaMemsetAsync(slab, 0, total, st);
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        unsigned char *p = slab + off;
+        off += slab_pad(bytes);
+        return (void *)p;
+    };
     for (auto &l : lv) {
-        size_t b = l.npts() * sizeof(double);
-        if (cudaMallocAsync(&l.x, b, st) != cudaSuccess || cudaMallocAsync(&l.r, b, st) != cudaSuccess ||
-            cudaMallocAsync(&l.res, b, st) != cudaSuccess)
-            return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
-        bytes_alloc += 3 * b;
-        cudaMemsetAsync(l.x, 0, b, st);
-        cudaMemsetAsync(l.r, 0, b, st);
-        cudaMemsetAsync(l.res, 0, b, st);
+        const size_t b = l.npts() * sizeof(double);
+        l.x = (double *)carve(b);
+        l.r = (double *)carve(b);
+        l.res = (double *)carve(b);
         if (mixed) {
-            size_t bf = l.npts() * sizeof(float);
-            if (cudaMallocAsync(&l.xs, bf, st) != cudaSuccess || cudaMallocAsync(&l.rs, bf, st) != cudaSuccess ||
-                cudaMallocAsync(&l.ress, bf, st) != cudaSuccess)
-                return fail(RMT3D_ERR_OOM, "multigrid allocation failed");
-            bytes_alloc += 3 * bf;
-            cudaMemsetAsync(l.xs, 0, bf, st);
-            cudaMemsetAsync(l.rs, 0, bf, st);
-            cudaMemsetAsync(l.ress, 0, bf, st);
+            const size_t bf = l.npts() * sizeof(float);
+            l.xs = (float *)carve(bf);
+            l.rs = (float *)carve(bf);
+            l.ress = (float *)carve(bf);
         }
     }
     if (build_dense(st)) return fail(RMT3D_ERR_OOM, "coarse inverse allocation failed");

@@ -75,6 +75,9 @@ constexpr int kMgMaxCycles = 4096;  // bound on the cycles of one solve
 struct graph_builder;
 struct pmg_args;
 
+// sizes of the arrays carved out of one allocation: 256-byte multiples
+inline size_t slab_pad(size_t bytes) { return (bytes + 255) & ~(size_t)255; }
+
 class mg_solver {
   public:
     mg_kind kind;
@@ -113,6 +116,7 @@ class mg_solver {
     // device bytes setup() allocates for this hierarchy (0 if it cannot coarsen)
     static size_t footprint(mg_kind k, const int n[3], const int prd[3], bool mixed_form);
     size_t bytes_alloc = 0;  // device bytes held
+    unsigned char *slab = nullptr;  // every level's arrays, one allocation
     double *rhs() { return lv[0].r; }
     double *sol() { return lv[0].x; }
     double *dense = nullptr;  // inverse of the coarsest operator (row-major), or null

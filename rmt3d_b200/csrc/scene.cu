@@ -82,6 +82,19 @@ struct host_obj {
 
 inline dim3 blk() { return dim3(32, 4, 2); }
 inline dim3 grd(int a, int b, int c) { return dim3((a + 31) / 32, (b + 3) / 4, (c + 1) / 2); }
+// Block shapes (x, y, z) of the bulk stencil kernels of the step, 256 threads
+// each: the tile of cells a block covers, chosen per kind of scene by the
+// batch autotuner (rmt3d_scene_set_block_shape).  Shape 0 is the default.
+constexpr int kBlockShapes[][3] = {{32, 4, 2}, {32, 8, 1}, {64, 4, 1}, {32, 2, 4}, {128, 2, 1}};
+constexpr int kNumBlockShapes = (int)(sizeof(kBlockShapes) / sizeof(kBlockShapes[0]));
+static_assert(kNumBlockShapes == RMT3D_BLOCK_SHAPES, "block shape table and header disagree");
+inline dim3 blk_of(int shape) {
+    return dim3(kBlockShapes[shape][0], kBlockShapes[shape][1], kBlockShapes[shape][2]);
+}
+inline dim3 grd_of(int shape, int a, int b, int c) {
+    const dim3 t = blk_of(shape);
+    return dim3((a + t.x - 1) / t.x, (b + t.y - 1) / t.y, (c + t.z - 1) / t.z);
+}
 inline unsigned lin_blocks(int n) { return (unsigned)((n + 255) / 256); }
 
 }  // namespace
@@ -141,6 +154,7 @@ struct rmt3d_scene {
     // velocity edge states through TMA-staged tiles (k_edge_vel_tma): the
     // tensor maps of vel[0..2], made when the rows are 16-byte aligned
     bool edge_tma = false;
+    int bshape = 0;  // block shape of the bulk stencil kernels (kBlockShapes)
     CUtensorMap tm_vel[3];
     int *mlist = nullptr, *mcnt = nullptr;  // cells holding a map, for the stress kernel
     // passive tracers (dump_code bit 1 and ntracers > 0, fluid_3d.cc:217-219)
@@ -172,6 +186,34 @@ struct rmt3d_scene {
     // dimensions; the FEM levels' cells are the same), FP64 and FP32
     std::vector<double *> rinv;
     std::vector<float *> rinvs;
+
+    // The per-cell arrays in one allocation: plan() records each array in
+    // order, commit_slab() allocates their total and carves them at 256-byte
+    // boundaries.  One pool request instead of about a hundred, and the
+    // arrays' relative placement is the same for every scene whatever the
+    // state of the memory pool.
+    std::vector<std::pair<void **, size_t>> slab_req;
+    template <typename T>
+    int plan(T **p, size_t n) {
+        slab_req.push_back({(void **)p, slab_pad(n * sizeof(T))});
+        return 0;
+    }
+    int commit_slab() {
+        size_t total = 0;
+        for (auto &r : slab_req) total += r.second;
+        unsigned char *b = nullptr;
+        if (cudaMallocAsync((void **)&b, total, st) != cudaSuccess) return fail(RMT3D_ERR_OOM, "device allocation failed");
+        allocs.push_back(b);
+        dev_bytes += total;
+        cudaMemsetAsync(b, 0, total, st);
+        size_t off = 0;
+        for (auto &r : slab_req) {
+            *r.first = b + off;
+            off += r.second;
+        }
+        slab_req.clear();
+        return 0;
+    }
 
     // stream-ordered allocation from the device's memory pool (no device-wide
     // synchronisation when scenes are created or destroyed)
@@ -777,7 +819,7 @@ static void compute_stress(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     const bool maps = g.n_obj > 0;
     if (maps) cudaMemsetAsync(s->mcnt, 0, sizeof(int), s->st);
-    k_stress_fluid<<<grd(g.sm + 4, g.sn + 4, g.so + 4), blk(), 0, s->st>>>(g, s->dF, maps ? s->mlist : nullptr,
+    k_stress_fluid<<<grd_of(s->bshape, g.sm + 4, g.sn + 4, g.so + 4), blk_of(s->bshape), 0, s->st>>>(g, s->dF, maps ? s->mlist : nullptr,
                                                                           s->mcnt);
     s->count();
     if (maps) {
@@ -813,14 +855,14 @@ static void ph_edges(rmt3d_scene *s) {
         launch_edge_vel_tma(g, s->dF, s->tm_vel, s->lx, s->ly, s->lz, s->dt, &s->ctl->time, s->d.var_den,
                             s->counters + 7, s->st);
     else if (g.f32face)
-        k_edge_vel<float><<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
+        k_edge_vel<float><<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
                                                                        &s->ctl->time, s->d.var_den);
     else
-        k_edge_vel<double><<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
+        k_edge_vel<double><<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
                                                                         &s->ctl->time, s->d.var_den);
     s->count();
     if (g.n_obj > 0) {
-        k_edge_refmap<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->counters + 5);
+        k_edge_refmap<<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, s->dt, s->counters + 5);
         s->count();
     }
     advance_half(s);
@@ -831,8 +873,8 @@ static void ph_upwind(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     fill_boundary_cf(s);
     comm_face_maps(s);
-    if (g.f32face) k_upwind<float><<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
-    else k_upwind<double><<<grd(g.sm + 1, g.sn + 1, g.so + 1), blk(), 0, s->st>>>(g, s->dF);
+    if (g.f32face) k_upwind<float><<<grd_of(s->bshape, g.sm + 1, g.sn + 1, g.so + 1), blk_of(s->bshape), 0, s->st>>>(g, s->dF);
+    else k_upwind<double><<<grd_of(s->bshape, g.sm + 1, g.sn + 1, g.so + 1), blk_of(s->bshape), 0, s->st>>>(g, s->dF);
     s->count();
     fill_boundary_cf(s);
 }
@@ -844,7 +886,7 @@ static void ph_upwind(rmt3d_scene *s) {
 static void ph_mac_pre(rmt3d_scene *s, double cdt) {
     const grid_dev &g = s->g;
     update_rinv(s);
-    k_mac_rhs<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.rhs(), cdt);
+    k_mac_rhs<<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, s->mac.rhs(), cdt);
     s->count();
 }
 
@@ -853,7 +895,7 @@ static void ph_mac_post(rmt3d_scene *s, double cdt) {
     k_mac_extract<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->mac.sol());
     s->count();
     comm_pressure(s);
-    k_sub_qgrad<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, cdt, s->d.var_den);
+    k_sub_qgrad<<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, cdt, s->d.var_den);
     s->count();
     fill_boundary_cf(s);
 }
@@ -865,7 +907,7 @@ static void ph_refmap(rmt3d_scene *s, double cdt) {
     // without a periodic axis nothing changes the codes between the snapshot
     // and the extrapolation, so the snapshot pass sets the layer tags too
     const bool prd = g.prd[0] || g.prd[1] || g.prd[2];
-    k_refmap_predict<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, cdt);
+    k_refmap_predict<<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, cdt);
     k_snapshot_reset<<<lin_blocks(g.ncell), 256, 0, s->st>>>(g, s->dF, prd ? nullptr : s->lay, s->inl);
     s->count(2);
     comm_primary(s);
@@ -884,10 +926,10 @@ static void ph_revert(rmt3d_scene *s) {
 static void ph_ustar(rmt3d_scene *s) {
     const grid_dev &g = s->g;
     if (g.f32face)
-        k_ustar<float><<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
+        k_ustar<float><<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
                                                                     &s->ctl->time, s->d.var_den);
     else
-        k_ustar<double><<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
+        k_ustar<double><<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, s->lx, s->ly, s->lz, s->dt,
                                                                      &s->ctl->time, s->d.var_den);
     s->count();
     fill_boundary_cc(s);
@@ -937,7 +979,7 @@ static void ph_pp_pre(rmt3d_scene *s) {
     // the density is already that of the current maps: update_rho ran after
     // the reference-map update, and nothing since has moved a map
     update_rinv(s);
-    k_fem_rhs<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
+    k_fem_rhs<<<grd_of(s->bshape, g.fm, g.fn, g.fo), blk_of(s->bshape), 0, s->st>>>(g, s->dF, s->fem.rhs(), s->gradphi);
     s->count();
 }
 
@@ -948,7 +990,7 @@ static void ph_pp_post(rmt3d_scene *s) {
     k_fem_extract<<<grd(g.fm, g.fn, g.fo), blk(), 0, s->st>>>(g, s->dF, s->fem.sol(), s->d_mean);
     s->count(2);
     comm_pressure(s);
-    k_sub_pgrad<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->dt, s->d.var_den);
+    k_sub_pgrad<<<grd_of(s->bshape, g.sm, g.sn, g.so), blk_of(s->bshape), 0, s->st>>>(g, s->dF, s->dt, s->d.var_den);
     s->count();
 }
 
@@ -1883,28 +1925,31 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     int e = 0;
     fields_dev &F = s->hF;
     memset(&F, 0, sizeof(F));
-    for (int c = 0; c < 3 && !e; c++) e |= s->alloc(&F.vel[c], n) | s->alloc(&F.dvel[c], n);
-    e |= s->alloc(&F.p, n) | s->alloc(&F.dp, n) | s->alloc(&F.q, n);
-    for (int c = 0; c < 18 && !e; c++) e |= g.f32face ? s->alloc(&F.fvel32[c], n) : s->alloc(&F.fvel[c], n);
-    for (int c = 0; c < 9 && !e; c++) e |= s->alloc(&F.sigma[c], n);
-    if (d.var_den) e |= s->alloc(&F.rho, n);
-    for (int o = 0; o < d.n_obj && !e; o++) {
+    for (int c = 0; c < 3; c++) s->plan(&F.vel[c], n), s->plan(&F.dvel[c], n);
+    s->plan(&F.p, n), s->plan(&F.dp, n), s->plan(&F.q, n);
+    for (int c = 0; c < 18; c++) g.f32face ? s->plan(&F.fvel32[c], n) : s->plan(&F.fvel[c], n);
+    for (int c = 0; c < 9; c++) s->plan(&F.sigma[c], n);
+    if (d.var_den) s->plan(&F.rho, n);
+    for (int o = 0; o < d.n_obj; o++) {
         objmap_dev &m = F.om[o];
-        e |= s->alloc(&m.code, n) | s->alloc(&m.code_prev, n);
-        for (int c = 0; c < 3; c++) e |= s->alloc(&m.x[c], n) | s->alloc(&m.xp[c], n) | s->alloc(&m.x_prev[c], n) | s->alloc(&m.det[c], n) |
-                                         s->alloc(&m.el[c], n);
-        for (int c = 0; c < 18; c++) e |= s->alloc(&m.fx[c], n);
-        for (int c = 0; c < 9; c++) e |= s->alloc(&m.gp[c], n) | s->alloc(&m.gp_prev[c], n);
-        cudaMemsetAsync(m.code, 0xff, n * sizeof(int), s->st);
-        cudaMemsetAsync(m.code_prev, 0xff, n * sizeof(int), s->st);
+        s->plan(&m.code, n), s->plan(&m.code_prev, n);
+        for (int c = 0; c < 3; c++)
+            s->plan(&m.x[c], n), s->plan(&m.xp[c], n), s->plan(&m.x_prev[c], n), s->plan(&m.det[c], n), s->plan(&m.el[c], n);
+        for (int c = 0; c < 18; c++) s->plan(&m.fx[c], n);
+        for (int c = 0; c < 9; c++) s->plan(&m.gp[c], n), s->plan(&m.gp_prev[c], n);
+    }
+    if (d.n_obj > 0) {
+        const size_t no = (size_t)d.n_obj * n;
+        s->plan(&s->lay, no), s->plan(&s->inl, no), s->plan(&s->front[0], no), s->plan(&s->front[1], no);
+        s->plan(&s->fcnt, 2 * kMaxObj), s->plan(&s->mlist, n), s->plan(&s->mcnt, 1);
+    }
+    e |= s->commit_slab();
+    for (int o = 0; o < d.n_obj && !e; o++) {
+        cudaMemsetAsync(F.om[o].code, 0xff, n * sizeof(int), s->st);
+        cudaMemsetAsync(F.om[o].code_prev, 0xff, n * sizeof(int), s->st);
     }
     e |= s->alloc(&s->lx, g.sm4) | s->alloc(&s->ly, g.sn4) | s->alloc(&s->lz, g.so4);
     e |= s->alloc(&s->dF, 1);
-    if (d.n_obj > 0) {
-        const size_t no = (size_t)d.n_obj * n;
-        e |= s->alloc(&s->lay, no) | s->alloc(&s->inl, no) | s->alloc(&s->front[0], no) | s->alloc(&s->front[1], no) |
-             s->alloc(&s->fcnt, 2 * kMaxObj) | s->alloc(&s->mlist, n) | s->alloc(&s->mcnt, 1);
-    }
     if ((d.run.dump_code & 1) && d.run.ntracers > 0) {
         s->ntr = d.run.ntracers;
         e |= s->alloc(&s->tr_pc, 3 * (size_t)s->ntr) | s->alloc(&s->tr_rp, 6 * (size_t)s->ntr) |
@@ -2839,6 +2884,14 @@ extern "C" int rmt3d_scene_set_coarse_cluster(rmt3d_scene *s, int pts) {
     return RMT3D_OK;
 }
 
+extern "C" int rmt3d_scene_set_block_shape(rmt3d_scene *s, int shape) {
+    if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
+    if (shape < 0 || shape >= kNumBlockShapes) return fail(RMT3D_ERR_INVALID, "block shape index out of range");
+    s->bshape = shape;
+    mark_dirty(s);
+    return RMT3D_OK;
+}
+
 extern "C" int rmt3d_scene_set_smoother(rmt3d_scene *s, int mode) {
     if (!s) return fail(RMT3D_ERR_INVALID, "null scene");
     if (mode < 0 || mode > 1) return fail(RMT3D_ERR_INVALID, "smoother mode must be 0 (colour passes) or 1 (tiled sweeps)");
@@ -2853,11 +2906,15 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
     // mirrors the allocations of rmt3d_scene_create and mg_solver::setup
     if (!d || d->sys_size[0] < 1 || d->sys_size[1] < 1 || d->sys_size[2] < 1) return 0;
     const size_t n = (size_t)(d->sys_size[0] + 4) * (d->sys_size[1] + 4) * (d->sys_size[2] + 4);
-    size_t b = n * sizeof(double) * (18 + (d->var_den ? 1 : 0)) + n * 18 * (face32(*d) ? sizeof(float) : sizeof(double));
-    b += (size_t)d->n_obj * n * (2 * sizeof(int) + 51 * sizeof(double));
-    if (d->n_obj > 0)
-        b += (size_t)d->n_obj * n * (sizeof(uint8_t) + 3 * sizeof(int)) + 2 * kMaxObj * sizeof(int) +
-             n * sizeof(int) + sizeof(int);
+    // the per-cell slab (commit_slab): arrays at 256-byte boundaries
+    size_t b = slab_pad(n * sizeof(double)) * (18 + (d->var_den ? 1 : 0)) +
+               18 * slab_pad(n * (face32(*d) ? sizeof(float) : sizeof(double)));
+    b += (size_t)d->n_obj * (2 * slab_pad(n * sizeof(int)) + 51 * slab_pad(n * sizeof(double)));
+    if (d->n_obj > 0) {
+        const size_t no = (size_t)d->n_obj * n;
+        b += slab_pad(no * sizeof(uint8_t)) + 3 * slab_pad(no * sizeof(int)) + slab_pad(2 * kMaxObj * sizeof(int)) +
+             slab_pad(n * sizeof(int)) + slab_pad(sizeof(int));
+    }
     if ((d->run.dump_code & 1) && d->run.ntracers > 0)
         b += (size_t)d->run.ntracers * (3 * sizeof(int) + 6 * sizeof(double) + sizeof(uint8_t));
     b += (size_t)(d->sys_size[0] + 4 + d->sys_size[1] + 4 + d->sys_size[2] + 4) * sizeof(double);

@@ -97,9 +97,10 @@ def test_autotune_choices_and_results(tmp_path):
         tuned = b.autotune(probe_steps=2)
         sizes = sorted({d.sys_size[0] * d.sys_size[1] * d.sys_size[2] for d in descs})
         assert sorted(tuned) == sizes
-        for vd, vu, cl, sm, cc in tuned.values():
+        for vd, vu, cl, sm, cc, bs in tuned.values():
             assert (vd, vu) in [(2, 2), (1, 1), (1, 2), (2, 1), (3, 3)]
             assert cl in (0, 1) and sm in (0, 1) and cc in (0, 5000, 40000)
+            assert 0 <= bs < R._lib.BLOCK_SHAPES
         assert b.step(3) == [R.NORMAL_EXIT] * len(descs)
         # another smoothing schedule converges to the same tolerance: the
         # fields agree with the default schedule at the solver's tolerance
