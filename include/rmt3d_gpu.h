@@ -49,6 +49,14 @@ extern "C" {
 /* arithmetic forms */
 #define RMT3D_FP64 0   /* plain form: FP64 throughout */
 #define RMT3D_MIXED 1  /* FP32 multigrid V-cycles inside FP64 iterative refinement */
+/* RMT3D_MIXED plus the advection stencil in FP32: FP32 velocity face states,
+ * FP32 limited slopes, half-step extrapolation, upwinding and advective
+ * increment added to the FP64 velocity.  2-3% faster per single-scene step
+ * at 64^3-128^3; its perturbations are larger, and over the 64 seeded scenes
+ * of the batched workload after 100 steps one scene's error against FP64
+ * rose from 3.4e-7 (RMT3D_MIXED) to 9.3e-6 (a discrete change of the flow
+ * there), against a budget of 1e-5.  No counterpart in the reference. */
+#define RMT3D_MIXED_BULK32 2
 
 /* One object: Sim/sim_params.cc:248-288 (basic_specs, extra_specs, srho,
  * shear_mod, object_list). */
@@ -106,7 +114,7 @@ typedef struct {
     double wt_n, ex_visc_mult, ev_trans_mult, sdt_pad, dt_ex_pad, weight_fac, gravity;
     rmt3d_object_desc obj[RMT3D_MAX_OBJ];
     int var_den;   /* compile-time VAR_DEN in the reference (Execs/Makefile:37-42) */
-    int precision; /* RMT3D_FP64 or RMT3D_MIXED */
+    int precision; /* RMT3D_FP64, RMT3D_MIXED or RMT3D_MIXED_BULK32 */
     int mg_exact;  /* 0: the reference's V-cycle control (residual tolerance of
                       mg_probs.hh:483-518); 1: additionally iterate every
                       Poisson solve until its residual stops shrinking, so

@@ -18,7 +18,7 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import FP64, MIXED, PROJECTION_ERR, REFMAP_UPDATE_ERR, STEADY_SOLN_EXIT  # noqa: F401
+from ._lib import FP64, MIXED, MIXED_BULK32, PROJECTION_ERR, REFMAP_UPDATE_ERR, STEADY_SOLN_EXIT  # noqa: F401
 from ._lib import OK as NORMAL_EXIT
 from ._lib import RMT3DError, SceneDesc
 
@@ -283,7 +283,7 @@ class Scene:
         """Start copying the named fields to host buffers (objects with
         data_ptr(), e.g. pinned torch tensors of ncell doubles) without
         waiting; snapshot_wait() returns once they are in host memory."""
-        which = (ctypes.c_int * len(names))(*[FIELD_INDEX[n] for n in names])
+        which = (ctypes.c_int * len(names))(*[FIELD_INDEX[n] if isinstance(n, str) else int(n) for n in names])
         dst = (ctypes.c_void_p * len(names))(*[b.data_ptr() for b in host_bufs])
         _lib.check(lib().rmt3d_snapshot_fields(self._h, which, len(names), dst))
 

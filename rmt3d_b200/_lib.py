@@ -28,7 +28,7 @@ ERR_TOO_LARGE = -8
 
 SIM_FTEST, SIM_STEST, SIM_OBJECTS = 0, 1, 2
 OBJ_BASIC_SPHERE, OBJ_SPHERE = 0, 1
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_BULK32 = 0, 1, 2
 
 
 class ObjectDesc(ctypes.Structure):

@@ -287,7 +287,8 @@ extern "C" int rmt3d_desc_from_cfg(const char *path, rmt3d_scene_desc *d) {
             // extension keyword: selects the reference's VAR_DEN build semantics
             d->var_den = t.next_int();
         } else if (k == "precision") {
-            // extension keyword: 0 FP64, 1 FP32 V-cycles inside FP64 refinement
+            // extension keyword: 0 FP64, 1 FP32 V-cycles inside FP64 refinement,
+            // 2 that and the advection stencil in FP32
             d->precision = t.next_int();
         } else if (k == "mixed_rtol") {
             // extension keyword: relative solve tolerance of the mixed form

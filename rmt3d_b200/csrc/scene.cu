@@ -257,13 +257,10 @@ static cudaError_t copy_sync(rmt3d_scene *s, void *dst, const void *src, size_t 
 // The velocity face states are FP32 in the mixed form (g.f32face): zeroed,
 // read and written from the host through these, widened to and narrowed from
 // FP64 on the host side.
-// The mixed form keeps the face states in FP32 unless the environment sets
-// RMT3D_FACE32=0 (a measurement switch; the plain form is always FP64).
-static bool face32(const rmt3d_scene_desc &d) {
-    if (d.precision != RMT3D_MIXED) return false;
-    const char *e = getenv("RMT3D_FACE32");
-    return !(e && e[0] == '0');
-}
+// FP32 face states and advection arithmetic: the RMT3D_MIXED_BULK32 form
+static bool face32(const rmt3d_scene_desc &d) { return d.precision == RMT3D_MIXED_BULK32; }
+// FP32 V-cycles inside FP64 refinement: both mixed forms
+static bool mixed_form(int precision) { return precision == RMT3D_MIXED || precision == RMT3D_MIXED_BULK32; }
 
 static cudaError_t zero_faces(rmt3d_scene *s) {
     const size_t n = s->g.ncell;
@@ -782,7 +779,7 @@ __global__ void k_rinv_coarse(int f0, int f1, int c0, int c1, int c2, const doub
 static void update_rinv(rmt3d_scene *s) {
     if (!s->d.var_den) return;
     const grid_dev &g = s->g;
-    const bool f32 = s->d.precision == RMT3D_MIXED;
+    const bool f32 = mixed_form(s->d.precision);
     k_rinv_fine<<<grd(g.sm, g.sn, g.so), blk(), 0, s->st>>>(g, s->dF, s->rinv[0], f32 ? s->rinvs[0] : nullptr);
     s->count();
     for (size_t l = 1; l < s->rinv.size(); l++) {
@@ -1741,6 +1738,8 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
         if (d.obj[o].type != RMT3D_OBJ_BASIC_SPHERE && d.obj[o].type != RMT3D_OBJ_SPHERE)
             return fail(RMT3D_ERR_UNSUPPORTED, "object type " + std::to_string(d.obj[o].type) + " is outside this path");
     if (d.nlayers < 1 || d.nlayers > 60) return fail(RMT3D_ERR_INVALID, "nlayers outside 1..60");
+    if (d.precision < RMT3D_FP64 || d.precision > RMT3D_MIXED_BULK32)
+        return fail(RMT3D_ERR_INVALID, "precision must be RMT3D_FP64, RMT3D_MIXED or RMT3D_MIXED_BULK32");
 
     rmt3d_scene *s = new rmt3d_scene();
     s->d = d;
@@ -2010,7 +2009,7 @@ extern "C" int rmt3d_scene_create(const rmt3d_scene_desc *desc, void *stream, rm
     s->mac.prof = &s->prof;
     s->fem.prof = &s->prof;
     int nm[3] = {g.sm, g.sn, g.so}, nf[3] = {g.fm, g.fn, g.fo};
-    bool mixed = d.precision == RMT3D_MIXED;
+    bool mixed = mixed_form(d.precision);
     s->mac.exact = s->fem.exact = d.mg_exact != 0;
     s->mac.rtol = s->fem.rtol = (mixed && d.mixed_rtol > 0) ? d.mixed_rtol : 0;
     s->mac.vd = s->fem.vd = d.var_den != 0;
@@ -2926,7 +2925,7 @@ extern "C" size_t rmt3d_scene_footprint(const rmt3d_scene_desc *d) {
         nm[a] = d->sys_size[a];
         nf[a] = d->sys_size[a] + (prd[a] ? 0 : 1);
     }
-    const bool mixed = d->precision == RMT3D_MIXED;
+    const bool mixed = mixed_form(d->precision);
     const size_t mac = mg_solver::footprint(MG_MAC, nm, prd, mixed), fem = mg_solver::footprint(MG_FEM, nf, prd, mixed);
     if (!mac || !fem) return 0;
     if (d->var_den) {

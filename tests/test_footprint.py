@@ -5,8 +5,6 @@ multigrid set-up; the GPU tests check it equals what a scene holds.  Here:
 the per-cell arithmetic and the multigrid hierarchy terms for the grids of
 the synthetic workloads.
 """
-import os
-
 import rmt3d_b200 as R
 from rmt3d_b200 import scenes
 
@@ -38,15 +36,12 @@ def test_objects_precision_and_size_order(tmp_path):
                                                     pad(4))
     mixed = _desc(tmp_path, scenes.cavity_sphere(64), "m64.cfg")
     mixed.precision = R.MIXED
-    # the mixed form adds FP32 copies of the multigrid hierarchies and keeps
-    # its 18 face-state arrays in FP32 (RMT3D_FACE32=0 keeps them FP64)
-    os.environ["RMT3D_FACE32"] = "0"
-    try:
-        mixed_f64_faces = R.footprint(mixed)
-    finally:
-        del os.environ["RMT3D_FACE32"]
-    assert mixed_f64_faces > R.footprint(sph)
-    assert mixed_f64_faces - R.footprint(mixed) == 18 * n * 4
+    # the mixed form adds FP32 copies of the multigrid hierarchies; its FP32
+    # advection form keeps the 18 face-state arrays in FP32
+    assert R.footprint(mixed) > R.footprint(sph)
+    bulk = _desc(tmp_path, scenes.cavity_sphere(64), "b64.cfg")
+    bulk.precision = R.MIXED_BULK32
+    assert R.footprint(mixed) - R.footprint(bulk) == 18 * n * 4
     sizes = [R.footprint(_desc(tmp_path, scenes.cavity(k), "k%d.cfg" % k)) for k in (32, 48, 64, 96, 128)]
     assert sizes == sorted(sizes)
 

@@ -113,15 +113,17 @@ def test_cluster_solve_matches_phase_launches(tmp_path, kind):
         assert e < 1e-10, (f, e)
 
 
-def test_mixed_form_accuracy(tmp_path):
-    """The mixed form (FP32 V-cycles inside FP64 refinement, solves ended at
-    mixed_rtol x max|rhs|) stays within its 1e-5 rel-L2 budget against the FP64
-    form over 60 steps of a 32^3 cavity with a sphere.  Velocity is measured
-    against the norm of the whole velocity field (v alone is a near-zero
-    cross-flow whose own norm magnifies round-off), pressure against its own."""
+@pytest.mark.parametrize("form", [R.MIXED, R.MIXED_BULK32])
+def test_mixed_form_accuracy(tmp_path, form):
+    """The mixed forms (FP32 V-cycles inside FP64 refinement, solves ended at
+    mixed_rtol x max|rhs|; the second also with the advection stencil in FP32)
+    stay within their 1e-5 rel-L2 budget against the FP64 form over 60 steps
+    of a 32^3 cavity with a sphere.  Velocity is measured against the norm of
+    the whole velocity field (v alone is a near-zero cross-flow whose own norm
+    magnifies round-off), pressure against its own."""
     path = scenes.write(str(tmp_path / "m.cfg"), scenes.cavity_sphere(32, steps=60, radius=0.25))
     out = {}
-    for prec in (R.FP64, R.MIXED):
+    for prec in (R.FP64, form):
         sc = R.Scene.from_cfg(path, precision=prec)
         try:
             sc.prepare()
@@ -129,12 +131,38 @@ def test_mixed_form_accuracy(tmp_path):
             out[prec] = ({f: sc.field(f)[H.INTERIOR] for f in ("u", "v", "w", "p")}, sc.scalar(7) + sc.scalar(8))
         finally:
             sc.close()
-    a, b = out[R.FP64][0], out[R.MIXED][0]
+    a, b = out[R.FP64][0], out[form][0]
     va, vb = np.stack([a[f] for f in "uvw"]), np.stack([b[f] for f in "uvw"])
     assert np.linalg.norm(vb - va) / np.linalg.norm(va) < 1e-5
     assert H.rel_l2(b["p"], a["p"]) < 1e-5
     # the relaxed solves need fewer V-cycles
-    assert out[R.MIXED][1] < out[R.FP64][1]
+    assert out[form][1] < out[R.FP64][1]
+
+
+def test_fp32_face_states_read_back(tmp_path):
+    """The FP32 advection form keeps the face states in FP32 on the device;
+    reading them widens them to FP64 (the values the step computed, finite,
+    close to the FP64 form's), and a snapshot, which copies FP64 arrays,
+    refuses them."""
+    path = scenes.write(str(tmp_path / "f.cfg"), scenes.cavity_sphere(24, steps=4, radius=0.25))
+    faces = {}
+    for prec in (R.FP64, R.MIXED_BULK32):
+        sc = R.Scene.from_cfg(path, precision=prec)
+        try:
+            sc.prepare()
+            assert sc.run(2) == R.NORMAL_EXIT
+            faces[prec] = np.stack([sc.field(9 + a) for a in range(18)])
+            if prec == R.MIXED_BULK32:
+                import torch
+                buf = torch.empty((sc.so4, sc.sn4, sc.sm4), dtype=torch.float64, pin_memory=True)
+                with pytest.raises(R.RMT3DError):
+                    sc.snapshot((9,), [buf])
+        finally:
+            sc.close()
+    f64, f32 = faces[R.FP64], faces[R.MIXED_BULK32]
+    assert np.all(np.isfinite(f32))
+    assert np.array_equal(f32, f32.astype(np.float32).astype(np.float64))
+    assert np.linalg.norm(f32 - f64) / np.linalg.norm(f64) < 1e-4
 
 
 def test_graph_rebuilt_after_dt_change(tmp_path):
