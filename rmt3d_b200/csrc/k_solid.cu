@@ -221,6 +221,7 @@ __global__ void k_lay_push(grid_dev g, const int *front, const int *cnt, int fro
     }
     int total = 0;
     for (int o = 0; o < g.n_obj; o++) total += cnt[o];
+    if (blockIdx.x * blockDim.x >= total) return;  // no frontier entry in any round
     for (int t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < total; t0 += gridDim.x * blockDim.x) {
         int t = t0, o;
         if (!front_entry(g.n_obj, cnt, t, o)) break;
@@ -406,14 +407,18 @@ __global__ void k_extrap_layer(grid_dev g, const fields_dev *__restrict__ F, con
                                int max_rs, double wt, const double *lx, const double *ly, const double *lz,
                                int *err) {
     __shared__ double wpow[kPowTab];
+    int total = 0;
+    for (int o = 0; o < g.n_obj; o++) total += cnt[o];
+    // the grid is sized for the largest frontiers: a block whose first lane
+    // group is past this layer's frontier has no cell in any round and leaves
+    // before building its weight table (the whole block, so no barrier waits)
+    if (blockIdx.x * (blockDim.x / LANES) >= total) return;
     const int npow = 3 * max_rs + 1;
     for (int q = threadIdx.x; q < kPowTab && q < npow; q += blockDim.x) wpow[q] = pow(wt, (double)q);
     __syncthreads();
     const int lane = threadIdx.x & (LANES - 1);
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / LANES;
     const int nwarps = (gridDim.x * blockDim.x) / LANES;
-    int total = 0;
-    for (int o = 0; o < g.n_obj; o++) total += cnt[o];
     for (int t0 = warp; t0 < total; t0 += nwarps) {
         int t = t0, o;
         if (!front_entry(g.n_obj, cnt, t, o)) break;
