@@ -251,15 +251,16 @@ extern "C" int rmt3d_batch_scene(rmt3d_batch *b, int i, rmt3d_scene **out) {
 
 // Autotune the multigrid schedule per kind of scene (grid shape,
 // periodicity, precision and density form, the keys build_groups groups by):
-// a probe copy of the first scene of each kind is set up and stepped
-// `probe_steps` times per candidate and the fastest candidate that ran
-// without error is applied to every scene of that kind.  The candidates are
+// a probe copy of the first scene of each kind is set up, every candidate is
+// stepped `probe_steps` times in each of three rounds, and the candidate with
+// the least total time that ran without error is applied to every scene of
+// that kind.  The candidates are
 // the smoothing counts (v_down, v_up), each solve as one thread-block-cluster
 // launch or as per-phase launches, and for the latter the smoother (one
 // launch per colour pass, or one per whole sweep on shared-memory tiles) and
 // the levels (none, up to 5000 or up to 40000 points) whose part of each
 // V-cycle runs as one cluster launch.  With the fastest of those, the block
-// shapes of the bulk stencil kernels are timed in turn
+// shapes of the bulk stencil kernels are timed the same way
 // (rmt3d_scene_set_block_shape).  tuned_out (optional, 7 ints per kind:
 // cells, v_down, v_up, cluster launch, smoother, coarse cluster points,
 // block shape) receives the choices.
@@ -283,51 +284,69 @@ extern "C" int rmt3d_batch_autotune(rmt3d_batch *b, int probe_steps, int *tuned_
             rmt3d_scene_destroy(probe);
             return e;
         }
-        double best = 1e300;
-        int bd = 2, bu = 2, bc = 0, bs = 0, bcc = 0;
+        // The probe steps on through the search, and a flow's steps get
+        // cheaper as it settles, so candidates are timed in rounds: every
+        // round times each candidate still in the race for probe_steps steps,
+        // in alternating order (forward, backward, forward), and a candidate's
+        // time is its sum over the rounds.  After the first round candidates
+        // slower than 1.5x the fastest leave the race.
+        struct cand {
+            int vd, vu, cl, sm, cc, bs;
+            double t;
+            bool ok;
+        };
+        auto race = [&](std::vector<cand> &cs) {
+            for (int round = 0; round < 3; round++) {
+                for (size_t q = 0; q < cs.size(); q++) {
+                    cand &c = cs[round % 2 ? cs.size() - 1 - q : q];
+                    if (!c.ok) continue;
+                    if (rmt3d_scene_set_mg_launch(probe, c.cl) || rmt3d_scene_set_coarse_cluster(probe, c.cc) ||
+                        rmt3d_scene_set_schedule(probe, c.vd, c.vu, 0) || rmt3d_scene_set_smoother(probe, c.sm) ||
+                        rmt3d_scene_set_block_shape(probe, c.bs)) {
+                        c.ok = false;  // e.g. clusters unavailable on this device
+                        continue;
+                    }
+                    int st = 0;
+                    // settle the cycle predictor, build the graph
+                    if (rmt3d_run(probe, 1, &st) || rmt3d_sync(probe) || st) {
+                        c.ok = false;
+                        continue;
+                    }
+                    auto t0 = std::chrono::steady_clock::now();
+                    const int er = rmt3d_run(probe, probe_steps, &st);
+                    const int es = rmt3d_sync(probe);
+                    if (er || es || st) {
+                        c.ok = false;
+                        continue;
+                    }
+                    c.t += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                }
+                if (round == 0) {
+                    double tmin = 1e300;
+                    for (auto &c : cs)
+                        if (c.ok) tmin = std::min(tmin, c.t);
+                    for (auto &c : cs)
+                        if (c.ok && c.t > 1.5 * tmin) c.ok = false;
+                }
+            }
+            int bi = -1;
+            for (size_t q = 0; q < cs.size(); q++)
+                if (cs[q].ok && (bi < 0 || cs[q].t < cs[bi].t)) bi = (int)q;
+            return bi;
+        };
+        std::vector<cand> cs;
         for (auto &ln : launch)
-            for (auto &c : smooth) {
-                if (rmt3d_scene_set_mg_launch(probe, ln[0])) continue;  // clusters unavailable
-                if (rmt3d_scene_set_coarse_cluster(probe, ln[2])) continue;  // clusters unavailable
-                if ((e = rmt3d_scene_set_schedule(probe, c[0], c[1], 0)) ||
-                    (e = rmt3d_scene_set_smoother(probe, ln[1]))) {
-                    rmt3d_scene_destroy(probe);
-                    return e;
-                }
-                int st = 0;
-                // settle the cycle predictor, build the graph
-                if (rmt3d_run(probe, 1, &st) || rmt3d_sync(probe) || st) continue;
-                auto t0 = std::chrono::steady_clock::now();
-                const int er = rmt3d_run(probe, probe_steps, &st);
-                const int es = rmt3d_sync(probe);
-                double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-                if (er == 0 && es == 0 && st == 0 && dt < best) {
-                    best = dt;
-                    bd = c[0];
-                    bu = c[1];
-                    bc = ln[0];
-                    bs = ln[1];
-                    bcc = ln[2];
-                }
-            }
-        // block shapes of the bulk kernels under the chosen schedule (shape 0
-        // keeps the time measured above)
-        int bb = 0;
-        if (!rmt3d_scene_set_mg_launch(probe, bc) && !rmt3d_scene_set_coarse_cluster(probe, bcc) &&
-            !rmt3d_scene_set_schedule(probe, bd, bu, 0) && !rmt3d_scene_set_smoother(probe, bs))
-            for (int shape = 1; shape < RMT3D_BLOCK_SHAPES; shape++) {
-                if (rmt3d_scene_set_block_shape(probe, shape)) break;
-                int st = 0;
-                if (rmt3d_run(probe, 1, &st) || rmt3d_sync(probe) || st) continue;
-                auto t0 = std::chrono::steady_clock::now();
-                const int er = rmt3d_run(probe, probe_steps, &st);
-                const int es = rmt3d_sync(probe);
-                double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-                if (er == 0 && es == 0 && st == 0 && dt < best) {
-                    best = dt;
-                    bb = shape;
-                }
-            }
+            for (auto &c : smooth) cs.push_back({c[0], c[1], ln[0], ln[1], ln[2], 0, 0.0, true});
+        int bi = race(cs);
+        int bd = 2, bu = 2, bc = 0, bs = 0, bcc = 0, bb = 0;
+        if (bi >= 0) {
+            bd = cs[bi].vd, bu = cs[bi].vu, bc = cs[bi].cl, bs = cs[bi].sm, bcc = cs[bi].cc;
+            // then the block shapes of the bulk kernels under that schedule
+            std::vector<cand> shapes;
+            for (int shape = 0; shape < RMT3D_BLOCK_SHAPES; shape++) shapes.push_back({bd, bu, bc, bs, bcc, shape, 0.0, true});
+            const int si = race(shapes);
+            if (si >= 0) bb = shapes[si].bs;
+        }
         rmt3d_scene_destroy(probe);
         b->tuned[kv.first] = {bd, bu, bc, bs, bcc, bb};
         for (size_t i = 0; i < b->descs.size(); i++)
