@@ -43,7 +43,7 @@ struct grid_dev {
     int n_obj;
     int sim_type;
     int has_exact;
-    int f32face;          // face states stored in FP32 (the mixed form), else FP64
+    int f32face;          // face states stored in FP32 (RMT3D_MIXED_BULK32), else FP64
     double gravity;
     double K_stiff, wall_dist, winv, min_wall_acc, wall_acc_mult;
     int walls[6];
@@ -76,7 +76,7 @@ __device__ inline double mono_diff(double u0, double u1, double u2, double u3, d
     return rsign(cen) * rmin(dlim, fabs(4.0 / 3.0 * cen - neigh_delf));
 }
 
-// The same slope in FP32 (the mixed form's advection stencil), written on the
+// The same slope in FP32 (the FP32-advection form's stencil), written on the
 // successive differences d0 = u1 - u0, ..., d3 = u4 - u3, of which every term
 // of mono_diff is a sum.
 __device__ __forceinline__ float del_lim_f(float a, float b) {
@@ -147,8 +147,8 @@ struct fields_dev {
     double *vel[3];
     double *p, *dp, *q;
     double *dvel[3];
-    double *fvel[18];     // face states, FP64 form (null in the mixed form)
-    float *fvel32[18];    // face states, mixed form (null in the FP64 form)
+    double *fvel[18];     // face states in FP64 (null when they are FP32)
+    float *fvel32[18];    // face states in FP32 (RMT3D_MIXED_BULK32 only)
     double *sigma[9];
     double *rho;  // VAR_DEN density per cell (fluid_3d.hh:160)
     objmap_dev om[kMaxObj];
@@ -157,11 +157,12 @@ struct fields_dev {
 
 // Velocity face states fvel[f][c] (fields.hh:296), written by the edge
 // extrapolation and read by the upwinding, both projections and the momentum
-// update.  The plain form keeps them in FP64; the mixed form keeps them in
-// FP32, as intermediate values of the advection stencils (the velocity, the
-// pressure and the reference maps stay FP64).  face_ptr picks the array of a
-// kernel instantiated for one form; face_ld / face_st serve kernels that run
-// in both forms and read g.f32face, which is uniform over the launch.
+// update.  The FP64 and mixed forms keep them in FP64; the FP32-advection
+// form (RMT3D_MIXED_BULK32) keeps them in FP32, as intermediate values of the
+// advection stencils (the velocity, the pressure and the reference maps stay
+// FP64).  face_ptr picks the array of a kernel instantiated for one storage
+// type; face_ld / face_st serve kernels that run with either and read
+// g.f32face, which is uniform over the launch.
 template <typename FT>
 __device__ __forceinline__ FT *face_ptr(const fields_dev *__restrict__ F, int a);
 template <>

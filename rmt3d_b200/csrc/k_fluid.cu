@@ -566,7 +566,8 @@ __device__ __forceinline__ void edge_store_f64(const grid_dev &g, const fields_d
         for (int c = 0; c < 3; c++) F->fvel[3 * f + c][ind] = vel[c] + d * nv[dim][c] + adv[c] + dt2 * acc[c];
     }
 }
-// The mixed form's FP32 face states: the same formula in FP32 with fused
+// The FP32 face states of the FP32-advection form (RMT3D_MIXED_BULK32): the
+// same formula in FP32 with fused
 // multiply-adds (the acceleration is formed in FP64 and rounded once).
 __device__ __forceinline__ void edge_store_f32(const grid_dev &g, const fields_dev *__restrict__ F, int ind,
                                                const float (&vel)[3], const float (&nv)[3][3],
@@ -1009,7 +1010,7 @@ __global__ void __launch_bounds__(256, 3) k_ustar(grid_dev g, const fields_dev *
         }
         for (int d = 0; d < 3; d++) dv[d] += acc[d];
     } else {
-        // the mixed form: the advective increment in FP32 from the FP32 face
+        // the FP32-advection form: the advective increment in FP32 from the FP32 face
         // states, added to the FP64 velocity with the FP64 acceleration term
         const float hdt = (float)(-0.5 * cdt);
         const float avgs[3] = {hdt * (fv[0] + fv[3]) * (float)g.dxsp, hdt * (fv[3 * 2 + 1] + fv[3 * 3 + 1]) * (float)g.dysp,

@@ -48,7 +48,7 @@ __global__ void k_bc_cc(grid_dev g, int n, bc_face lo, bc_face hi, double *u, do
 __global__ void k_bc_cf(grid_dev g, int walls, bc_faces bcs, const fields_dev *F);
 __global__ void k_stress(grid_dev g, const fields_dev *__restrict__ F, const int *list, const int *cnt);
 __global__ void k_stress_fluid(grid_dev g, const fields_dev *__restrict__ F, int *list, int *cnt);
-// FT: the face states' type, double in the plain form, float in the mixed form
+// FT: the face states' type: float in the FP32-advection form (RMT3D_MIXED_BULK32), else double
 template <typename FT>
 __global__ void k_edge_vel(grid_dev g, const fields_dev *__restrict__ F, const double *lx, const double *ly,
                            const double *lz, double cdt, const double *time_p, int var_den);

@@ -254,7 +254,7 @@ static cudaError_t copy_sync(rmt3d_scene *s, void *dst, const void *src, size_t 
     return cudaStreamSynchronize(s->st);
 }
 
-// The velocity face states are FP32 in the mixed form (g.f32face): zeroed,
+// The velocity face states are FP32 in the FP32-advection form (g.f32face): zeroed,
 // read and written from the host through these, widened to and narrowed from
 // FP64 on the host side.
 // FP32 face states and advection arithmetic: the RMT3D_MIXED_BULK32 form
@@ -2365,7 +2365,7 @@ static double *field_ptr(rmt3d_scene *s, int which) {
     if (which == 4) return F.dp;
     if (which == 5) return F.q;
     if (which >= 6 && which < 9) return F.dvel[which - 6];
-    if (which >= 9 && which < 27) return F.fvel[which - 9];  // null for the mixed form's FP32 faces
+    if (which >= 9 && which < 27) return F.fvel[which - 9];  // null when the faces are FP32
     if (which >= 27 && which < 36) return F.sigma[which - 27];
     return nullptr;
 }
