@@ -12,7 +12,7 @@ and pressure after the listed steps.
   FMA contraction after 1, 5 and 20 steps; the bound is ENV_FACTOR times the
   reference's own rounding envelope (with against without contraction), the
   largest up to that step.  Measured on a B200: 1.0e-9 after one step, 3.1e-9
-  after 20 (envelope 0.9e-9 and 3.0e-9); the north star's 1e-10 per field is
+  after 20 (envelope 0.9e-9 and 3.0e-9); the plain form's 1e-10 per-field target is
   below the reference's own spread between two roundings at this size.
 * The mixed form (FP32 V-cycles inside FP64 refinement, the reference's
   residual-tolerance control) after 100 steps of that workload, against the
