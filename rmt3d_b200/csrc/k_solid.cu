@@ -298,7 +298,11 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
         if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
         if (kk + r > g.so4 - 1 || kk + r < 0) continue;
         int qi = ind + p + g.sm4 * q + g.smn4 * r;
-        int cd = m.code[qi];
+        // the candidate's map values are loaded together with its code (qi is
+        // inside the box), so the two loads do not wait on each other; they
+        // are used only when the code makes the candidate eligible
+        const int cd = m.code[qi];
+        const double xv[3] = {m.xp[0][qi], m.xp[1][qi], m.xp[2][qi]};
         if (cd < 0 || cd >= L) continue;
         double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
         double wgt = wpw(abs(p) + abs(q) + abs(r));
@@ -319,7 +323,7 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
         cnt++;
         for (int c = 0; c < 3; c++) {
             sd[c] += d[c] * wgt;
-            sr[c] += m.xp[c][qi] * wgt;
+            sr[c] += xv[c] * wgt;
         }
     }
     const unsigned gm = group_mask<LANES>();
@@ -343,7 +347,8 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
         if (jj + q > g.sn4 - 1 || jj + q < 0) continue;
         if (kk + r > g.so4 - 1 || kk + r < 0) continue;
         int qi = ind + p + g.sm4 * q + g.smn4 * r;
-        int cd = m.code[qi];
+        const int cd = m.code[qi];
+        const double xv[3] = {m.xp[0][qi], m.xp[1][qi], m.xp[2][qi]};
         if (cd < 0 || cd >= L) continue;
         double d[3] = {lx[ii + p], ly[jj + q], lz[kk + r]};
         double Q = wpw(abs(p) + abs(q) + abs(r));
@@ -368,7 +373,7 @@ __device__ bool ls_radius(const grid_dev &g, const objmap_dev &m, int R, int L, 
         a[4] += Q * e0 * e2;
         a[5] += Q * e1 * e2;
         for (int c = 0; c < 3; c++) {
-            double lr = Q * (m.xp[c][qi] - ravg[c]);
+            double lr = Q * (xv[c] - ravg[c]);
             rhs[3 * c + 0] += e0 * lr;
             rhs[3 * c + 1] += e1 * lr;
             rhs[3 * c + 2] += e2 * lr;
