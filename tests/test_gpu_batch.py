@@ -114,7 +114,7 @@ def test_autotune_choices_and_results(tmp_path):
 
 def test_footprint_is_what_a_scene_allocates(tmp_path):
     for d in _descs(tmp_path):
-        for prec in (R.FP64, R.MIXED):
+        for prec in (R.FP64, R.MIXED, R.MIXED_BULK32):
             d.precision = prec
             sc = R.Scene(d)
             try:
@@ -192,11 +192,12 @@ def _group_descs(tmp_path, precision=R.FP64, var_den=0):
     return out
 
 
-@pytest.mark.parametrize("form", ["fp64", "mixed_vd"])
+@pytest.mark.parametrize("form", ["fp64", "mixed_vd", "bulk32_vd"])
 def test_group_matches_alone(tmp_path, form):
     """Equally sized scenes step as one group (batched multigrid over the
     group); each scene's result is its solo result to round-off."""
-    descs = _group_descs(tmp_path, R.MIXED if form == "mixed_vd" else R.FP64, 1 if form == "mixed_vd" else 0)
+    prec = {"fp64": R.FP64, "mixed_vd": R.MIXED, "bulk32_vd": R.MIXED_BULK32}[form]
+    descs = _group_descs(tmp_path, prec, 0 if form == "fp64" else 1)
     b = R.Batch(descs, host_threads=2)
     try:
         b.prepare()
