@@ -74,3 +74,17 @@ def test_random_scene_is_seeded_and_disjoint(tmp_path):
             ca, cb = np.array(d.obj[a].basic[:3]), np.array(d.obj[b].basic[:3])
             gap = np.linalg.norm(ca - cb) - d.obj[a].basic[3] - d.obj[b].basic[3]
             assert gap >= 2 * dx
+
+
+def test_precision_forms(tmp_path):
+    """The extension keywords select the arithmetic form and the mixed forms'
+    solve tolerance; a form outside the three is refused before any device
+    work."""
+    text = scenes.cavity(16, 4) + "precision 2\nmixed_rtol 1e-6\n"
+    d = R.desc_from_cfg(scenes.write(str(tmp_path / "p.cfg"), text))
+    assert d.precision == R.MIXED_BULK32 and d.mixed_rtol == 1e-6
+    assert R.desc_from_cfg(scenes.write(str(tmp_path / "q.cfg"), scenes.cavity(16, 4))).precision == R.FP64
+    d.precision = 3
+    with pytest.raises(R.RMT3DError) as e:
+        R.Scene(d)
+    assert "precision" in str(e.value)
