@@ -92,3 +92,22 @@ def test_ftest_error_restatement_matches_reference_report():
     printed = fx["runsim_err"]
     assert st["time"] == pytest.approx(printed[0], rel=1e-12)
     assert np.allclose(e, printed[3:], rtol=0, atol=6e-11), (e, printed)
+
+
+@needs_ref
+def test_compact_field_dumps_match_full_dumps(tmp_path):
+    """The compact dumps the configuration-size GPU tests read
+    (`ref_driver ... fields k1,k2,...`) carry the same velocity and pressure
+    bits as the full dumps the fixtures were made from, at every listed step."""
+    fx = H.load_fixture("cavity16")
+    cfg = H.fixture_cfg(fx, str(tmp_path / "case.cfg"))
+    env = dict(os.environ, RMT3D_SHIM_EXACT="1")
+    subprocess.run([DRIVER, cfg, "8", "out", "fields", "1,8"], check=True, capture_output=True, cwd=str(tmp_path),
+                   env=env)
+    for k in (1, 8):
+        d = refdump.read_fields(str(tmp_path / ("out_s%d.f64" % k)))
+        st = H.state(fx, k)
+        assert d["steps"] == k and d["dt"] == st["dt"] and d["time"] == st["time"]
+        for c, name in enumerate("uvw"):
+            assert np.array_equal(d[name].ravel(), st["vel"][c]), (k, name)
+        assert np.array_equal(d["p"].ravel(), st["p"]), k
